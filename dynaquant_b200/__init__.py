@@ -1,0 +1,169 @@
+"""dynaquant_b200 — B200 (sm_100a) stochastic-Hamiltonian exciton propagator.
+
+Python front end of the C ABI in include/dq.h (libdq.so, built in-tree by
+dynaquant_b200/build.py).  The names follow the reference's step sequence
+(propagate.cu:211-254): ``prop_step`` is lanczosClass::doLanczos +
+padeClass::doPade + propagateSystem + renormalizeAndStoreNorm for one
+trajectory; ``run`` is the ensemble loop over all trajectories.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import (DOT_BILINEAR, DOT_HERMITIAN, NOISE_GAUSS, NOISE_NONE, NOISE_OU, NORM_COMPLEX,
+                   NORM_REAL_ONLY, PREC_FP64, PREC_MIXED, DQError)
+
+__all__ = ["Propagator", "DQError", "NOISE_NONE", "NOISE_GAUSS", "NOISE_OU", "DOT_BILINEAR", "DOT_HERMITIAN",
+           "NORM_REAL_ONLY", "NORM_COMPLEX", "PREC_FP64", "PREC_MIXED", "reference_hbar"]
+
+
+def reference_hbar() -> float:
+    """hbar in cm^-1 fs as cppUtility.cpp:19-22 computes it (c = 299792548 m/s)."""
+    import math
+    return (1 / 100.) * 1e15 * 1. / (299792548. * 2 * (math.atan(1.0) * 4.0))
+
+
+class Propagator:
+    """One context of the C ABI: a system, its trajectories and observables."""
+
+    def __init__(self, n_sites, m=16, n_traj=1, dt=1.0, hbar=0.0, noise=NOISE_NONE, ka_substeps=1,
+                 sigma_static=0.0, seed=0, dot=DOT_HERMITIAN, norm=NORM_COMPLEX, precision=PREC_MIXED,
+                 reorth=0, pop_every=1, max_steps=1024, device=0):
+        self.L = _lib.load()
+        cfg = _lib.Config()
+        self.L.dq_config_default(C.byref(cfg))
+        cfg.n_sites, cfg.m, cfg.n_traj, cfg.dt, cfg.hbar = n_sites, m, n_traj, dt, hbar
+        cfg.noise_model, cfg.ka_substeps, cfg.sigma_static, cfg.seed = noise, ka_substeps, sigma_static, seed
+        cfg.dot_mode, cfg.norm_mode, cfg.precision, cfg.reorth = dot, norm, precision, reorth
+        cfg.pop_every, cfg.max_steps, cfg.device = pop_every, max_steps, device
+        self.cfg = cfg
+        self.n = n_sites
+        self.n_traj = n_traj
+        h = C.c_void_p()
+        rc = self.L.dq_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise DQError(rc, "dq_create failed (bad config or CUDA unavailable)")
+        self.h = h
+
+    # -- lifecycle -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.dq_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise DQError(rc, self.L.dq_last_error(self.h).decode(errors="replace"))
+
+    @property
+    def stream(self) -> int:
+        return self.L.dq_get_stream(self.h)
+
+    # -- system ----------------------------------------------------------------
+    def set_hamiltonian_csr(self, rowptr, col, val):
+        self._rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self._col = np.ascontiguousarray(col, dtype=np.int32)
+        self._val = np.ascontiguousarray(val, dtype=np.float64)
+        self._check(self.L.dq_set_hamiltonian_csr(self.h, self.n, _lib.iptr(self._rp), _lib.iptr(self._col),
+                                                  _lib.dptr(self._val)))
+
+    def set_system(self, system):
+        self.set_hamiltonian_csr(system.rowptr, system.col, system.val)
+
+    def set_coupling_classes(self, cls, scales):
+        cls = np.ascontiguousarray(cls, dtype=np.int32)
+        scales = np.ascontiguousarray(scales, dtype=np.float64)
+        self._check(self.L.dq_set_coupling_classes(self.h, _lib.iptr(cls), len(scales), _lib.dptr(scales)))
+
+    def set_noise_params(self, sigma, tau=None):
+        sigma = np.ascontiguousarray(np.broadcast_to(sigma, (self.n,)), dtype=np.float64)
+        tau = None if tau is None else np.ascontiguousarray(np.broadcast_to(tau, (self.n,)), dtype=np.float64)
+        self._check(self.L.dq_set_noise_params(self.h, _lib.dptr(sigma), _lib.dptr(tau)))
+
+    def set_static_energies(self, eps):
+        eps = None if eps is None else np.ascontiguousarray(eps, dtype=np.float64)
+        self._check(self.L.dq_set_static_energies(self.h, _lib.dptr(eps)))
+
+    def set_initial_state(self, psi0):
+        psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
+        self._check(self.L.dq_set_initial_state(self.h, _lib.dptr(psi0.view(np.float64))))
+
+    def reset(self):
+        self._check(self.L.dq_reset(self.h))
+
+    # -- propagation -------------------------------------------------------------
+    def prop_step(self, traj, step, psi_in_ptr, psi_out_ptr, want_error=False):
+        """One plain FP64 step on device buffers (raw CUDA pointers, N complex128)."""
+        err = C.c_double()
+        self._check(self.L.dq_prop_step(self.h, traj, step, C.c_void_p(psi_in_ptr), C.c_void_p(psi_out_ptr),
+                                        C.byref(err) if want_error else None))
+        return err.value if want_error else None
+
+    def run_plain(self, n_steps):
+        self._check(self.L.dq_run_plain(self.h, n_steps))
+
+    def run(self, n_steps):
+        self._check(self.L.dq_run(self.h, n_steps))
+
+    def profile_step(self, n_steps=1):
+        """Eager steps with CUDA events between kernels: {kind: (ms per launch, launches)}."""
+        nk = len(_lib.KIND_NAMES)
+        ms = np.zeros(nk)
+        cnt = np.zeros(nk, dtype=np.int32)
+        self._check(self.L.dq_profile_step(self.h, n_steps, _lib.dptr(ms), _lib.iptr(cnt), nk))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.KIND_NAMES)}
+
+    # -- observables -------------------------------------------------------------
+    def populations(self) -> np.ndarray:
+        nrec = C.c_int()
+        self._check(self.L.dq_get_populations(self.h, None, C.byref(nrec)))
+        out = np.zeros((nrec.value, self.n))
+        self._check(self.L.dq_get_populations(self.h, _lib.dptr(out), C.byref(nrec)))
+        return out
+
+    def correlation(self) -> np.ndarray:
+        npts = C.c_int()
+        self._check(self.L.dq_get_correlation(self.h, None, C.byref(npts)))
+        out = np.zeros(npts.value, dtype=np.complex128)
+        self._check(self.L.dq_get_correlation(self.h, _lib.dptr(out.view(np.float64)), C.byref(npts)))
+        return out
+
+    def states(self) -> np.ndarray:
+        out = np.zeros((self.n_traj, self.n), dtype=np.complex128)
+        self._check(self.L.dq_get_states(self.h, _lib.dptr(out.view(np.float64))))
+        return out
+
+    def error_accum(self) -> np.ndarray:
+        out = np.zeros(self.n_traj)
+        self._check(self.L.dq_get_error_accum(self.h, _lib.dptr(out)))
+        return out
+
+    def spectrum(self, length) -> np.ndarray:
+        out = np.zeros(length, dtype=np.complex128)
+        self._check(self.L.dq_get_spectrum(self.h, length, _lib.dptr(out.view(np.float64))))
+        return out
+
+    def noise_state(self, traj):
+        eps = np.zeros(self.n)
+        deps = np.zeros(self.n)
+        self._check(self.L.dq_get_noise_state(self.h, traj, _lib.dptr(eps), _lib.dptr(deps)))
+        return eps, deps
+
+    @property
+    def steps_done(self) -> int:
+        return self.L.dq_steps_done(self.h)

@@ -1,0 +1,120 @@
+"""ctypes binding of libdq.so (include/dq.h).
+
+The library is built in-tree (dynaquant_b200/build.py).  Loading fails
+loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdq.so")
+
+DQ_OK, DQ_ERR_ARG, DQ_ERR_CUDA, DQ_ERR_BREAKDOWN, DQ_ERR_NAN, DQ_ERR_TIMEOUT, DQ_ERR_SCALING, DQ_ERR_STATE, \
+    DQ_ERR_SINGULAR = range(9)
+NOISE_NONE, NOISE_GAUSS, NOISE_OU = 0, 1, 2
+DOT_BILINEAR, DOT_HERMITIAN = 0, 1
+NORM_REAL_ONLY, NORM_COMPLEX = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+KIND_NAMES = ["noise", "spmm_alpha", "axpy_beta", "spmm_norm", "pade", "combine", "pop"]
+
+# every symbol include/dq.h declares
+EXPORTS = [
+    "dq_config_default", "dq_create", "dq_destroy", "dq_last_error", "dq_get_stream",
+    "dq_set_hamiltonian_csr", "dq_set_coupling_classes", "dq_set_noise_params", "dq_set_static_energies",
+    "dq_set_initial_state", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
+    "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
+    "dq_get_noise_state", "dq_profile_step",
+]
+
+
+class Config(C.Structure):
+    _fields_ = [
+        ("n_sites", C.c_int),
+        ("m", C.c_int),
+        ("n_traj", C.c_int),
+        ("dt", C.c_double),
+        ("hbar", C.c_double),
+        ("noise_model", C.c_int),
+        ("ka_substeps", C.c_int),
+        ("sigma_static", C.c_double),
+        ("seed", C.c_uint64),
+        ("dot_mode", C.c_int),
+        ("norm_mode", C.c_int),
+        ("precision", C.c_int),
+        ("reorth", C.c_int),
+        ("pop_every", C.c_int),
+        ("m_min", C.c_int),
+        ("m_tol", C.c_double),
+        ("max_steps", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+class CDouble(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads libdq.so and declares its signatures; raises if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m dynaquant_b200.build` "
+                           "(the propagator has no CPU fallback)")
+    L = C.CDLL(path)
+    vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+    cfgp = C.POINTER(Config)
+    L.dq_config_default.argtypes = [cfgp]
+    L.dq_config_default.restype = None
+    L.dq_create.argtypes = [cfgp, C.POINTER(vp)]
+    L.dq_destroy.argtypes = [vp]
+    L.dq_destroy.restype = None
+    L.dq_last_error.argtypes = [vp]
+    L.dq_last_error.restype = C.c_char_p
+    L.dq_get_stream.argtypes = [vp]
+    L.dq_get_stream.restype = vp
+    L.dq_set_hamiltonian_csr.argtypes = [vp, C.c_int, ip, ip, dp]
+    L.dq_set_coupling_classes.argtypes = [vp, ip, C.c_int, dp]
+    L.dq_set_noise_params.argtypes = [vp, dp, dp]
+    L.dq_set_static_energies.argtypes = [vp, dp]
+    L.dq_set_initial_state.argtypes = [vp, dp]
+    L.dq_reset.argtypes = [vp]
+    L.dq_prop_step.argtypes = [vp, C.c_int, C.c_int, vp, vp, dp]
+    L.dq_run_plain.argtypes = [vp, C.c_int]
+    L.dq_run.argtypes = [vp, C.c_int]
+    L.dq_get_populations.argtypes = [vp, dp, ip]
+    L.dq_get_correlation.argtypes = [vp, dp, ip]
+    L.dq_get_states.argtypes = [vp, dp]
+    L.dq_get_error_accum.argtypes = [vp, dp]
+    L.dq_steps_done.argtypes = [vp]
+    L.dq_steps_done.restype = C.c_int
+    L.dq_get_spectrum.argtypes = [vp, C.c_int, dp]
+    L.dq_get_noise_state.argtypes = [vp, C.c_int, dp, dp]
+    L.dq_profile_step.argtypes = [vp, C.c_int, dp, ip, C.c_int]
+    for name in EXPORTS:
+        if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def dptr(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def iptr(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+class DQError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"dq error {code}: {msg}")
+        self.code = code

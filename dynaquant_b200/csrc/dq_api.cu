@@ -1,0 +1,409 @@
+// dq_api.cu — the C ABI (include/dq.h): context life cycle, system set-up,
+// the plain drop-in step, the ensemble drivers and the observable getters.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "dq_internal.h"
+
+using namespace dq;
+
+namespace {
+
+double reference_hbar() {
+    // cppUtility.cpp:19-22, including the reference's c = 299792548 m/s
+    double pi = atan(1.0) * 4.0;
+    double lightspeed = 299792548.;
+    return (1 / 100.) * (1e15) * 1. / (lightspeed * 2 * pi);
+}
+
+dq_status fail(dq_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define DQ_CU(call)                                                     \
+    do {                                                                \
+        dq_status _s = check_cuda(c, (call), #call);                    \
+        if (_s != DQ_OK) return _s;                                     \
+    } while (0)
+
+template <typename T>
+dq_status upload(dq_ctx* c, T** dptr, const T* host, size_t count) {
+    if (*dptr) { cudaFree(*dptr); *dptr = nullptr; }
+    if (count == 0) return DQ_OK;
+    DQ_CU(cudaMalloc(dptr, sizeof(T) * count));
+    DQ_CU(cudaMemcpyAsync(*dptr, host, sizeof(T) * count, cudaMemcpyHostToDevice, c->stream));
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    return DQ_OK;
+}
+
+dq_status upload_couplings(dq_ctx* c) {
+    c->val.resize(c->val_base.size());
+    for (size_t k = 0; k < c->val_base.size(); ++k) {
+        double s = 1.0;
+        if (!c->cls.empty()) s = c->scales[c->cls[k]];
+        c->val[k] = s * c->val_base[k];
+    }
+    std::vector<float> vf(c->val.begin(), c->val.end());
+    dq_status st = upload(c, &c->d_val, c->val.data(), c->val.size());
+    if (st) return st;
+    return upload(c, &c->d_valf, vf.data(), vf.size());
+}
+
+}  // namespace
+
+extern "C" {
+
+void dq_config_default(dq_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->m = 16;
+    cfg->n_traj = 1;
+    cfg->dt = 1.0;
+    cfg->hbar = 0.0;
+    cfg->noise_model = DQ_NOISE_NONE;
+    cfg->ka_substeps = 1;
+    cfg->dot_mode = DQ_DOT_HERMITIAN;
+    cfg->norm_mode = DQ_NORM_COMPLEX;
+    cfg->precision = DQ_PREC_MIXED;
+    cfg->pop_every = 1;
+    cfg->max_steps = 1024;
+}
+
+dq_status dq_create(const dq_config* cfg, dq_ctx** out) {
+    if (!cfg || !out) return DQ_ERR_ARG;
+    *out = nullptr;
+    if (cfg->n_sites < 2 || cfg->m < 2 || cfg->m > kMaxM || cfg->n_traj < 1 || !(cfg->dt > 0) ||
+        cfg->pop_every < 1 || cfg->max_steps < 1 || cfg->ka_substeps < 0 ||
+        cfg->noise_model < DQ_NOISE_NONE || cfg->noise_model > DQ_NOISE_OU ||
+        (cfg->reorth && cfg->dot_mode != DQ_DOT_HERMITIAN) || cfg->m > cfg->n_sites)
+        return DQ_ERR_ARG;
+    if ((cfg->n_sites + kPlainThreads - 1) / kPlainThreads > kMaxPartials) return DQ_ERR_ARG;
+    dq_ctx* c = new (std::nothrow) dq_ctx();
+    if (!c) return DQ_ERR_CUDA;
+    c->cfg = *cfg;
+    if (c->cfg.ka_substeps == 0) c->cfg.ka_substeps = 1;
+    c->n = cfg->n_sites;
+    c->hbar = cfg->hbar > 0 ? cfg->hbar : reference_hbar();
+    c->tau_im = -cfg->dt / c->hbar;   // propagate.cu:90-93: expCoeff = (0, -dt/hbar)
+    dq_status st = DQ_OK;
+    do {
+        if ((st = check_cuda(c, cudaSetDevice(cfg->device), "cudaSetDevice"))) break;
+        if ((st = check_cuda(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream"))) break;
+        c->n_rec_max = cfg->max_steps / cfg->pop_every + 1;
+        if ((st = check_cuda(c, cudaMalloc(&c->d_pops, sizeof(double) * (size_t)c->n_rec_max * c->n), "pops"))) break;
+        if ((st = check_cuda(c, cudaMalloc(&c->d_corr, sizeof(cd) * (size_t)(cfg->max_steps + 1)), "corr"))) break;
+        if ((st = check_cuda(c, cudaMalloc(&c->d_erracc, sizeof(double) * cfg->n_traj), "erracc"))) break;
+        if ((st = check_cuda(c, cudaMalloc(&c->d_psi0, sizeof(cd) * c->n), "psi0"))) break;
+        if ((st = plain_alloc(c))) break;
+        if ((st = plain_clear_observables(c))) break;
+    } while (0);
+    if (st != DQ_OK) {
+        dq_destroy(c);
+        return st;
+    }
+    *out = c;
+    return DQ_OK;
+}
+
+void dq_destroy(dq_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->cfg.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    batched_free(c);
+    plain_free(c);
+    cudaFree(c->d_rowptr); cudaFree(c->d_col); cudaFree(c->d_val); cudaFree(c->d_valf); cudaFree(c->d_h0);
+    cudaFree(c->d_static); cudaFree(c->d_sigma); cudaFree(c->d_invtau); cudaFree(c->d_coeff);
+    cudaFree(c->d_psi0); cudaFree(c->d_pops); cudaFree(c->d_corr); cudaFree(c->d_erracc);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* dq_last_error(const dq_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void* dq_get_stream(dq_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+dq_status dq_set_hamiltonian_csr(dq_ctx* c, int n, const int* rowptr, const int* col, const double* val) {
+    if (!c) return DQ_ERR_ARG;
+    if (n != c->n || !rowptr || !col || !val) return fail(c, DQ_ERR_ARG, "hamiltonian: size or null pointer");
+    if (rowptr[0] != 0) return fail(c, DQ_ERR_ARG, "hamiltonian: rowptr[0] != 0");
+    for (int i = 0; i < n; ++i)
+        if (rowptr[i + 1] < rowptr[i]) return fail(c, DQ_ERR_ARG, "hamiltonian: rowptr not monotone");
+    const int nnz = rowptr[n];
+    std::vector<int> rp(n + 1, 0), cl;
+    std::vector<double> vb, h0(n, 0.0);
+    cl.reserve(nnz);
+    vb.reserve(nnz);
+    for (int i = 0; i < n; ++i) {
+        for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) {
+            int j = col[p];
+            if (j < 0 || j >= n) return fail(c, DQ_ERR_ARG, "hamiltonian: column index out of range");
+            if (!std::isfinite(val[p])) return fail(c, DQ_ERR_ARG, "hamiltonian: non-finite value");
+            if (j == i) h0[i] += val[p];
+            else { cl.push_back(j); vb.push_back(val[p]); }
+        }
+        rp[i + 1] = (int)cl.size();
+    }
+    c->rowptr = rp;
+    c->col = cl;
+    c->val_base = vb;
+    c->h0diag = h0;
+    c->nnz_off = (int)cl.size();
+    c->cls.clear();
+    c->scales.clear();
+    dq_status st;
+    if ((st = upload(c, &c->d_rowptr, c->rowptr.data(), c->rowptr.size()))) return st;
+    if ((st = upload(c, &c->d_col, c->col.data(), c->col.size()))) return st;
+    if ((st = upload(c, &c->d_h0, c->h0diag.data(), c->h0diag.size()))) return st;
+    if ((st = upload_couplings(c))) return st;
+    if (c->nnz_off == 0) {
+        // keep valid (non-null) pointers for kernels
+        static const int zi = 0;
+        static const double zd = 0.0;
+        static const float zf = 0.f;
+        if ((st = upload(c, &c->d_col, &zi, 1))) return st;
+        if ((st = upload(c, &c->d_val, &zd, 1))) return st;
+        if ((st = upload(c, &c->d_valf, &zf, 1))) return st;
+    }
+    c->have_ham = true;
+    c->ready = false;
+    return DQ_OK;
+}
+
+dq_status dq_set_coupling_classes(dq_ctx* c, const int* cls, int n_classes, const double* scales) {
+    if (!c) return DQ_ERR_ARG;
+    if (!c->have_ham) return fail(c, DQ_ERR_STATE, "coupling classes: set the Hamiltonian first");
+    if (!cls || !scales || n_classes < 1) return fail(c, DQ_ERR_ARG, "coupling classes: null or empty");
+    std::vector<int> off(cls, cls + c->nnz_off);
+    for (int v : off)
+        if (v < 0 || v >= n_classes) return fail(c, DQ_ERR_ARG, "coupling classes: class out of range");
+    c->cls = off;
+    c->scales.assign(scales, scales + n_classes);
+    return upload_couplings(c);
+}
+
+dq_status dq_set_noise_params(dq_ctx* c, const double* sigma, const double* tau) {
+    if (!c) return DQ_ERR_ARG;
+    if (!sigma) return fail(c, DQ_ERR_ARG, "noise params: sigma is null");
+    if (c->cfg.noise_model == DQ_NOISE_OU && !tau) return fail(c, DQ_ERR_ARG, "noise params: OU needs tau");
+    const int n = c->n;
+    c->sigma.assign(sigma, sigma + n);
+    std::vector<double> invtau(n, 0.0), coeff(n, 0.0);
+    if (tau) {
+        c->tau.assign(tau, tau + n);
+        for (int i = 0; i < n; ++i) {
+            if (!(tau[i] > 0)) return fail(c, DQ_ERR_ARG, "noise params: tau must be > 0");
+            // systemClass.cu:1033-1034
+            invtau[i] = 1. / tau[i];
+            coeff[i] = sigma[i] * sqrt(2. / tau[i]);
+        }
+    }
+    dq_status st;
+    if ((st = upload(c, &c->d_sigma, c->sigma.data(), (size_t)n))) return st;
+    if ((st = upload(c, &c->d_invtau, invtau.data(), (size_t)n))) return st;
+    if ((st = upload(c, &c->d_coeff, coeff.data(), (size_t)n))) return st;
+    c->have_noise = true;
+    return DQ_OK;
+}
+
+dq_status dq_set_static_energies(dq_ctx* c, const double* eps) {
+    if (!c) return DQ_ERR_ARG;
+    if (!eps) {
+        c->static_eps.clear();
+        cudaFree(c->d_static);
+        c->d_static = nullptr;
+        return DQ_OK;
+    }
+    c->static_eps.assign(eps, eps + c->n);
+    return upload(c, &c->d_static, c->static_eps.data(), (size_t)c->n);
+}
+
+dq_status dq_set_initial_state(dq_ctx* c, const dq_cdouble* psi0) {
+    if (!c) return DQ_ERR_ARG;
+    if (!psi0) return fail(c, DQ_ERR_ARG, "initial state is null");
+    c->psi0.assign(psi0, psi0 + c->n);
+    DQ_CU(cudaMemcpyAsync(c->d_psi0, psi0, sizeof(cd) * c->n, cudaMemcpyHostToDevice, c->stream));
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    c->have_psi0 = true;
+    return DQ_OK;
+}
+
+static dq_status check_ready(dq_ctx* c) {
+    if (!c->have_ham) return fail(c, DQ_ERR_STATE, "no Hamiltonian set");
+    if (c->cfg.noise_model != DQ_NOISE_NONE && !c->have_noise) return fail(c, DQ_ERR_STATE, "no noise parameters set");
+    if (!c->have_psi0) return fail(c, DQ_ERR_STATE, "no initial state set");
+    return DQ_OK;
+}
+
+dq_status dq_reset(dq_ctx* c) {
+    if (!c) return DQ_ERR_ARG;
+    dq_status st;
+    if ((st = check_ready(c))) return st;
+    if ((st = plain_traj_init(c))) return st;
+    if ((st = plain_clear_observables(c))) return st;
+    c->steps_done = 0;
+    c->plain_traj_done = 0;
+    if (c->bat) {
+        if ((st = batched_reset(c))) return st;
+    }
+    c->ready = true;
+    return DQ_OK;
+}
+
+dq_status dq_prop_step(dq_ctx* c, int traj, int step, const dq_cdouble* psi_in, dq_cdouble* psi_out, double* err_est) {
+    if (!c) return DQ_ERR_ARG;
+    if (traj < 0 || traj >= c->cfg.n_traj || step < 0 || !psi_in || !psi_out || psi_in == psi_out)
+        return fail(c, DQ_ERR_ARG, "prop_step: bad trajectory, step or pointers");
+    dq_status st;
+    if (!c->ready) {
+        if ((st = dq_reset(c))) return st;
+    }
+    if ((st = plain_step(c, traj, step, reinterpret_cast<const cd*>(psi_in), reinterpret_cast<cd*>(psi_out), false, -1)))
+        return st;
+    if (err_est) {
+        DQ_CU(cudaStreamSynchronize(c->stream));
+        PlainScalars h;
+        DQ_CU(cudaMemcpy(&h, c->d_ps, sizeof(h), cudaMemcpyDeviceToHost));
+        *err_est = h.err;
+        if (h.status) {
+            int code = h.status;
+            cudaMemsetAsync(&c->d_ps->status, 0, sizeof(int), c->stream);
+            return read_status(c, code, "prop_step");
+        }
+    }
+    return DQ_OK;
+}
+
+dq_status dq_run_plain(dq_ctx* c, int n_steps) {
+    if (!c) return DQ_ERR_ARG;
+    if (n_steps < 0 || n_steps > c->cfg.max_steps) return fail(c, DQ_ERR_ARG, "run_plain: n_steps out of range");
+    dq_status st;
+    if ((st = dq_reset(c))) return st;
+    const int n = c->n, pe = c->cfg.pop_every;
+    for (int t = 0; t < c->cfg.n_traj; ++t) {
+        if ((st = plain_observe_initial(c))) return st;
+        cd* src = c->d_psi_a;
+        cd* dst = c->d_psi_b;
+        DQ_CU(cudaMemcpyAsync(src, c->d_psi0, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->stream));
+        for (int k = 0; k < n_steps; ++k) {
+            int rec = ((k + 1) % pe == 0) ? (k + 1) / pe : -1;
+            if ((st = plain_step(c, t, k, src, dst, true, rec))) return st;
+            std::swap(src, dst);
+        }
+    }
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    PlainScalars h;
+    DQ_CU(cudaMemcpy(&h, c->d_ps, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h.status) return read_status(c, h.status, "run_plain");
+    c->steps_done = n_steps;
+    c->plain_traj_done = c->cfg.n_traj;
+    c->last_path = 0;
+    c->ready = false;   // the ensemble form restarts from dq_reset
+    return DQ_OK;
+}
+
+dq_status dq_run(dq_ctx* c, int n_steps) {
+    if (!c) return DQ_ERR_ARG;
+    if (n_steps < 0 || c->steps_done + n_steps > c->cfg.max_steps)
+        return fail(c, DQ_ERR_ARG, "run: steps exceed max_steps");
+    dq_status st;
+    if (!c->bat) {
+        if ((st = batched_alloc(c))) return st;
+        c->ready = false;
+    }
+    if (!c->ready) {
+        if ((st = dq_reset(c))) return st;
+    }
+    c->last_path = 1;
+    return batched_run(c, n_steps);
+}
+
+dq_status dq_get_populations(dq_ctx* c, double* out, int* n_records) {
+    if (!c) return DQ_ERR_ARG;
+    int nrec = c->steps_done / c->cfg.pop_every + 1;
+    if (n_records) *n_records = nrec;
+    if (!out) return DQ_OK;
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    DQ_CU(cudaMemcpy(out, c->d_pops, sizeof(double) * (size_t)nrec * c->n, cudaMemcpyDeviceToHost));
+    const double inv = 1.0 / c->cfg.n_traj;
+    for (size_t x = 0; x < (size_t)nrec * c->n; ++x) out[x] *= inv;
+    return DQ_OK;
+}
+
+dq_status dq_get_correlation(dq_ctx* c, dq_cdouble* out, int* n_points) {
+    if (!c) return DQ_ERR_ARG;
+    int np = c->steps_done + 1;
+    if (n_points) *n_points = np;
+    if (!out) return DQ_OK;
+    if (c->last_path == 1 && c->bat) {
+        dq_status st = batched_collect_corr(c);
+        if (st) return st;
+    }
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    DQ_CU(cudaMemcpy(out, c->d_corr, sizeof(cd) * np, cudaMemcpyDeviceToHost));
+    const double inv = 1.0 / c->cfg.n_traj;
+    for (int k = 0; k < np; ++k) { out[k].re *= inv; out[k].im *= inv; }
+    return DQ_OK;
+}
+
+dq_status dq_get_states(dq_ctx* c, dq_cdouble* out) {
+    if (!c || !out) return DQ_ERR_ARG;
+    if (!c->bat) return fail(c, DQ_ERR_STATE, "get_states: no ensemble state (run dq_run first)");
+    return batched_get_states(c, out);
+}
+
+dq_status dq_get_error_accum(dq_ctx* c, double* out) {
+    if (!c || !out) return DQ_ERR_ARG;
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    DQ_CU(cudaMemcpy(out, c->d_erracc, sizeof(double) * c->cfg.n_traj, cudaMemcpyDeviceToHost));
+    return DQ_OK;
+}
+
+int dq_steps_done(const dq_ctx* c) { return c ? c->steps_done : -1; }
+
+}  // extern "C"
+
+extern "C" dq_status dq_get_noise_state(dq_ctx* c, int traj, double* eps, double* deps) {
+    if (!c) return DQ_ERR_ARG;
+    if (traj < 0 || traj >= c->cfg.n_traj) return fail(c, DQ_ERR_ARG, "noise_state: bad trajectory");
+    const int n = c->n;
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    if (c->last_path == 1 && c->bat) {
+        const double* e = nullptr;
+        const double* d = nullptr;
+        batched_noise_arrays(c, &e, &d);
+        const size_t pitch = sizeof(double) * c->cfg.n_traj;
+        if (eps) DQ_CU(cudaMemcpy2D(eps, sizeof(double), e + traj, pitch, sizeof(double), n, cudaMemcpyDeviceToHost));
+        if (deps) DQ_CU(cudaMemcpy2D(deps, sizeof(double), d + traj, pitch, sizeof(double), n, cudaMemcpyDeviceToHost));
+    } else {
+        if (eps) DQ_CU(cudaMemcpy(eps, c->d_eps_p + (size_t)traj * n, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        if (deps) DQ_CU(cudaMemcpy(deps, c->d_deps_p + (size_t)traj * n, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    }
+    return DQ_OK;
+}
+
+extern "C" dq_status dq_profile_step(dq_ctx* c, int n_steps, double* ms_per_launch, int* launches, int n_kinds) {
+    if (!c || !ms_per_launch || n_kinds < 1) return DQ_ERR_ARG;
+    if (n_steps < 1 || c->steps_done + n_steps > c->cfg.max_steps)
+        return fail(c, DQ_ERR_ARG, "profile_step: steps exceed max_steps");
+    dq_status st;
+    if (!c->bat) {
+        if ((st = batched_alloc(c))) return st;
+        c->ready = false;
+    }
+    if (!c->ready) {
+        if ((st = dq_reset(c))) return st;
+    }
+    c->last_path = 1;
+    const int nk = n_kinds < DQ_KIND_COUNT ? n_kinds : DQ_KIND_COUNT;
+    std::vector<double> ms(DQ_KIND_COUNT, 0.0);
+    std::vector<int> cnt(DQ_KIND_COUNT, 0);
+    if ((st = batched_profile(c, n_steps, ms.data(), cnt.data(), DQ_KIND_COUNT))) return st;
+    for (int k = 0; k < nk; ++k) {
+        ms_per_launch[k] = cnt[k] ? ms[k] / cnt[k] : 0.0;
+        if (launches) launches[k] = cnt[k];
+    }
+    return DQ_OK;
+}

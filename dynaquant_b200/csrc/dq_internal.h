@@ -1,0 +1,110 @@
+// dq_internal.h — the context behind the C ABI (include/dq.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/dq.h"
+#include "dq_common.cuh"
+#include "dq_pade.cuh"
+
+namespace dq {
+
+// Scalars of the plain per-trajectory path (device resident).
+struct PlainScalars {
+    cd alpha[kMaxL];
+    cd beta[kMaxL];
+    double sc[kMaxL];     // slab j holds q_j / sc[j] (unnormalised Lanczos residual)
+    cd yt[kMaxL];         // y_{j-1} * sc[j]: combine weights
+    double nav;           // ||H q_{m+1}||
+    double norm;          // ||psi_out|| before renormalisation
+    double invnorm;
+    double err;           // EXPOKIT estimate of the last step
+    int s;                // Padé squarings of the last step
+    int status;           // DQ_OK or a DQ_ERR_* code raised on the device
+    unsigned int ticket[4];
+};
+
+constexpr int kPlainThreads = 256;
+constexpr int kMaxPartials = 4096;
+
+struct BatchedState;   // dq_batched.cu
+
+}  // namespace dq
+
+struct dq_ctx {
+    dq_config cfg{};
+    std::string err;
+    cudaStream_t stream = nullptr;
+    double hbar = 0.0;
+    double tau_im = 0.0;  // tau = (0, tau_im) = -i dt / hbar
+
+    // host copies of the system
+    int n = 0;
+    std::vector<int> rowptr, col;          // off-diagonal CSR
+    std::vector<double> val_base, val;     // couplings before / after class scaling
+    std::vector<int> cls;                  // coupling class per off-diagonal entry
+    std::vector<double> scales;
+    std::vector<double> h0diag;
+    std::vector<double> sigma, tau;
+    std::vector<double> static_eps;        // explicit static energies (empty = h0 + disorder)
+    std::vector<dq_cdouble> psi0;
+    bool have_ham = false, have_noise = false, have_psi0 = false, ready = false;
+
+    // device: shared structure
+    int* d_rowptr = nullptr;
+    int* d_col = nullptr;
+    double* d_val = nullptr;
+    float* d_valf = nullptr;
+    double* d_h0 = nullptr;
+    double* d_static = nullptr;            // explicit static energies (or null)
+    double* d_sigma = nullptr;
+    double* d_invtau = nullptr;
+    double* d_coeff = nullptr;
+    dq::cd* d_psi0 = nullptr;
+    int nnz_off = 0;
+
+    // plain path: per trajectory state [traj][site], work buffers
+    double* d_eps_p = nullptr;
+    double* d_deps_p = nullptr;
+    double* d_diag = nullptr;
+    dq::cd* d_Q = nullptr;        // (m+2) slabs of n
+    dq::cd* d_w = nullptr;
+    dq::cd* d_psi_a = nullptr;    // ensemble driver ping-pong states
+    dq::cd* d_psi_b = nullptr;
+    double* d_partial = nullptr;  // kMaxPartials x 2
+    dq::PlainScalars* d_ps = nullptr;
+
+    // observables (sums over trajectories; divided by n_traj on read)
+    int n_rec_max = 0;
+    double* d_pops = nullptr;     // n_rec_max x n
+    dq::cd* d_corr = nullptr;     // max_steps + 1
+    double* d_erracc = nullptr;   // n_traj
+    int steps_done = 0;
+    int plain_traj_done = 0;      // trajectories completed by dq_run_plain
+    int last_path = 0;            // 0: observables from dq_run_plain, 1: from dq_run
+
+    dq::BatchedState* bat = nullptr;
+};
+
+namespace dq {
+// implemented in dq_plain.cu
+dq_status plain_alloc(dq_ctx* c);
+void plain_free(dq_ctx* c);
+dq_status plain_traj_init(dq_ctx* c);
+dq_status plain_step(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_out, bool observe, int rec);
+dq_status plain_clear_observables(dq_ctx* c);
+dq_status plain_observe_initial(dq_ctx* c);
+dq_status check_cuda(dq_ctx* c, cudaError_t e, const char* what);
+dq_status read_status(dq_ctx* c, int code, const char* what);
+// implemented in dq_batched.cu
+dq_status batched_alloc(dq_ctx* c);
+void batched_free(dq_ctx* c);
+dq_status batched_reset(dq_ctx* c);
+dq_status batched_run(dq_ctx* c, int n_steps);
+dq_status batched_get_states(dq_ctx* c, dq_cdouble* out);
+dq_status batched_collect_corr(dq_ctx* c);
+dq_status batched_profile(dq_ctx* c, int n_steps, double* ms, int* cnt, int nk);
+void batched_noise_arrays(dq_ctx* c, const double** eps, const double** deps);
+}  // namespace dq

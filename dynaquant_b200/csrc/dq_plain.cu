@@ -1,0 +1,350 @@
+// dq_plain.cu — the plain FP64 per-trajectory form: the drop-in for one
+// reference time step (propagate.cu:211-254).
+//
+// Per step, all on the context's stream, no host synchronisation:
+//   k_noise          OU / Gaussian update of this trajectory's diagonal
+//                    (gpuSysHelper.cu:32-128, Philox instead of cuRAND)
+//   m x { k_spmv_alpha, k_axpy_norm }
+//                    one Lanczos iteration (lanczosClass.cu:405-526): the
+//                    SpMV, alpha, both axpys, beta and the scaling collapse
+//                    into two kernels; the residual is stored unnormalised
+//                    with a per-slab scale, so no third pass is needed
+//   k_spmv_norm      ||H q_{m+1}|| (lanczosClass.cu:537-570)
+//   k_pade           exp(tau Tbar), weights, EXPOKIT error (one CTA)
+//   k_combine        psi = V y, ||psi||^2 (propStep.cu:31-44)
+//   k_renorm         psi /= ||psi|| (+ population / correlation sums)
+// Cross-block reductions use the last-block ticket, so every reduction is
+// deterministic and costs no extra launch.
+#include <cstdio>
+
+#include "dq_internal.h"
+#include "dq_rng.cuh"
+
+namespace dq {
+
+__global__ void k_traj_init_plain(int n, int n_traj, uint64_t seed, const double* __restrict__ h0,
+                                  const double* __restrict__ static_eps, double sigma_static,
+                                  const double* __restrict__ sigma, int noise, double* __restrict__ eps,
+                                  double* __restrict__ deps) {
+    size_t total = (size_t)n * n_traj;
+    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
+        int t = (int)(x / n), i = (int)(x % n);
+        double e;
+        if (static_eps) e = static_eps[i];
+        else e = __dadd_rn(__dmul_rn(sigma_static, normal(seed, P_STATIC, t, 0, i, 0)), h0[i]);
+        eps[x] = e;
+        deps[x] = (noise == DQ_NOISE_OU) ? __dmul_rn(sigma[i], normal(seed, P_OU_INIT, t, 0, i, 0)) : 0.0;
+    }
+}
+
+__global__ void k_noise(int n, int traj, int step, int noise, int ns, double subdt, double sqrt_subdt,
+                        uint64_t seed, const double* __restrict__ sigma, const double* __restrict__ invtau,
+                        const double* __restrict__ coeff, const double* __restrict__ eps,
+                        double* __restrict__ deps, double* __restrict__ diag, PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) ps->sc[1] = 1.0;   // q_1 = psi_in
+    if (i >= n) return;
+    if (noise == DQ_NOISE_OU) {
+        double cur = ou_update(deps[i], invtau[i], coeff[i], subdt, sqrt_subdt, ns, seed, traj, step, i);
+        deps[i] = cur;
+        diag[i] = __dadd_rn(cur, eps[i]);
+    } else if (noise == DQ_NOISE_GAUSS) {
+        double xi = normal(seed, P_GAUSS, traj, step, i, 0);
+        diag[i] = __dadd_rn(__dmul_rn(xi, sigma[i]), eps[i]);
+    } else {
+        diag[i] = eps[i];
+    }
+}
+
+// Reduce 2 doubles per block into partial[2*blockIdx]; the last block sums
+// the partials in block order into out2 (and returns true in that block).
+__device__ __forceinline__ bool reduce2_last(double a, double b, double* partial, unsigned int* ticket,
+                                             double* out2) {
+    __shared__ double scratch[kPlainThreads / 32];
+    double ra = block_sum(a, scratch);
+    double rb = block_sum(b, scratch);
+    if (threadIdx.x == 0) { partial[2 * blockIdx.x] = ra; partial[2 * blockIdx.x + 1] = rb; }
+    bool last = last_block_ticket(ticket, gridDim.x);
+    if (last) {
+        double sa = 0.0, sb = 0.0;
+        if (threadIdx.x == 0) {
+            for (unsigned int k = 0; k < gridDim.x; ++k) {
+                sa += __ldcg(&partial[2 * k]);
+                sb += __ldcg(&partial[2 * k + 1]);
+            }
+            out2[0] = sa;
+            out2[1] = sb;
+            *ticket = 0;
+        }
+        __syncthreads();
+    }
+    return last;
+}
+
+// w = H q_j (q_j = sc_j * r_j), alpha_j = <q_j, w> (bilinear or Hermitian)
+template <bool kBilinear>
+__global__ void __launch_bounds__(kPlainThreads) k_spmv_alpha(int n, int j, const int* __restrict__ rowptr,
+                                                             const int* __restrict__ col,
+                                                             const double* __restrict__ val,
+                                                             const double* __restrict__ diag, const cd* rj,
+                                                             cd* __restrict__ w, double* partial,
+                                                             PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ar = 0.0, ai = 0.0;
+    if (i < n) {
+        const double sc = ps->sc[j];
+        cd x = rj[i];
+        cd acc = cscale(x, diag[i]);
+        for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) acc = cadd(acc, cscale(rj[col[p]], val[p]));
+        cd u = cscale(acc, sc);
+        w[i] = u;
+        cd q = cscale(x, sc);
+        cd pr = kBilinear ? cmul(q, u) : cmul(cconj(q), u);
+        ar = pr.x;
+        ai = pr.y;
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(ar, ai, partial, &ps->ticket[0], out2) && threadIdx.x == 0) {
+        ps->alpha[j] = cmk(out2[0], out2[1]);
+    }
+}
+
+// r_{j+1} = w - alpha_j q_j - beta_{j-1} q_{j-1};  beta_j = ||r_{j+1}||
+__global__ void __launch_bounds__(kPlainThreads) k_axpy_norm(int n, int j, const cd* __restrict__ w,
+                                                            const cd* rj, const cd* rjm, cd* rjp,
+                                                            double* partial, PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double nn = 0.0;
+    if (i < n) {
+        const cd a = ps->alpha[j];
+        cd r = csub(w[i], cmul(a, cscale(rj[i], ps->sc[j])));
+        if (j > 1) r = csub(r, cmul(ps->beta[j - 1], cscale(rjm[i], ps->sc[j - 1])));
+        rjp[i] = r;
+        nn = cabs2(r);
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(nn, 0.0, partial, &ps->ticket[1], out2) && threadIdx.x == 0) {
+        double b = sqrt(out2[0]);
+        if (!isfinite(b)) atomicCAS(&ps->status, 0, DQ_ERR_NAN);
+        // lucky breakdown: the Krylov space is invariant, q_{j+1} = 0 makes
+        // the remaining block of T decouple and the result exact
+        const double scale = sqrt(cabs2(ps->alpha[j])) + (j > 1 ? ps->beta[j - 1].x : 0.0);
+        if (b <= kBreakdownRel * scale) b = 0.0;
+        ps->beta[j] = cmk(b, 0.0);
+        ps->sc[j + 1] = b > 0.0 ? 1.0 / b : 0.0;
+    }
+}
+
+// ||H q_{m+1}||
+__global__ void __launch_bounds__(kPlainThreads) k_spmv_norm(int n, int j, const int* __restrict__ rowptr,
+                                                            const int* __restrict__ col,
+                                                            const double* __restrict__ val,
+                                                            const double* __restrict__ diag, const cd* rj,
+                                                            double* partial, PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double nn = 0.0;
+    if (i < n) {
+        cd acc = cscale(rj[i], diag[i]);
+        for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) acc = cadd(acc, cscale(rj[col[p]], val[p]));
+        nn = cabs2(cscale(acc, ps->sc[j]));
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(nn, 0.0, partial, &ps->ticket[2], out2) && threadIdx.x == 0) ps->nav = sqrt(out2[0]);
+}
+
+__global__ void k_pade_plain(int m, double tau_im, int norm_mode, PlainScalars* ps, double* erracc, int traj) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ cd y[kMaxM];
+    PadeOut o = pade_exp_tbar(m, ps->alpha, ps->beta, cmk(0.0, tau_im), norm_mode, y, smem);
+    if (o.s < 0) {
+        if (threadIdx.x == 0) atomicCAS(&ps->status, 0, (o.s == -1) ? DQ_ERR_SCALING : DQ_ERR_SINGULAR);
+        return;
+    }
+    __syncthreads();
+    if (threadIdx.x < m) ps->yt[threadIdx.x + 1] = cscale(y[threadIdx.x], ps->sc[threadIdx.x + 1]);
+    if (threadIdx.x == 0) {
+        ps->s = o.s;
+        double est = expokit_error(ps->beta[m].x, ps->nav, o.e_m1_m, o.e_m1_mp1);
+        ps->err = est;
+        if (erracc) erracc[traj] += est;
+    }
+}
+
+// psi_out = sum_j yt_j r_j, ||psi_out||^2
+__global__ void __launch_bounds__(kPlainThreads) k_combine(int n, int m, const cd* psi_in, const cd* Q,
+                                                          cd* __restrict__ out, double* partial,
+                                                          PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double nn = 0.0;
+    if (i < n) {
+        cd acc = cmul(psi_in[i], ps->yt[1]);
+        for (int j = 2; j <= m; ++j) acc = cadd(acc, cmul(Q[(size_t)j * n + i], ps->yt[j]));
+        out[i] = acc;
+        nn = cabs2(acc);
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(nn, 0.0, partial, &ps->ticket[0], out2) && threadIdx.x == 0) {
+        double nrm = sqrt(out2[0]);
+        ps->norm = nrm;
+        ps->invnorm = 1. / nrm;
+        if (!(nrm > 0.0) || !isfinite(nrm)) atomicCAS(&ps->status, 0, DQ_ERR_NAN);
+    }
+}
+
+// psi_out *= 1/||psi_out||; optionally adds |psi|^2 into pops_row and
+// <psi0|psi> into corr_pt.
+__global__ void __launch_bounds__(kPlainThreads) k_renorm(int n, cd* out, const cd* __restrict__ psi0,
+                                                         double* pops_row, cd* corr_pt, double* partial,
+                                                         PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double cr = 0.0, ci = 0.0;
+    if (i < n) {
+        cd v = cscale(out[i], ps->invnorm);
+        out[i] = v;
+        if (pops_row) pops_row[i] += cabs2(v);
+        if (corr_pt) {
+            cd c = cmul(cconj(psi0[i]), v);
+            cr = c.x;
+            ci = c.y;
+        }
+    }
+    if (corr_pt) {
+        __shared__ double out2[2];
+        if (reduce2_last(cr, ci, partial, &ps->ticket[3], out2) && threadIdx.x == 0) {
+            corr_pt->x += out2[0];
+            corr_pt->y += out2[1];
+        }
+    }
+}
+
+__global__ void k_observe_initial(int n, const cd* __restrict__ psi0, double* pops_row, cd* corr_pt,
+                                  double* partial, PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double cr = 0.0, ci = 0.0;
+    if (i < n) {
+        cd v = psi0[i];
+        pops_row[i] += cabs2(v);
+        cd c = cmul(cconj(v), v);
+        cr = c.x;
+        ci = c.y;
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(cr, ci, partial, &ps->ticket[3], out2) && threadIdx.x == 0) {
+        corr_pt->x += out2[0];
+        corr_pt->y += out2[1];
+    }
+}
+
+// ------------------------------------------------------------------------
+dq_status check_cuda(dq_ctx* c, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return DQ_OK;
+    c->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return DQ_ERR_CUDA;
+}
+
+dq_status read_status(dq_ctx* c, int code, const char* what) {
+    if (code == DQ_OK) return DQ_OK;
+    static const char* names[] = {"ok", "argument", "cuda", "Lanczos breakdown (beta_j == 0)",
+                                  "non-finite value", "device wait timed out", "Padé scaling s >= 50",
+                                  "call out of order", "Padé denominator singular"};
+    c->err = std::string(what) + ": " + (code > 0 && code <= 8 ? names[code] : "unknown device error");
+    return code;
+}
+
+#define DQ_CU(call)                                                     \
+    do {                                                                \
+        dq_status _s = check_cuda(c, (call), #call);                    \
+        if (_s != DQ_OK) return _s;                                     \
+    } while (0)
+
+dq_status plain_alloc(dq_ctx* c) {
+    const int n = c->n, B = c->cfg.n_traj, m = c->cfg.m;
+    DQ_CU(cudaMalloc(&c->d_eps_p, sizeof(double) * (size_t)n * B));
+    DQ_CU(cudaMalloc(&c->d_deps_p, sizeof(double) * (size_t)n * B));
+    DQ_CU(cudaMalloc(&c->d_diag, sizeof(double) * n));
+    DQ_CU(cudaMalloc(&c->d_Q, sizeof(cd) * (size_t)n * (m + 2)));
+    DQ_CU(cudaMalloc(&c->d_w, sizeof(cd) * n));
+    DQ_CU(cudaMalloc(&c->d_psi_a, sizeof(cd) * n));
+    DQ_CU(cudaMalloc(&c->d_psi_b, sizeof(cd) * n));
+    DQ_CU(cudaMalloc(&c->d_partial, sizeof(double) * 2 * kMaxPartials));
+    DQ_CU(cudaMalloc(&c->d_ps, sizeof(PlainScalars)));
+    DQ_CU(cudaMemsetAsync(c->d_ps, 0, sizeof(PlainScalars), c->stream));
+    DQ_CU(cudaMemsetAsync(c->d_Q, 0, sizeof(cd) * (size_t)n * (m + 2), c->stream));
+    size_t smem = pade_smem_bytes(m + 2);
+    DQ_CU(cudaFuncSetAttribute(k_pade_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    return DQ_OK;
+}
+
+void plain_free(dq_ctx* c) {
+    cudaFree(c->d_eps_p); cudaFree(c->d_deps_p); cudaFree(c->d_diag); cudaFree(c->d_Q); cudaFree(c->d_w);
+    cudaFree(c->d_psi_a); cudaFree(c->d_psi_b); cudaFree(c->d_partial); cudaFree(c->d_ps);
+    c->d_eps_p = c->d_deps_p = c->d_diag = c->d_partial = nullptr;
+    c->d_Q = c->d_w = c->d_psi_a = c->d_psi_b = nullptr;
+    c->d_ps = nullptr;
+}
+
+dq_status plain_traj_init(dq_ctx* c) {
+    const int n = c->n, B = c->cfg.n_traj;
+    size_t total = (size_t)n * B;
+    int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    k_traj_init_plain<<<blocks, 256, 0, c->stream>>>(n, B, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
+                                                     c->d_sigma, c->cfg.noise_model, c->d_eps_p, c->d_deps_p);
+    DQ_CU(cudaGetLastError());
+    DQ_CU(cudaMemsetAsync(&c->d_ps->status, 0, sizeof(int), c->stream));
+    return DQ_OK;
+}
+
+dq_status plain_clear_observables(dq_ctx* c) {
+    DQ_CU(cudaMemsetAsync(c->d_pops, 0, sizeof(double) * (size_t)c->n_rec_max * c->n, c->stream));
+    DQ_CU(cudaMemsetAsync(c->d_corr, 0, sizeof(cd) * (size_t)(c->cfg.max_steps + 1), c->stream));
+    DQ_CU(cudaMemsetAsync(c->d_erracc, 0, sizeof(double) * c->cfg.n_traj, c->stream));
+    return DQ_OK;
+}
+
+// One plain step.  observe: add the result into the observable sums; rec >= 0
+// selects the population record to add |psi|^2 into (or -1).
+dq_status plain_step(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_out, bool observe, int rec) {
+    const int n = c->n, m = c->cfg.m;
+    const int T = kPlainThreads;
+    const int G = (n + T - 1) / T;
+    cudaStream_t st = c->stream;
+    const int ns = c->cfg.ka_substeps > 0 ? c->cfg.ka_substeps : 1;
+    const double subdt = c->cfg.dt / (double)ns;
+    const double sqrt_subdt = sqrt(subdt);
+    const double* eps = c->d_eps_p + (size_t)traj * n;
+    double* deps = c->d_deps_p + (size_t)traj * n;
+    k_noise<<<G, T, 0, st>>>(n, traj, step, c->cfg.noise_model, ns, subdt, sqrt_subdt, c->cfg.seed, c->d_sigma,
+                             c->d_invtau, c->d_coeff, eps, deps, c->d_diag, c->d_ps);
+    for (int j = 1; j <= m; ++j) {
+        const cd* rj = (j == 1) ? psi_in : c->d_Q + (size_t)j * n;
+        const cd* rjm = (j <= 1) ? nullptr : (j == 2 ? psi_in : c->d_Q + (size_t)(j - 1) * n);
+        cd* rjp = c->d_Q + (size_t)(j + 1) * n;
+        if (c->cfg.dot_mode == DQ_DOT_BILINEAR)
+            k_spmv_alpha<true><<<G, T, 0, st>>>(n, j, c->d_rowptr, c->d_col, c->d_val, c->d_diag, rj, c->d_w,
+                                                c->d_partial, c->d_ps);
+        else
+            k_spmv_alpha<false><<<G, T, 0, st>>>(n, j, c->d_rowptr, c->d_col, c->d_val, c->d_diag, rj, c->d_w,
+                                                 c->d_partial, c->d_ps);
+        k_axpy_norm<<<G, T, 0, st>>>(n, j, c->d_w, rj, rjm, rjp, c->d_partial, c->d_ps);
+    }
+    k_spmv_norm<<<G, T, 0, st>>>(n, m + 1, c->d_rowptr, c->d_col, c->d_val, c->d_diag, c->d_Q + (size_t)(m + 1) * n,
+                                 c->d_partial, c->d_ps);
+    k_pade_plain<<<1, 256, pade_smem_bytes(m + 2), st>>>(m, c->tau_im, c->cfg.norm_mode, c->d_ps,
+                                                         observe ? c->d_erracc : nullptr, traj);
+    k_combine<<<G, T, 0, st>>>(n, m, psi_in, c->d_Q, psi_out, c->d_partial, c->d_ps);
+    double* prow = (observe && rec >= 0) ? c->d_pops + (size_t)rec * n : nullptr;
+    cd* cpt = observe ? c->d_corr + (step + 1) : nullptr;
+    k_renorm<<<G, T, 0, st>>>(n, psi_out, c->d_psi0, prow, cpt, c->d_partial, c->d_ps);
+    DQ_CU(cudaGetLastError());
+    return DQ_OK;
+}
+
+dq_status plain_observe_initial(dq_ctx* c) {
+    const int n = c->n;
+    const int G = (n + kPlainThreads - 1) / kPlainThreads;
+    k_observe_initial<<<G, kPlainThreads, 0, c->stream>>>(n, c->d_psi0, c->d_pops, c->d_corr, c->d_partial, c->d_ps);
+    DQ_CU(cudaGetLastError());
+    return DQ_OK;
+}
+
+}  // namespace dq

@@ -1,0 +1,185 @@
+/*
+ * dq.h — C ABI of dynaquant_b200, a B200 (sm_100a) implementation of
+ * DynaQuant's stochastic-Hamiltonian exciton propagator.
+ *
+ * One time step of the reference is four calls on three objects
+ * (propagate.cu:226-248):
+ *     lanczosClass::doLanczos(psi_src)      lanczosClass.cu:232
+ *     padeClass::doPade()                   padeClass.cu:206
+ *     propagateSystem(sys, lan, pade, dest) propStep.cu:10
+ *     systemClass::renormalizeAndStoreNorm  systemClass.cu:1771
+ * preceded by systemClass::updateHamiltonian(t) (systemClass.cu:1883), and
+ * followed by calculateErrorEstimate (systemClass.cu:2057).  dq_prop_step
+ * below is that whole sequence as one stream-ordered call; dq_run is the
+ * batched ensemble form of propagate.cu's run loop (propagate.cu:167-298).
+ *
+ * Conventions: every function returns dq_status (0 = DQ_OK);
+ * dq_last_error(ctx) gives the message of the last failure.  Host arrays are
+ * copied and stay owned by the caller.  A context is single-threaded; work is
+ * ordered on the context's stream (dq_get_stream).  Units: energies cm^-1,
+ * time fs.
+ */
+#ifndef DQ_H
+#define DQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define DQ_API __attribute__((visibility("default")))
+#else
+#define DQ_API
+#endif
+
+typedef struct dq_ctx dq_ctx;
+typedef int dq_status;
+typedef struct { double re, im; } dq_cdouble;
+
+enum {
+    DQ_OK = 0,
+    DQ_ERR_ARG = 1,       /* invalid argument or size */
+    DQ_ERR_CUDA = 2,      /* CUDA runtime error (allocation, launch) */
+    DQ_ERR_BREAKDOWN = 3, /* Lanczos beta_j == 0 (lucky breakdown) */
+    DQ_ERR_NAN = 4,       /* non-finite value or norm drift detected */
+    DQ_ERR_TIMEOUT = 5,   /* a bounded device wait gave up */
+    DQ_ERR_SCALING = 6,   /* Padé scaling s >= 50 (padeClass.cu:618-623) */
+    DQ_ERR_STATE = 7,     /* call out of order (e.g. backward before forward) */
+    DQ_ERR_SINGULAR = 8   /* Padé denominator singular (padeClass.cu:735-738) */
+};
+
+/* Noise on the diagonal site energies (includeFiles.cu:19-25). */
+enum { DQ_NOISE_NONE = 0, DQ_NOISE_GAUSS = 1 /* SIM_TYPE_HSR */, DQ_NOISE_OU = 2 /* SIM_TYPE_KUBO_ANDERSON */ };
+/* Lanczos alpha: DQ_DOT_BILINEAR is the reference's unconjugated cublasZdotu
+ * (lanczosClass.cu:421); DQ_DOT_HERMITIAN the Hermitian inner product. */
+enum { DQ_DOT_BILINEAR = 0, DQ_DOT_HERMITIAN = 1 };
+/* Padé scaling norm: DQ_NORM_REAL_ONLY sums |Re| as gpuPadeHelper.cu:25 does;
+ * DQ_NORM_COMPLEX sums |.|. */
+enum { DQ_NORM_REAL_ONLY = 0, DQ_NORM_COMPLEX = 1 };
+/* Ensemble path precision: complex128 everywhere, or complex64 vectors with
+ * FP64 Lanczos scalars and FP64 Padé. */
+enum { DQ_PREC_FP64 = 0, DQ_PREC_MIXED = 1 };
+
+typedef struct dq_config {
+    int n_sites;            /* N */
+    int m;                  /* Krylov dimension (2..32); the maximum when adaptive */
+    int n_traj;             /* trajectories held by the context (B) */
+    double dt;              /* fs */
+    double hbar;            /* cm^-1 fs; <= 0 selects the reference's value (cppUtility.cpp:19-22) */
+    int noise_model;        /* DQ_NOISE_* */
+    int ka_substeps;        /* OU Euler-Maruyama substeps per step (ka_substeps key) */
+    double sigma_static;    /* static disorder sigma (cm^-1), redrawn per trajectory */
+    uint64_t seed;          /* Philox key */
+    int dot_mode;           /* DQ_DOT_* */
+    int norm_mode;          /* DQ_NORM_* */
+    int precision;          /* DQ_PREC_*: ensemble path (dq_run) */
+    int reorth;             /* 1: full reorthogonalisation (Hermitian dot only) */
+    int pop_every;          /* record ensemble populations every k steps */
+    int m_min;              /* adaptive Krylov dimension: lower bound (0 = fixed m) */
+    double m_tol;           /* adaptive Krylov dimension: EXPOKIT error tolerance */
+    int max_steps;          /* capacity of the correlation / population records */
+    int device;             /* CUDA device ordinal */
+} dq_config;
+
+/* Fills defaults: m 16, dt 1, reference hbar, no noise, 1 substep,
+ * Hermitian dot, complex norm, mixed precision, pop_every 1, max_steps 1024. */
+DQ_API void dq_config_default(dq_config *cfg);
+
+DQ_API dq_status dq_create(const dq_config *cfg, dq_ctx **out);
+DQ_API void dq_destroy(dq_ctx *ctx);
+DQ_API const char *dq_last_error(const dq_ctx *ctx);
+/* cudaStream_t the context orders its work on. */
+DQ_API void *dq_get_stream(dq_ctx *ctx);
+
+/* Hamiltonian as CSR including every diagonal entry (the reference requires
+ * all diagonals for a fluctuating Hamiltonian, sparseMatrixClasses.cu:173-251).
+ * Replaces matCooClass::readInFile + matCsrClass::pointToCooAndConvert +
+ * systemClass::prepForNonConstHam (sparseMatrixClasses.cu:75-540,
+ * systemClass.cu:810-870).  The diagonal becomes the static site energies;
+ * off-diagonal couplings are stored once and shared by all trajectories. */
+DQ_API dq_status dq_set_hamiltonian_csr(dq_ctx *ctx, int n, const int *rowptr, const int *col,
+                                        const double *val);
+/* Optional coupling classes: cls[k] in [0, n_classes) for the k-th
+ * OFF-DIAGONAL entry of the CSR given to dq_set_hamiltonian_csr (CSR order,
+ * diagonal entries skipped); that coupling is scaled by scales[cls[k]]. */
+DQ_API dq_status dq_set_coupling_classes(dq_ctx *ctx, const int *cls, int n_classes, const double *scales);
+/* Per-site noise parameters: sigma (cm^-1) and, for OU, tau (fs).
+ * Replaces prepForKA / prepForHsr (systemClass.cu:912-1071). */
+DQ_API dq_status dq_set_noise_params(dq_ctx *ctx, const double *sigma, const double *tau);
+/* Explicit static site energies shared by all trajectories (replaces the
+ * Hamiltonian diagonal plus static disorder); NULL restores them. */
+DQ_API dq_status dq_set_static_energies(dq_ctx *ctx, const double *eps);
+/* Initial state (host, N complex); replaces setInitState /
+ * initStateAsBasisVector / spectraClass::prepInitState. */
+DQ_API dq_status dq_set_initial_state(dq_ctx *ctx, const dq_cdouble *psi0);
+/* Redraws static disorder and OU offsets for every trajectory, sets every
+ * trajectory to psi0 and clears the observable records (prepAnalysesForNextRun,
+ * systemClass.cu:1554-1608). */
+DQ_API dq_status dq_reset(dq_ctx *ctx);
+
+/* ---- plain FP64 per-trajectory form: the drop-in for propStep ---- */
+/* One step of trajectory `traj` at step index `step`: noise update of that
+ * trajectory's diagonal, m-step Lanczos, Padé exp, psi_out = V exp(tau T) e1,
+ * renormalisation.  psi_in/psi_out are DEVICE pointers to N complex128
+ * (may not alias).  If err_est is non-NULL the call synchronises and writes
+ * the EXPOKIT error estimate there.  Steps of a trajectory must be issued in
+ * order (its OU offsets advance with each call). */
+DQ_API dq_status dq_prop_step(dq_ctx *ctx, int traj, int step, const dq_cdouble *psi_in_dev,
+                              dq_cdouble *psi_out_dev, double *err_est);
+/* Runs every trajectory through dq_prop_step's kernels one after another for
+ * n_steps, accumulating populations / correlation / error on the device. */
+DQ_API dq_status dq_run_plain(dq_ctx *ctx, int n_steps);
+
+/* ---- batched ensemble form ---- */
+/* Advances all trajectories by n_steps with the configured precision
+ * (shared-structure SpMM Lanczos over all trajectories, batched FP64 Padé,
+ * fused combine/observables), the step loop captured in a CUDA graph. */
+DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
+
+/* Kernel kinds of one ensemble step, for dq_profile_step. */
+enum {
+    DQ_KIND_NOISE = 0,      /* OU / Gaussian diagonal update */
+    DQ_KIND_SPMM = 1,       /* SpMM w = H q_j fused with alpha_j */
+    DQ_KIND_AXPY = 2,       /* r_{j+1} = w - alpha q_j - beta q_{j-1}, beta_j */
+    DQ_KIND_SPMM_NORM = 3,  /* ||H q_{m+1}|| for the error estimate */
+    DQ_KIND_PADE = 4,       /* batched Padé exponential */
+    DQ_KIND_COMBINE = 5,    /* psi = V y, norms, correlation */
+    DQ_KIND_POP = 6,        /* population record */
+    DQ_KIND_COUNT = 7
+};
+/* Advances all trajectories by n_steps exactly like dq_run, but launches the
+ * step's kernels eagerly with CUDA events between them; ms_per_launch[k]
+ * receives the mean device time of one launch of kind k (n_kinds entries,
+ * up to DQ_KIND_COUNT) and launches[k] their count (may be NULL). */
+DQ_API dq_status dq_profile_step(dq_ctx *ctx, int n_steps, double *ms_per_launch, int *launches, int n_kinds);
+
+/* ---- observables (host outputs, caller-owned) ---- */
+/* Ensemble-averaged populations, records at steps 0, pop_every, ...:
+ * (*n_records) x N doubles. Pass out = NULL to query n_records. */
+DQ_API dq_status dq_get_populations(dq_ctx *ctx, double *out, int *n_records);
+/* Ensemble-averaged <psi0|psi(t_k)> for k = 0..steps done (spectraClass.cu:510-571). */
+DQ_API dq_status dq_get_correlation(dq_ctx *ctx, dq_cdouble *out, int *n_points);
+/* Current normalised states, n_traj x N complex128. */
+DQ_API dq_status dq_get_states(dq_ctx *ctx, dq_cdouble *out);
+/* Accumulated EXPOKIT error per trajectory (systemClass.cu:2057-2085). */
+DQ_API dq_status dq_get_error_accum(dq_ctx *ctx, double *out);
+/* Steps done since dq_reset. */
+DQ_API int dq_steps_done(const dq_ctx *ctx);
+/* Static energies and OU offsets (FP64, N each) of one trajectory in the
+ * path that ran last; the step's diagonal is eps + deps for OU noise.  The
+ * counterpart of the reference's debug_diags dump (propagate.cu:214-223).
+ * Either pointer may be NULL. */
+DQ_API dq_status dq_get_noise_state(dq_ctx *ctx, int traj, double *eps, double *deps);
+
+/* Inverse DFT (cuFFT INVERSE convention, unnormalised) of the first
+ * n_in correlation points zero-padded to len (a power of two), on the GPU.
+ * Replaces spectraClass::singleSpectraCalc's cufftExecZ2Z (spectraClass.cu:621). */
+DQ_API dq_status dq_get_spectrum(dq_ctx *ctx, int len, dq_cdouble *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DQ_H */

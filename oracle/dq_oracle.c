@@ -1,0 +1,585 @@
+/*
+ * dq_oracle.c — CPU FP64 restatement of DynaQuant's stochastic-Hamiltonian
+ * Krylov propagator.  TEST INFRASTRUCTURE ONLY (the checker for the CUDA
+ * path; never linked into the product library).
+ *
+ * Follows, in order (files of nicolassawaya/DynaQuant):
+ *   gpuSysHelper.cu:73-128   OU (Kubo-Anderson) Euler-Maruyama noise update
+ *   gpuSysHelper.cu:32-66    Gaussian (Haken-Strobl-Reineker) noise
+ *   systemClass.cu:993-1036  OU parameters: coeff = sigma*sqrt(2/tau), subdt
+ *   systemClass.cu:760-804   static disorder eps = H0_ii + N(0, sigma_static)
+ *   lanczosClass.cu:397-531  Lanczos recurrence (q1 = psi, Q column 0 = 0)
+ *   lanczosClass.cu:537-570  ||H q_{m+1}|| for the error estimate
+ *   gpuLanczosHelper.cu:14-60 augmented tridiagonal T (EXPOKIT Theorem 1)
+ *   padeClass.cu:161-168     Padé c_k
+ *   padeClass.cu:206-487     Padé(6,6): A^2, A^4, A^6, odd/even parts, solve
+ *   padeClass.cu:585-706     scaling (|Re| row sums) and squaring
+ *   propStep.cu:31-44        psi_dest = Q[:,1..m] * E[0..m-1, 0]
+ *   systemClass.cu:1771-1829 renormalisation
+ *   padeClass.cu:750-782     EXPOKIT Algorithm 3.2 error estimate
+ *   spectraClass.cu:510-571  correlation <psi0|psi(t)> (Zdotc)
+ *   spectraClass.cu:621-626  inverse FFT (cuFFT INVERSE convention)
+ *
+ * Noise: the reference draws from cuRAND MRG32k3a / Boost mt19937 with
+ * wall-clock seeds.  This restatement instead keys Philox4x32-10 (Salmon,
+ * Moraes, Dror, Shaw, SC'11) by (seed, purpose, trajectory, step, site,
+ * substep) and turns uniforms into normals by Box-Muller with its own log
+ * (atanh series after binary range reduction) and sin/cos (octant reduction
+ * plus Taylor polynomials), all with explicit fma so the CUDA kernels
+ * reproduce every draw bit for bit.  Build with -ffp-contract=off.
+ */
+#include "dq_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Philox4x32-10                                                       */
+/* ------------------------------------------------------------------ */
+#define PHILOX_M0 0xD2511F53u
+#define PHILOX_M1 0xCD9E8D57u
+#define PHILOX_W0 0x9E3779B9u
+#define PHILOX_W1 0xBB67AE85u
+
+void dqo_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int r = 0; r < 10; ++r) {
+        if (r) { k0 += PHILOX_W0; k1 += PHILOX_W1; }
+        uint64_t p0 = (uint64_t)PHILOX_M0 * c0;
+        uint64_t p1 = (uint64_t)PHILOX_M1 * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* ------------------------------------------------------------------ */
+/* Elementary functions written from their series (bit-identical with  */
+/* the device versions: same operations, explicit fma).                */
+/* ------------------------------------------------------------------ */
+static const double LOG_C[12] = {
+    0x1.0000000000000p+0, 0x1.5555555555555p-2, 0x1.999999999999ap-3, 0x1.2492492492492p-3,
+    0x1.c71c71c71c71cp-4, 0x1.745d1745d1746p-4, 0x1.3b13b13b13b14p-4, 0x1.1111111111111p-4,
+    0x1.e1e1e1e1e1e1ep-5, 0x1.af286bca1af28p-5, 0x1.8618618618618p-5, 0x1.642c8590b2164p-5};
+static const double LN2_HI = 0x1.62e42fee00000p-1;
+static const double LN2_LO = 0x1.a39ef35793c76p-33;
+static const double SQRT2 = 0x1.6a09e667f3bcdp+0;
+/* sin: (-1)^k/(2k+1)!, cos: (-1)^k/(2k)!, k = 0..9 */
+static const double SIN_C[10] = {
+    0x1.0000000000000p+0, -0x1.5555555555555p-3, 0x1.1111111111111p-7, -0x1.a01a01a01a01ap-13,
+    0x1.71de3a556c734p-19, -0x1.ae64567f544e4p-26, 0x1.6124613a86d09p-33, -0x1.ae7f3e733b81fp-41,
+    0x1.952c77030ad4ap-49, -0x1.2f49b46814157p-57};
+static const double COS_C[10] = {
+    0x1.0000000000000p+0, -0x1.0000000000000p-1, 0x1.5555555555555p-5, -0x1.6c16c16c16c17p-10,
+    0x1.a01a01a01a01ap-16, -0x1.27e4fb7789f5cp-22, 0x1.1eed8eff8d898p-29, -0x1.93974a8c07c9dp-37,
+    0x1.ae7f3e733b81fp-45, -0x1.6827863b97d97p-53};
+static const double PIO4_HI = 0x1.921fb54442d18p-1;
+static const double PIO4_LO = 0x1.1a62633145c07p-55;
+
+/* natural log of a positive normal double: x = 2^e f, f in [sqrt(1/2), sqrt(2)),
+ * log f = 2 atanh(s), s = (f-1)/(f+1), series in s^2. */
+double dqo_log(double x) {
+    uint64_t b;
+    memcpy(&b, &x, 8);
+    int e = (int)((b >> 52) & 0x7ff) - 1023;
+    uint64_t mb = (b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL;
+    double f;
+    memcpy(&f, &mb, 8);
+    if (f > SQRT2) { f = f * 0.5; e += 1; }
+    double s = (f - 1.0) / (f + 1.0);
+    double z = s * s;
+    double p = LOG_C[11];
+    for (int k = 10; k >= 0; --k) p = fma(p, z, LOG_C[k]);
+    double ls = (s + s) * p;
+    double de = (double)e;
+    return fma(de, LN2_HI, fma(de, LN2_LO, ls));
+}
+
+static void sincos_pio4(double g, double *s, double *c) {
+    /* x = g*pi/4, g in [0,1] */
+    double x = fma(g, PIO4_HI, g * PIO4_LO);
+    double y = x * x;
+    double ps = SIN_C[9];
+    for (int k = 8; k >= 0; --k) ps = fma(ps, y, SIN_C[k]);
+    double pc = COS_C[9];
+    for (int k = 8; k >= 0; --k) pc = fma(pc, y, COS_C[k]);
+    *s = x * ps;
+    *c = pc;
+}
+
+/* sin and cos of 2*pi*u for u in [0,1): octant reduction on 8u (exact). */
+void dqo_sincos_2pi(double u, double *s, double *c) {
+    double t = u * 8.0;
+    int k = (int)t;
+    double f = t - (double)k;
+    double sa, ca;
+    if (k & 1) sincos_pio4(1.0 - f, &sa, &ca);
+    else sincos_pio4(f, &sa, &ca);
+    double S, C;
+    switch (k & 7) {
+        case 0: S = sa;  C = ca;  break;
+        case 1: S = ca;  C = sa;  break;
+        case 2: S = ca;  C = -sa; break;
+        case 3: S = sa;  C = -ca; break;
+        case 4: S = -sa; C = -ca; break;
+        case 5: S = -ca; C = -sa; break;
+        case 6: S = -ca; C = sa;  break;
+        default: S = -sa; C = ca; break;
+    }
+    *s = S;
+    *c = C;
+}
+
+/* Normal draw keyed by (seed, purpose, traj, step, site, sub).  One Philox
+ * block gives two uniforms of 53 bits and Box-Muller gives two normals; the
+ * even substep takes the cosine branch, the odd one the sine branch. */
+double dqo_normal(uint64_t seed, uint32_t purpose, uint32_t traj, uint32_t step,
+                  uint32_t site, uint32_t sub) {
+    uint32_t ctr[4] = {site, step, traj, (purpose << 24) | (sub >> 1)};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t o[4];
+    dqo_philox4x32_10(ctr, key, o);
+    uint64_t a = ((uint64_t)o[1] << 32) | o[0];
+    uint64_t b = ((uint64_t)o[3] << 32) | o[2];
+    double u1 = (double)((a >> 11) + 1) * 0x1.0p-53; /* (0,1] */
+    double u2 = (double)(b >> 11) * 0x1.0p-53;       /* [0,1) */
+    double r = sqrt(-2.0 * dqo_log(u1));
+    double sn, cs;
+    dqo_sincos_2pi(u2, &sn, &cs);
+    return (sub & 1) ? r * sn : r * cs;
+}
+
+/* hbar in cm^-1 fs exactly as cppUtility.cpp:19-22 computes it (note the
+ * reference's speed of light 299792548 m/s). */
+double dqo_hbar_reference(void) {
+    double pi = atan(1.0) * 4.0;
+    double lightspeed = 299792548.;
+    return (1 / 100.) * (1e15) * 1. / (lightspeed * 2 * pi);
+}
+
+/* padeClass.cu:161-168 */
+void dqo_pade_ck(int p, double *ck) {
+    ck[0] = 1.0;
+    double fp = (double)p;
+    for (int k = 1; k <= p; ++k) {
+        double fk = (double)k;
+        ck[k] = ck[k - 1] * (fp + 1. - fk) / ((2 * fp + 1. - fk) * fk);
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* complex helpers (interleaved re, im)                                */
+/* ------------------------------------------------------------------ */
+typedef struct { double re, im; } cx;
+static inline cx cmul(cx a, cx b) { cx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; return r; }
+static inline cx cadd(cx a, cx b) { cx r = {a.re + b.re, a.im + b.im}; return r; }
+static inline cx csub(cx a, cx b) { cx r = {a.re - b.re, a.im - b.im}; return r; }
+static inline cx cscale(cx a, double s) { cx r = {a.re * s, a.im * s}; return r; }
+static inline cx cconj(cx a) { cx r = {a.re, -a.im}; return r; }
+static inline double cabs2(cx a) { return a.re * a.re + a.im * a.im; }
+static inline cx cdiv(cx a, cx b) {
+    double d = b.re * b.re + b.im * b.im;
+    cx r = {(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+    return r;
+}
+
+/* C = A * B for L x L row-major complex */
+static void mat_mul(int L, const cx *A, const cx *B, cx *C) {
+    for (int i = 0; i < L; ++i)
+        for (int j = 0; j < L; ++j) {
+            cx s = {0, 0};
+            for (int k = 0; k < L; ++k) s = cadd(s, cmul(A[i * L + k], B[k * L + j]));
+            C[i * L + j] = s;
+        }
+}
+
+/* Solve D X = Nm in place (Nm overwritten with X); LU with partial pivoting
+ * by |.|^2.  Stands in for culaDeviceZgesv (padeClass.cu:715-745). */
+static int lu_solve(int L, cx *D, cx *Nm) {
+    for (int k = 0; k < L; ++k) {
+        int piv = k;
+        double best = cabs2(D[k * L + k]);
+        for (int i = k + 1; i < L; ++i) {
+            double v = cabs2(D[i * L + k]);
+            if (v > best) { best = v; piv = i; }
+        }
+        if (best == 0.0) return -1;
+        if (piv != k) {
+            for (int j = 0; j < L; ++j) {
+                cx t = D[k * L + j]; D[k * L + j] = D[piv * L + j]; D[piv * L + j] = t;
+                t = Nm[k * L + j]; Nm[k * L + j] = Nm[piv * L + j]; Nm[piv * L + j] = t;
+            }
+        }
+        cx inv = cdiv((cx){1.0, 0.0}, D[k * L + k]);
+        for (int i = k + 1; i < L; ++i) {
+            cx f = cmul(D[i * L + k], inv);
+            D[i * L + k] = f;
+            for (int j = k + 1; j < L; ++j) D[i * L + j] = csub(D[i * L + j], cmul(f, D[k * L + j]));
+            for (int j = 0; j < L; ++j) Nm[i * L + j] = csub(Nm[i * L + j], cmul(f, Nm[k * L + j]));
+        }
+    }
+    for (int k = L - 1; k >= 0; --k) {
+        cx inv = cdiv((cx){1.0, 0.0}, D[k * L + k]);
+        for (int j = 0; j < L; ++j) {
+            cx s = Nm[k * L + j];
+            for (int c = k + 1; c < L; ++c) s = csub(s, cmul(D[k * L + c], Nm[c * L + j]));
+            Nm[k * L + j] = cmul(s, inv);
+        }
+    }
+    return 0;
+}
+
+/* Padé(6,6) with scaling and squaring (padeClass.cu:206-487, 585-706).
+ * A is the already-scaled tau*Tbar. */
+int dqo_pade_exp(int L, const double *Ain, double *Eout, int norm_mode) {
+    size_t L2 = (size_t)L * L;
+    cx *A = (cx *)malloc(L2 * sizeof(cx) * 9);
+    cx *A2 = A + L2, *A4 = A2 + L2, *A6 = A4 + L2, *U = A6 + L2, *V = U + L2, *T1 = V + L2,
+       *D = T1 + L2, *E = D + L2;
+    memcpy(A, Ain, L2 * sizeof(cx));
+    double ck[7];
+    dqo_pade_ck(6, ck);
+    /* infinity norm: reference sums |Re| only (gpuPadeHelper.cu:25) */
+    double nrm = 0.0;
+    for (int i = 0; i < L; ++i) {
+        double rs = 0.0;
+        for (int j = 0; j < L; ++j) {
+            cx a = A[i * L + j];
+            rs += (norm_mode == DQO_NORM_REAL_ONLY) ? fabs(a.re) : sqrt(cabs2(a));
+        }
+        if (rs > nrm) nrm = rs;
+    }
+    int s = 0;
+    while (nrm > 0.5) { nrm *= 0.5; s++; }
+    if (s >= 50) { free(A); return -1; }
+    double sc = ldexp(1.0, -s);
+    for (size_t i = 0; i < L2; ++i) A[i] = cscale(A[i], sc);
+    mat_mul(L, A, A, A2);
+    mat_mul(L, A2, A2, A4);
+    mat_mul(L, A2, A4, A6);
+    /* odd part U = A (c1 I + c3 A^2 + c5 A^4) */
+    for (int i = 0; i < L; ++i)
+        for (int j = 0; j < L; ++j) {
+            size_t x = (size_t)i * L + j;
+            cx t = cadd(cscale(A2[x], ck[3]), cscale(A4[x], ck[5]));
+            if (i == j) t.re += ck[1];
+            T1[x] = t;
+        }
+    mat_mul(L, A, T1, U);
+    /* even part V = c0 I + c2 A^2 + c4 A^4 + c6 A^6 */
+    for (int i = 0; i < L; ++i)
+        for (int j = 0; j < L; ++j) {
+            size_t x = (size_t)i * L + j;
+            cx t = cadd(cadd(cscale(A2[x], ck[2]), cscale(A4[x], ck[4])), cscale(A6[x], ck[6]));
+            if (i == j) t.re += ck[0];
+            V[x] = t;
+            D[x] = csub(t, U[x]);
+        }
+    if (lu_solve(L, D, U) != 0) { free(A); return -2; }
+    for (int i = 0; i < L; ++i)
+        for (int j = 0; j < L; ++j) {
+            size_t x = (size_t)i * L + j;
+            cx t = cscale(U[x], 2.0);
+            if (i == j) t.re += 1.0;
+            E[x] = t;
+        }
+    for (int k = 0; k < s; ++k) {
+        mat_mul(L, E, E, T1);
+        memcpy(E, T1, L2 * sizeof(cx));
+    }
+    memcpy(Eout, E, L2 * sizeof(cx));
+    free(A);
+    return s;
+}
+
+/* ------------------------------------------------------------------ */
+/* noise                                                               */
+/* ------------------------------------------------------------------ */
+void dqo_traj_init(const dqo_system *sys, int traj, double *eps, double *deps) {
+    for (int i = 0; i < sys->n; ++i) {
+        if (sys->static_eps) {
+            eps[i] = sys->static_eps[i];
+        } else {
+            double z = dqo_normal(sys->seed, DQO_P_STATIC, (uint32_t)traj, 0, (uint32_t)i, 0);
+            eps[i] = sys->sigma_static * z + sys->h0diag[i];
+        }
+        if (sys->noise == DQO_NOISE_OU) {
+            double z = dqo_normal(sys->seed, DQO_P_OU_INIT, (uint32_t)traj, 0, (uint32_t)i, 0);
+            deps[i] = sys->sigma[i] * z;
+        } else {
+            deps[i] = 0.0;
+        }
+    }
+}
+
+void dqo_noise_update(const dqo_system *sys, int traj, int step, const double *eps, double *deps,
+                      double *diag) {
+    int n = sys->n;
+    if (sys->noise == DQO_NOISE_OU) {
+        int ns = sys->ka_substeps > 0 ? sys->ka_substeps : 1;
+        double subdt = sys->dt / (double)ns;
+        double sqrt_subdt = sqrt(subdt);
+        for (int i = 0; i < n; ++i) {
+            double inv_tau = 1. / sys->tau[i];
+            double coeff = sys->sigma[i] * sqrt(2. / sys->tau[i]);
+            double cur = deps[i];
+            for (int s = 0; s < ns; ++s) {
+                double xi = dqo_normal(sys->seed, DQO_P_OU, (uint32_t)traj, (uint32_t)step, (uint32_t)i,
+                                       (uint32_t)s);
+                cur = cur - cur * inv_tau * subdt + coeff * xi * sqrt_subdt;
+            }
+            deps[i] = cur;
+            diag[i] = cur + eps[i];
+        }
+    } else if (sys->noise == DQO_NOISE_GAUSS) {
+        for (int i = 0; i < n; ++i) {
+            double xi = dqo_normal(sys->seed, DQO_P_GAUSS, (uint32_t)traj, (uint32_t)step, (uint32_t)i, 0);
+            double noise = xi * sys->sigma[i];
+            diag[i] = noise + eps[i];
+        }
+    } else {
+        for (int i = 0; i < n; ++i) diag[i] = eps[i];
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Lanczos                                                             */
+/* ------------------------------------------------------------------ */
+static void spmv(const dqo_system *sys, const double *diag, const cx *x, cx *y) {
+    for (int i = 0; i < sys->n; ++i) {
+        cx s = cscale(x[i], diag[i]);
+        for (int p = sys->rowptr[i]; p < sys->rowptr[i + 1]; ++p) s = cadd(s, cscale(x[sys->col[p]], sys->val[p]));
+        y[i] = s;
+    }
+}
+
+double dqo_lanczos(const dqo_system *sys, const double *diag, const double *q1, double *Qd,
+                   double *alpha_d, double *beta_d) {
+    int n = sys->n, m = sys->m;
+    cx *Q = (cx *)Qd;
+    cx *alpha = (cx *)alpha_d, *beta = (cx *)beta_d;
+    cx *w = (cx *)malloc(sizeof(cx) * n);
+    memset(Q, 0, sizeof(cx) * (size_t)n * (m + 2));
+    memset(alpha, 0, sizeof(cx) * (m + 2));
+    memset(beta, 0, sizeof(cx) * (m + 2));
+    memcpy(Q + n, q1, sizeof(cx) * n);
+    for (int j = 1; j <= m; ++j) {
+        cx *qj = Q + (size_t)j * n, *qjm = Q + (size_t)(j - 1) * n, *qjp = Q + (size_t)(j + 1) * n;
+        spmv(sys, diag, qj, w);
+        cx a = {0, 0};
+        for (int i = 0; i < n; ++i)
+            a = cadd(a, cmul(sys->dot_mode == DQO_DOT_BILINEAR ? qj[i] : cconj(qj[i]), w[i]));
+        alpha[j] = a;
+        for (int i = 0; i < n; ++i) {
+            w[i] = csub(w[i], cmul(a, qj[i]));
+            w[i] = csub(w[i], cmul(beta[j - 1], qjm[i]));
+        }
+        double nn = 0.0;
+        for (int i = 0; i < n; ++i) nn += cabs2(w[i]);
+        double b = sqrt(nn);
+        /* lucky breakdown (the reference divides by zero here,
+         * gpuSimpleOps.cu:24-28): the Krylov space is invariant; q_{j+1} = 0
+         * decouples the rest of T and the step stays exact. */
+        if (b <= 1e-12 * (sqrt(cabs2(a)) + (j > 1 ? beta[j - 1].re : 0.0))) b = 0.0;
+        beta[j].re = b;
+        beta[j].im = 0.0;
+        double inv = b > 0.0 ? 1.0 / b : 0.0;
+        for (int i = 0; i < n; ++i) qjp[i] = cscale(w[i], inv);
+    }
+    spmv(sys, diag, Q + (size_t)(m + 1) * n, w);
+    double nn = 0.0;
+    for (int i = 0; i < n; ++i) nn += cabs2(w[i]);
+    free(w);
+    return sqrt(nn);
+}
+
+/* gpuLanczosHelper.cu:14-60, row-major L x L with L = m+2 */
+void dqo_build_tbar(int m, const double *alpha_d, const double *beta_d, double *Td) {
+    int L = m + 2;
+    const cx *alpha = (const cx *)alpha_d, *beta = (const cx *)beta_d;
+    cx *T = (cx *)Td;
+    memset(T, 0, sizeof(cx) * L * L);
+    for (int i = 0; i < m; ++i) {
+        T[i * L + i] = alpha[i + 1];
+        if (i + 1 < m) {
+            T[i * L + i + 1] = beta[i + 1];
+            T[(i + 1) * L + i] = beta[i + 1];
+        }
+    }
+    T[0 * L + m].re = 1.0;
+    T[m * L + m + 1].re = 1.0;
+}
+
+int dqo_krylov_step(const dqo_system *sys, const double *diag, const double *psi_in, double *psi_out,
+                    double *err_est, double *norm_out, int *s_out) {
+    int n = sys->n, m = sys->m, L = m + 2;
+    double *Q = (double *)malloc(sizeof(cx) * (size_t)n * (m + 2));
+    double *al = (double *)malloc(sizeof(cx) * (m + 2));
+    double *be = (double *)malloc(sizeof(cx) * (m + 2));
+    double *T = (double *)malloc(sizeof(cx) * L * L);
+    double *E = (double *)malloc(sizeof(cx) * L * L);
+    double nrm_av = dqo_lanczos(sys, diag, psi_in, Q, al, be);
+    dqo_build_tbar(m, al, be, T);
+    cx tau = {0.0, -sys->dt / sys->hbar};
+    cx *Tc = (cx *)T;
+    for (int i = 0; i < L * L; ++i) Tc[i] = cmul(tau, Tc[i]);
+    int s = dqo_pade_exp(L, T, E, sys->norm_mode);
+    if (s_out) *s_out = s;
+    if (s < 0) { free(Q); free(al); free(be); free(T); free(E); return s; }
+    cx *Ec = (cx *)E, *Qc = (cx *)Q, *out = (cx *)psi_out;
+    for (int i = 0; i < n; ++i) {
+        cx acc = {0, 0};
+        for (int j = 0; j < m; ++j) acc = cadd(acc, cmul(Qc[(size_t)(j + 1) * n + i], Ec[j * L + 0]));
+        out[i] = acc;
+    }
+    double nn = 0.0;
+    for (int i = 0; i < n; ++i) nn += cabs2(out[i]);
+    double nrm = sqrt(nn);
+    if (norm_out) *norm_out = nrm;
+    double inv = 1. / nrm;
+    for (int i = 0; i < n; ++i) out[i] = cscale(out[i], inv);
+    /* EXPOKIT Alg. 3.2 (padeClass.cu:750-782; systemClass.cu:2075-2077) */
+    if (err_est) {
+        cx *bec = (cx *)be;
+        double hm = sqrt(cabs2(bec[m]));
+        double err1 = hm * sqrt(cabs2(Ec[(m - 1) * L + m]));
+        double err2 = hm * nrm_av * sqrt(cabs2(Ec[(m - 1) * L + m + 1]));
+        double est = (err1 > err2) ? err2 / (1 - err2 / err1) : err1;
+        if (est < 1.110223e-16) est = 1.110223e-16;
+        *err_est = est;
+    }
+    free(Q); free(al); free(be); free(T); free(E);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* ensemble                                                            */
+/* ------------------------------------------------------------------ */
+int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const double *psi0d, int pop_every,
+            double *pops, double *corr, double *psi_final, double *err_acc, int n_threads) {
+    int n = sys->n;
+    int n_rec = n_steps / pop_every + 1;
+    int nt = 1;
+#ifdef _OPENMP
+    nt = n_threads > 0 ? n_threads : omp_get_max_threads();
+    if (nt > n_traj) nt = n_traj;
+    if (nt < 1) nt = 1;
+#endif
+    double *pacc = (double *)calloc((size_t)nt * n_rec * n, sizeof(double));
+    double *cacc = (double *)calloc((size_t)nt * (n_steps + 1) * 2, sizeof(double));
+    int status = 0;
+    const cx *psi0 = (const cx *)psi0d;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nt)
+#endif
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double *myp = pacc + (size_t)tid * n_rec * n;
+        double *myc = cacc + (size_t)tid * (n_steps + 1) * 2;
+        double *eps = (double *)malloc(sizeof(double) * n * 3);
+        double *deps = eps + n, *diag = deps + n;
+        cx *psi = (cx *)malloc(sizeof(cx) * n * 2);
+        cx *tmp = psi + n;
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+        for (int t = 0; t < n_traj; ++t) {
+            int traj = traj0 + t;
+            dqo_traj_init(sys, traj, eps, deps);
+            memcpy(psi, psi0, sizeof(cx) * n);
+            double errsum = 0.0;
+            cx c = {0, 0};
+            for (int i = 0; i < n; ++i) c = cadd(c, cmul(cconj(psi0[i]), psi[i]));
+            myc[0] += c.re; myc[1] += c.im;
+            for (int i = 0; i < n; ++i) myp[i] += cabs2(psi[i]);
+            for (int k = 0; k < n_steps; ++k) {
+                dqo_noise_update(sys, traj, k, eps, deps, diag);
+                double est;
+                int rc = dqo_krylov_step(sys, diag, (const double *)psi, (double *)tmp, &est, NULL, NULL);
+                if (rc != 0) { status = rc; break; }
+                errsum += est;
+                memcpy(psi, tmp, sizeof(cx) * n);
+                c.re = 0; c.im = 0;
+                for (int i = 0; i < n; ++i) c = cadd(c, cmul(cconj(psi0[i]), psi[i]));
+                myc[2 * (k + 1)] += c.re; myc[2 * (k + 1) + 1] += c.im;
+                if ((k + 1) % pop_every == 0) {
+                    double *row = myp + (size_t)((k + 1) / pop_every) * n;
+                    for (int i = 0; i < n; ++i) row[i] += cabs2(psi[i]);
+                }
+            }
+            if (psi_final) memcpy(psi_final + (size_t)t * n * 2, psi, sizeof(cx) * n);
+            if (err_acc) err_acc[t] = errsum;
+        }
+        free(eps);
+        free(psi);
+    }
+    double inv = 1.0 / n_traj;
+    if (pops) {
+        for (size_t x = 0; x < (size_t)n_rec * n; ++x) {
+            double s = 0.0;
+            for (int t = 0; t < nt; ++t) s += pacc[(size_t)t * n_rec * n + x];
+            pops[x] = s * inv;
+        }
+    }
+    if (corr) {
+        for (int x = 0; x < (n_steps + 1) * 2; ++x) {
+            double s = 0.0;
+            for (int t = 0; t < nt; ++t) s += cacc[(size_t)t * (n_steps + 1) * 2 + x];
+            corr[x] = s * inv;
+        }
+    }
+    free(pacc);
+    free(cacc);
+    return status;
+}
+
+/* ------------------------------------------------------------------ */
+/* inverse DFT, cuFFT INVERSE convention: X_k = sum_j x_j e^{+2 pi i jk/n} */
+/* ------------------------------------------------------------------ */
+void dqo_ifft(int n, double *xd) {
+    cx *x = (cx *)xd;
+    if (n <= 1) return;
+    if ((n & (n - 1)) == 0) {
+        for (int i = 1, j = 0; i < n; ++i) {
+            int bit = n >> 1;
+            for (; j & bit; bit >>= 1) j ^= bit;
+            j ^= bit;
+            if (i < j) { cx t = x[i]; x[i] = x[j]; x[j] = t; }
+        }
+        for (int len = 2; len <= n; len <<= 1) {
+            double ang = 2.0 * M_PI / len;
+            for (int i = 0; i < n; i += len) {
+                for (int k = 0; k < len / 2; ++k) {
+                    cx w = {cos(ang * k), sin(ang * k)};
+                    cx u = x[i + k], v = cmul(x[i + k + len / 2], w);
+                    x[i + k] = cadd(u, v);
+                    x[i + k + len / 2] = csub(u, v);
+                }
+            }
+        }
+    } else {
+        cx *y = (cx *)malloc(sizeof(cx) * n);
+        for (int k = 0; k < n; ++k) {
+            cx s = {0, 0};
+            for (int j = 0; j < n; ++j) {
+                double ang = 2.0 * M_PI * (double)(((long long)j * k) % n) / n;
+                cx w = {cos(ang), sin(ang)};
+                s = cadd(s, cmul(x[j], w));
+            }
+            y[k] = s;
+        }
+        memcpy(x, y, sizeof(cx) * n);
+        free(y);
+    }
+}

@@ -1,0 +1,102 @@
+/*
+ * dq_oracle.h — CPU FP64 restatement of DynaQuant's stochastic-Hamiltonian
+ * Krylov step.  TEST INFRASTRUCTURE ONLY: the checker that the CUDA path is
+ * compared against.  Nothing in the product library links or calls it; only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ *
+ * Parity pins: Padé c_k and hbar/expCoeff against the reference's captured
+ * log (out:76-83), the Padé exponential against scipy.linalg.expm, the full
+ * step against dense expm(-i dt H/hbar), Philox against the published
+ * Random123 known answers and cuRAND's device generator.  The reference's
+ * own trajectories are not reproducible (wall-clock seeds, missing
+ * Hamiltonian file), so trajectory-level golden vectors are generated by
+ * this oracle with fixed Philox seeds (tests/golden/make_golden.py).
+ */
+#ifndef DQ_ORACLE_H
+#define DQ_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Noise models (reference enum simulationType, includeFiles.cu:19-25). */
+enum { DQO_NOISE_NONE = 0, DQO_NOISE_GAUSS = 1, DQO_NOISE_OU = 2 };
+/* Lanczos alpha: reference-exact unconjugated dot (lanczosClass.cu:421,
+ * cublasZdotu) or the Hermitian inner product. */
+enum { DQO_DOT_BILINEAR = 0, DQO_DOT_HERMITIAN = 1 };
+/* Padé scaling norm: reference |Re|-only row sums (gpuPadeHelper.cu:25) or
+ * the complex-modulus infinity norm. */
+enum { DQO_NORM_REAL_ONLY = 0, DQO_NORM_COMPLEX = 1 };
+/* Philox purposes (the fourth counter word's top byte). */
+enum { DQO_P_OU = 1, DQO_P_GAUSS = 2, DQO_P_OU_INIT = 3, DQO_P_STATIC = 4 };
+
+typedef struct {
+    int n;                 /* sites */
+    const int *rowptr;     /* off-diagonal CSR, n+1 */
+    const int *col;        /* off-diagonal column indices */
+    const double *val;     /* off-diagonal couplings (cm^-1), already scaled */
+    const double *h0diag;  /* diagonal of the input Hamiltonian (cm^-1), n */
+    int m;                 /* Krylov dimension */
+    double dt;             /* fs */
+    double hbar;           /* cm^-1 fs */
+    int dot_mode;
+    int norm_mode;
+    int noise;             /* DQO_NOISE_* */
+    int ka_substeps;       /* OU Euler-Maruyama substeps per step */
+    const double *sigma;   /* per-site noise sigma (cm^-1), n (or NULL) */
+    const double *tau;     /* per-site OU correlation time (fs), n (or NULL) */
+    double sigma_static;   /* static disorder sigma, redrawn per trajectory */
+    const double *static_eps; /* optional explicit static energies (n), replaces h0diag+disorder */
+    uint64_t seed;
+} dqo_system;
+
+/* ---- building blocks ---- */
+void dqo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+double dqo_log(double x);
+void dqo_sincos_2pi(double u, double *s, double *c);
+double dqo_normal(uint64_t seed, uint32_t purpose, uint32_t traj, uint32_t step,
+                  uint32_t site, uint32_t sub);
+double dqo_hbar_reference(void);
+void dqo_pade_ck(int p, double *ck);
+/* exp of an L x L complex matrix A (row-major interleaved re/im), Padé(6,6)
+ * with scaling and squaring; returns s (or -1 when s >= 50). */
+int dqo_pade_exp(int L, const double *A, double *E, int norm_mode);
+
+/* ---- one trajectory ---- */
+/* Per-trajectory state: static energies eps (n), OU offsets deps (n). */
+void dqo_traj_init(const dqo_system *sys, int traj, double *eps, double *deps);
+/* Noise update for step `step` (gpuSysHelper.cu:73-128 / :32-66): writes the
+ * step's diagonal into diag (n) and advances deps. */
+void dqo_noise_update(const dqo_system *sys, int traj, int step, const double *eps,
+                      double *deps, double *diag);
+/* Lanczos + Padé + combine + renorm for one step. psi_in/psi_out are n complex
+ * (interleaved).  Returns 0 on success; err_est gets the EXPOKIT estimate,
+ * norm_out the pre-renormalisation norm, s_out the Padé scaling. */
+int dqo_krylov_step(const dqo_system *sys, const double *diag, const double *psi_in,
+                    double *psi_out, double *err_est, double *norm_out, int *s_out);
+/* Lanczos only: Q (m+2) columns of n complex each (column 0 zero), alpha and
+ * beta (m+2 complex each), returns ||H q_{m+1}||. */
+double dqo_lanczos(const dqo_system *sys, const double *diag, const double *q1,
+                   double *Q, double *alpha, double *beta);
+void dqo_build_tbar(int m, const double *alpha, const double *beta, double *T);
+
+/* ---- ensemble run ---- */
+/* Runs trajectories traj0..traj0+n_traj-1 for n_steps from psi0 (n complex).
+ * pops: (n_steps/pop_every + 1) x n, ensemble-averaged |psi|^2 at steps
+ * 0, pop_every, ...; corr: (n_steps+1) complex, averaged <psi0|psi(t)>;
+ * psi_final: n_traj x n complex (may be NULL); err_acc: n_traj (may be NULL).
+ * Returns 0 or a negative error code. */
+int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const double *psi0,
+            int pop_every, double *pops, double *corr, double *psi_final, double *err_acc,
+            int n_threads);
+
+/* ---- spectrum ---- */
+/* In-place inverse DFT (sign +1, unnormalised, cuFFT INVERSE convention) of
+ * n complex values; radix-2 when n is a power of two, direct sum otherwise. */
+void dqo_ifft(int n, double *x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

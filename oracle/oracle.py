@@ -1,0 +1,220 @@
+"""ctypes front end of the CPU FP64 oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY.  tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg import this module as the checker; the product library
+(dynaquant_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+
+NOISE_NONE, NOISE_GAUSS, NOISE_OU = 0, 1, 2
+DOT_BILINEAR, DOT_HERMITIAN = 0, 1
+NORM_REAL_ONLY, NORM_COMPLEX = 0, 1
+P_OU, P_GAUSS, P_OU_INIT, P_STATIC = 1, 2, 3, 4
+
+
+def build() -> str:
+    """Compile liboracle.so with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+class _System(C.Structure):
+    _fields_ = [
+        ("n", C.c_int),
+        ("rowptr", C.POINTER(C.c_int)),
+        ("col", C.POINTER(C.c_int)),
+        ("val", C.POINTER(C.c_double)),
+        ("h0diag", C.POINTER(C.c_double)),
+        ("m", C.c_int),
+        ("dt", C.c_double),
+        ("hbar", C.c_double),
+        ("dot_mode", C.c_int),
+        ("norm_mode", C.c_int),
+        ("noise", C.c_int),
+        ("ka_substeps", C.c_int),
+        ("sigma", C.POINTER(C.c_double)),
+        ("tau", C.POINTER(C.c_double)),
+        ("sigma_static", C.c_double),
+        ("static_eps", C.POINTER(C.c_double)),
+        ("seed", C.c_uint64),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = C.CDLL(_LIB)
+        dp = C.POINTER(C.c_double)
+        L.dqo_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.dqo_log.argtypes = [C.c_double]
+        L.dqo_log.restype = C.c_double
+        L.dqo_sincos_2pi.argtypes = [C.c_double, dp, dp]
+        L.dqo_normal.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.dqo_normal.restype = C.c_double
+        L.dqo_hbar_reference.restype = C.c_double
+        L.dqo_pade_ck.argtypes = [C.c_int, dp]
+        L.dqo_pade_exp.argtypes = [C.c_int, dp, dp, C.c_int]
+        L.dqo_pade_exp.restype = C.c_int
+        sp = C.POINTER(_System)
+        L.dqo_traj_init.argtypes = [sp, C.c_int, dp, dp]
+        L.dqo_noise_update.argtypes = [sp, C.c_int, C.c_int, dp, dp, dp]
+        L.dqo_krylov_step.argtypes = [sp, dp, dp, dp, dp, dp, C.POINTER(C.c_int)]
+        L.dqo_krylov_step.restype = C.c_int
+        L.dqo_lanczos.argtypes = [sp, dp, dp, dp, dp, dp]
+        L.dqo_lanczos.restype = C.c_double
+        L.dqo_build_tbar.argtypes = [C.c_int, dp, dp, dp]
+        L.dqo_run.argtypes = [sp, C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_int]
+        L.dqo_run.restype = C.c_int
+        L.dqo_ifft.argtypes = [C.c_int, dp]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double)) if a is not None else None
+
+
+def philox(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    lib().dqo_philox4x32_10(c, k, o)
+    return list(o)
+
+
+def log(x):
+    return lib().dqo_log(float(x))
+
+
+def sincos_2pi(u):
+    s, c = C.c_double(), C.c_double()
+    lib().dqo_sincos_2pi(float(u), C.byref(s), C.byref(c))
+    return s.value, c.value
+
+
+def normal(seed, purpose, traj, step, site, sub=0):
+    return lib().dqo_normal(seed, purpose, traj, step, site, sub)
+
+
+def hbar_reference():
+    return lib().dqo_hbar_reference()
+
+
+def pade_ck(p=6):
+    ck = np.zeros(p + 1)
+    lib().dqo_pade_ck(p, _dp(ck))
+    return ck
+
+
+def pade_exp(A, norm_mode=NORM_COMPLEX):
+    A = np.ascontiguousarray(A, dtype=np.complex128)
+    L = A.shape[0]
+    E = np.zeros_like(A)
+    s = lib().dqo_pade_exp(L, _dp(A.view(np.float64)), _dp(E.view(np.float64)), norm_mode)
+    return E, s
+
+
+def ifft(x):
+    x = np.array(x, dtype=np.complex128)
+    lib().dqo_ifft(len(x), _dp(x.view(np.float64)))
+    return x
+
+
+class System:
+    """Python holder for a dqo_system (keeps the numpy buffers alive).
+
+    rowptr/col/val is the OFF-DIAGONAL CSR; h0diag the input diagonal."""
+
+    def __init__(self, rowptr, col, val, h0diag, m, dt, hbar=None, dot_mode=DOT_BILINEAR,
+                 norm_mode=NORM_COMPLEX, noise=NOISE_NONE, ka_substeps=1, sigma=None, tau=None,
+                 sigma_static=0.0, static_eps=None, seed=0):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self.col = np.ascontiguousarray(col, dtype=np.int32)
+        self.val = np.ascontiguousarray(val, dtype=np.float64)
+        self.h0diag = np.ascontiguousarray(h0diag, dtype=np.float64)
+        self.n = len(self.h0diag)
+        self.sigma = None if sigma is None else np.ascontiguousarray(np.broadcast_to(sigma, (self.n,)), dtype=np.float64)
+        self.tau = None if tau is None else np.ascontiguousarray(np.broadcast_to(tau, (self.n,)), dtype=np.float64)
+        self.static_eps = None if static_eps is None else np.ascontiguousarray(static_eps, dtype=np.float64)
+        self.m = m
+        self.dt = dt
+        self.hbar = hbar_reference() if hbar is None else hbar
+        self.s = _System(
+            self.n,
+            self.rowptr.ctypes.data_as(C.POINTER(C.c_int)),
+            self.col.ctypes.data_as(C.POINTER(C.c_int)),
+            _dp(self.val),
+            _dp(self.h0diag),
+            m, dt, self.hbar, dot_mode, norm_mode, noise, ka_substeps,
+            _dp(self.sigma), _dp(self.tau), float(sigma_static), _dp(self.static_eps), seed,
+        )
+
+    def dense(self, diag=None):
+        H = np.zeros((self.n, self.n))
+        for i in range(self.n):
+            for p in range(self.rowptr[i], self.rowptr[i + 1]):
+                H[i, self.col[p]] += self.val[p]
+        H[np.arange(self.n), np.arange(self.n)] += self.h0diag if diag is None else diag
+        return H
+
+    def traj_init(self, traj):
+        eps = np.zeros(self.n)
+        deps = np.zeros(self.n)
+        lib().dqo_traj_init(C.byref(self.s), traj, _dp(eps), _dp(deps))
+        return eps, deps
+
+    def noise_update(self, traj, step, eps, deps):
+        diag = np.zeros(self.n)
+        lib().dqo_noise_update(C.byref(self.s), traj, step, _dp(eps), _dp(deps), _dp(diag))
+        return diag
+
+    def krylov_step(self, diag, psi):
+        psi = np.ascontiguousarray(psi, dtype=np.complex128)
+        out = np.zeros_like(psi)
+        err, nrm, s = C.c_double(), C.c_double(), C.c_int()
+        rc = lib().dqo_krylov_step(C.byref(self.s), _dp(np.ascontiguousarray(diag, dtype=np.float64)),
+                                   _dp(psi.view(np.float64)), _dp(out.view(np.float64)),
+                                   C.byref(err), C.byref(nrm), C.byref(s))
+        if rc != 0:
+            raise RuntimeError(f"oracle krylov step failed ({rc})")
+        return out, err.value, nrm.value, s.value
+
+    def lanczos(self, diag, q1):
+        n, m = self.n, self.m
+        Q = np.zeros((m + 2, n), dtype=np.complex128)
+        al = np.zeros(m + 2, dtype=np.complex128)
+        be = np.zeros(m + 2, dtype=np.complex128)
+        q1 = np.ascontiguousarray(q1, dtype=np.complex128)
+        nav = lib().dqo_lanczos(C.byref(self.s), _dp(np.ascontiguousarray(diag, dtype=np.float64)),
+                                _dp(q1.view(np.float64)), _dp(Q.view(np.float64)),
+                                _dp(al.view(np.float64)), _dp(be.view(np.float64)))
+        return Q, al, be, nav
+
+    def run(self, n_traj, n_steps, psi0, pop_every=1, traj0=0, threads=0, want_final=False):
+        n = self.n
+        psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
+        n_rec = n_steps // pop_every + 1
+        pops = np.zeros((n_rec, n))
+        corr = np.zeros(n_steps + 1, dtype=np.complex128)
+        fin = np.zeros((n_traj, n), dtype=np.complex128) if want_final else None
+        err = np.zeros(n_traj)
+        rc = lib().dqo_run(C.byref(self.s), traj0, n_traj, n_steps, _dp(psi0.view(np.float64)), pop_every,
+                           _dp(pops), _dp(corr.view(np.float64)),
+                           _dp(fin.view(np.float64)) if fin is not None else None, _dp(err), threads)
+        if rc != 0:
+            raise RuntimeError(f"oracle run failed ({rc})")
+        return {"pops": pops, "corr": corr, "psi_final": fin, "err": err}

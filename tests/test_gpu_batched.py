@@ -1,0 +1,114 @@
+"""Parity of the batched ensemble path (shared-CSR SpMM Lanczos, batched
+FP64 Padé, fused combine) with the CPU oracle: complex128 to 1e-10,
+complex64 mixed precision to 1e-6 in populations."""
+import numpy as np
+import pytest
+
+from tests.golden import make_golden as G
+
+pytestmark = pytest.mark.gpu
+
+POP_TOL_FP64 = 1e-10
+POP_TOL_MIXED = 1e-6
+
+
+def _golden():
+    return np.load(G.__file__.replace("make_golden.py", "golden_chain.npz"))
+
+
+def _chain_prop(precision, dot, n_traj=None, steps=None):
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    c = G.CHAIN
+    s = systems.chain(c["n"], c["J"])
+    p = dq.Propagator(s.n, m=c["m"], n_traj=n_traj or c["n_traj"], dt=c["dt"], noise=dq.NOISE_OU,
+                      sigma_static=c["sigma_static"], seed=c["seed"], dot=dot, pop_every=c["pop_every"],
+                      max_steps=steps or c["n_steps"], precision=precision)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, c["sigma"]), np.full(s.n, c["tau"]))
+    p.set_initial_state(G.chain_psi0())
+    return p
+
+
+@pytest.mark.parametrize("tag,dot", [("herm", 1), ("bil", 0)])
+def test_batched_fp64_matches_golden(tag, dot):
+    import dynaquant_b200 as dq
+    g = _golden()
+    p = _chain_prop(dq.PREC_FP64, dot)
+    p.run(G.CHAIN["n_steps"])
+    assert np.abs(p.populations() - g[f"{tag}_pops"]).max() < POP_TOL_FP64
+    assert np.abs(p.correlation() - g[f"{tag}_corr"]).max() < POP_TOL_FP64
+    if tag == "herm":
+        assert np.abs(p.states() - g["herm_psi_final"]).max() < 1e-10
+    assert np.allclose(p.error_accum(), g[f"{tag}_err"], rtol=1e-3, atol=1e-14)
+    e1, d1 = p.noise_state(1)
+    assert np.array_equal(e1, g["noise_traj1_eps"]) and np.array_equal(d1, g["noise_traj1_deps"])
+    p.close()
+
+
+def test_batched_fp64_incremental_equals_single_call():
+    import dynaquant_b200 as dq
+    g = _golden()
+    p = _chain_prop(dq.PREC_FP64, 1)
+    for k in (7, 13, 40):
+        p.run(k)
+    assert p.steps_done == 60
+    assert np.abs(p.populations() - g["herm_pops"]).max() < POP_TOL_FP64
+    p.close()
+
+
+def test_batched_mixed_matches_oracle():
+    import dynaquant_b200 as dq
+    g = _golden()
+    p = _chain_prop(dq.PREC_MIXED, 1)
+    p.run(G.CHAIN["n_steps"])
+    err = np.abs(p.populations() - g["herm_pops"]).max()
+    assert err < POP_TOL_MIXED, err
+    assert np.abs(p.correlation() - g["herm_corr"]).max() < 1e-5
+    p.close()
+
+
+def test_batched_mixed_tube_matches_oracle(oracle):
+    """Dipole-coupled tube (480 sites, ~28 couplings/row), OU noise, 32
+    trajectories x 40 steps: mixed precision vs FP64 oracle."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 24)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=20, dt=0.5, dot_mode=1, noise=2, sigma=250.0, tau=50.0,
+                      sigma_static=150.0, seed=9)
+    B, T = 32, 40
+    psi0 = s.bright_state()
+    ref = S.run(B, T, psi0, pop_every=8, threads=4)
+    for prec, tol in ((dq.PREC_MIXED, POP_TOL_MIXED), (dq.PREC_FP64, POP_TOL_FP64)):
+        p = dq.Propagator(s.n, m=20, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=9, dot=1,
+                          pop_every=8, max_steps=T, precision=prec)
+        p.set_system(s)
+        p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+        p.set_initial_state(psi0)
+        p.run(T)
+        err = np.abs(p.populations() - ref["pops"]).max()
+        assert err < tol, (prec, err)
+        assert np.abs(p.correlation() - ref["corr"]).max() < tol * 10
+        p.close()
+
+
+def test_batched_states_are_normalised():
+    import dynaquant_b200 as dq
+    p = _chain_prop(dq.PREC_MIXED, 1, n_traj=8)
+    p.run(20)
+    st = p.states()
+    assert np.allclose(np.linalg.norm(st, axis=1), 1.0, atol=1e-12)
+    p.close()
+
+
+def test_spectrum_matches_numpy():
+    import dynaquant_b200 as dq
+    p = _chain_prop(dq.PREC_FP64, 1)
+    p.run(G.CHAIN["n_steps"])
+    corr = p.correlation()
+    spec = p.spectrum(128)
+    x = np.zeros(128, complex)
+    x[:len(corr)] = corr
+    assert np.abs(spec - np.fft.ifft(x) * 128).max() < 1e-10
+    p.close()
