@@ -191,6 +191,7 @@ def run_ours(args, rank, world, local_rank):
     seed = w["seed"] + 7919 * rank
     # ---- device-resident throughput ----------------------------------------
     p = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=W + K + 8)
+    tiling = p.autotune()
     p.reset()
     p.run(W)
     stream = torch.cuda.ExternalStream(p.stream)
@@ -224,6 +225,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     p2 = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=K + 8)
+    p2.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"])
     p2.reset()
     p2.run(K)
     pops = p2.populations()
@@ -279,7 +281,8 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": w["name"], "n_sites": s.n, "nnz_per_row": (s.nnz - s.n) / s.n, "m": w["m"],
                    "trajectories_per_gpu": B, "dt_fs": w["dt"], "noise": "OU 250/50 fs + static 150",
                    "l2": "inputs larger than L2 (Krylov slabs %.1f GB)" % (8.0 * s.n * B * (w["m"] + 2) / 1e9),
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "ms_per_iter")}},
         "e2e": e2e,
         "gpu_launches": int(kernels_per_step * K),
         "roofline": {"bound": "hbm", "kernel": "k_spmm (SpMM + alpha)", "achieved": achieved, "peak": peak,

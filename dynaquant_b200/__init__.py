@@ -120,6 +120,25 @@ class Propagator:
     def run(self, n_steps):
         self._check(self.L.dq_run(self.h, n_steps))
 
+    def set_tiling(self, traj_chunk, vec, ctas_per_sm):
+        self._check(self.L.dq_set_tiling(self.h, traj_chunk, vec, ctas_per_sm))
+
+    def get_tiling(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.L.dq_get_tiling(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def autotune_raw(self, reps=5):
+        ms = C.c_double()
+        self._check(self.L.dq_autotune(self.h, reps, C.byref(ms)))
+        return ms.value
+
+    def autotune(self, reps=5, use_cache=True):
+        """Picks the ensemble tiling (JSON-cached per GPU and size class)."""
+        from . import autotune as _at
+        nnz = int(self._rp[-1]) if getattr(self, "_rp", None) is not None else 0
+        return _at.tune(self, nnz, reps=reps, use_cache=use_cache)
+
     def profile_step(self, n_steps=1):
         """Eager steps with CUDA events between kernels: {kind: (ms per launch, launches)}."""
         nk = len(_lib.KIND_NAMES)

@@ -407,3 +407,57 @@ extern "C" dq_status dq_profile_step(dq_ctx* c, int n_steps, double* ms_per_laun
     }
     return DQ_OK;
 }
+
+static dq_status ensure_batched(dq_ctx* c) {
+    dq_status st;
+    if (!c->bat) {
+        if ((st = check_ready(c))) return st;
+        if ((st = batched_alloc(c))) return st;
+        c->ready = false;
+    }
+    return DQ_OK;
+}
+
+extern "C" dq_status dq_set_tiling(dq_ctx* c, int traj_chunk, int vec, int ctas_per_sm) {
+    if (!c) return DQ_ERR_ARG;
+    dq_status st;
+    if ((st = ensure_batched(c))) return st;
+    if ((st = batched_set_tiling(c, traj_chunk, vec, ctas_per_sm)))
+        return fail(c, st, "set_tiling: invalid tiling for this system");
+    c->ready = false;
+    return DQ_OK;
+}
+
+extern "C" dq_status dq_get_tiling(dq_ctx* c, int* traj_chunk, int* vec, int* ctas_per_sm) {
+    if (!c) return DQ_ERR_ARG;
+    dq_status st;
+    if ((st = ensure_batched(c))) return st;
+    batched_get_tiling(c, traj_chunk, vec, ctas_per_sm);
+    return DQ_OK;
+}
+
+extern "C" dq_status dq_autotune(dq_ctx* c, int reps, double* best_ms) {
+    if (!c) return DQ_ERR_ARG;
+    if (reps < 1) reps = 5;
+    dq_status st;
+    if ((st = ensure_batched(c))) return st;
+    if ((st = dq_reset(c))) return st;
+    int b_tc = 0, b_vec = 0, b_cps = 0;
+    double best = 1e30;
+    const int vecs[2] = {2, 1};
+    for (int vi = 0; vi < 2; ++vi) {
+        for (int tc = 4; tc <= 64; tc <<= 1) {
+            for (int cps = 1; cps <= 8; cps <<= 1) {
+                if (batched_set_tiling(c, tc, vecs[vi], cps) != DQ_OK) continue;
+                double ms = 0.0;
+                if ((st = batched_time_iteration(c, reps, &ms))) return st;
+                if (ms < best) { best = ms; b_tc = tc; b_vec = vecs[vi]; b_cps = cps; }
+            }
+        }
+    }
+    if (!b_tc) return fail(c, DQ_ERR_ARG, "autotune: no valid tiling");
+    if ((st = batched_set_tiling(c, b_tc, b_vec, b_cps))) return st;
+    if (best_ms) *best_ms = best;
+    c->ready = false;
+    return dq_reset(c);
+}

@@ -9,19 +9,22 @@
 //   slab j (j = 1..m+1): r_j[site][traj], complex64 (mixed) or complex128
 //                        (fp64); q_j = sc_j[traj] * r_j (unnormalised Lanczos
 //                        residuals, slab 1 = psi itself)
-//   w[site][traj]      : SpMM output of the current iteration
+//   slab 0             : w[site][traj], SpMM output of the current iteration
 //   d[site][traj]      : this step's diagonal, real (float or double)
 //   eps, deps          : FP64 static energies and OU offsets [site][traj]
 // Per-trajectory FP64 scalars live in [j][traj] arrays.
 //
-// Grid: blockIdx.y picks a chunk of TC trajectories, blockIdx.x strides over
-// rows; a thread owns TPT consecutive trajectories of one row at a time
-// (16-byte vector loads).  Per-trajectory reductions (alpha, beta, norms,
-// correlation) go through per-chunk partials and a per-chunk last-block
-// ticket, so they are deterministic and need no extra launch.
+// Tiling: blockIdx.y picks a chunk of TC trajectories; blockIdx.x owns a
+// CONTIGUOUS range of rows, so the neighbour rows one row gathers are the
+// ones its predecessors just gathered and stay in L1.  A thread owns TPT
+// consecutive trajectories of one row at a time (8- or 16-byte vector
+// loads).  TC, TPT and CTAs per SM are chosen by dq_autotune.
+// Per-trajectory reductions (alpha, beta, norms, correlation) go through
+// per-chunk partials and a per-chunk last-block ticket: deterministic, no
+// extra launch, no block ever waits for another.
 //
 // One time step (propagate.cu:199-259 for all trajectories at once):
-//   k_noise_b, m x {k_spmm_alpha, k_axpy_beta}, k_spmm_norm, k_pade_b,
+//   k_noise_b, m x {k_spmm, k_axpy_beta}, k_spmm (norm), k_pade_b,
 //   k_combine_b, k_pop_b
 // captured once into a CUDA graph and replayed per step; the step index lives
 // in device memory.
@@ -34,27 +37,26 @@
 
 namespace dq {
 
-template <typename Real> struct VecT;
-template <> struct VecT<float> {
-    static constexpr int TPT = 2;   // complex64 per thread: one float4
-    using L = float4;
-};
-template <> struct VecT<double> {
-    static constexpr int TPT = 1;   // complex128 per thread: one double2
-    using L = double2;
-};
+constexpr int kBThreads = 256;
+constexpr int kMaxTC = 64;
+constexpr int kMaxCtasPerChunk = 4096;
 
-template <typename Real>
-struct CV {   // TPT complex values held in registers
-    Real re[VecT<Real>::TPT], im[VecT<Real>::TPT];
-};
+// ---- vector access of TPT consecutive complex values ----------------------
+template <typename Real, int TPT> struct VL;
+template <> struct VL<float, 1> { using T = float2; };
+template <> struct VL<float, 2> { using T = float4; };
+template <> struct VL<double, 1> { using T = double2; };
 
-template <typename Real>
-__device__ __forceinline__ CV<Real> ldv(const Real* base, size_t idx2) {
-    // idx2 = index in complex elements; base points at interleaved re/im
-    CV<Real> v;
-    typename VecT<Real>::L t = *reinterpret_cast<const typename VecT<Real>::L*>(base + 2 * idx2);
-    if constexpr (VecT<Real>::TPT == 2) {
+template <typename Real, int TPT>
+struct CV { Real re[TPT], im[TPT]; };
+
+template <typename Real, int TPT, bool kLdg>
+__device__ __forceinline__ CV<Real, TPT> ldv(const Real* base, size_t idx) {
+    using T = typename VL<Real, TPT>::T;
+    const T* p = reinterpret_cast<const T*>(base + 2 * idx);
+    T t = kLdg ? __ldg(p) : *p;
+    CV<Real, TPT> v;
+    if constexpr (TPT == 2) {
         v.re[0] = t.x; v.im[0] = t.y; v.re[1] = t.z; v.im[1] = t.w;
     } else {
         v.re[0] = t.x; v.im[0] = t.y;
@@ -62,39 +64,52 @@ __device__ __forceinline__ CV<Real> ldv(const Real* base, size_t idx2) {
     return v;
 }
 
-template <typename Real>
-__device__ __forceinline__ void stv(Real* base, size_t idx2, const CV<Real>& v) {
-    typename VecT<Real>::L t;
-    if constexpr (VecT<Real>::TPT == 2) {
+template <typename Real, int TPT>
+__device__ __forceinline__ void stv(Real* base, size_t idx, const CV<Real, TPT>& v) {
+    using T = typename VL<Real, TPT>::T;
+    T t;
+    if constexpr (TPT == 2) {
         t.x = v.re[0]; t.y = v.im[0]; t.z = v.re[1]; t.w = v.im[1];
     } else {
         t.x = v.re[0]; t.y = v.im[0];
     }
-    *reinterpret_cast<typename VecT<Real>::L*>(base + 2 * idx2) = t;
+    *reinterpret_cast<T*>(base + 2 * idx) = t;
 }
 
-constexpr int kBThreads = 256;
-constexpr int kMaxTC = 64;
-
 struct BatchedScalars {
-    // all [kMaxL][B] row-major by j, allocated separately (B is runtime)
-    double* alpha;    // complex: 2 doubles per entry
-    double* beta;
-    double* sc;       // sc[j][b]
-    double* yt;       // complex combine weights
-    double* nav;      // [B]
+    double* alpha;    // [kMaxL][B] complex (2 doubles)
+    double* beta;     // [kMaxL][B]
+    double* sc;       // [kMaxL][B]; q_j = sc_j r_j
+    double* yt;       // [kMaxL][B] complex combine weights y_{j-1} sc_j
+    double* nav;      // [B] ||H q_{m+1}||
     double* norm2;    // [B] ||psi||^2 of the stored (unnormalised) psi
-    double* partial;  // [chunks][gx][TC][2]
-    unsigned int* tickets;  // [8][chunks]
+    double* partial;  // 2 regions of [chunks][gx][TC][2]
+    unsigned int* tickets;  // [8][chunks] + step ticket
     int* status;      // [1]
     int* step;        // [1] current step index
     double* corr;     // [(max_steps+1)][chunks][2]
 };
 
+// Thread -> (row lane, trajectory lane) map and the CTA's row range.
+template <int TPT>
+struct Tile {
+    int tr, rl, RPC, b0, r0, r1;
+    __device__ __forceinline__ Tile(int TC, int rows_per_cta, int n) {
+        const int TPR = TC / TPT;
+        tr = threadIdx.x % TPR;
+        rl = threadIdx.x / TPR;
+        RPC = blockDim.x / TPR;
+        b0 = blockIdx.y * TC + tr * TPT;
+        r0 = blockIdx.x * rows_per_cta;
+        r1 = min(n, r0 + rows_per_cta);
+    }
+};
+
 }  // namespace dq
 
 struct dq::BatchedState {
-    int B = 0, TC = 0, chunks = 0, gx = 0;
+    int B = 0, TC = 0, TPT = 2, chunks = 0, gx = 0, rpc = 0, ctas_per_sm = 2;
+    int sms = 148;
     bool mixed = true;
     void* slabs = nullptr;      // (m+2) slabs (slab 0 = w)
     void* diag = nullptr;       // Real [n][B]
@@ -102,6 +117,7 @@ struct dq::BatchedState {
     double* deps = nullptr;     // [n][B]
     dq::BatchedScalars s{};
     double* scal_mem = nullptr;
+    size_t partial_cap = 0;     // doubles per partial region
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
@@ -111,15 +127,15 @@ namespace dq {
 // ---------------------------------------------------------------------------
 // per-chunk reduction of TC complex partials per block
 // ---------------------------------------------------------------------------
-// acc[t] for this thread's TPT trajectories; threads with the same traj lane
-// across the RPC row lanes are summed in shared memory, the block partial
-// goes to partial[chunk][blockIdx.x][TC]; the last block of the chunk sums the
-// gx partials in order.  Returns true in the last block; red_out[tcl] holds
-// the chunk's totals (TC complex) in shared memory for threads < TC.
+// ar/ai: this thread's partials for its TPT trajectories.  Threads of the
+// same trajectory lane are summed in shared memory; the block partial goes to
+// partial[chunk][blockIdx.x][TC]; the last block of the chunk sums the
+// gridDim.x partials in block order.  Returns true in that block, with the
+// chunk's totals in red_out[0..TC).
 template <int TPT>
 __device__ __forceinline__ bool chunk_reduce(const double (&ar)[TPT], const double (&ai)[TPT], int TC,
                                              double* partial, unsigned int* ticket, double2* red_out) {
-    __shared__ double2 sm[kBThreads * 2];   // RPC * TC <= kBThreads * TPT
+    __shared__ double2 sm[kBThreads * 2];
     const int TPR = TC / TPT;
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int RPC = blockDim.x / TPR;
@@ -160,86 +176,94 @@ __global__ void k_traj_init_b(int n, int B, uint64_t seed, const double* __restr
                               const double* __restrict__ static_eps, double sigma_static,
                               const double* __restrict__ sigma, int noise, double* __restrict__ eps,
                               double* __restrict__ deps) {
-    size_t total = (size_t)n * B;
-    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-        int i = (int)(x / B), b = (int)(x % B);
-        double e;
-        if (static_eps) e = static_eps[i];
-        else e = __dadd_rn(__dmul_rn(sigma_static, normal(seed, P_STATIC, b, 0, i, 0)), h0[i]);
-        eps[x] = e;
-        deps[x] = (noise == DQ_NOISE_OU) ? __dmul_rn(sigma[i], normal(seed, P_OU_INIT, b, 0, i, 0)) : 0.0;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        for (int b = threadIdx.x; b < B; b += blockDim.x) {
+            const size_t x = (size_t)i * B + b;
+            double e;
+            if (static_eps) e = static_eps[i];
+            else e = __dadd_rn(__dmul_rn(sigma_static, normal(seed, P_STATIC, b, 0, i, 0)), h0[i]);
+            eps[x] = e;
+            deps[x] = (noise == DQ_NOISE_OU) ? __dmul_rn(sigma[i], normal(seed, P_OU_INIT, b, 0, i, 0)) : 0.0;
+        }
     }
 }
 
 template <typename Real>
 __global__ void k_set_psi0_b(int n, int B, const cd* __restrict__ psi0, Real* __restrict__ r1) {
-    size_t total = (size_t)n * B;
-    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-        int i = (int)(x / B);
-        r1[2 * x] = (Real)psi0[i].x;
-        r1[2 * x + 1] = (Real)psi0[i].y;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const cd p = psi0[i];
+        for (int b = threadIdx.x; b < B; b += blockDim.x) {
+            const size_t x = (size_t)i * B + b;
+            r1[2 * x] = (Real)p.x;
+            r1[2 * x + 1] = (Real)p.y;
+        }
     }
 }
 
-template <typename Real>
-__global__ void k_noise_b(int n, int B, int noise, int ns, double subdt, double sqrt_subdt, uint64_t seed,
-                          const double* __restrict__ sigma, const double* __restrict__ invtau,
-                          const double* __restrict__ coeff, const double* __restrict__ eps,
-                          double* __restrict__ deps, Real* __restrict__ d, BatchedScalars S) {
+// OU / Gaussian update of every trajectory's diagonal for this step
+// (gpuSysHelper.cu:32-128 with Philox keys instead of shared cuRAND states)
+template <typename Real, int TPT>
+__global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int TC, int rpc, int noise, int ns, double subdt,
+                                                      double sqrt_subdt, uint64_t seed,
+                                                      const double* __restrict__ sigma,
+                                                      const double* __restrict__ invtau,
+                                                      const double* __restrict__ coeff,
+                                                      const double* __restrict__ eps, double* __restrict__ deps,
+                                                      Real* __restrict__ d, BatchedScalars S) {
+    const Tile<TPT> T(TC, rpc, n);
     const int step = *S.step;
-    size_t total = (size_t)n * B;
-    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-        int i = (int)(x / B), b = (int)(x % B);
-        double v;
-        if (noise == DQ_NOISE_OU) {
-            double cur = ou_update(deps[x], invtau[i], coeff[i], subdt, sqrt_subdt, ns, seed, b, step, i);
-            deps[x] = cur;
-            v = __dadd_rn(cur, eps[x]);
-        } else if (noise == DQ_NOISE_GAUSS) {
-            double xi = normal(seed, P_GAUSS, b, step, i, 0);
-            v = __dadd_rn(__dmul_rn(xi, sigma[i]), eps[x]);
-        } else {
-            v = eps[x];
+    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+            const int b = T.b0 + t;
+            const size_t x = (size_t)row * B + b;
+            double v;
+            if (noise == DQ_NOISE_OU) {
+                double cur = ou_update(deps[x], invtau[row], coeff[row], subdt, sqrt_subdt, ns, seed, b, step, row);
+                deps[x] = cur;
+                v = __dadd_rn(cur, eps[x]);
+            } else if (noise == DQ_NOISE_GAUSS) {
+                double xi = normal(seed, P_GAUSS, b, step, row, 0);
+                v = __dadd_rn(__dmul_rn(xi, sigma[row]), eps[x]);
+            } else {
+                v = eps[x];
+            }
+            d[x] = (Real)v;
         }
-        d[x] = (Real)v;
     }
 }
 
-// w = H q_j for all trajectories; alpha_j[b] = <q_j, w>_b
-template <typename Real, bool kBilinear, bool kWrite>
-__global__ void __launch_bounds__(kBThreads) k_spmm(int n, int B, int TC, int j, const int* __restrict__ rowptr,
-                                                   const int* __restrict__ col, const Real* __restrict__ val,
-                                                   const Real* __restrict__ d, const Real* __restrict__ rj,
-                                                   Real* __restrict__ w, BatchedScalars S) {
-    constexpr int TPT = VecT<Real>::TPT;
-    const int TPR = TC / TPT;
-    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
-    const int RPC = blockDim.x / TPR;
-    const int b0 = blockIdx.y * TC + tr * TPT;
-    double sc[TPT];
+// w = H q_j for all trajectories and alpha_j[b] = <q_j, w>_b  (kWrite), or
+// ||H q_j||_b only (!kWrite, for the EXPOKIT error estimate)
+template <typename Real, int TPT, bool kBilinear, bool kWrite>
+__global__ void __launch_bounds__(kBThreads) k_spmm(int n, int B, int TC, int rpc, int j,
+                                                   const int* __restrict__ rowptr, const int* __restrict__ col,
+                                                   const Real* __restrict__ val, const Real* __restrict__ d,
+                                                   const Real* __restrict__ rj, Real* __restrict__ w,
+                                                   BatchedScalars S) {
+    const Tile<TPT> T(TC, rpc, n);
+    double sc[TPT], ar[TPT], ai[TPT];
 #pragma unroll
-    for (int t = 0; t < TPT; ++t) sc[t] = S.sc[(size_t)j * B + b0 + t];
-    double ar[TPT], ai[TPT];
+    for (int t = 0; t < TPT; ++t) {
+        sc[t] = S.sc[(size_t)j * B + T.b0 + t];
+        ar[t] = 0.0;
+        ai[t] = 0.0;
+    }
+    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+        const size_t base = (size_t)row * B + T.b0;
+        const CV<Real, TPT> x = ldv<Real, TPT, true>(rj, base);
+        CV<Real, TPT> u;
 #pragma unroll
-    for (int t = 0; t < TPT; ++t) { ar[t] = 0.0; ai[t] = 0.0; }
-    for (int row = blockIdx.x * RPC + rl; row < n; row += gridDim.x * RPC) {
-        const size_t base = (size_t)row * B + b0;
-        CV<Real> x = ldv(rj, base);
-        CV<Real> u;
-        {
-            const Real* dp = d + base;
-#pragma unroll
-            for (int t = 0; t < TPT; ++t) {
-                Real dd = dp[t];
-                u.re[t] = dd * x.re[t];
-                u.im[t] = dd * x.im[t];
-            }
+        for (int t = 0; t < TPT; ++t) {
+            const Real dd = __ldg(d + base + t);
+            u.re[t] = dd * x.re[t];
+            u.im[t] = dd * x.im[t];
         }
-        const int p1 = rowptr[row + 1];
-        for (int p = rowptr[row]; p < p1; ++p) {
+        const int p1 = __ldg(rowptr + row + 1);
+        for (int p = __ldg(rowptr + row); p < p1; ++p) {
             const int c = __ldg(col + p);
             const Real v = __ldg(val + p);
-            CV<Real> y = ldv(rj, (size_t)c * B + b0);
+            const CV<Real, TPT> y = ldv<Real, TPT, true>(rj, (size_t)c * B + T.b0);
 #pragma unroll
             for (int t = 0; t < TPT; ++t) {
                 u.re[t] = fma(v, y.re[t], u.re[t]);
@@ -247,20 +271,17 @@ __global__ void __launch_bounds__(kBThreads) k_spmm(int n, int B, int TC, int j,
             }
         }
         if (kWrite) {
-            CV<Real> o;
+            CV<Real, TPT> o;
 #pragma unroll
             for (int t = 0; t < TPT; ++t) {
                 o.re[t] = (Real)(sc[t] * (double)u.re[t]);
                 o.im[t] = (Real)(sc[t] * (double)u.im[t]);
-            }
-            stv(w, base, o);
-#pragma unroll
-            for (int t = 0; t < TPT; ++t) {
-                // alpha partial of the unscaled product; sc^2 applied at the end
-                double xr = x.re[t], xi = x.im[t], ur = u.re[t], ui = u.im[t];
+                // alpha partial from the unscaled product; sc^2 applied at the end
+                const double xr = x.re[t], xi = x.im[t], ur = u.re[t], ui = u.im[t];
                 if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
                 else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
             }
+            stv<Real, TPT>(w, base, o);
         } else {
 #pragma unroll
             for (int t = 0; t < TPT; ++t) ar[t] += (double)u.re[t] * u.re[t] + (double)u.im[t] * u.im[t];
@@ -271,7 +292,7 @@ __global__ void __launch_bounds__(kBThreads) k_spmm(int n, int B, int TC, int j,
         if (threadIdx.x < TC) {
             const int b = blockIdx.y * TC + threadIdx.x;
             const double s = S.sc[(size_t)j * B + b];
-            double2 v = red[threadIdx.x];
+            const double2 v = red[threadIdx.x];
             if (kWrite) {
                 S.alpha[2 * ((size_t)j * B + b)] = v.x * s * s;
                 S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s * s;
@@ -282,39 +303,33 @@ __global__ void __launch_bounds__(kBThreads) k_spmm(int n, int B, int TC, int j,
     }
 }
 
-// r_{j+1} = w - alpha_j q_j - beta_{j-1} q_{j-1}; beta_j = ||r_{j+1}||
-template <typename Real>
-__global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, int j, const Real* __restrict__ w,
-                                                        const Real* __restrict__ rj, const Real* __restrict__ rjm,
-                                                        Real* __restrict__ rjp, BatchedScalars S) {
-    constexpr int TPT = VecT<Real>::TPT;
-    const int TPR = TC / TPT;
-    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
-    const int RPC = blockDim.x / TPR;
-    const int b0 = blockIdx.y * TC + tr * TPT;
-    double ajr[TPT], aji[TPT], sj[TPT], bm[TPT];
+// r_{j+1} = w - alpha_j q_j - beta_{j-1} q_{j-1};  beta_j = ||r_{j+1}||
+template <typename Real, int TPT>
+__global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, int rpc, int j,
+                                                        const Real* __restrict__ w, const Real* __restrict__ rj,
+                                                        const Real* __restrict__ rjm, Real* __restrict__ rjp,
+                                                        BatchedScalars S) {
+    const Tile<TPT> T(TC, rpc, n);
+    double ajr[TPT], aji[TPT], bm[TPT], nn[TPT], zero[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) {
-        const size_t k = (size_t)j * B + b0 + t;
+        const size_t k = (size_t)j * B + T.b0 + t;
         ajr[t] = S.alpha[2 * k] * S.sc[k];
         aji[t] = S.alpha[2 * k + 1] * S.sc[k];
-        sj[t] = S.sc[k];
-        bm[t] = (j > 1) ? S.beta[(size_t)(j - 1) * B + b0 + t] * S.sc[(size_t)(j - 1) * B + b0 + t] : 0.0;
+        bm[t] = (j > 1) ? S.beta[(size_t)(j - 1) * B + T.b0 + t] * S.sc[(size_t)(j - 1) * B + T.b0 + t] : 0.0;
+        nn[t] = 0.0;
+        zero[t] = 0.0;
     }
-    double nn[TPT], dummy[TPT];
-#pragma unroll
-    for (int t = 0; t < TPT; ++t) { nn[t] = 0.0; dummy[t] = 0.0; }
-    for (int row = blockIdx.x * RPC + rl; row < n; row += gridDim.x * RPC) {
-        const size_t base = (size_t)row * B + b0;
-        CV<Real> u = ldv(w, base);
-        CV<Real> x = ldv(rj, base);
-        CV<Real> xm;
-        if (j > 1) xm = ldv(rjm, base);
-        CV<Real> o;
+    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+        const size_t base = (size_t)row * B + T.b0;
+        const CV<Real, TPT> u = ldv<Real, TPT, false>(w, base);
+        const CV<Real, TPT> x = ldv<Real, TPT, false>(rj, base);
+        CV<Real, TPT> xm;
+        if (j > 1) xm = ldv<Real, TPT, false>(rjm, base);
+        CV<Real, TPT> o;
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
-            // alpha * (sc_j r_j): (ajr + i aji) (xr + i xi)
-            double xr = x.re[t], xi = x.im[t];
+            const double xr = x.re[t], xi = x.im[t];
             double rr = (double)u.re[t] - (ajr[t] * xr - aji[t] * xi);
             double ri = (double)u.im[t] - (ajr[t] * xi + aji[t] * xr);
             if (j > 1) {
@@ -325,11 +340,10 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
             o.im[t] = (Real)ri;
             nn[t] += (double)o.re[t] * o.re[t] + (double)o.im[t] * o.im[t];
         }
-        stv(rjp, base, o);
+        stv<Real, TPT>(rjp, base, o);
     }
-    (void)sj;
     __shared__ double2 red[kMaxTC];
-    if (chunk_reduce<TPT>(nn, dummy, TC, S.partial, S.tickets + 1 * gridDim.y, red)) {
+    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 1 * gridDim.y, red)) {
         if (threadIdx.x < TC) {
             const int b = blockIdx.y * TC + threadIdx.x;
             double bt = sqrt(red[threadIdx.x].x);
@@ -364,48 +378,49 @@ __global__ void k_pade_b(int m, int B, double tau_im, int norm_mode, BatchedScal
     __syncthreads();
     for (int j = threadIdx.x; j < m; j += blockDim.x) {
         const size_t k = (size_t)(j + 1) * B + b;
-        cd v = cscale(y[j], S.sc[k]);
+        const cd v = cscale(y[j], S.sc[k]);
         S.yt[2 * k] = v.x;
         S.yt[2 * k + 1] = v.y;
     }
-    if (threadIdx.x == 0) {
-        double est = expokit_error(be[m].x, S.nav[b], o.e_m1_m, o.e_m1_mp1);
-        erracc[b] += est;
-    }
+    if (threadIdx.x == 0) erracc[b] += expokit_error(be[m].x, S.nav[b], o.e_m1_m, o.e_m1_mp1);
 }
 
 // psi = sum_j yt_j r_j written over slab 1; ||psi||^2 and <psi0|psi> per
-// trajectory; correlation point step+1 per chunk.
-template <typename Real>
-__global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, int m, Real* __restrict__ slabs,
-                                                        size_t slab_stride, const cd* __restrict__ psi0,
-                                                        BatchedScalars S) {
-    constexpr int TPT = VecT<Real>::TPT;
-    const int TPR = TC / TPT;
-    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
-    const int RPC = blockDim.x / TPR;
-    const int b0 = blockIdx.y * TC + tr * TPT;
+// trajectory; correlation point step+1 per chunk (propStep.cu:31-44,
+// systemClass.cu:1771-1829, spectraClass.cu:510-571)
+template <typename Real, int TPT>
+__global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, int rpc, int m,
+                                                        Real* __restrict__ slabs, size_t slab_stride,
+                                                        const cd* __restrict__ psi0, BatchedScalars S) {
+    const Tile<TPT> T(TC, rpc, n);
     const int step = *S.step;
+    __shared__ double2 yts[kMaxM * kMaxTC];
+    for (int e = threadIdx.x; e < m * TC; e += blockDim.x) {
+        const int j = 1 + e / TC, b = blockIdx.y * TC + e % TC;
+        const size_t k = (size_t)j * B + b;
+        yts[e] = make_double2(S.yt[2 * k], S.yt[2 * k + 1]);
+    }
+    __syncthreads();
+    const int tl = T.b0 - blockIdx.y * TC;   // trajectory lane within the chunk
     double nn[TPT], cr[TPT], ci[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) { nn[t] = 0.0; cr[t] = 0.0; ci[t] = 0.0; }
-    Real* r1 = slabs + 2 * slab_stride;   // slab 1
-    for (int row = blockIdx.x * RPC + rl; row < n; row += gridDim.x * RPC) {
-        const size_t base = (size_t)row * B + b0;
+    Real* r1 = slabs + 2 * slab_stride;
+    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+        const size_t base = (size_t)row * B + T.b0;
         double accr[TPT], acci[TPT];
 #pragma unroll
         for (int t = 0; t < TPT; ++t) { accr[t] = 0.0; acci[t] = 0.0; }
         for (int j = 1; j <= m; ++j) {
-            CV<Real> x = ldv(slabs + 2 * slab_stride * j, base);
+            const CV<Real, TPT> x = ldv<Real, TPT, false>(slabs + 2 * slab_stride * j, base);
 #pragma unroll
             for (int t = 0; t < TPT; ++t) {
-                const size_t k = (size_t)j * B + b0 + t;
-                const double yr = S.yt[2 * k], yi = S.yt[2 * k + 1];
-                accr[t] += yr * x.re[t] - yi * x.im[t];
-                acci[t] += yr * x.im[t] + yi * x.re[t];
+                const double2 yv = yts[(j - 1) * TC + tl + t];
+                accr[t] += yv.x * x.re[t] - yv.y * x.im[t];
+                acci[t] += yv.x * x.im[t] + yv.y * x.re[t];
             }
         }
-        CV<Real> o;
+        CV<Real, TPT> o;
         const cd p0 = psi0[row];
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
@@ -416,28 +431,25 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
             cr[t] += p0.x * vr + p0.y * vi;   // conj(psi0) * psi
             ci[t] += p0.x * vi - p0.y * vr;
         }
-        stv(r1, base, o);
+        stv<Real, TPT>(r1, base, o);
     }
     __shared__ double2 red[kMaxTC];
-    // norms
     double zero[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) zero[t] = 0.0;
     if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 3 * gridDim.y, red)) {
         if (threadIdx.x < TC) {
             const int b = blockIdx.y * TC + threadIdx.x;
-            double n2 = red[threadIdx.x].x;
+            const double n2 = red[threadIdx.x].x;
             S.norm2[b] = n2;
-            double s1 = 1.0 / sqrt(n2);
-            S.sc[B + b] = s1;   // sc[1][b]: next step's q_1 = psi / ||psi||
+            S.sc[B + b] = 1.0 / sqrt(n2);   // sc[1][b]: next step's q_1 = psi / ||psi||
             if (!(n2 > 0.0) || !isfinite(n2)) atomicCAS(S.status, 0, DQ_ERR_NAN);
         }
     }
     __syncthreads();
-    // correlation, normalised per trajectory by this step's ||psi||: the
-    // norms are final once the norm reduction above has completed in every
-    // block; the correlation therefore uses a second partial pass whose last
-    // block divides by the norms (published by then through the ticket order)
+    // correlation of the normalised state: the last block of the second
+    // ticket runs after every block of the chunk passed the first one, so the
+    // chunk's norms are published by then
     double* part2 = S.partial + (size_t)gridDim.y * gridDim.x * TC * 2;
     if (chunk_reduce<TPT>(cr, ci, TC, part2, S.tickets + 4 * gridDim.y, red)) {
         if (threadIdx.x == 0) {
@@ -456,7 +468,7 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
 }
 
 // populations: one warp per row, all trajectories, fixed order; advances the
-// step counter in its last block.
+// step counter in its last block
 template <typename Real>
 __global__ void k_pop_b(int n, int B, int pop_every, const Real* __restrict__ r1, double* __restrict__ pops,
                         BatchedScalars S, unsigned int* ticket) {
@@ -485,7 +497,7 @@ __global__ void k_pop_b(int n, int B, int pop_every, const Real* __restrict__ r1
     }
 }
 
-// initial record: pops[0] += B |psi0|^2, corr[0] = B <psi0|psi0>, norms
+// initial record: pops[0] += B |psi0|^2, corr[0] = B <psi0|psi0>
 __global__ void k_init_obs_b(int n, int B, const cd* __restrict__ psi0, double* pops, BatchedScalars S,
                              int chunks) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -521,11 +533,24 @@ __global__ void k_set_norms_b(int n, int B, const cd* __restrict__ psi0, Batched
 
 template <typename Real>
 __global__ void k_get_states_b(int n, int B, const Real* __restrict__ r1, const BatchedScalars S, cd* __restrict__ out) {
-    size_t total = (size_t)n * B;
-    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-        int i = (int)(x / B), b = (int)(x % B);
-        double s = 1.0 / sqrt(S.norm2[b]);
-        out[(size_t)b * n + i] = cmk(r1[2 * x] * s, r1[2 * x + 1] * s);
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        for (int b = threadIdx.x; b < B; b += blockDim.x) {
+            const size_t x = (size_t)i * B + b;
+            const double s = 1.0 / sqrt(S.norm2[b]);
+            out[(size_t)b * n + i] = cmk(r1[2 * x] * s, r1[2 * x + 1] * s);
+        }
+    }
+}
+
+// correlation sums over chunks -> d_corr (called by the getters)
+__global__ void k_corr_collect(int np, int chunks, const double* __restrict__ corr_chunks, cd* __restrict__ out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+        double sr = 0.0, si = 0.0;
+        for (int ch = 0; ch < chunks; ++ch) {
+            sr += corr_chunks[((size_t)k * chunks + ch) * 2];
+            si += corr_chunks[((size_t)k * chunks + ch) * 2 + 1];
+        }
+        out[k] = cmk(sr, si);
     }
 }
 
@@ -536,10 +561,36 @@ __global__ void k_get_states_b(int n, int B, const Real* __restrict__ r1, const 
         if (_s != DQ_OK) return _s;                                     \
     } while (0)
 
-static int pick_tc(int B, int tpt) {
-    for (int tc = kMaxTC; tc >= tpt; tc >>= 1)
-        if (B % tc == 0 && tc / tpt <= kBThreads) return tc;
-    return 0;
+static void drop_graph(BatchedState* bs) {
+    if (bs->exec) cudaGraphExecDestroy(bs->exec);
+    if (bs->graph) cudaGraphDestroy(bs->graph);
+    bs->exec = nullptr;
+    bs->graph = nullptr;
+}
+
+// Tiling: TC trajectories per chunk, TPT per thread, ~ctas_per_sm CTAs per SM.
+dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm) {
+    BatchedState* bs = c->bat;
+    const int B = bs->B, n = c->n;
+    if (tpt != 1 && tpt != 2) return DQ_ERR_ARG;
+    if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
+    if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
+    if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
+    const int chunks = B / tc;
+    const int TPR = tc / tpt, RPC = kBThreads / TPR;
+    int gx = std::max(1, (bs->sms * ctas_per_sm) / chunks);
+    int rpc = (n + gx - 1) / gx;
+    rpc = ((rpc + RPC - 1) / RPC) * RPC;
+    gx = (n + rpc - 1) / rpc;
+    if (gx > kMaxCtasPerChunk || (size_t)gx * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
+    bs->TC = tc;
+    bs->TPT = tpt;
+    bs->chunks = chunks;
+    bs->gx = gx;
+    bs->rpc = rpc;
+    bs->ctas_per_sm = ctas_per_sm;
+    drop_graph(bs);
+    return DQ_OK;
 }
 
 dq_status batched_alloc(dq_ctx* c) {
@@ -548,19 +599,11 @@ dq_status batched_alloc(dq_ctx* c) {
     c->bat = bs;
     bs->B = B;
     bs->mixed = c->cfg.precision == DQ_PREC_MIXED;
-    const int tpt = bs->mixed ? VecT<float>::TPT : VecT<double>::TPT;
-    bs->TC = pick_tc(B, tpt);
-    if (!bs->TC) {
-        c->err = "batched: n_traj must be a multiple of 2 for the mixed path";
+    cudaDeviceGetAttribute(&bs->sms, cudaDevAttrMultiProcessorCount, c->cfg.device);
+    if (B % 2 && bs->mixed) {
+        c->err = "batched: n_traj must be even for the mixed path";
         return DQ_ERR_ARG;
     }
-    bs->chunks = B / bs->TC;
-    int dev_sms = 148;
-    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->cfg.device);
-    const int TPR = bs->TC / tpt, RPC = kBThreads / TPR;
-    int gx = std::max(1, (dev_sms * 4) / bs->chunks);
-    gx = std::min(gx, (n + RPC - 1) / RPC);
-    bs->gx = gx;
     const size_t real_sz = bs->mixed ? sizeof(float) : sizeof(double);
     const size_t slab = (size_t)n * B * 2 * real_sz;
     DQ_CU(cudaMalloc(&bs->slabs, slab * (m + 2)));
@@ -568,11 +611,11 @@ dq_status batched_alloc(dq_ctx* c) {
     DQ_CU(cudaMalloc(&bs->diag, (size_t)n * B * real_sz));
     DQ_CU(cudaMalloc(&bs->eps, sizeof(double) * (size_t)n * B));
     DQ_CU(cudaMalloc(&bs->deps, sizeof(double) * (size_t)n * B));
-    // scalars
     const size_t LB = (size_t)kMaxL * B;
-    const size_t partial_n = (size_t)bs->chunks * gx * bs->TC * 2 * 2;
-    const size_t corr_n = (size_t)(c->cfg.max_steps + 1) * bs->chunks * 2;
-    const size_t total = LB * 2 /*alpha*/ + LB /*beta*/ + LB /*sc*/ + LB * 2 /*yt*/ + B + B + partial_n + corr_n;
+    // partial capacity: up to 16 CTAs per SM over all chunks, 2 doubles per trajectory
+    bs->partial_cap = (size_t)std::min(kMaxCtasPerChunk, bs->sms * 16) * B * 2;
+    const size_t corr_n = (size_t)(c->cfg.max_steps + 1) * B * 2;   // chunks <= B
+    const size_t total = LB * 2 + LB + LB + LB * 2 + B + B + 2 * bs->partial_cap + corr_n;
     DQ_CU(cudaMalloc(&bs->scal_mem, sizeof(double) * total));
     DQ_CU(cudaMemsetAsync(bs->scal_mem, 0, sizeof(double) * total, c->stream));
     double* p = bs->scal_mem;
@@ -582,22 +625,32 @@ dq_status batched_alloc(dq_ctx* c) {
     bs->s.yt = p; p += LB * 2;
     bs->s.nav = p; p += B;
     bs->s.norm2 = p; p += B;
-    bs->s.partial = p; p += partial_n;
+    bs->s.partial = p; p += 2 * bs->partial_cap;
     bs->s.corr = p; p += corr_n;
-    DQ_CU(cudaMalloc(&bs->s.tickets, sizeof(unsigned int) * 8 * bs->chunks + sizeof(unsigned int) * 8));
-    DQ_CU(cudaMemsetAsync(bs->s.tickets, 0, sizeof(unsigned int) * 8 * bs->chunks + sizeof(unsigned int) * 8, c->stream));
+    const size_t nt = (size_t)8 * B + 8;
+    DQ_CU(cudaMalloc(&bs->s.tickets, sizeof(unsigned int) * nt));
+    DQ_CU(cudaMemsetAsync(bs->s.tickets, 0, sizeof(unsigned int) * nt, c->stream));
     DQ_CU(cudaMalloc(&bs->s.status, sizeof(int) * 2));
     bs->s.step = bs->s.status + 1;
     DQ_CU(cudaMemsetAsync(bs->s.status, 0, sizeof(int) * 2, c->stream));
     DQ_CU(cudaFuncSetAttribute(k_pade_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pade_smem_bytes(m + 2)));
+    // default tiling (dq_autotune refines it)
+    int tpt = bs->mixed ? 2 : 1;
+    int tc = 16;
+    while (tc > tpt && B % tc) tc >>= 1;
+    if (B % tc) tc = tpt;
+    dq_status st = batched_set_tiling(c, tc, tpt, 2);
+    if (st) {
+        c->err = "batched: no valid tiling for n_traj";
+        return st;
+    }
     return DQ_OK;
 }
 
 void batched_free(dq_ctx* c) {
     BatchedState* bs = c->bat;
     if (!bs) return;
-    if (bs->exec) cudaGraphExecDestroy(bs->exec);
-    if (bs->graph) cudaGraphDestroy(bs->graph);
+    drop_graph(bs);
     cudaFree(bs->slabs); cudaFree(bs->diag); cudaFree(bs->eps); cudaFree(bs->deps);
     cudaFree(bs->scal_mem); cudaFree(bs->s.tickets); cudaFree(bs->s.status);
     delete bs;
@@ -607,19 +660,19 @@ void batched_free(dq_ctx* c) {
 dq_status batched_reset(dq_ctx* c) {
     BatchedState* bs = c->bat;
     const int n = c->n, B = bs->B;
-    size_t total = (size_t)n * B;
-    int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
-    k_traj_init_b<<<blocks, 256, 0, c->stream>>>(n, B, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
+    const int blocks = std::min(n, bs->sms * 8);
+    const int thr = std::min(256, ((B + 31) / 32) * 32);
+    k_traj_init_b<<<blocks, thr, 0, c->stream>>>(n, B, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
                                                  c->d_sigma, c->cfg.noise_model, bs->eps, bs->deps);
     const size_t real_sz = bs->mixed ? sizeof(float) : sizeof(double);
     const size_t slab = (size_t)n * B * 2 * real_sz;
     if (bs->mixed)
-        k_set_psi0_b<float><<<blocks, 256, 0, c->stream>>>(n, B, c->d_psi0, (float*)((char*)bs->slabs + slab));
+        k_set_psi0_b<float><<<blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, (float*)((char*)bs->slabs + slab));
     else
-        k_set_psi0_b<double><<<blocks, 256, 0, c->stream>>>(n, B, c->d_psi0, (double*)((char*)bs->slabs + slab));
+        k_set_psi0_b<double><<<blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, (double*)((char*)bs->slabs + slab));
     k_set_norms_b<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, bs->s);
-    k_init_obs_b<<<std::max(1, std::min(148, (n + 255) / 256)), 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops,
-                                                                                     bs->s, bs->chunks);
+    k_init_obs_b<<<std::max(1, std::min(bs->sms, (n + 255) / 256)), 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops,
+                                                                                        bs->s, bs->chunks);
     DQ_CU(cudaGetLastError());
     return DQ_OK;
 }
@@ -649,51 +702,73 @@ struct StepTimer {
     }
 };
 
-template <typename Real>
-static dq_status enqueue_step(dq_ctx* c, StepTimer* tm = nullptr) {
+template <typename Real, int TPT>
+static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm) {
+    BatchedState* bs = c->bat;
+    const int n = c->n, B = bs->B, TC = bs->TC, rpc = bs->rpc;
+    cudaStream_t st = c->stream;
+    const size_t se = (size_t)n * B;
+    Real* slabs = (Real*)bs->slabs;
+    auto slab = [&](int k) { return slabs + 2 * se * k; };
+    const Real* val = bs->mixed ? (const Real*)c->d_valf : (const Real*)c->d_val;
+    const dim3 grid(bs->gx, bs->chunks);
+    if (tm) tm->mark(DQ_KIND_SPMM, st);
+    if (c->cfg.dot_mode == DQ_DOT_BILINEAR)
+        k_spmm<Real, TPT, true, true><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, c->d_rowptr, c->d_col, val,
+                                                                  (const Real*)bs->diag, slab(j), slab(0), bs->s);
+    else
+        k_spmm<Real, TPT, false, true><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, c->d_rowptr, c->d_col, val,
+                                                                   (const Real*)bs->diag, slab(j), slab(0), bs->s);
+    if (tm) tm->mark(DQ_KIND_AXPY, st);
+    k_axpy_beta<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slab(0), slab(j), slab(j - 1),
+                                                       slab(j + 1), bs->s);
+    return DQ_OK;
+}
+
+template <typename Real, int TPT>
+static dq_status enqueue_step(dq_ctx* c, StepTimer* tm) {
     BatchedState* bs = c->bat;
     auto mark = [&](int k) { if (tm) tm->mark(k, c->stream); };
-    const int n = c->n, B = bs->B, m = c->cfg.m, TC = bs->TC;
+    const int n = c->n, B = bs->B, m = c->cfg.m, TC = bs->TC, rpc = bs->rpc;
     cudaStream_t st = c->stream;
-    const size_t slab_elems = (size_t)n * B;   // complex elements per slab
+    const size_t se = (size_t)n * B;
     Real* slabs = (Real*)bs->slabs;
-    auto slab = [&](int j) { return slabs + 2 * slab_elems * j; };
-    Real* w = slab(0);
+    auto slab = [&](int k) { return slabs + 2 * se * k; };
     const int ns = c->cfg.ka_substeps > 0 ? c->cfg.ka_substeps : 1;
     const double subdt = c->cfg.dt / (double)ns;
     const double sqrt_subdt = sqrt(subdt);
-    size_t total = (size_t)n * B;
-    int nblocks = (int)std::min<size_t>((total + 255) / 256, 148 * 8);
+    const dim3 grid(bs->gx, bs->chunks);
     mark(DQ_KIND_NOISE);
-    k_noise_b<Real><<<nblocks, 256, 0, st>>>(n, B, c->cfg.noise_model, ns, subdt, sqrt_subdt, c->cfg.seed, c->d_sigma,
-                                             c->d_invtau, c->d_coeff, bs->eps, bs->deps, (Real*)bs->diag, bs->s);
+    k_noise_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, c->cfg.noise_model, ns, subdt, sqrt_subdt,
+                                                     c->cfg.seed, c->d_sigma, c->d_invtau, c->d_coeff, bs->eps,
+                                                     bs->deps, (Real*)bs->diag, bs->s);
+    for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm);
     const Real* val = bs->mixed ? (const Real*)c->d_valf : (const Real*)c->d_val;
-    dim3 grid(bs->gx, bs->chunks);
-    const bool bil = c->cfg.dot_mode == DQ_DOT_BILINEAR;
-    for (int j = 1; j <= m; ++j) {
-        mark(DQ_KIND_SPMM);
-        if (bil)
-            k_spmm<Real, true, true><<<grid, kBThreads, 0, st>>>(n, B, TC, j, c->d_rowptr, c->d_col, val,
-                                                                 (const Real*)bs->diag, slab(j), w, bs->s);
-        else
-            k_spmm<Real, false, true><<<grid, kBThreads, 0, st>>>(n, B, TC, j, c->d_rowptr, c->d_col, val,
-                                                                  (const Real*)bs->diag, slab(j), w, bs->s);
-        mark(DQ_KIND_AXPY);
-        k_axpy_beta<Real><<<grid, kBThreads, 0, st>>>(n, B, TC, j, w, slab(j), slab(j - 1), slab(j + 1), bs->s);
-    }
     mark(DQ_KIND_SPMM_NORM);
-    k_spmm<Real, false, false><<<grid, kBThreads, 0, st>>>(n, B, TC, m + 1, c->d_rowptr, c->d_col, val,
-                                                           (const Real*)bs->diag, slab(m + 1), nullptr, bs->s);
+    k_spmm<Real, TPT, false, false><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, m + 1, c->d_rowptr, c->d_col, val,
+                                                                (const Real*)bs->diag, slab(m + 1), nullptr, bs->s);
     mark(DQ_KIND_PADE);
     k_pade_b<<<B, 128, pade_smem_bytes(m + 2), st>>>(m, B, c->tau_im, c->cfg.norm_mode, bs->s, c->d_erracc);
     mark(DQ_KIND_COMBINE);
-    k_combine_b<Real><<<grid, kBThreads, 0, st>>>(n, B, TC, m, slabs, slab_elems, c->d_psi0, bs->s);
-    int pblocks = std::max(1, std::min(148 * 4, (n + 7) / 8));
+    k_combine_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, m, slabs, se, c->d_psi0, bs->s);
+    const int pblocks = std::max(1, std::min(bs->sms * 4, (n + 7) / 8));
     mark(DQ_KIND_POP);
     k_pop_b<Real><<<pblocks, 256, 0, st>>>(n, B, c->cfg.pop_every, slab(1), c->d_pops, bs->s,
-                                           bs->s.tickets + 8 * bs->chunks);
+                                           bs->s.tickets + 8 * B);
     mark(-1);
     return check_cuda(c, cudaGetLastError(), "batched step launch");
+}
+
+static dq_status enqueue_step_any(dq_ctx* c, StepTimer* tm) {
+    BatchedState* bs = c->bat;
+    if (!bs->mixed) return enqueue_step<double, 1>(c, tm);
+    return bs->TPT == 2 ? enqueue_step<float, 2>(c, tm) : enqueue_step<float, 1>(c, tm);
+}
+
+static dq_status enqueue_iteration_any(dq_ctx* c, int j) {
+    BatchedState* bs = c->bat;
+    if (!bs->mixed) return enqueue_iteration<double, 1>(c, j, nullptr);
+    return bs->TPT == 2 ? enqueue_iteration<float, 2>(c, j, nullptr) : enqueue_iteration<float, 1>(c, j, nullptr);
 }
 
 dq_status batched_run(dq_ctx* c, int n_steps) {
@@ -701,7 +776,7 @@ dq_status batched_run(dq_ctx* c, int n_steps) {
     if (n_steps == 0) return DQ_OK;
     if (!bs->exec) {
         DQ_CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        dq_status st = bs->mixed ? enqueue_step<float>(c) : enqueue_step<double>(c);
+        dq_status st = enqueue_step_any(c, nullptr);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         if (st) return st;
@@ -722,7 +797,7 @@ dq_status batched_profile(dq_ctx* c, int n_steps, double* ms, int* cnt, int nk) 
     BatchedState* bs = c->bat;
     StepTimer tm;
     for (int k = 0; k < n_steps; ++k) {
-        dq_status st = bs->mixed ? enqueue_step<float>(c, &tm) : enqueue_step<double>(c, &tm);
+        dq_status st = enqueue_step_any(c, &tm);
         if (st) return st;
         DQ_CU(cudaStreamSynchronize(c->stream));
         tm.collect(ms, cnt, nk);
@@ -734,6 +809,31 @@ dq_status batched_profile(dq_ctx* c, int n_steps, double* ms, int* cnt, int nk) 
     return DQ_OK;
 }
 
+// Mean device time of one Lanczos iteration (SpMM + axpy) under the current
+// tiling: reps launches of iteration 1 between two events.
+dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
+    cudaEvent_t e0, e1;
+    DQ_CU(cudaEventCreate(&e0));
+    DQ_CU(cudaEventCreate(&e1));
+    enqueue_iteration_any(c, 1);   // warm-up
+    DQ_CU(cudaEventRecord(e0, c->stream));
+    for (int r = 0; r < reps; ++r) enqueue_iteration_any(c, 1);
+    DQ_CU(cudaEventRecord(e1, c->stream));
+    DQ_CU(cudaEventSynchronize(e1));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / reps;
+    return check_cuda(c, cudaGetLastError(), "time iteration");
+}
+
+void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps) {
+    if (tc) *tc = c->bat->TC;
+    if (tpt) *tpt = c->bat->TPT;
+    if (cps) *cps = c->bat->ctas_per_sm;
+}
+
 dq_status batched_get_states(dq_ctx* c, dq_cdouble* out) {
     BatchedState* bs = c->bat;
     const int n = c->n, B = bs->B;
@@ -741,11 +841,12 @@ dq_status batched_get_states(dq_ctx* c, dq_cdouble* out) {
     DQ_CU(cudaMalloc(&tmp, sizeof(cd) * (size_t)n * B));
     const size_t real_sz = bs->mixed ? sizeof(float) : sizeof(double);
     const size_t slab = (size_t)n * B * 2 * real_sz;
-    int blocks = (int)std::min<size_t>(((size_t)n * B + 255) / 256, 148 * 16);
+    const int blocks = std::min(n, bs->sms * 8);
+    const int thr = std::min(256, ((B + 31) / 32) * 32);
     if (bs->mixed)
-        k_get_states_b<float><<<blocks, 256, 0, c->stream>>>(n, B, (const float*)((char*)bs->slabs + slab), bs->s, tmp);
+        k_get_states_b<float><<<blocks, thr, 0, c->stream>>>(n, B, (const float*)((char*)bs->slabs + slab), bs->s, tmp);
     else
-        k_get_states_b<double><<<blocks, 256, 0, c->stream>>>(n, B, (const double*)((char*)bs->slabs + slab), bs->s, tmp);
+        k_get_states_b<double><<<blocks, thr, 0, c->stream>>>(n, B, (const double*)((char*)bs->slabs + slab), bs->s, tmp);
     cudaError_t e = cudaMemcpyAsync(out, tmp, sizeof(cd) * (size_t)n * B, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(tmp);
@@ -757,23 +858,11 @@ void batched_noise_arrays(dq_ctx* c, const double** eps, const double** deps) {
     *deps = c->bat->deps;
 }
 
-// correlation sums over chunks -> d_corr (called by the getter)
-__global__ void k_corr_collect(int np, int chunks, const double* __restrict__ corr_chunks, cd* __restrict__ out) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
-        double sr = 0.0, si = 0.0;
-        for (int ch = 0; ch < chunks; ++ch) {
-            sr += corr_chunks[((size_t)k * chunks + ch) * 2];
-            si += corr_chunks[((size_t)k * chunks + ch) * 2 + 1];
-        }
-        out[k] = cmk(sr, si);
-    }
-}
-
 dq_status batched_collect_corr(dq_ctx* c) {
     BatchedState* bs = c->bat;
     const int np = c->steps_done + 1;
-    k_corr_collect<<<std::max(1, std::min(148, (np + 255) / 256)), 256, 0, c->stream>>>(np, bs->chunks, bs->s.corr,
-                                                                                          c->d_corr);
+    k_corr_collect<<<std::max(1, std::min(bs->sms, (np + 255) / 256)), 256, 0, c->stream>>>(np, bs->chunks, bs->s.corr,
+                                                                                              c->d_corr);
     return check_cuda(c, cudaGetLastError(), "corr collect");
 }
 

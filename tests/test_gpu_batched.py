@@ -112,3 +112,33 @@ def test_spectrum_matches_numpy():
     x[:len(corr)] = corr
     assert np.abs(spec - np.fft.ifft(x) * 128).max() < 1e-10
     p.close()
+
+
+@pytest.mark.parametrize("tiling", [(2, 2, 1), (4, 1, 2), (4, 2, 8), (2, 1, 4)])
+def test_every_tiling_matches_oracle(tiling):
+    """Tilings only change the schedule: each must reproduce the oracle."""
+    import dynaquant_b200 as dq
+    g = _golden()
+    p = _chain_prop(dq.PREC_MIXED, 1)
+    p.set_tiling(*tiling)
+    assert p.get_tiling() == tiling
+    p.run(G.CHAIN["n_steps"])
+    assert np.abs(p.populations() - g["herm_pops"]).max() < POP_TOL_MIXED
+    p.close()
+
+
+def test_autotune_picks_valid_tiling_and_keeps_parity(tmp_path, monkeypatch):
+    import dynaquant_b200 as dq
+    monkeypatch.setenv("DQ_TUNE_CACHE", str(tmp_path / "tiling.json"))
+    g = _golden()
+    p = _chain_prop(dq.PREC_MIXED, 1)
+    r = p.autotune(reps=2)
+    assert not r["cached"] and r["ms_per_iter"] > 0
+    assert (tmp_path / "tiling.json").exists()
+    p.run(G.CHAIN["n_steps"])
+    assert np.abs(p.populations() - g["herm_pops"]).max() < POP_TOL_MIXED
+    p.close()
+    q = _chain_prop(dq.PREC_MIXED, 1)
+    r2 = q.autotune(reps=2)
+    assert r2["cached"] and q.get_tiling() == (r["traj_chunk"], r["vec"], r["ctas_per_sm"])
+    q.close()

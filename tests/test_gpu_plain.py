@@ -104,14 +104,17 @@ def test_tube_plain_matches_oracle(oracle):
     p.set_initial_state(psi0)
     p.reset()
     eps, deps = S.traj_init(1)
-    a = torch.tensor(psi0, dtype=torch.complex128, device="cuda")
-    b = torch.empty_like(a)
-    psi = psi0.copy()
-    for k in range(25):
-        p.prop_step(1, k, a.data_ptr(), b.data_ptr())
-        psi, _, _, _ = S.krylov_step(S.noise_update(1, k, eps, deps), psi)
-        a, b = b, a
-    got = a.cpu().numpy()
+    # dq_prop_step is ordered on the context's stream: create, use and read
+    # the buffers on that same stream
+    with torch.cuda.stream(torch.cuda.ExternalStream(p.stream)):
+        a = torch.tensor(psi0, dtype=torch.complex128, device="cuda")
+        b = torch.empty_like(a)
+        psi = psi0.copy()
+        for k in range(25):
+            p.prop_step(1, k, a.data_ptr(), b.data_ptr())
+            psi, _, _, _ = S.krylov_step(S.noise_update(1, k, eps, deps), psi)
+            a, b = b, a
+        got = a.cpu().numpy()
     assert np.abs(np.abs(got) ** 2 - np.abs(psi) ** 2).max() < POP_TOL
     p.close()
 
