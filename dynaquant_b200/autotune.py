@@ -64,20 +64,20 @@ def store(k: str, entry: dict) -> None:
 
 def tune(prop, nnz: int, reps: int = 5, use_cache: bool = True) -> dict:
     """Chooses the tiling for `prop` (a dynaquant_b200.Propagator with its
-    system set); returns {"traj_chunk", "vec", "ctas_per_sm", "ms_per_iter",
-    "cached"}.  The ensemble is reset afterwards."""
+    system set); returns {"traj_chunk", "vec", "ctas_per_sm", "rows_per_block",
+    "ms_per_iter", "cached"}.  The ensemble is reset afterwards."""
     k = key(prop, nnz)
     if use_cache:
         e = load_cache().get(k)
         if e:
             try:
-                prop.set_tiling(e["traj_chunk"], e["vec"], e["ctas_per_sm"])
+                prop.set_tiling(e["traj_chunk"], e["vec"], e["ctas_per_sm"], e["rows_per_block"])
                 prop.reset()
                 return dict(e, cached=True)
             except Exception:
                 pass
     ms = prop.autotune_raw(reps)
-    tc, vec, cps = prop.get_tiling()
-    entry = {"traj_chunk": tc, "vec": vec, "ctas_per_sm": cps, "ms_per_iter": ms}
+    tc, vec, cps, rpb = prop.get_tiling()
+    entry = {"traj_chunk": tc, "vec": vec, "ctas_per_sm": cps, "rows_per_block": rpb, "ms_per_iter": ms}
     store(k, entry)
     return dict(entry, cached=False)

@@ -107,8 +107,22 @@ struct Tile {
 
 }  // namespace dq
 
+// Row-blocked column-union form of the off-diagonal couplings: block k holds
+// rows [kR, kR+R); its entries are the sorted union of those rows' neighbour
+// columns, each with R coefficients (zero where a row lacks that column), so
+// one gathered trajectory row serves R output rows.
+struct BlockFmt {
+    int R = 0, nb = 0;
+    size_t nunion = 0;
+    int* bptr = nullptr;     // nb + 1
+    int* bcol = nullptr;     // nunion
+    void* bcoef = nullptr;   // nunion x R (Real)
+};
+
 struct dq::BatchedState {
     int B = 0, TC = 0, TPT = 2, chunks = 0, gx = 0, rpc = 0, ctas_per_sm = 2;
+    int R = 4, gxs = 0, bpc = 0;          // SpMM: rows per block, CTAs per chunk, blocks per CTA
+    ::BlockFmt fmt[4];                    // R = 1, 2, 4, 8 (built on demand)
     int sms = 148;
     bool mixed = true;
     void* slabs = nullptr;      // (m+2) slabs (slab 0 = w)
@@ -233,58 +247,107 @@ __global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int TC, int
     }
 }
 
-// w = H q_j for all trajectories and alpha_j[b] = <q_j, w>_b  (kWrite), or
-// ||H q_j||_b only (!kWrite, for the EXPOKIT error estimate)
-template <typename Real, int TPT, bool kBilinear, bool kWrite>
-__global__ void __launch_bounds__(kBThreads) k_spmm(int n, int B, int TC, int rpc, int j,
-                                                   const int* __restrict__ rowptr, const int* __restrict__ col,
-                                                   const Real* __restrict__ val, const Real* __restrict__ d,
-                                                   const Real* __restrict__ rj, Real* __restrict__ w,
-                                                   BatchedScalars S) {
-    const Tile<TPT> T(TC, rpc, n);
+template <typename Real, int R>
+__device__ __forceinline__ void ld_coef(const Real* __restrict__ base, int e, Real (&c)[R]) {
+    const Real* p = base + (size_t)e * R;
+    if constexpr (R == 1) {
+        c[0] = __ldg(p);
+    } else if constexpr (sizeof(Real) * R == 8) {
+        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
+        c[0] = t.x;
+        c[1] = t.y;
+    } else {
+        constexpr int NV = (int)(sizeof(Real) * R / 16);
+        constexpr int PER = 16 / (int)sizeof(Real);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(p) + v);
+            union { float4 f; Real r[PER]; } u;
+            u.f = t;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) c[v * PER + k] = u.r[k];
+        }
+    }
+}
+
+// Row-blocked SpMM: w = H q_j for all trajectories of the chunk, R rows per
+// block.  kWrite: also alpha_j[b] = <q_j, w>_b; !kWrite: ||H q_j||_b only.
+template <typename Real, int TPT, int R, bool kBilinear, bool kWrite>
+__global__ void __launch_bounds__(kBThreads) k_spmm_blk(int n, int B, int TC, int bpc, int nb, int j,
+                                                       const int* __restrict__ bptr, const int* __restrict__ bcol,
+                                                       const Real* __restrict__ bcoef, const Real* __restrict__ d,
+                                                       const Real* __restrict__ rj, Real* __restrict__ w,
+                                                       BatchedScalars S) {
+    const int TPR = TC / TPT;
+    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int RPC = blockDim.x / TPR;
+    const int b0 = blockIdx.y * TC + tr * TPT;
+    const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
     double sc[TPT], ar[TPT], ai[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) {
-        sc[t] = S.sc[(size_t)j * B + T.b0 + t];
+        sc[t] = S.sc[(size_t)j * B + b0 + t];
         ar[t] = 0.0;
         ai[t] = 0.0;
     }
-    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
-        const size_t base = (size_t)row * B + T.b0;
-        const CV<Real, TPT> x = ldv<Real, TPT, true>(rj, base);
-        CV<Real, TPT> u;
+    for (int k = k0 + rl; k < k1; k += RPC) {
+        const int row0 = k * R;
+        CV<Real, TPT> acc[R];
 #pragma unroll
-        for (int t = 0; t < TPT; ++t) {
-            const Real dd = __ldg(d + base + t);
-            u.re[t] = dd * x.re[t];
-            u.im[t] = dd * x.im[t];
-        }
-        const int p1 = __ldg(rowptr + row + 1);
-        for (int p = __ldg(rowptr + row); p < p1; ++p) {
-            const int c = __ldg(col + p);
-            const Real v = __ldg(val + p);
-            const CV<Real, TPT> y = ldv<Real, TPT, true>(rj, (size_t)c * B + T.b0);
+        for (int i = 0; i < R; ++i) {
+            const int row = row0 + i;
+            if (row < n) {
+                const size_t base = (size_t)row * B + b0;
+                const CV<Real, TPT> x = ldv<Real, TPT, true>(rj, base);
 #pragma unroll
-            for (int t = 0; t < TPT; ++t) {
-                u.re[t] = fma(v, y.re[t], u.re[t]);
-                u.im[t] = fma(v, y.im[t], u.im[t]);
+                for (int t = 0; t < TPT; ++t) {
+                    const Real dd = __ldg(d + base + t);
+                    acc[i].re[t] = dd * x.re[t];
+                    acc[i].im[t] = dd * x.im[t];
+                }
+            } else {
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) { acc[i].re[t] = 0; acc[i].im[t] = 0; }
             }
         }
-        if (kWrite) {
-            CV<Real, TPT> o;
+        const int pe = __ldg(bptr + k + 1);
+#pragma unroll 4
+        for (int p = __ldg(bptr + k); p < pe; ++p) {
+            const int c = __ldg(bcol + p);
+            Real cf[R];
+            ld_coef<Real, R>(bcoef, p, cf);
+            const CV<Real, TPT> y = ldv<Real, TPT, true>(rj, (size_t)c * B + b0);
 #pragma unroll
-            for (int t = 0; t < TPT; ++t) {
-                o.re[t] = (Real)(sc[t] * (double)u.re[t]);
-                o.im[t] = (Real)(sc[t] * (double)u.im[t]);
-                // alpha partial from the unscaled product; sc^2 applied at the end
-                const double xr = x.re[t], xi = x.im[t], ur = u.re[t], ui = u.im[t];
-                if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
-                else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+            for (int i = 0; i < R; ++i) {
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    acc[i].re[t] = fma(cf[i], y.re[t], acc[i].re[t]);
+                    acc[i].im[t] = fma(cf[i], y.im[t], acc[i].im[t]);
+                }
             }
-            stv<Real, TPT>(w, base, o);
-        } else {
+        }
 #pragma unroll
-            for (int t = 0; t < TPT; ++t) ar[t] += (double)u.re[t] * u.re[t] + (double)u.im[t] * u.im[t];
+        for (int i = 0; i < R; ++i) {
+            const int row = row0 + i;
+            if (row >= n) break;
+            const size_t base = (size_t)row * B + b0;
+            if (kWrite) {
+                const CV<Real, TPT> x = ldv<Real, TPT, true>(rj, base);
+                CV<Real, TPT> o;
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    o.re[t] = (Real)(sc[t] * (double)acc[i].re[t]);
+                    o.im[t] = (Real)(sc[t] * (double)acc[i].im[t]);
+                    const double xr = x.re[t], xi = x.im[t], ur = acc[i].re[t], ui = acc[i].im[t];
+                    if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
+                    else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+                }
+                stv<Real, TPT>(w, base, o);
+            } else {
+#pragma unroll
+                for (int t = 0; t < TPT; ++t)
+                    ar[t] += (double)acc[i].re[t] * acc[i].re[t] + (double)acc[i].im[t] * acc[i].im[t];
+            }
         }
     }
     __shared__ double2 red[kMaxTC];
@@ -568,27 +631,101 @@ static void drop_graph(BatchedState* bs) {
     bs->graph = nullptr;
 }
 
-// Tiling: TC trajectories per chunk, TPT per thread, ~ctas_per_sm CTAs per SM.
-dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm) {
+static int r_index(int R) { return R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : -1; }
+
+static void free_fmt(BlockFmt& f) {
+    cudaFree(f.bptr); cudaFree(f.bcol); cudaFree(f.bcoef);
+    f = BlockFmt();
+}
+
+void batched_invalidate_blocks(dq_ctx* c) {
+    if (!c->bat) return;
+    for (auto& f : c->bat->fmt) free_fmt(f);
+    drop_graph(c->bat);
+}
+
+// Builds the row-blocked column-union form of the (scaled) off-diagonal CSR.
+static dq_status build_fmt(dq_ctx* c, int R, BlockFmt& f) {
+    BatchedState* bs = c->bat;
+    const int n = c->n, nb = (n + R - 1) / R;
+    std::vector<int> bptr(nb + 1, 0), bcol;
+    std::vector<double> coef;
+    std::vector<int> cols;
+    bcol.reserve((size_t)c->nnz_off + nb);
+    coef.reserve(((size_t)c->nnz_off + nb) * R);
+    for (int k = 0; k < nb; ++k) {
+        const int r0 = k * R, r1 = std::min(n, r0 + R);
+        cols.clear();
+        for (int r = r0; r < r1; ++r)
+            for (int p = c->rowptr[r]; p < c->rowptr[r + 1]; ++p) cols.push_back(c->col[p]);
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        const size_t base = bcol.size();
+        bcol.insert(bcol.end(), cols.begin(), cols.end());
+        coef.resize(bcol.size() * R, 0.0);
+        for (int r = r0; r < r1; ++r)
+            for (int p = c->rowptr[r]; p < c->rowptr[r + 1]; ++p) {
+                const size_t u = base + (std::lower_bound(cols.begin(), cols.end(), c->col[p]) - cols.begin());
+                coef[u * R + (r - r0)] += c->val[p];
+            }
+        bptr[k + 1] = (int)bcol.size();
+    }
+    f.R = R;
+    f.nb = nb;
+    f.nunion = bcol.size();
+    const size_t nu = std::max<size_t>(f.nunion, 1);
+    DQ_CU(cudaMalloc(&f.bptr, sizeof(int) * (nb + 1)));
+    DQ_CU(cudaMalloc(&f.bcol, sizeof(int) * nu));
+    DQ_CU(cudaMemcpy(f.bptr, bptr.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice));
+    if (f.nunion) DQ_CU(cudaMemcpy(f.bcol, bcol.data(), sizeof(int) * f.nunion, cudaMemcpyHostToDevice));
+    if (bs->mixed) {
+        std::vector<float> cf(coef.begin(), coef.end());
+        DQ_CU(cudaMalloc(&f.bcoef, sizeof(float) * nu * R));
+        if (f.nunion) DQ_CU(cudaMemcpy(f.bcoef, cf.data(), sizeof(float) * f.nunion * R, cudaMemcpyHostToDevice));
+    } else {
+        DQ_CU(cudaMalloc(&f.bcoef, sizeof(double) * nu * R));
+        if (f.nunion) DQ_CU(cudaMemcpy(f.bcoef, coef.data(), sizeof(double) * f.nunion * R, cudaMemcpyHostToDevice));
+    }
+    return DQ_OK;
+}
+
+// Tiling: TC trajectories per chunk, TPT per thread, ~ctas_per_sm CTAs per
+// SM, R rows per SpMM block.
+dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R) {
     BatchedState* bs = c->bat;
     const int B = bs->B, n = c->n;
     if (tpt != 1 && tpt != 2) return DQ_ERR_ARG;
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
+    const int ri = r_index(R);
+    if (ri < 0) return DQ_ERR_ARG;
     const int chunks = B / tc;
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
     int gx = std::max(1, (bs->sms * ctas_per_sm) / chunks);
     int rpc = (n + gx - 1) / gx;
     rpc = ((rpc + RPC - 1) / RPC) * RPC;
     gx = (n + rpc - 1) / rpc;
+    const int nb = (n + R - 1) / R;
+    int gxs = std::max(1, (bs->sms * ctas_per_sm) / chunks);
+    int bpc = (nb + gxs - 1) / gxs;
+    bpc = ((bpc + RPC - 1) / RPC) * RPC;
+    gxs = (nb + bpc - 1) / bpc;
     if (gx > kMaxCtasPerChunk || (size_t)gx * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
+    if (gxs > kMaxCtasPerChunk || (size_t)gxs * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
+    if (!bs->fmt[ri].bptr) {
+        dq_status st = build_fmt(c, R, bs->fmt[ri]);
+        if (st) return st;
+    }
     bs->TC = tc;
     bs->TPT = tpt;
     bs->chunks = chunks;
     bs->gx = gx;
     bs->rpc = rpc;
     bs->ctas_per_sm = ctas_per_sm;
+    bs->R = R;
+    bs->gxs = gxs;
+    bs->bpc = bpc;
     drop_graph(bs);
     return DQ_OK;
 }
@@ -639,7 +776,7 @@ dq_status batched_alloc(dq_ctx* c) {
     int tc = 16;
     while (tc > tpt && B % tc) tc >>= 1;
     if (B % tc) tc = tpt;
-    dq_status st = batched_set_tiling(c, tc, tpt, 2);
+    dq_status st = batched_set_tiling(c, tc, tpt, 2, 4);
     if (st) {
         c->err = "batched: no valid tiling for n_traj";
         return st;
@@ -651,6 +788,7 @@ void batched_free(dq_ctx* c) {
     BatchedState* bs = c->bat;
     if (!bs) return;
     drop_graph(bs);
+    for (auto& f : bs->fmt) free_fmt(f);
     cudaFree(bs->slabs); cudaFree(bs->diag); cudaFree(bs->eps); cudaFree(bs->deps);
     cudaFree(bs->scal_mem); cudaFree(bs->s.tickets); cudaFree(bs->s.status);
     delete bs;
@@ -702,6 +840,26 @@ struct StepTimer {
     }
 };
 
+template <typename Real, int TPT, bool kBil, bool kWrite>
+static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w) {
+    BatchedState* bs = c->bat;
+    const BlockFmt& f = bs->fmt[r_index(bs->R)];
+    const dim3 grid(bs->gxs, bs->chunks);
+    const int n = c->n, B = bs->B, TC = bs->TC;
+    const Real* cf = (const Real*)f.bcoef;
+    const Real* d = (const Real*)bs->diag;
+#define DQ_SPMM_R(RR)                                                                                             \
+    k_spmm_blk<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j, f.bptr, \
+                                                                               f.bcol, cf, d, rj, w, bs->s)
+    switch (bs->R) {
+        case 1: DQ_SPMM_R(1); break;
+        case 2: DQ_SPMM_R(2); break;
+        case 4: DQ_SPMM_R(4); break;
+        default: DQ_SPMM_R(8); break;
+    }
+#undef DQ_SPMM_R
+}
+
 template <typename Real, int TPT>
 static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm) {
     BatchedState* bs = c->bat;
@@ -710,15 +868,10 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm) {
     const size_t se = (size_t)n * B;
     Real* slabs = (Real*)bs->slabs;
     auto slab = [&](int k) { return slabs + 2 * se * k; };
-    const Real* val = bs->mixed ? (const Real*)c->d_valf : (const Real*)c->d_val;
     const dim3 grid(bs->gx, bs->chunks);
     if (tm) tm->mark(DQ_KIND_SPMM, st);
-    if (c->cfg.dot_mode == DQ_DOT_BILINEAR)
-        k_spmm<Real, TPT, true, true><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, c->d_rowptr, c->d_col, val,
-                                                                  (const Real*)bs->diag, slab(j), slab(0), bs->s);
-    else
-        k_spmm<Real, TPT, false, true><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, c->d_rowptr, c->d_col, val,
-                                                                   (const Real*)bs->diag, slab(j), slab(0), bs->s);
+    if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_spmm<Real, TPT, true, true>(c, j, slab(j), slab(0));
+    else launch_spmm<Real, TPT, false, true>(c, j, slab(j), slab(0));
     if (tm) tm->mark(DQ_KIND_AXPY, st);
     k_axpy_beta<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slab(0), slab(j), slab(j - 1),
                                                        slab(j + 1), bs->s);
@@ -743,10 +896,8 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm) {
                                                      c->cfg.seed, c->d_sigma, c->d_invtau, c->d_coeff, bs->eps,
                                                      bs->deps, (Real*)bs->diag, bs->s);
     for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm);
-    const Real* val = bs->mixed ? (const Real*)c->d_valf : (const Real*)c->d_val;
     mark(DQ_KIND_SPMM_NORM);
-    k_spmm<Real, TPT, false, false><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, m + 1, c->d_rowptr, c->d_col, val,
-                                                                (const Real*)bs->diag, slab(m + 1), nullptr, bs->s);
+    launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr);
     mark(DQ_KIND_PADE);
     k_pade_b<<<B, 128, pade_smem_bytes(m + 2), st>>>(m, B, c->tau_im, c->cfg.norm_mode, bs->s, c->d_erracc);
     mark(DQ_KIND_COMBINE);
@@ -828,10 +979,11 @@ dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
     return check_cuda(c, cudaGetLastError(), "time iteration");
 }
 
-void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps) {
+void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R) {
     if (tc) *tc = c->bat->TC;
     if (tpt) *tpt = c->bat->TPT;
     if (cps) *cps = c->bat->ctas_per_sm;
+    if (R) *R = c->bat->R;
 }
 
 dq_status batched_get_states(dq_ctx* c, dq_cdouble* out) {

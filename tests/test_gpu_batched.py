@@ -114,7 +114,7 @@ def test_spectrum_matches_numpy():
     p.close()
 
 
-@pytest.mark.parametrize("tiling", [(2, 2, 1), (4, 1, 2), (4, 2, 8), (2, 1, 4)])
+@pytest.mark.parametrize("tiling", [(2, 2, 1, 1), (4, 1, 2, 2), (4, 2, 8, 4), (2, 1, 4, 8), (4, 2, 2, 8)])
 def test_every_tiling_matches_oracle(tiling):
     """Tilings only change the schedule: each must reproduce the oracle."""
     import dynaquant_b200 as dq
@@ -140,5 +140,5 @@ def test_autotune_picks_valid_tiling_and_keeps_parity(tmp_path, monkeypatch):
     p.close()
     q = _chain_prop(dq.PREC_MIXED, 1)
     r2 = q.autotune(reps=2)
-    assert r2["cached"] and q.get_tiling() == (r["traj_chunk"], r["vec"], r["ctas_per_sm"])
+    assert r2["cached"] and q.get_tiling() == (r["traj_chunk"], r["vec"], r["ctas_per_sm"], r["rows_per_block"])
     q.close()
