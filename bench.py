@@ -282,7 +282,8 @@ def run_ours(args, rank, world, local_rank):
                    "trajectories_per_gpu": B, "dt_fs": w["dt"], "noise": "OU 250/50 fs + static 150",
                    "l2": "inputs larger than L2 (Krylov slabs %.1f GB)" % (8.0 * s.n * B * (w["m"] + 2) / 1e9),
                    "parallelism": f"replicas x{world}",
-                   "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "ms_per_iter")}},
+                   "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged",
+                                                    "ms_per_iter")}},
         "e2e": e2e,
         "gpu_launches": int(kernels_per_step * K),
         "roofline": {"bound": "hbm", "kernel": "k_spmm (SpMM + alpha)", "achieved": achieved, "peak": peak,

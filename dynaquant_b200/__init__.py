@@ -120,13 +120,13 @@ class Propagator:
     def run(self, n_steps):
         self._check(self.L.dq_run(self.h, n_steps))
 
-    def set_tiling(self, traj_chunk, vec, ctas_per_sm, rows_per_block=4):
-        self._check(self.L.dq_set_tiling(self.h, traj_chunk, vec, ctas_per_sm, rows_per_block))
+    def set_tiling(self, traj_chunk, vec, ctas_per_sm, rows_per_block=4, staged=0):
+        self._check(self.L.dq_set_tiling(self.h, traj_chunk, vec, ctas_per_sm, rows_per_block, staged))
 
     def get_tiling(self):
-        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        self._check(self.L.dq_get_tiling(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
-        return a.value, b.value, c.value, d.value
+        a, b, c, d, e = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        self._check(self.L.dq_get_tiling(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(e)))
+        return a.value, b.value, c.value, d.value, e.value
 
     def autotune_raw(self, reps=5):
         ms = C.c_double()

@@ -99,8 +99,8 @@ def load(path: str = LIB_PATH):
     L.dq_get_spectrum.argtypes = [vp, C.c_int, dp]
     L.dq_get_noise_state.argtypes = [vp, C.c_int, dp, dp]
     L.dq_profile_step.argtypes = [vp, C.c_int, dp, ip, C.c_int]
-    L.dq_set_tiling.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
-    L.dq_get_tiling.argtypes = [vp, ip, ip, ip, ip]
+    L.dq_set_tiling.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.dq_get_tiling.argtypes = [vp, ip, ip, ip, ip, ip]
     L.dq_autotune.argtypes = [vp, C.c_int, dp]
     for name in EXPORTS:
         if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done"):

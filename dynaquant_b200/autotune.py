@@ -71,13 +71,14 @@ def tune(prop, nnz: int, reps: int = 5, use_cache: bool = True) -> dict:
         e = load_cache().get(k)
         if e:
             try:
-                prop.set_tiling(e["traj_chunk"], e["vec"], e["ctas_per_sm"], e["rows_per_block"])
+                prop.set_tiling(e["traj_chunk"], e["vec"], e["ctas_per_sm"], e["rows_per_block"], e["staged"])
                 prop.reset()
                 return dict(e, cached=True)
             except Exception:
                 pass
     ms = prop.autotune_raw(reps)
-    tc, vec, cps, rpb = prop.get_tiling()
-    entry = {"traj_chunk": tc, "vec": vec, "ctas_per_sm": cps, "rows_per_block": rpb, "ms_per_iter": ms}
+    tc, vec, cps, rpb, staged = prop.get_tiling()
+    entry = {"traj_chunk": tc, "vec": vec, "ctas_per_sm": cps, "rows_per_block": rpb, "staged": staged,
+             "ms_per_iter": ms}
     store(k, entry)
     return dict(entry, cached=False)

@@ -32,8 +32,11 @@
 #include <cstdio>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "dq_internal.h"
 #include "dq_rng.cuh"
+#include "dq_tma.cuh"
 
 namespace dq {
 
@@ -122,6 +125,10 @@ struct BlockFmt {
 struct dq::BatchedState {
     int B = 0, TC = 0, TPT = 2, chunks = 0, gx = 0, rpc = 0, ctas_per_sm = 2;
     int R = 4, gxs = 0, bpc = 0;          // SpMM: rows per block, CTAs per chunk, blocks per CTA
+    int staged = 0;                       // 1: TMA-staged shared-memory window SpMM
+    int halo = 0, wmask = 0, rpc_win = 0, gxw = 0, bw = 0;   // window geometry, matrix bandwidth
+    size_t win_smem = 0;
+    std::vector<CUtensorMap> tmaps;       // one per slab (window variant)
     ::BlockFmt fmt[4];                    // R = 1, 2, 4, 8 (built on demand)
     int sms = 148;
     bool mixed = true;
@@ -227,6 +234,30 @@ __global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int TC, int
     const Tile<TPT> T(TC, rpc, n);
     const int step = *S.step;
     for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+        if constexpr (TPT == 2) {
+            // trajectories b0, b0+1 form one Philox pair (b0 is even)
+            const size_t x = (size_t)row * B + T.b0;
+            double v0, v1;
+            if (noise == DQ_NOISE_OU) {
+                double c0 = deps[x], c1 = deps[x + 1];
+                ou_update_pair(c0, c1, invtau[row], coeff[row], subdt, sqrt_subdt, ns, seed, T.b0 >> 1, step, row);
+                deps[x] = c0;
+                deps[x + 1] = c1;
+                v0 = __dadd_rn(c0, eps[x]);
+                v1 = __dadd_rn(c1, eps[x + 1]);
+            } else if (noise == DQ_NOISE_GAUSS) {
+                double z0, z1;
+                normal_pair(seed, P_GAUSS, T.b0 >> 1, step, row, 0, z0, z1);
+                v0 = __dadd_rn(__dmul_rn(z0, sigma[row]), eps[x]);
+                v1 = __dadd_rn(__dmul_rn(z1, sigma[row]), eps[x + 1]);
+            } else {
+                v0 = eps[x];
+                v1 = eps[x + 1];
+            }
+            d[x] = (Real)v0;
+            d[x + 1] = (Real)v1;
+            continue;
+        }
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
             const int b = T.b0 + t;
@@ -366,6 +397,151 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_blk(int n, int B, int TC, in
     }
 }
 
+// Row-blocked SpMM with the gathered trajectory rows staged in shared
+// memory.  The CTA owns rows [r0, r1) of one trajectory chunk and walks them
+// in steps of SR rows; a ring of W = wmask+1 rows holds [a-halo, a+SR+halo)
+// for the current step a, where halo >= the matrix bandwidth.  Thread 0
+// issues the next step's SR new rows as one 2-D TMA box before the current
+// step computes, so the copy overlaps the gathers (the ring holds two
+// windows: W >= 2 halo + 2 SR).  Rows outside [0, n) arrive as zeros.
+template <typename Real, int TPT, int R, bool kBilinear, bool kWrite>
+__global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, int rows_per_cta, int halo, int wmask,
+                                                       int j, const int* __restrict__ bptr,
+                                                       const int* __restrict__ bcol, const Real* __restrict__ bcoef,
+                                                       const Real* __restrict__ d, Real* __restrict__ w,
+                                                       BatchedScalars S, const __grid_constant__ CUtensorMap tmap) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    Real* win = reinterpret_cast<Real*>(smem_raw);   // [W][TC] complex
+    __shared__ __align__(8) uint64_t bars[2];
+    const int TPR = TC / TPT;
+    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int BPS = blockDim.x / TPR;   // row blocks per step
+    const int SR = BPS * R;             // rows per step
+    const int tl = tr * TPT;
+    const int b0 = blockIdx.y * TC + tl;
+    const int r0 = blockIdx.x * rows_per_cta;
+    const int r1 = min(n, r0 + rows_per_cta);
+    const int nsteps = r1 > r0 ? (r1 - r0 + SR - 1) / SR : 0;
+    const int xc = blockIdx.y * TC * 2;
+    const uint32_t box_bytes = (uint32_t)(SR * TC * 2 * sizeof(Real));
+    auto slot = [&](int row) { return win + (size_t)(row & wmask) * TC * 2; };
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && nsteps > 0) {
+        const int nbox = (2 * halo + SR) / SR;
+        mbar_arrive_expect_tx(&bars[0], box_bytes * nbox);
+        for (int q = 0; q < nbox; ++q) {
+            const int y = r0 - halo + q * SR;
+            tma_load_2d(slot(y), &tmap, &bars[0], xc, y);
+        }
+    }
+    double sc[TPT], ar[TPT], ai[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        sc[t] = S.sc[(size_t)j * B + b0 + t];
+        ar[t] = 0.0;
+        ai[t] = 0.0;
+    }
+    int issued = 0;   // highest step whose load was issued
+    for (int s = 0; s < nsteps; ++s) {
+        const int a = r0 + s * SR;
+        __syncthreads();   // step s-1 done: the rows the next load overwrites are free
+        if (threadIdx.x == 0 && s + 1 < nsteps) {
+            const int y = a + SR + halo;
+            mbar_arrive_expect_tx(&bars[(s + 1) & 1], box_bytes);
+            tma_load_2d(slot(y), &tmap, &bars[(s + 1) & 1], xc, y);
+        }
+        if (s + 1 < nsteps) issued = s + 1;
+        const bool ok = mbar_wait_bounded(&bars[s & 1], (uint32_t)((s >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            // a copy never completed: flag it, give the copy in flight a
+            // bounded chance to land, and leave without reducing
+            if (threadIdx.x == 0) atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
+            if (issued > s) mbar_wait_bounded(&bars[issued & 1], (uint32_t)((issued >> 1) & 1));
+            return;
+        }
+        const int k = a / R + rl;
+        const int row0 = k * R;
+        if (row0 < r1) {
+            CV<Real, TPT> acc[R];
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const int row = row0 + i;
+                const CV<Real, TPT> x = ldv<Real, TPT, false>(slot(row), tl);
+                if (row < n) {
+                    const size_t base = (size_t)row * B + b0;
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) {
+                        const Real dd = __ldg(d + base + t);
+                        acc[i].re[t] = dd * x.re[t];
+                        acc[i].im[t] = dd * x.im[t];
+                    }
+                } else {
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) { acc[i].re[t] = 0; acc[i].im[t] = 0; }
+                }
+            }
+            const int pe = __ldg(bptr + k + 1);
+#pragma unroll 4
+            for (int p = __ldg(bptr + k); p < pe; ++p) {
+                const int c = __ldg(bcol + p);
+                Real cf[R];
+                ld_coef<Real, R>(bcoef, p, cf);
+                const CV<Real, TPT> y = ldv<Real, TPT, false>(slot(c), tl);
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) {
+                        acc[i].re[t] = fma(cf[i], y.re[t], acc[i].re[t]);
+                        acc[i].im[t] = fma(cf[i], y.im[t], acc[i].im[t]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const int row = row0 + i;
+                if (row >= r1) break;
+                const size_t base = (size_t)row * B + b0;
+                if (kWrite) {
+                    const CV<Real, TPT> x = ldv<Real, TPT, false>(slot(row), tl);
+                    CV<Real, TPT> o;
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) {
+                        o.re[t] = (Real)(sc[t] * (double)acc[i].re[t]);
+                        o.im[t] = (Real)(sc[t] * (double)acc[i].im[t]);
+                        const double xr = x.re[t], xi = x.im[t], ur = acc[i].re[t], ui = acc[i].im[t];
+                        if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
+                        else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+                    }
+                    stv<Real, TPT>(w, base, o);
+                } else {
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t)
+                        ar[t] += (double)acc[i].re[t] * acc[i].re[t] + (double)acc[i].im[t] * acc[i].im[t];
+                }
+            }
+        }
+    }
+    __shared__ double2 red[kMaxTC];
+    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * gridDim.y, red)) {
+        if (threadIdx.x < TC) {
+            const int b = blockIdx.y * TC + threadIdx.x;
+            const double s2 = S.sc[(size_t)j * B + b];
+            const double2 v = red[threadIdx.x];
+            if (kWrite) {
+                S.alpha[2 * ((size_t)j * B + b)] = v.x * s2 * s2;
+                S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s2 * s2;
+            } else {
+                S.nav[b] = sqrt(v.x) * s2;
+            }
+        }
+    }
+}
+
 // r_{j+1} = w - alpha_j q_j - beta_{j-1} q_{j-1};  beta_j = ||r_{j+1}||
 template <typename Real, int TPT>
 __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, int rpc, int j,
@@ -383,27 +559,40 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
         nn[t] = 0.0;
         zero[t] = 0.0;
     }
-    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+    // two rows per trip so six independent loads are in flight per thread
+    for (int row = T.r0 + T.rl; row < T.r1; row += 2 * T.RPC) {
+        const int row2 = row + T.RPC;
+        const bool has2 = row2 < T.r1;
         const size_t base = (size_t)row * B + T.b0;
-        const CV<Real, TPT> u = ldv<Real, TPT, false>(w, base);
-        const CV<Real, TPT> x = ldv<Real, TPT, false>(rj, base);
-        CV<Real, TPT> xm;
-        if (j > 1) xm = ldv<Real, TPT, false>(rjm, base);
-        CV<Real, TPT> o;
-#pragma unroll
-        for (int t = 0; t < TPT; ++t) {
-            const double xr = x.re[t], xi = x.im[t];
-            double rr = (double)u.re[t] - (ajr[t] * xr - aji[t] * xi);
-            double ri = (double)u.im[t] - (ajr[t] * xi + aji[t] * xr);
-            if (j > 1) {
-                rr -= bm[t] * (double)xm.re[t];
-                ri -= bm[t] * (double)xm.im[t];
-            }
-            o.re[t] = (Real)rr;
-            o.im[t] = (Real)ri;
-            nn[t] += (double)o.re[t] * o.re[t] + (double)o.im[t] * o.im[t];
+        const size_t base2 = (size_t)(has2 ? row2 : row) * B + T.b0;
+        CV<Real, TPT> u[2], x[2], xm[2];
+        u[0] = ldv<Real, TPT, false>(w, base);
+        x[0] = ldv<Real, TPT, false>(rj, base);
+        u[1] = ldv<Real, TPT, false>(w, base2);
+        x[1] = ldv<Real, TPT, false>(rj, base2);
+        if (j > 1) {
+            xm[0] = ldv<Real, TPT, false>(rjm, base);
+            xm[1] = ldv<Real, TPT, false>(rjm, base2);
         }
-        stv<Real, TPT>(rjp, base, o);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (h == 1 && !has2) break;
+            CV<Real, TPT> o;
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                const double xr = x[h].re[t], xi = x[h].im[t];
+                double rr = (double)u[h].re[t] - (ajr[t] * xr - aji[t] * xi);
+                double ri = (double)u[h].im[t] - (ajr[t] * xi + aji[t] * xr);
+                if (j > 1) {
+                    rr -= bm[t] * (double)xm[h].re[t];
+                    ri -= bm[t] * (double)xm[h].im[t];
+                }
+                o.re[t] = (Real)rr;
+                o.im[t] = (Real)ri;
+                nn[t] += (double)o.re[t] * o.re[t] + (double)o.im[t] * o.im[t];
+            }
+            stv<Real, TPT>(rjp, h ? base2 : base, o);
+        }
     }
     __shared__ double2 red[kMaxTC];
     if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 1 * gridDim.y, red)) {
@@ -474,7 +663,22 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
         double accr[TPT], acci[TPT];
 #pragma unroll
         for (int t = 0; t < TPT; ++t) { accr[t] = 0.0; acci[t] = 0.0; }
-        for (int j = 1; j <= m; ++j) {
+        // four slabs per trip: four independent loads in flight per thread
+        int j = 1;
+        for (; j + 3 <= m; j += 4) {
+            CV<Real, TPT> x[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x[q] = ldv<Real, TPT, false>(slabs + 2 * slab_stride * (j + q), base);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    const double2 yv = yts[(j + q - 1) * TC + tl + t];
+                    accr[t] += yv.x * x[q].re[t] - yv.y * x[q].im[t];
+                    acci[t] += yv.x * x[q].im[t] + yv.y * x[q].re[t];
+                }
+        }
+        for (; j <= m; ++j) {
             const CV<Real, TPT> x = ldv<Real, TPT, false>(slabs + 2 * slab_stride * j, base);
 #pragma unroll
             for (int t = 0; t < TPT; ++t) {
@@ -670,6 +874,10 @@ static dq_status build_fmt(dq_ctx* c, int R, BlockFmt& f) {
             }
         bptr[k + 1] = (int)bcol.size();
     }
+    int bw = 0;
+    for (int r = 0; r < n; ++r)
+        for (int p = c->rowptr[r]; p < c->rowptr[r + 1]; ++p) bw = std::max(bw, std::abs(c->col[p] - r));
+    bs->bw = bw;
     f.R = R;
     f.nb = nb;
     f.nunion = bcol.size();
@@ -689,15 +897,80 @@ static dq_status build_fmt(dq_ctx* c, int R, BlockFmt& f) {
     return DQ_OK;
 }
 
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// One 2-D tensor map per slab: rows of 2B reals, boxes of SR rows x 2TC reals.
+static dq_status build_tmaps(dq_ctx* c, int tc, int sr) {
+    BatchedState* bs = c->bat;
+    auto enc = tensor_map_encoder();
+    if (!enc) {
+        c->err = "cuTensorMapEncodeTiled unavailable";
+        return DQ_ERR_CUDA;
+    }
+    const int n = c->n, B = bs->B, m = c->cfg.m;
+    const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
+    bs->tmaps.assign(m + 2, CUtensorMap{});
+    for (int j = 0; j <= m + 1; ++j) {
+        void* base = (char*)bs->slabs + (size_t)j * n * B * 2 * rsz;
+        cuuint64_t dims[2] = {(cuuint64_t)(2 * B), (cuuint64_t)n};
+        cuuint64_t strides[1] = {(cuuint64_t)(2 * B * rsz)};
+        cuuint32_t box[2] = {(cuuint32_t)(2 * tc), (cuuint32_t)sr};
+        cuuint32_t estr[2] = {1, 1};
+        CUresult r = enc(&bs->tmaps[j], bs->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            c->err = "cuTensorMapEncodeTiled failed";
+            return DQ_ERR_CUDA;
+        }
+    }
+    return DQ_OK;
+}
+
+template <typename Real, int TPT, int R>
+static cudaError_t win_attr(int bytes) {
+    cudaError_t e = cudaSuccess;
+    e = cudaFuncSetAttribute(k_spmm_win<Real, TPT, R, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spmm_win<Real, TPT, R, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spmm_win<Real, TPT, R, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 bytes);
+    return e;
+}
+
+template <typename Real, int TPT>
+static cudaError_t win_attr_r(int R, int bytes) {
+    switch (R) {
+        case 1: return win_attr<Real, TPT, 1>(bytes);
+        case 2: return win_attr<Real, TPT, 2>(bytes);
+        case 4: return win_attr<Real, TPT, 4>(bytes);
+        default: return win_attr<Real, TPT, 8>(bytes);
+    }
+}
+
+constexpr size_t kWinSmemMax = 200 * 1024;
+
 // Tiling: TC trajectories per chunk, TPT per thread, ~ctas_per_sm CTAs per
-// SM, R rows per SpMM block.
-dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R) {
+// SM, R rows per SpMM block, staged: TMA shared-memory window SpMM.
+dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R, int staged) {
     BatchedState* bs = c->bat;
     const int B = bs->B, n = c->n;
     if (tpt != 1 && tpt != 2) return DQ_ERR_ARG;
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
+    if (staged != 0 && staged != 1) return DQ_ERR_ARG;
     const int ri = r_index(R);
     if (ri < 0) return DQ_ERR_ARG;
     const int chunks = B / tc;
@@ -717,6 +990,30 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R)
         dq_status st = build_fmt(c, R, bs->fmt[ri]);
         if (st) return st;
     }
+    int halo = 0, wmask = 0, rpc_win = 0, gxw = 0;
+    size_t smem = 0;
+    if (staged) {
+        const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
+        const int SR = RPC * R;
+        if (SR > 256 || 2 * tc > 256 || tc * 2 * rsz < 16) return DQ_ERR_ARG;
+        halo = ((bs->bw + SR - 1) / SR) * SR;
+        int W = 1;
+        while (W < 2 * halo + 2 * SR) W <<= 1;
+        smem = (size_t)W * tc * 2 * rsz;
+        if (smem > kWinSmemMax) return DQ_ERR_ARG;
+        wmask = W - 1;
+        const int fit = std::max(1, (int)((228 * 1024) / (smem + 12 * 1024)));
+        gxw = std::max(1, (bs->sms * std::min(ctas_per_sm, fit)) / chunks);
+        rpc_win = (n + gxw - 1) / gxw;
+        rpc_win = ((rpc_win + SR - 1) / SR) * SR;
+        gxw = (n + rpc_win - 1) / rpc_win;
+        if (gxw > kMaxCtasPerChunk || (size_t)gxw * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
+        cudaError_t e = bs->mixed ? (tpt == 2 ? win_attr_r<float, 2>(R, (int)smem) : win_attr_r<float, 1>(R, (int)smem))
+                                  : win_attr_r<double, 1>(R, (int)smem);
+        if (e != cudaSuccess) return DQ_ERR_ARG;
+        dq_status st = build_tmaps(c, tc, SR);
+        if (st) return st;
+    }
     bs->TC = tc;
     bs->TPT = tpt;
     bs->chunks = chunks;
@@ -726,6 +1023,12 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R)
     bs->R = R;
     bs->gxs = gxs;
     bs->bpc = bpc;
+    bs->staged = staged;
+    bs->halo = halo;
+    bs->wmask = wmask;
+    bs->rpc_win = rpc_win;
+    bs->gxw = gxw;
+    bs->win_smem = smem;
     drop_graph(bs);
     return DQ_OK;
 }
@@ -776,7 +1079,7 @@ dq_status batched_alloc(dq_ctx* c) {
     int tc = 16;
     while (tc > tpt && B % tc) tc >>= 1;
     if (B % tc) tc = tpt;
-    dq_status st = batched_set_tiling(c, tc, tpt, 2, 4);
+    dq_status st = batched_set_tiling(c, tc, tpt, 2, 4, 0);
     if (st) {
         c->err = "batched: no valid tiling for n_traj";
         return st;
@@ -808,6 +1111,7 @@ dq_status batched_reset(dq_ctx* c) {
         k_set_psi0_b<float><<<blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, (float*)((char*)bs->slabs + slab));
     else
         k_set_psi0_b<double><<<blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, (double*)((char*)bs->slabs + slab));
+    DQ_CU(cudaMemsetAsync(bs->s.tickets, 0, sizeof(unsigned int) * ((size_t)8 * B + 8), c->stream));
     k_set_norms_b<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, bs->s);
     k_init_obs_b<<<std::max(1, std::min(bs->sms, (n + 255) / 256)), 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops,
                                                                                         bs->s, bs->chunks);
@@ -844,10 +1148,25 @@ template <typename Real, int TPT, bool kBil, bool kWrite>
 static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w) {
     BatchedState* bs = c->bat;
     const BlockFmt& f = bs->fmt[r_index(bs->R)];
-    const dim3 grid(bs->gxs, bs->chunks);
     const int n = c->n, B = bs->B, TC = bs->TC;
     const Real* cf = (const Real*)f.bcoef;
     const Real* d = (const Real*)bs->diag;
+    if (bs->staged) {
+        const dim3 grid(bs->gxw, bs->chunks);
+        const CUtensorMap& tm = bs->tmaps[j];
+#define DQ_WIN_R(RR)                                                                                       \
+    k_spmm_win<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, bs->win_smem, c->stream>>>(                  \
+        n, B, TC, bs->rpc_win, bs->halo, bs->wmask, j, f.bptr, f.bcol, cf, d, w, bs->s, tm)
+        switch (bs->R) {
+            case 1: DQ_WIN_R(1); break;
+            case 2: DQ_WIN_R(2); break;
+            case 4: DQ_WIN_R(4); break;
+            default: DQ_WIN_R(8); break;
+        }
+#undef DQ_WIN_R
+        return;
+    }
+    const dim3 grid(bs->gxs, bs->chunks);
 #define DQ_SPMM_R(RR)                                                                                             \
     k_spmm_blk<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j, f.bptr, \
                                                                                f.bcol, cf, d, rj, w, bs->s)
@@ -979,7 +1298,8 @@ dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
     return check_cuda(c, cudaGetLastError(), "time iteration");
 }
 
-void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R) {
+void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged) {
+    if (staged) *staged = c->bat->staged;
     if (tc) *tc = c->bat->TC;
     if (tpt) *tpt = c->bat->TPT;
     if (cps) *cps = c->bat->ctas_per_sm;

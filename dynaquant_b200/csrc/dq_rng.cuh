@@ -2,7 +2,8 @@
 //
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
 // easy as 1, 2, 3", SC'11) keyed by the 64-bit seed, with counter
-// {site, step, traj, purpose<<24 | substep/2}.  Uniforms become normals by
+// {site, step, traj/2, purpose<<24 | substep}; the two normals of a block
+// belong to the even and the odd trajectory of the pair.  Uniforms become normals by
 // Box-Muller; log, sin and cos are this file's own series (binary range
 // reduction + atanh series for log, octant reduction + Taylor polynomials for
 // sin/cos) evaluated with explicit fma and intrinsics that are never
@@ -98,12 +99,12 @@ __device__ __forceinline__ void own_sincos_2pi(double u, double& S, double& C) {
     }
 }
 
-// Both normals of one Philox block: z[0] (cosine branch, even substep) and
-// z[1] (sine branch, odd substep).
-__device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t purpose, uint32_t traj,
-                                            uint32_t step, uint32_t site, uint32_t pair,
+// Both normals of one Philox block, keyed by the trajectory pair: z0 (cosine
+// branch) belongs to trajectory 2*tpair, z1 (sine branch) to 2*tpair + 1.
+__device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t purpose, uint32_t tpair,
+                                            uint32_t step, uint32_t site, uint32_t sub,
                                             double& z0, double& z1) {
-    uint32_t c[4] = {site, step, traj, (purpose << 24) | pair};
+    uint32_t c[4] = {site, step, tpair, (purpose << 24) | sub};
     philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
     unsigned long long a = ((unsigned long long)c[1] << 32) | c[0];
     unsigned long long b = ((unsigned long long)c[3] << 32) | c[2];
@@ -119,26 +120,42 @@ __device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t purpose, uin
 __device__ __forceinline__ double normal(uint64_t seed, uint32_t purpose, uint32_t traj, uint32_t step,
                                          uint32_t site, uint32_t sub) {
     double z0, z1;
-    normal_pair(seed, purpose, traj, step, site, sub >> 1, z0, z1);
-    return (sub & 1) ? z1 : z0;
+    normal_pair(seed, purpose, traj >> 1, step, site, sub, z0, z1);
+    return (traj & 1) ? z1 : z0;
 }
 
-// One OU (Kubo-Anderson) Euler-Maruyama update of a site's offset over
-// `ns` substeps, in the reference's operation order (gpuSysHelper.cu:112):
+// One Euler-Maruyama substep of the OU (Kubo-Anderson) offset in the
+// reference's operation order (gpuSysHelper.cu:112):
 // cur = cur - cur*invTau*subdt + coeff*xi*sqrt_subdt.
+__device__ __forceinline__ double ou_substep(double cur, double inv_tau, double coeff, double subdt,
+                                             double sqrt_subdt, double xi) {
+    return __dadd_rn(__dsub_rn(cur, __dmul_rn(__dmul_rn(cur, inv_tau), subdt)),
+                     __dmul_rn(__dmul_rn(coeff, xi), sqrt_subdt));
+}
+
+// `ns` OU substeps of one trajectory's offset.
 __device__ __forceinline__ double ou_update(double cur, double inv_tau, double coeff, double subdt,
                                             double sqrt_subdt, int ns, uint64_t seed, uint32_t traj,
                                             uint32_t step, uint32_t site) {
-    for (int s = 0; s < ns; s += 2) {
+    for (int s = 0; s < ns; ++s) {
         double z0, z1;
-        normal_pair(seed, P_OU, traj, step, site, (uint32_t)(s >> 1), z0, z1);
-        cur = __dadd_rn(__dsub_rn(cur, __dmul_rn(__dmul_rn(cur, inv_tau), subdt)),
-                        __dmul_rn(__dmul_rn(coeff, z0), sqrt_subdt));
-        if (s + 1 < ns)
-            cur = __dadd_rn(__dsub_rn(cur, __dmul_rn(__dmul_rn(cur, inv_tau), subdt)),
-                            __dmul_rn(__dmul_rn(coeff, z1), sqrt_subdt));
+        normal_pair(seed, P_OU, traj >> 1, step, site, (uint32_t)s, z0, z1);
+        cur = ou_substep(cur, inv_tau, coeff, subdt, sqrt_subdt, (traj & 1) ? z1 : z0);
     }
     return cur;
+}
+
+// `ns` OU substeps of the offsets of trajectories 2*tpair and 2*tpair + 1,
+// one Philox block and one Box-Muller transform per substep.
+__device__ __forceinline__ void ou_update_pair(double& c0, double& c1, double inv_tau, double coeff, double subdt,
+                                               double sqrt_subdt, int ns, uint64_t seed, uint32_t tpair,
+                                               uint32_t step, uint32_t site) {
+    for (int s = 0; s < ns; ++s) {
+        double z0, z1;
+        normal_pair(seed, P_OU, tpair, step, site, (uint32_t)s, z0, z1);
+        c0 = ou_substep(c0, inv_tau, coeff, subdt, sqrt_subdt, z0);
+        c1 = ou_substep(c1, inv_tau, coeff, subdt, sqrt_subdt, z1);
+    }
 }
 
 }  // namespace dq

@@ -144,10 +144,14 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * thread (8- or 16-byte loads; 1 in FP64), about ctas_per_sm CTAs per SM,
  * each owning a contiguous range of sites, and rows_per_block (1, 2, 4 or 8)
  * rows computed together by the SpMM over the union of their neighbour
- * columns.  Changing it restarts the ensemble at the next dq_run (as
- * dq_reset does). */
-DQ_API dq_status dq_set_tiling(dq_ctx *ctx, int traj_chunk, int vec, int ctas_per_sm, int rows_per_block);
-DQ_API dq_status dq_get_tiling(dq_ctx *ctx, int *traj_chunk, int *vec, int *ctas_per_sm, int *rows_per_block);
+ * columns.  staged = 1 stages the gathered trajectory rows in a shared-memory
+ * window filled by TMA (needs the matrix bandwidth to fit the window; the
+ * call fails otherwise), 0 gathers through L1.  Changing it restarts the
+ * ensemble at the next dq_run (as dq_reset does). */
+DQ_API dq_status dq_set_tiling(dq_ctx *ctx, int traj_chunk, int vec, int ctas_per_sm, int rows_per_block,
+                               int staged);
+DQ_API dq_status dq_get_tiling(dq_ctx *ctx, int *traj_chunk, int *vec, int *ctas_per_sm, int *rows_per_block,
+                               int *staged);
 /* Times one Lanczos iteration (SpMM + axpy) of the current system under
  * every valid tiling, keeps the fastest and resets the ensemble.  best_ms
  * (may be NULL) gets its time per iteration. */

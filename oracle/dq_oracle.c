@@ -140,10 +140,12 @@ void dqo_sincos_2pi(double u, double *s, double *c) {
 
 /* Normal draw keyed by (seed, purpose, traj, step, site, sub).  One Philox
  * block gives two uniforms of 53 bits and Box-Muller gives two normals; the
- * even substep takes the cosine branch, the odd one the sine branch. */
+ * block is keyed by the trajectory PAIR (traj >> 1), the even trajectory
+ * takes the cosine branch and the odd one the sine branch, so both normals
+ * of every block are used. */
 double dqo_normal(uint64_t seed, uint32_t purpose, uint32_t traj, uint32_t step,
                   uint32_t site, uint32_t sub) {
-    uint32_t ctr[4] = {site, step, traj, (purpose << 24) | (sub >> 1)};
+    uint32_t ctr[4] = {site, step, traj >> 1, (purpose << 24) | sub};
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
     uint32_t o[4];
     dqo_philox4x32_10(ctr, key, o);
@@ -154,7 +156,7 @@ double dqo_normal(uint64_t seed, uint32_t purpose, uint32_t traj, uint32_t step,
     double r = sqrt(-2.0 * dqo_log(u1));
     double sn, cs;
     dqo_sincos_2pi(u2, &sn, &cs);
-    return (sub & 1) ? r * sn : r * cs;
+    return (traj & 1) ? r * sn : r * cs;
 }
 
 /* hbar in cm^-1 fs exactly as cppUtility.cpp:19-22 computes it (note the
