@@ -225,7 +225,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     p2 = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=K + 8)
-    p2.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"])
+    p2.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
+                  tiling["staged"], tiling["groups"])
     p2.reset()
     p2.run(K)
     pops = p2.populations()
@@ -283,7 +284,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (Krylov slabs %.1f GB)" % (8.0 * s.n * B * (w["m"] + 2) / 1e9),
                    "parallelism": f"replicas x{world}",
                    "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged",
-                                                    "ms_per_iter")}},
+                                                    "groups", "ms_per_iter")}},
         "e2e": e2e,
         "gpu_launches": int(kernels_per_step * K),
         "roofline": {"bound": "hbm", "kernel": "k_spmm (SpMM + alpha)", "achieved": achieved, "peak": peak,

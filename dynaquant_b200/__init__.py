@@ -120,13 +120,19 @@ class Propagator:
     def run(self, n_steps):
         self._check(self.L.dq_run(self.h, n_steps))
 
-    def set_tiling(self, traj_chunk, vec, ctas_per_sm, rows_per_block=4, staged=0):
-        self._check(self.L.dq_set_tiling(self.h, traj_chunk, vec, ctas_per_sm, rows_per_block, staged))
+    def set_tiling(self, traj_chunk, vec, ctas_per_sm, rows_per_block=4, staged=0, groups=1):
+        self._check(self.L.dq_set_tiling(self.h, traj_chunk, vec, ctas_per_sm, rows_per_block, staged, groups))
 
     def get_tiling(self):
-        a, b, c, d, e = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        self._check(self.L.dq_get_tiling(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(d), C.byref(e)))
-        return a.value, b.value, c.value, d.value, e.value
+        v = [C.c_int() for _ in range(6)]
+        self._check(self.L.dq_get_tiling(self.h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def time_iteration(self, reps=10):
+        """Mean device ms of one Lanczos iteration (SpMM + axpy) under the current tiling."""
+        ms = C.c_double()
+        self._check(self.L.dq_time_iteration(self.h, reps, C.byref(ms)))
+        return ms.value
 
     def autotune_raw(self, reps=5):
         ms = C.c_double()

@@ -27,7 +27,7 @@ EXPORTS = [
     "dq_set_hamiltonian_csr", "dq_set_coupling_classes", "dq_set_noise_params", "dq_set_static_energies",
     "dq_set_initial_state", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
-    "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune",
+    "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
 ]
 
 
@@ -99,9 +99,10 @@ def load(path: str = LIB_PATH):
     L.dq_get_spectrum.argtypes = [vp, C.c_int, dp]
     L.dq_get_noise_state.argtypes = [vp, C.c_int, dp, dp]
     L.dq_profile_step.argtypes = [vp, C.c_int, dp, ip, C.c_int]
-    L.dq_set_tiling.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
-    L.dq_get_tiling.argtypes = [vp, ip, ip, ip, ip, ip]
+    L.dq_set_tiling.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.dq_get_tiling.argtypes = [vp, ip, ip, ip, ip, ip, ip]
     L.dq_autotune.argtypes = [vp, C.c_int, dp]
+    L.dq_time_iteration.argtypes = [vp, C.c_int, dp]
     for name in EXPORTS:
         if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done"):
             getattr(L, name).restype = C.c_int

@@ -71,14 +71,15 @@ def tune(prop, nnz: int, reps: int = 5, use_cache: bool = True) -> dict:
         e = load_cache().get(k)
         if e:
             try:
-                prop.set_tiling(e["traj_chunk"], e["vec"], e["ctas_per_sm"], e["rows_per_block"], e["staged"])
+                prop.set_tiling(e["traj_chunk"], e["vec"], e["ctas_per_sm"], e["rows_per_block"], e["staged"],
+                                e["groups"])
                 prop.reset()
                 return dict(e, cached=True)
             except Exception:
                 pass
     ms = prop.autotune_raw(reps)
-    tc, vec, cps, rpb, staged = prop.get_tiling()
+    tc, vec, cps, rpb, staged, groups = prop.get_tiling()
     entry = {"traj_chunk": tc, "vec": vec, "ctas_per_sm": cps, "rows_per_block": rpb, "staged": staged,
-             "ms_per_iter": ms}
+             "groups": groups, "ms_per_iter": ms}
     store(k, entry)
     return dict(entry, cached=False)

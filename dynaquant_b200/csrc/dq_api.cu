@@ -420,22 +420,22 @@ static dq_status ensure_batched(dq_ctx* c) {
 }
 
 extern "C" dq_status dq_set_tiling(dq_ctx* c, int traj_chunk, int vec, int ctas_per_sm, int rows_per_block,
-                                   int staged) {
+                                   int staged, int groups) {
     if (!c) return DQ_ERR_ARG;
     dq_status st;
     if ((st = ensure_batched(c))) return st;
-    if ((st = batched_set_tiling(c, traj_chunk, vec, ctas_per_sm, rows_per_block, staged)))
+    if ((st = batched_set_tiling(c, traj_chunk, vec, ctas_per_sm, rows_per_block, staged, groups)))
         return fail(c, st, "set_tiling: invalid tiling for this system");
     c->ready = false;
     return DQ_OK;
 }
 
 extern "C" dq_status dq_get_tiling(dq_ctx* c, int* traj_chunk, int* vec, int* ctas_per_sm, int* rows_per_block,
-                                   int* staged) {
+                                   int* staged, int* groups) {
     if (!c) return DQ_ERR_ARG;
     dq_status st;
     if ((st = ensure_batched(c))) return st;
-    batched_get_tiling(c, traj_chunk, vec, ctas_per_sm, rows_per_block, staged);
+    batched_get_tiling(c, traj_chunk, vec, ctas_per_sm, rows_per_block, staged, groups);
     return DQ_OK;
 }
 
@@ -445,22 +445,37 @@ extern "C" dq_status dq_autotune(dq_ctx* c, int reps, double* best_ms) {
     dq_status st;
     if ((st = ensure_batched(c))) return st;
     if ((st = dq_reset(c))) return st;
-    int b_tc = 0, b_vec = 0, b_cps = 0, b_r = 0, b_st = 0;
+    int b_tc = 0, b_vec = 0, b_cps = 0, b_r = 0, b_st = 0, b_g = 1;
     double best = 1e30;
     const int vecs[2] = {2, 1};
-    for (int staged = 0; staged <= 1; ++staged)
-        for (int vi = 0; vi < 2; ++vi)
-            for (int tc = 4; tc <= 64; tc <<= 1)
-                for (int cps = 1; cps <= 8; cps <<= 1)
-                    for (int R = 1; R <= 8; R <<= 1) {
-                        if (batched_set_tiling(c, tc, vecs[vi], cps, R, staged) != DQ_OK) continue;
-                        double ms = 0.0;
-                        if ((st = batched_time_iteration(c, reps, &ms))) return st;
-                        if (ms < best) { best = ms; b_tc = tc; b_vec = vecs[vi]; b_cps = cps; b_r = R; b_st = staged; }
-                    }
+    for (int groups = 1; groups <= 8; groups <<= 1)
+        for (int staged = 0; staged <= 1; ++staged)
+            for (int vi = 0; vi < 2; ++vi)
+                for (int tc = 4; tc <= 64; tc <<= 1)
+                    for (int cps = 1; cps <= 8; cps <<= 1)
+                        for (int R : {1, 2, 3, 4, 8}) {
+                            if (batched_set_tiling(c, tc, vecs[vi], cps, R, staged, groups) != DQ_OK) continue;
+                            double ms = 0.0;
+                            if ((st = batched_time_iteration(c, reps, &ms))) return st;
+                            if (ms < best) {
+                                best = ms; b_tc = tc; b_vec = vecs[vi]; b_cps = cps; b_r = R; b_st = staged;
+                                b_g = groups;
+                            }
+                        }
     if (!b_tc) return fail(c, DQ_ERR_ARG, "autotune: no valid tiling");
-    if ((st = batched_set_tiling(c, b_tc, b_vec, b_cps, b_r, b_st))) return st;
+    if ((st = batched_set_tiling(c, b_tc, b_vec, b_cps, b_r, b_st, b_g))) return st;
     if (best_ms) *best_ms = best;
     c->ready = false;
     return dq_reset(c);
+}
+
+extern "C" dq_status dq_time_iteration(dq_ctx* c, int reps, double* ms) {
+    if (!c || !ms) return DQ_ERR_ARG;
+    if (reps < 1) reps = 5;
+    dq_status st;
+    if ((st = ensure_batched(c))) return st;
+    if ((st = dq_reset(c))) return st;
+    if ((st = batched_time_iteration(c, reps, ms))) return st;
+    c->ready = false;
+    return DQ_OK;
 }

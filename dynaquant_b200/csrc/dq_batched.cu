@@ -30,6 +30,7 @@
 // in device memory.
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -51,7 +52,7 @@ template <> struct VL<float, 2> { using T = float4; };
 template <> struct VL<double, 1> { using T = double2; };
 
 template <typename Real, int TPT>
-struct CV { Real re[TPT], im[TPT]; };
+struct CV { Real v[2 * TPT]; };   // interleaved (re, im) per trajectory
 
 template <typename Real, int TPT, bool kLdg>
 __device__ __forceinline__ CV<Real, TPT> ldv(const Real* base, size_t idx) {
@@ -60,9 +61,9 @@ __device__ __forceinline__ CV<Real, TPT> ldv(const Real* base, size_t idx) {
     T t = kLdg ? __ldg(p) : *p;
     CV<Real, TPT> v;
     if constexpr (TPT == 2) {
-        v.re[0] = t.x; v.im[0] = t.y; v.re[1] = t.z; v.im[1] = t.w;
+        v.v[0] = t.x; v.v[1] = t.y; v.v[2] = t.z; v.v[3] = t.w;
     } else {
-        v.re[0] = t.x; v.im[0] = t.y;
+        v.v[0] = t.x; v.v[1] = t.y;
     }
     return v;
 }
@@ -72,11 +73,32 @@ __device__ __forceinline__ void stv(Real* base, size_t idx, const CV<Real, TPT>&
     using T = typename VL<Real, TPT>::T;
     T t;
     if constexpr (TPT == 2) {
-        t.x = v.re[0]; t.y = v.im[0]; t.z = v.re[1]; t.w = v.im[1];
+        t.x = v.v[0]; t.y = v.v[1]; t.z = v.v[2]; t.w = v.v[3];
     } else {
-        t.x = v.re[0]; t.y = v.im[0];
+        t.x = v.v[0]; t.y = v.v[1];
     }
     *reinterpret_cast<T*>(base + 2 * idx) = t;
+}
+
+// acc += c * y for TPT complex values; packed FP32x2 FMA on sm_100 for the
+// complex64 path (one instruction per complex element)
+template <typename Real, int TPT>
+__device__ __forceinline__ void cfma(CV<Real, TPT>& acc, Real c, const CV<Real, TPT>& y) {
+    if constexpr (sizeof(Real) == 4) {
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+            const float2 r = __ffma2_rn(make_float2(c, c), make_float2(y.v[2 * t], y.v[2 * t + 1]),
+                                        make_float2(acc.v[2 * t], acc.v[2 * t + 1]));
+            acc.v[2 * t] = r.x;
+            acc.v[2 * t + 1] = r.y;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+            acc.v[2 * t] = fma(c, y.v[2 * t], acc.v[2 * t]);
+            acc.v[2 * t + 1] = fma(c, y.v[2 * t + 1], acc.v[2 * t + 1]);
+        }
+    }
 }
 
 struct BatchedScalars {
@@ -96,13 +118,14 @@ struct BatchedScalars {
 // Thread -> (row lane, trajectory lane) map and the CTA's row range.
 template <int TPT>
 struct Tile {
-    int tr, rl, RPC, b0, r0, r1;
-    __device__ __forceinline__ Tile(int TC, int rows_per_cta, int n) {
+    int tr, rl, RPC, b0, r0, r1, chunk;
+    __device__ __forceinline__ Tile(int TC, int rows_per_cta, int n, int cy0 = 0) {
         const int TPR = TC / TPT;
         tr = threadIdx.x % TPR;
         rl = threadIdx.x / TPR;
         RPC = blockDim.x / TPR;
-        b0 = blockIdx.y * TC + tr * TPT;
+        chunk = blockIdx.y + cy0;
+        b0 = chunk * TC + tr * TPT;
         r0 = blockIdx.x * rows_per_cta;
         r1 = min(n, r0 + rows_per_cta);
     }
@@ -117,6 +140,7 @@ struct Tile {
 struct BlockFmt {
     int R = 0, nb = 0;
     size_t nunion = 0;
+    bool packed = false;     // 16-byte records {col, c0, c1, c2}, blocks padded to 4 entries
     int* bptr = nullptr;     // nb + 1
     int* bcol = nullptr;     // nunion
     void* bcoef = nullptr;   // nunion x R (Real)
@@ -126,10 +150,11 @@ struct dq::BatchedState {
     int B = 0, TC = 0, TPT = 2, chunks = 0, gx = 0, rpc = 0, ctas_per_sm = 2;
     int R = 4, gxs = 0, bpc = 0;          // SpMM: rows per block, CTAs per chunk, blocks per CTA
     int staged = 0;                       // 1: TMA-staged shared-memory window SpMM
+    int groups = 1;                       // trajectory groups iterated one after another
     int halo = 0, wmask = 0, rpc_win = 0, gxw = 0, bw = 0;   // window geometry, matrix bandwidth
     size_t win_smem = 0;
     std::vector<CUtensorMap> tmaps;       // one per slab (window variant)
-    ::BlockFmt fmt[4];                    // R = 1, 2, 4, 8 (built on demand)
+    ::BlockFmt fmt[5];                    // R = 1, 2, 3, 4, 8 (built on demand)
     int sms = 148;
     bool mixed = true;
     void* slabs = nullptr;      // (m+2) slabs (slab 0 = w)
@@ -155,7 +180,7 @@ namespace dq {
 // chunk's totals in red_out[0..TC).
 template <int TPT>
 __device__ __forceinline__ bool chunk_reduce(const double (&ar)[TPT], const double (&ai)[TPT], int TC,
-                                             double* partial, unsigned int* ticket, double2* red_out) {
+                                             double* partial, unsigned int* ticket, double2* red_out, int chunk) {
     __shared__ double2 sm[kBThreads * 2];
     const int TPR = TC / TPT;
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
@@ -163,7 +188,6 @@ __device__ __forceinline__ bool chunk_reduce(const double (&ar)[TPT], const doub
 #pragma unroll
     for (int t = 0; t < TPT; ++t) sm[rl * TC + tr * TPT + t] = make_double2(ar[t], ai[t]);
     __syncthreads();
-    const int chunk = blockIdx.y;
     double* mypart = partial + ((size_t)chunk * gridDim.x + blockIdx.x) * TC * 2;
     if (threadIdx.x < TC) {
         double sr = 0.0, si = 0.0;
@@ -177,14 +201,29 @@ __device__ __forceinline__ bool chunk_reduce(const double (&ar)[TPT], const doub
     }
     bool last = last_block_ticket(ticket + chunk, gridDim.x);
     if (last) {
+        // all threads of the last block: `per` threads per trajectory each sum
+        // a strided share of the block partials, then the shares are added in
+        // a fixed order (deterministic, no serial walk over every partial)
+        const int per = blockDim.x / TC;
+        const int tl = threadIdx.x % TC, part = threadIdx.x / TC;
+        const double* base = partial + (size_t)chunk * gridDim.x * TC * 2;
+        double sr = 0.0, si = 0.0;
+#pragma unroll 4
+        for (unsigned int g = part; g < gridDim.x; g += per) {
+            const double2 v = __ldcg(reinterpret_cast<const double2*>(base + ((size_t)g * TC + tl) * 2));
+            sr += v.x;
+            si += v.y;
+        }
+        __syncthreads();   // sm is reused for the shares
+        sm[part * TC + tl] = make_double2(sr, si);
+        __syncthreads();
         if (threadIdx.x < TC) {
-            double sr = 0.0, si = 0.0;
-            const double* base = partial + (size_t)chunk * gridDim.x * TC * 2;
-            for (unsigned int g = 0; g < gridDim.x; ++g) {
-                sr += __ldcg(&base[((size_t)g * TC + threadIdx.x) * 2]);
-                si += __ldcg(&base[((size_t)g * TC + threadIdx.x) * 2 + 1]);
+            double ar2 = 0.0, ai2 = 0.0;
+            for (int q = 0; q < per; ++q) {
+                ar2 += sm[q * TC + threadIdx.x].x;
+                ai2 += sm[q * TC + threadIdx.x].y;
             }
-            red_out[threadIdx.x] = make_double2(sr, si);
+            red_out[threadIdx.x] = make_double2(ar2, ai2);
         }
         if (threadIdx.x == 0) ticket[chunk] = 0;
         __syncthreads();
@@ -301,6 +340,164 @@ __device__ __forceinline__ void ld_coef(const Real* __restrict__ base, int e, Re
     }
 }
 
+// acc[i] += sum_p coef[p][i] * gather(col[p]) over the union entries
+// [pb, pe) of one row block.  The columns and coefficients of the next G
+// entries are loaded while the current G gather and accumulate, so the
+// index loads leave the gather's dependency chain.
+template <typename Real, int TPT, int R, int G, typename Gather>
+__device__ __forceinline__ void union_loop(int pb, int pe, const int* __restrict__ bcol,
+                                           const Real* __restrict__ bcoef, CV<Real, TPT> (&acc)[R],
+                                           Gather gather) {
+    if (pb >= pe) return;
+    int cc[G];
+    Real cf[G][R];
+#pragma unroll
+    for (int q = 0; q < G; ++q) {
+        const int p = min(pb + q, pe - 1);
+        cc[q] = __ldg(bcol + p);
+        ld_coef<Real, R>(bcoef, p, cf[q]);
+    }
+    for (int p0 = pb; p0 < pe; p0 += G) {
+        const bool more = p0 + G < pe;
+        int nc[G];
+        Real nf[G][R];
+        if (more) {
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                const int p = min(p0 + G + q, pe - 1);
+                nc[q] = __ldg(bcol + p);
+                ld_coef<Real, R>(bcoef, p, nf[q]);
+            }
+        }
+        CV<Real, TPT> y[G];
+#pragma unroll
+        for (int q = 0; q < G; ++q) y[q] = gather(cc[q]);
+#pragma unroll
+        for (int q = 0; q < G; ++q) {
+            if (p0 + q < pe) {
+#pragma unroll
+                for (int i = 0; i < R; ++i) cfma<Real, TPT>(acc[i], cf[q][i], y[q]);
+            }
+        }
+        if (more) {
+#pragma unroll
+            for (int q = 0; q < G; ++q) {
+                cc[q] = nc[q];
+#pragma unroll
+                for (int i = 0; i < R; ++i) cf[q][i] = nf[q][i];
+            }
+        }
+    }
+}
+
+template <int R> struct UnionGroup { static constexpr int G = R >= 4 ? 2 : 4; };
+
+// Packed form (complex64, R <= 3): one 16-byte record {col, c0, c1, c2} per
+// union entry, the block's record count a multiple of 4.  Two groups of four
+// records alternate so the next group loads while the current one gathers.
+template <int TPT, int R, typename Gather>
+__device__ __forceinline__ void union_loop_packed(int pb, int pe, const float4* __restrict__ rec,
+                                                  CV<float, TPT> (&acc)[R], Gather gather) {
+    if (pb >= pe) return;
+    float4 A[4], Bq[4];
+    auto process = [&](const float4 (&E)[4]) {
+        CV<float, TPT> y[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) y[q] = gather(__float_as_int(E[q].x));
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            cfma<float, TPT>(acc[0], E[q].y, y[q]);
+            if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], E[q].z, y[q]);
+            if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], E[q].w, y[q]);
+        }
+    };
+#pragma unroll
+    for (int q = 0; q < 4; ++q) A[q] = __ldg(rec + pb + q);
+    for (int p0 = pb;; p0 += 8) {
+        const bool hasB = p0 + 4 < pe;
+        if (hasB) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) Bq[q] = __ldg(rec + p0 + 4 + q);
+        }
+        process(A);
+        if (!hasB) break;
+        const bool hasA = p0 + 8 < pe;
+        if (hasA) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) A[q] = __ldg(rec + p0 + 8 + q);
+        }
+        process(Bq);
+        if (!hasA) break;
+    }
+}
+
+// Header of one row block with its first four packed records, fetched one
+// block ahead so the dependent bptr -> record loads leave the critical path.
+struct BlkPre {
+    int pb, pe;
+    float4 A[4];
+};
+
+__device__ __forceinline__ void blk_prefetch(BlkPre& P, bool valid, int k, const int* __restrict__ bptr,
+                                             const float4* __restrict__ rec) {
+    if (valid) {
+        P.pb = __ldg(bptr + k);
+        P.pe = __ldg(bptr + k + 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) P.A[q] = __ldg(rec + P.pb + q);
+    } else {
+        P.pb = P.pe = 0;
+    }
+}
+
+// union_loop_packed with the first group already in registers (P.A)
+template <int TPT, int R, typename Gather>
+__device__ __forceinline__ void union_loop_pre(const BlkPre& P, const float4* __restrict__ rec,
+                                               CV<float, TPT> (&acc)[R], Gather gather) {
+    const int pb = P.pb, pe = P.pe;
+    if (pb >= pe) return;
+    float4 A[4], Bq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) A[q] = P.A[q];
+    auto process = [&](const float4 (&E)[4]) {
+        CV<float, TPT> y[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) y[q] = gather(__float_as_int(E[q].x));
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            cfma<float, TPT>(acc[0], E[q].y, y[q]);
+            if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], E[q].z, y[q]);
+            if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], E[q].w, y[q]);
+        }
+    };
+    for (int p0 = pb;; p0 += 8) {
+        const bool hasB = p0 + 4 < pe;
+        if (hasB) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) Bq[q] = __ldg(rec + p0 + 4 + q);
+        }
+        process(A);
+        if (!hasB) break;
+        const bool hasA = p0 + 8 < pe;
+        if (hasA) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) A[q] = __ldg(rec + p0 + 8 + q);
+        }
+        process(Bq);
+        if (!hasA) break;
+    }
+}
+
+template <typename Real, int TPT, int R, typename Gather>
+__device__ __forceinline__ void union_any(int pb, int pe, const int* __restrict__ bcol,
+                                          const Real* __restrict__ bcoef, CV<Real, TPT> (&acc)[R], Gather gather) {
+    if constexpr (sizeof(Real) == 4 && R <= 3) {
+        union_loop_packed<TPT, R>(pb, pe, reinterpret_cast<const float4*>(bcoef), acc, gather);
+    } else {
+        union_loop<Real, TPT, R, UnionGroup<R>::G>(pb, pe, bcol, bcoef, acc, gather);
+    }
+}
+
 // Row-blocked SpMM: w = H q_j for all trajectories of the chunk, R rows per
 // block.  kWrite: also alpha_j[b] = <q_j, w>_b; !kWrite: ||H q_j||_b only.
 template <typename Real, int TPT, int R, bool kBilinear, bool kWrite>
@@ -308,11 +505,12 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_blk(int n, int B, int TC, in
                                                        const int* __restrict__ bptr, const int* __restrict__ bcol,
                                                        const Real* __restrict__ bcoef, const Real* __restrict__ d,
                                                        const Real* __restrict__ rj, Real* __restrict__ w,
-                                                       BatchedScalars S) {
+                                                       BatchedScalars S, int cy0, int nch) {
     const int TPR = TC / TPT;
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int RPC = blockDim.x / TPR;
-    const int b0 = blockIdx.y * TC + tr * TPT;
+    const int chunk = blockIdx.y + cy0;
+    const int b0 = chunk * TC + tr * TPT;
     const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
     double sc[TPT], ar[TPT], ai[TPT];
 #pragma unroll
@@ -321,55 +519,56 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_blk(int n, int B, int TC, in
         ar[t] = 0.0;
         ai[t] = 0.0;
     }
+    constexpr bool kPk = sizeof(Real) == 4 && R <= 3;
+    const float4* rec = reinterpret_cast<const float4*>(bcoef);
+    BlkPre P;
+    if constexpr (kPk) blk_prefetch(P, k0 + rl < k1, k0 + rl, bptr, rec);
     for (int k = k0 + rl; k < k1; k += RPC) {
         const int row0 = k * R;
-        CV<Real, TPT> acc[R];
+        BlkPre cur;
+        if constexpr (kPk) {
+            cur = P;
+            blk_prefetch(P, k + RPC < k1, k + RPC, bptr, rec);
+        }
+        // the block's own rows and diagonal are loaded first and used only
+        // after the union loop, so their latency hides under the gathers
+        CV<Real, TPT> acc[R], xo[R];
+        Real dd[R][TPT];
 #pragma unroll
         for (int i = 0; i < R; ++i) {
-            const int row = row0 + i;
-            if (row < n) {
-                const size_t base = (size_t)row * B + b0;
-                const CV<Real, TPT> x = ldv<Real, TPT, true>(rj, base);
+            const int row = min(row0 + i, n - 1);
+            const size_t base = (size_t)row * B + b0;
+            xo[i] = ldv<Real, TPT, true>(rj, base);
 #pragma unroll
-                for (int t = 0; t < TPT; ++t) {
-                    const Real dd = __ldg(d + base + t);
-                    acc[i].re[t] = dd * x.re[t];
-                    acc[i].im[t] = dd * x.im[t];
-                }
-            } else {
-#pragma unroll
-                for (int t = 0; t < TPT; ++t) { acc[i].re[t] = 0; acc[i].im[t] = 0; }
+            for (int t = 0; t < TPT; ++t) {
+                dd[i][t] = row0 + i < n ? __ldg(d + base + t) : Real(0);
+                acc[i].v[2 * t] = 0;
+                acc[i].v[2 * t + 1] = 0;
             }
         }
-        const int pe = __ldg(bptr + k + 1);
-#pragma unroll 4
-        for (int p = __ldg(bptr + k); p < pe; ++p) {
-            const int c = __ldg(bcol + p);
-            Real cf[R];
-            ld_coef<Real, R>(bcoef, p, cf);
-            const CV<Real, TPT> y = ldv<Real, TPT, true>(rj, (size_t)c * B + b0);
+        auto gather = [&](int c) { return ldv<Real, TPT, true>(rj, (size_t)c * B + b0); };
+        if constexpr (kPk) union_loop_pre<TPT, R>(cur, rec, acc, gather);
+        else union_any<Real, TPT, R>(__ldg(bptr + k), __ldg(bptr + k + 1), bcol, bcoef, acc, gather);
 #pragma unroll
-            for (int i = 0; i < R; ++i) {
+        for (int i = 0; i < R; ++i)
 #pragma unroll
-                for (int t = 0; t < TPT; ++t) {
-                    acc[i].re[t] = fma(cf[i], y.re[t], acc[i].re[t]);
-                    acc[i].im[t] = fma(cf[i], y.im[t], acc[i].im[t]);
-                }
+            for (int t = 0; t < TPT; ++t) {
+                acc[i].v[2 * t] = fma(dd[i][t], xo[i].v[2 * t], acc[i].v[2 * t]);
+                acc[i].v[2 * t + 1] = fma(dd[i][t], xo[i].v[2 * t + 1], acc[i].v[2 * t + 1]);
             }
-        }
 #pragma unroll
         for (int i = 0; i < R; ++i) {
             const int row = row0 + i;
             if (row >= n) break;
             const size_t base = (size_t)row * B + b0;
             if (kWrite) {
-                const CV<Real, TPT> x = ldv<Real, TPT, true>(rj, base);
+                const CV<Real, TPT>& x = xo[i];
                 CV<Real, TPT> o;
 #pragma unroll
                 for (int t = 0; t < TPT; ++t) {
-                    o.re[t] = (Real)(sc[t] * (double)acc[i].re[t]);
-                    o.im[t] = (Real)(sc[t] * (double)acc[i].im[t]);
-                    const double xr = x.re[t], xi = x.im[t], ur = acc[i].re[t], ui = acc[i].im[t];
+                    o.v[2 * t] = (Real)(sc[t] * (double)acc[i].v[2 * t]);
+                    o.v[2 * t + 1] = (Real)(sc[t] * (double)acc[i].v[2 * t + 1]);
+                    const double xr = x.v[2 * t], xi = x.v[2 * t + 1], ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
                     if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
                     else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
                 }
@@ -377,14 +576,14 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_blk(int n, int B, int TC, in
             } else {
 #pragma unroll
                 for (int t = 0; t < TPT; ++t)
-                    ar[t] += (double)acc[i].re[t] * acc[i].re[t] + (double)acc[i].im[t] * acc[i].im[t];
+                    ar[t] += (double)acc[i].v[2 * t] * acc[i].v[2 * t] + (double)acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
             }
         }
     }
     __shared__ double2 red[kMaxTC];
-    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * gridDim.y, red)) {
+    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk)) {
         if (threadIdx.x < TC) {
-            const int b = blockIdx.y * TC + threadIdx.x;
+            const int b = chunk * TC + threadIdx.x;
             const double s = S.sc[(size_t)j * B + b];
             const double2 v = red[threadIdx.x];
             if (kWrite) {
@@ -409,7 +608,8 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
                                                        int j, const int* __restrict__ bptr,
                                                        const int* __restrict__ bcol, const Real* __restrict__ bcoef,
                                                        const Real* __restrict__ d, Real* __restrict__ w,
-                                                       BatchedScalars S, const __grid_constant__ CUtensorMap tmap) {
+                                                       BatchedScalars S, int cy0, int nch,
+                                                       const __grid_constant__ CUtensorMap tmap) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     Real* win = reinterpret_cast<Real*>(smem_raw);   // [W][TC] complex
     __shared__ __align__(8) uint64_t bars[2];
@@ -418,11 +618,12 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
     const int BPS = blockDim.x / TPR;   // row blocks per step
     const int SR = BPS * R;             // rows per step
     const int tl = tr * TPT;
-    const int b0 = blockIdx.y * TC + tl;
+    const int chunk = blockIdx.y + cy0;
+    const int b0 = chunk * TC + tl;
     const int r0 = blockIdx.x * rows_per_cta;
     const int r1 = min(n, r0 + rows_per_cta);
     const int nsteps = r1 > r0 ? (r1 - r0 + SR - 1) / SR : 0;
-    const int xc = blockIdx.y * TC * 2;
+    const int xc = chunk * TC * 2;
     const uint32_t box_bytes = (uint32_t)(SR * TC * 2 * sizeof(Real));
     auto slot = [&](int row) { return win + (size_t)(row & wmask) * TC * 2; };
     if (threadIdx.x == 0) {
@@ -447,8 +648,18 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
         ai[t] = 0.0;
     }
     int issued = 0;   // highest step whose load was issued
+    constexpr bool kPk = sizeof(Real) == 4 && R <= 3;
+    const float4* rec = reinterpret_cast<const float4*>(bcoef);
+    BlkPre P;
+    if constexpr (kPk) blk_prefetch(P, r0 + rl * R < r1, r0 / R + rl, bptr, rec);
     for (int s = 0; s < nsteps; ++s) {
         const int a = r0 + s * SR;
+        BlkPre cur;
+        if constexpr (kPk) {
+            // this thread's block of the next step: rows a + SR + rl R
+            cur = P;
+            blk_prefetch(P, a + SR + rl * R < r1, (a + SR) / R + rl, bptr, rec);
+        }
         __syncthreads();   // step s-1 done: the rows the next load overwrites are free
         if (threadIdx.x == 0 && s + 1 < nsteps) {
             const int y = a + SR + halo;
@@ -467,38 +678,30 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
         const int k = a / R + rl;
         const int row0 = k * R;
         if (row0 < r1) {
+            // diagonal loads issued first, applied after the union loop
             CV<Real, TPT> acc[R];
+            Real dd[R][TPT];
 #pragma unroll
             for (int i = 0; i < R; ++i) {
                 const int row = row0 + i;
-                const CV<Real, TPT> x = ldv<Real, TPT, false>(slot(row), tl);
-                if (row < n) {
-                    const size_t base = (size_t)row * B + b0;
+                const size_t base = (size_t)min(row, n - 1) * B + b0;
 #pragma unroll
-                    for (int t = 0; t < TPT; ++t) {
-                        const Real dd = __ldg(d + base + t);
-                        acc[i].re[t] = dd * x.re[t];
-                        acc[i].im[t] = dd * x.im[t];
-                    }
-                } else {
-#pragma unroll
-                    for (int t = 0; t < TPT; ++t) { acc[i].re[t] = 0; acc[i].im[t] = 0; }
+                for (int t = 0; t < TPT; ++t) {
+                    dd[i][t] = row < n ? __ldg(d + base + t) : Real(0);
+                    acc[i].v[2 * t] = 0;
+                    acc[i].v[2 * t + 1] = 0;
                 }
             }
-            const int pe = __ldg(bptr + k + 1);
-#pragma unroll 4
-            for (int p = __ldg(bptr + k); p < pe; ++p) {
-                const int c = __ldg(bcol + p);
-                Real cf[R];
-                ld_coef<Real, R>(bcoef, p, cf);
-                const CV<Real, TPT> y = ldv<Real, TPT, false>(slot(c), tl);
+            auto gather = [&](int c) { return ldv<Real, TPT, false>(slot(c), tl); };
+            if constexpr (kPk) union_loop_pre<TPT, R>(cur, rec, acc, gather);
+            else union_any<Real, TPT, R>(__ldg(bptr + k), __ldg(bptr + k + 1), bcol, bcoef, acc, gather);
 #pragma unroll
-                for (int i = 0; i < R; ++i) {
+            for (int i = 0; i < R; ++i) {
+                const CV<Real, TPT> x = ldv<Real, TPT, false>(slot(row0 + i), tl);
 #pragma unroll
-                    for (int t = 0; t < TPT; ++t) {
-                        acc[i].re[t] = fma(cf[i], y.re[t], acc[i].re[t]);
-                        acc[i].im[t] = fma(cf[i], y.im[t], acc[i].im[t]);
-                    }
+                for (int t = 0; t < TPT; ++t) {
+                    acc[i].v[2 * t] = fma(dd[i][t], x.v[2 * t], acc[i].v[2 * t]);
+                    acc[i].v[2 * t + 1] = fma(dd[i][t], x.v[2 * t + 1], acc[i].v[2 * t + 1]);
                 }
             }
 #pragma unroll
@@ -511,9 +714,9 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
                     CV<Real, TPT> o;
 #pragma unroll
                     for (int t = 0; t < TPT; ++t) {
-                        o.re[t] = (Real)(sc[t] * (double)acc[i].re[t]);
-                        o.im[t] = (Real)(sc[t] * (double)acc[i].im[t]);
-                        const double xr = x.re[t], xi = x.im[t], ur = acc[i].re[t], ui = acc[i].im[t];
+                        o.v[2 * t] = (Real)(sc[t] * (double)acc[i].v[2 * t]);
+                        o.v[2 * t + 1] = (Real)(sc[t] * (double)acc[i].v[2 * t + 1]);
+                        const double xr = x.v[2 * t], xi = x.v[2 * t + 1], ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
                         if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
                         else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
                     }
@@ -521,15 +724,15 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
                 } else {
 #pragma unroll
                     for (int t = 0; t < TPT; ++t)
-                        ar[t] += (double)acc[i].re[t] * acc[i].re[t] + (double)acc[i].im[t] * acc[i].im[t];
+                        ar[t] += (double)acc[i].v[2 * t] * acc[i].v[2 * t] + (double)acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
                 }
             }
         }
     }
     __shared__ double2 red[kMaxTC];
-    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * gridDim.y, red)) {
+    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk)) {
         if (threadIdx.x < TC) {
-            const int b = blockIdx.y * TC + threadIdx.x;
+            const int b = chunk * TC + threadIdx.x;
             const double s2 = S.sc[(size_t)j * B + b];
             const double2 v = red[threadIdx.x];
             if (kWrite) {
@@ -547,8 +750,8 @@ template <typename Real, int TPT>
 __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, int rpc, int j,
                                                         const Real* __restrict__ w, const Real* __restrict__ rj,
                                                         const Real* __restrict__ rjm, Real* __restrict__ rjp,
-                                                        BatchedScalars S) {
-    const Tile<TPT> T(TC, rpc, n);
+                                                        BatchedScalars S, int cy0, int nch) {
+    const Tile<TPT> T(TC, rpc, n, cy0);
     double ajr[TPT], aji[TPT], bm[TPT], nn[TPT], zero[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) {
@@ -580,24 +783,24 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
             CV<Real, TPT> o;
 #pragma unroll
             for (int t = 0; t < TPT; ++t) {
-                const double xr = x[h].re[t], xi = x[h].im[t];
-                double rr = (double)u[h].re[t] - (ajr[t] * xr - aji[t] * xi);
-                double ri = (double)u[h].im[t] - (ajr[t] * xi + aji[t] * xr);
+                const double xr = x[h].v[2 * t], xi = x[h].v[2 * t + 1];
+                double rr = (double)u[h].v[2 * t] - (ajr[t] * xr - aji[t] * xi);
+                double ri = (double)u[h].v[2 * t + 1] - (ajr[t] * xi + aji[t] * xr);
                 if (j > 1) {
-                    rr -= bm[t] * (double)xm[h].re[t];
-                    ri -= bm[t] * (double)xm[h].im[t];
+                    rr -= bm[t] * (double)xm[h].v[2 * t];
+                    ri -= bm[t] * (double)xm[h].v[2 * t + 1];
                 }
-                o.re[t] = (Real)rr;
-                o.im[t] = (Real)ri;
-                nn[t] += (double)o.re[t] * o.re[t] + (double)o.im[t] * o.im[t];
+                o.v[2 * t] = (Real)rr;
+                o.v[2 * t + 1] = (Real)ri;
+                nn[t] += (double)o.v[2 * t] * o.v[2 * t] + (double)o.v[2 * t + 1] * o.v[2 * t + 1];
             }
             stv<Real, TPT>(rjp, h ? base2 : base, o);
         }
     }
     __shared__ double2 red[kMaxTC];
-    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 1 * gridDim.y, red)) {
+    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 1 * nch, red, T.chunk)) {
         if (threadIdx.x < TC) {
-            const int b = blockIdx.y * TC + threadIdx.x;
+            const int b = T.chunk * TC + threadIdx.x;
             double bt = sqrt(red[threadIdx.x].x);
             if (!isfinite(bt)) atomicCAS(S.status, 0, DQ_ERR_NAN);
             // lucky breakdown: invariant Krylov space, continue with q_{j+1} = 0
@@ -674,8 +877,8 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
 #pragma unroll
                 for (int t = 0; t < TPT; ++t) {
                     const double2 yv = yts[(j + q - 1) * TC + tl + t];
-                    accr[t] += yv.x * x[q].re[t] - yv.y * x[q].im[t];
-                    acci[t] += yv.x * x[q].im[t] + yv.y * x[q].re[t];
+                    accr[t] += yv.x * x[q].v[2 * t] - yv.y * x[q].v[2 * t + 1];
+                    acci[t] += yv.x * x[q].v[2 * t + 1] + yv.y * x[q].v[2 * t];
                 }
         }
         for (; j <= m; ++j) {
@@ -683,17 +886,17 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
 #pragma unroll
             for (int t = 0; t < TPT; ++t) {
                 const double2 yv = yts[(j - 1) * TC + tl + t];
-                accr[t] += yv.x * x.re[t] - yv.y * x.im[t];
-                acci[t] += yv.x * x.im[t] + yv.y * x.re[t];
+                accr[t] += yv.x * x.v[2 * t] - yv.y * x.v[2 * t + 1];
+                acci[t] += yv.x * x.v[2 * t + 1] + yv.y * x.v[2 * t];
             }
         }
         CV<Real, TPT> o;
         const cd p0 = psi0[row];
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
-            o.re[t] = (Real)accr[t];
-            o.im[t] = (Real)acci[t];
-            const double vr = o.re[t], vi = o.im[t];
+            o.v[2 * t] = (Real)accr[t];
+            o.v[2 * t + 1] = (Real)acci[t];
+            const double vr = o.v[2 * t], vi = o.v[2 * t + 1];
             nn[t] += vr * vr + vi * vi;
             cr[t] += p0.x * vr + p0.y * vi;   // conj(psi0) * psi
             ci[t] += p0.x * vi - p0.y * vr;
@@ -704,7 +907,7 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
     double zero[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) zero[t] = 0.0;
-    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 3 * gridDim.y, red)) {
+    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 3 * gridDim.y, red, T.chunk)) {
         if (threadIdx.x < TC) {
             const int b = blockIdx.y * TC + threadIdx.x;
             const double n2 = red[threadIdx.x].x;
@@ -718,7 +921,7 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
     // ticket runs after every block of the chunk passed the first one, so the
     // chunk's norms are published by then
     double* part2 = S.partial + (size_t)gridDim.y * gridDim.x * TC * 2;
-    if (chunk_reduce<TPT>(cr, ci, TC, part2, S.tickets + 4 * gridDim.y, red)) {
+    if (chunk_reduce<TPT>(cr, ci, TC, part2, S.tickets + 4 * gridDim.y, red, T.chunk)) {
         if (threadIdx.x == 0) {
             double sr = 0.0, si = 0.0;
             for (int t = 0; t < TC; ++t) {
@@ -835,7 +1038,7 @@ static void drop_graph(BatchedState* bs) {
     bs->graph = nullptr;
 }
 
-static int r_index(int R) { return R == 1 ? 0 : R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : -1; }
+static int r_index(int R) { return R == 1 ? 0 : R == 2 ? 1 : R == 3 ? 2 : R == 4 ? 3 : R == 8 ? 4 : -1; }
 
 static void free_fmt(BlockFmt& f) {
     cudaFree(f.bptr); cudaFree(f.bcol); cudaFree(f.bcoef);
@@ -846,6 +1049,12 @@ void batched_invalidate_blocks(dq_ctx* c) {
     if (!c->bat) return;
     for (auto& f : c->bat->fmt) free_fmt(f);
     drop_graph(c->bat);
+}
+
+static inline float __int_as_float_host(int v) {
+    float f;
+    std::memcpy(&f, &v, sizeof f);
+    return f;
 }
 
 // Builds the row-blocked column-union form of the (scaled) off-diagonal CSR.
@@ -880,6 +1089,40 @@ static dq_status build_fmt(dq_ctx* c, int R, BlockFmt& f) {
     bs->bw = bw;
     f.R = R;
     f.nb = nb;
+    if (bs->mixed && R <= 3) {
+        // 16-byte records {col, c0, c1, c2}; every block padded to a multiple of
+        // 4 records with zero coefficients on its own first row, so the kernel
+        // loop needs neither clamps nor guards
+        std::vector<float4> rec;
+        std::vector<int> pptr(nb + 1, 0);
+        for (int k = 0; k < nb; ++k) {
+            const int u0 = bptr[k], u1 = bptr[k + 1];
+            for (int u = u0; u < u1; ++u) {
+                float4 r;
+                r.x = __int_as_float_host(bcol[u]);
+                r.y = (float)coef[(size_t)u * R];
+                r.z = R > 1 ? (float)coef[(size_t)u * R + 1] : 0.f;
+                r.w = R > 2 ? (float)coef[(size_t)u * R + 2] : 0.f;
+                rec.push_back(r);
+            }
+            while ((rec.size() - (size_t)pptr[k]) % 4) {
+                float4 r;
+                r.x = __int_as_float_host(k * R);
+                r.y = r.z = r.w = 0.f;
+                rec.push_back(r);
+            }
+            pptr[k + 1] = (int)rec.size();
+        }
+        f.packed = true;
+        f.nunion = rec.size();
+        DQ_CU(cudaMalloc(&f.bptr, sizeof(int) * (nb + 1)));
+        DQ_CU(cudaMemcpy(f.bptr, pptr.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice));
+        DQ_CU(cudaMalloc(&f.bcoef, sizeof(float4) * std::max<size_t>(rec.size(), 1)));
+        if (!rec.empty()) DQ_CU(cudaMemcpy(f.bcoef, rec.data(), sizeof(float4) * rec.size(), cudaMemcpyHostToDevice));
+        DQ_CU(cudaMalloc(&f.bcol, sizeof(int)));
+        return DQ_OK;
+    }
+    if (R == 3) return DQ_ERR_ARG;   // three rows per block only in the packed (complex64) form
     f.nunion = bcol.size();
     const size_t nu = std::max<size_t>(f.nunion, 1);
     DQ_CU(cudaMalloc(&f.bptr, sizeof(int) * (nb + 1)));
@@ -954,6 +1197,7 @@ static cudaError_t win_attr_r(int R, int bytes) {
     switch (R) {
         case 1: return win_attr<Real, TPT, 1>(bytes);
         case 2: return win_attr<Real, TPT, 2>(bytes);
+        case 3: return sizeof(Real) == 4 ? win_attr<Real, TPT, 3>(bytes) : cudaErrorInvalidValue;
         case 4: return win_attr<Real, TPT, 4>(bytes);
         default: return win_attr<Real, TPT, 8>(bytes);
     }
@@ -963,7 +1207,7 @@ constexpr size_t kWinSmemMax = 200 * 1024;
 
 // Tiling: TC trajectories per chunk, TPT per thread, ~ctas_per_sm CTAs per
 // SM, R rows per SpMM block, staged: TMA shared-memory window SpMM.
-dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R, int staged) {
+dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R, int staged, int groups) {
     BatchedState* bs = c->bat;
     const int B = bs->B, n = c->n;
     if (tpt != 1 && tpt != 2) return DQ_ERR_ARG;
@@ -974,13 +1218,15 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     const int ri = r_index(R);
     if (ri < 0) return DQ_ERR_ARG;
     const int chunks = B / tc;
+    if (groups < 1 || chunks % groups) return DQ_ERR_ARG;
+    const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
-    int gx = std::max(1, (bs->sms * ctas_per_sm) / chunks);
+    int gx = std::max(1, (bs->sms * ctas_per_sm) / cpg);
     int rpc = (n + gx - 1) / gx;
     rpc = ((rpc + RPC - 1) / RPC) * RPC;
     gx = (n + rpc - 1) / rpc;
     const int nb = (n + R - 1) / R;
-    int gxs = std::max(1, (bs->sms * ctas_per_sm) / chunks);
+    int gxs = std::max(1, (bs->sms * ctas_per_sm) / cpg);
     int bpc = (nb + gxs - 1) / gxs;
     bpc = ((bpc + RPC - 1) / RPC) * RPC;
     gxs = (nb + bpc - 1) / bpc;
@@ -995,7 +1241,8 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (staged) {
         const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
         const int SR = RPC * R;
-        if (SR > 256 || 2 * tc > 256 || tc * 2 * rsz < 16) return DQ_ERR_ARG;
+        // boxes of SR rows tile the power-of-two ring without wrapping
+        if (SR > 256 || (SR & (SR - 1)) || 2 * tc > 256 || tc * 2 * rsz < 16) return DQ_ERR_ARG;
         halo = ((bs->bw + SR - 1) / SR) * SR;
         int W = 1;
         while (W < 2 * halo + 2 * SR) W <<= 1;
@@ -1003,7 +1250,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         if (smem > kWinSmemMax) return DQ_ERR_ARG;
         wmask = W - 1;
         const int fit = std::max(1, (int)((228 * 1024) / (smem + 12 * 1024)));
-        gxw = std::max(1, (bs->sms * std::min(ctas_per_sm, fit)) / chunks);
+        gxw = std::max(1, (bs->sms * std::min(ctas_per_sm, fit)) / cpg);
         rpc_win = (n + gxw - 1) / gxw;
         rpc_win = ((rpc_win + SR - 1) / SR) * SR;
         gxw = (n + rpc_win - 1) / rpc_win;
@@ -1024,6 +1271,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     bs->gxs = gxs;
     bs->bpc = bpc;
     bs->staged = staged;
+    bs->groups = groups;
     bs->halo = halo;
     bs->wmask = wmask;
     bs->rpc_win = rpc_win;
@@ -1079,7 +1327,7 @@ dq_status batched_alloc(dq_ctx* c) {
     int tc = 16;
     while (tc > tpt && B % tc) tc >>= 1;
     if (B % tc) tc = tpt;
-    dq_status st = batched_set_tiling(c, tc, tpt, 2, 4, 0);
+    dq_status st = batched_set_tiling(c, tc, tpt, 2, 4, 0, 1);
     if (st) {
         c->err = "batched: no valid tiling for n_traj";
         return st;
@@ -1145,34 +1393,37 @@ struct StepTimer {
 };
 
 template <typename Real, int TPT, bool kBil, bool kWrite>
-static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w) {
+static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w, int cy0, int ncy) {
     BatchedState* bs = c->bat;
     const BlockFmt& f = bs->fmt[r_index(bs->R)];
     const int n = c->n, B = bs->B, TC = bs->TC;
     const Real* cf = (const Real*)f.bcoef;
     const Real* d = (const Real*)bs->diag;
     if (bs->staged) {
-        const dim3 grid(bs->gxw, bs->chunks);
+        const dim3 grid(bs->gxw, ncy);
         const CUtensorMap& tm = bs->tmaps[j];
 #define DQ_WIN_R(RR)                                                                                       \
     k_spmm_win<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, bs->win_smem, c->stream>>>(                  \
-        n, B, TC, bs->rpc_win, bs->halo, bs->wmask, j, f.bptr, f.bcol, cf, d, w, bs->s, tm)
+        n, B, TC, bs->rpc_win, bs->halo, bs->wmask, j, f.bptr, f.bcol, cf, d, w, bs->s, cy0, bs->chunks, tm)
         switch (bs->R) {
             case 1: DQ_WIN_R(1); break;
             case 2: DQ_WIN_R(2); break;
+            case 3: if constexpr (sizeof(Real) == 4) DQ_WIN_R(3); break;
             case 4: DQ_WIN_R(4); break;
             default: DQ_WIN_R(8); break;
         }
 #undef DQ_WIN_R
         return;
     }
-    const dim3 grid(bs->gxs, bs->chunks);
+    const dim3 grid(bs->gxs, ncy);
 #define DQ_SPMM_R(RR)                                                                                             \
     k_spmm_blk<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j, f.bptr, \
-                                                                               f.bcol, cf, d, rj, w, bs->s)
+                                                                               f.bcol, cf, d, rj, w, bs->s, cy0,    \
+                                                                               bs->chunks)
     switch (bs->R) {
         case 1: DQ_SPMM_R(1); break;
         case 2: DQ_SPMM_R(2); break;
+        case 3: if constexpr (sizeof(Real) == 4) DQ_SPMM_R(3); break;
         case 4: DQ_SPMM_R(4); break;
         default: DQ_SPMM_R(8); break;
     }
@@ -1180,20 +1431,20 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w) {
 }
 
 template <typename Real, int TPT>
-static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm) {
+static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int ncy) {
     BatchedState* bs = c->bat;
     const int n = c->n, B = bs->B, TC = bs->TC, rpc = bs->rpc;
     cudaStream_t st = c->stream;
     const size_t se = (size_t)n * B;
     Real* slabs = (Real*)bs->slabs;
     auto slab = [&](int k) { return slabs + 2 * se * k; };
-    const dim3 grid(bs->gx, bs->chunks);
+    const dim3 grid(bs->gx, ncy);
     if (tm) tm->mark(DQ_KIND_SPMM, st);
-    if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_spmm<Real, TPT, true, true>(c, j, slab(j), slab(0));
-    else launch_spmm<Real, TPT, false, true>(c, j, slab(j), slab(0));
+    if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_spmm<Real, TPT, true, true>(c, j, slab(j), slab(0), cy0, ncy);
+    else launch_spmm<Real, TPT, false, true>(c, j, slab(j), slab(0), cy0, ncy);
     if (tm) tm->mark(DQ_KIND_AXPY, st);
     k_axpy_beta<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slab(0), slab(j), slab(j - 1),
-                                                       slab(j + 1), bs->s);
+                                                       slab(j + 1), bs->s, cy0, bs->chunks);
     return DQ_OK;
 }
 
@@ -1214,9 +1465,14 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm) {
     k_noise_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, c->cfg.noise_model, ns, subdt, sqrt_subdt,
                                                      c->cfg.seed, c->d_sigma, c->d_invtau, c->d_coeff, bs->eps,
                                                      bs->deps, (Real*)bs->diag, bs->s);
-    for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm);
-    mark(DQ_KIND_SPMM_NORM);
-    launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr);
+    // trajectory groups one after another: a group's Krylov slabs stay in L2
+    // across its m iterations
+    const int cpg = bs->chunks / bs->groups;
+    for (int g = 0; g < bs->groups; ++g) {
+        for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm, g * cpg, cpg);
+        mark(DQ_KIND_SPMM_NORM);
+        launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, g * cpg, cpg);
+    }
     mark(DQ_KIND_PADE);
     k_pade_b<<<B, 128, pade_smem_bytes(m + 2), st>>>(m, B, c->tau_im, c->cfg.norm_mode, bs->s, c->d_erracc);
     mark(DQ_KIND_COMBINE);
@@ -1237,8 +1493,13 @@ static dq_status enqueue_step_any(dq_ctx* c, StepTimer* tm) {
 
 static dq_status enqueue_iteration_any(dq_ctx* c, int j) {
     BatchedState* bs = c->bat;
-    if (!bs->mixed) return enqueue_iteration<double, 1>(c, j, nullptr);
-    return bs->TPT == 2 ? enqueue_iteration<float, 2>(c, j, nullptr) : enqueue_iteration<float, 1>(c, j, nullptr);
+    const int cpg = bs->chunks / bs->groups;
+    for (int g = 0; g < bs->groups; ++g) {
+        if (!bs->mixed) enqueue_iteration<double, 1>(c, j, nullptr, g * cpg, cpg);
+        else if (bs->TPT == 2) enqueue_iteration<float, 2>(c, j, nullptr, g * cpg, cpg);
+        else enqueue_iteration<float, 1>(c, j, nullptr, g * cpg, cpg);
+    }
+    return DQ_OK;
 }
 
 dq_status batched_run(dq_ctx* c, int n_steps) {
@@ -1298,8 +1559,9 @@ dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
     return check_cuda(c, cudaGetLastError(), "time iteration");
 }
 
-void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged) {
+void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged, int* groups) {
     if (staged) *staged = c->bat->staged;
+    if (groups) *groups = c->bat->groups;
     if (tc) *tc = c->bat->TC;
     if (tpt) *tpt = c->bat->TPT;
     if (cps) *cps = c->bat->ctas_per_sm;

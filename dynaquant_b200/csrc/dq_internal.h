@@ -106,8 +106,8 @@ dq_status batched_run(dq_ctx* c, int n_steps);
 dq_status batched_get_states(dq_ctx* c, dq_cdouble* out);
 dq_status batched_collect_corr(dq_ctx* c);
 dq_status batched_profile(dq_ctx* c, int n_steps, double* ms, int* cnt, int nk);
-dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R, int staged);
-void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged);
+dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R, int staged, int groups);
+void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged, int* groups);
 void batched_invalidate_blocks(dq_ctx* c);
 dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms);
 void batched_noise_arrays(dq_ctx* c, const double** eps, const double** deps);

@@ -66,12 +66,15 @@ __device__ __forceinline__ bool reduce2_last(double a, double b, double* partial
     if (threadIdx.x == 0) { partial[2 * blockIdx.x] = ra; partial[2 * blockIdx.x + 1] = rb; }
     bool last = last_block_ticket(ticket, gridDim.x);
     if (last) {
+        // every thread sums a strided share, then a fixed-order block sum
         double sa = 0.0, sb = 0.0;
+        for (unsigned int k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+            sa += __ldcg(&partial[2 * k]);
+            sb += __ldcg(&partial[2 * k + 1]);
+        }
+        sa = block_sum(sa, scratch);
+        sb = block_sum(sb, scratch);
         if (threadIdx.x == 0) {
-            for (unsigned int k = 0; k < gridDim.x; ++k) {
-                sa += __ldcg(&partial[2 * k]);
-                sb += __ldcg(&partial[2 * k + 1]);
-            }
             out2[0] = sa;
             out2[1] = sb;
             *ticket = 0;

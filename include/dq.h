@@ -146,16 +146,22 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * rows computed together by the SpMM over the union of their neighbour
  * columns.  staged = 1 stages the gathered trajectory rows in a shared-memory
  * window filled by TMA (needs the matrix bandwidth to fit the window; the
- * call fails otherwise), 0 gathers through L1.  Changing it restarts the
- * ensemble at the next dq_run (as dq_reset does). */
+ * call fails otherwise), 0 gathers through L1.  groups splits the
+ * trajectory chunks into groups whose m Lanczos iterations run one group
+ * after another, so a group's Krylov slabs stay resident in L2 (must divide
+ * n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run
+ * (as dq_reset does). */
 DQ_API dq_status dq_set_tiling(dq_ctx *ctx, int traj_chunk, int vec, int ctas_per_sm, int rows_per_block,
-                               int staged);
+                               int staged, int groups);
 DQ_API dq_status dq_get_tiling(dq_ctx *ctx, int *traj_chunk, int *vec, int *ctas_per_sm, int *rows_per_block,
-                               int *staged);
+                               int *staged, int *groups);
 /* Times one Lanczos iteration (SpMM + axpy) of the current system under
  * every valid tiling, keeps the fastest and resets the ensemble.  best_ms
  * (may be NULL) gets its time per iteration. */
 DQ_API dq_status dq_autotune(dq_ctx *ctx, int reps, double *best_ms);
+/* Mean device time of one Lanczos iteration (SpMM + axpy) under the current
+ * tiling, over reps launches; the ensemble restarts at the next dq_run. */
+DQ_API dq_status dq_time_iteration(dq_ctx *ctx, int reps, double *ms);
 
 /* Kernel kinds of one ensemble step, for dq_profile_step. */
 enum {

@@ -114,8 +114,9 @@ def test_spectrum_matches_numpy():
     p.close()
 
 
-@pytest.mark.parametrize("tiling", [(2, 2, 1, 1, 0), (4, 1, 2, 2, 0), (4, 2, 8, 4, 0), (2, 1, 4, 8, 0),
-                                    (4, 2, 2, 8, 0), (4, 2, 1, 1, 1), (2, 2, 2, 2, 1), (4, 1, 1, 4, 1)])
+@pytest.mark.parametrize("tiling", [(2, 2, 1, 1, 0, 1), (4, 1, 2, 2, 0, 1), (4, 2, 8, 4, 0, 1), (2, 1, 4, 8, 0, 2),
+                                    (4, 2, 2, 8, 0, 1), (4, 2, 1, 1, 1, 1), (2, 2, 2, 1, 1, 2), (4, 1, 1, 4, 1, 1),
+                                    (1, 1, 2, 4, 0, 4)])
 def test_every_tiling_matches_oracle(tiling):
     """Tilings only change the schedule: each must reproduce the oracle."""
     import dynaquant_b200 as dq
@@ -142,12 +143,13 @@ def test_autotune_picks_valid_tiling_and_keeps_parity(tmp_path, monkeypatch):
     q = _chain_prop(dq.PREC_MIXED, 1)
     r2 = q.autotune(reps=2)
     assert r2["cached"] and q.get_tiling() == (r["traj_chunk"], r["vec"], r["ctas_per_sm"], r["rows_per_block"],
-                                               r["staged"])
+                                               r["staged"], r["groups"])
     q.close()
 
 
-@pytest.mark.parametrize("R,staged", [(1, 1), (4, 1), (8, 1), (4, 0)])
-def test_tube_tilings_match_oracle(oracle, R, staged):
+@pytest.mark.parametrize("R,staged,groups", [(1, 1, 1), (2, 1, 1), (3, 0, 1), (4, 1, 1), (8, 1, 1), (4, 0, 1),
+                                             (3, 0, 2), (2, 1, 2), (2, 0, 2)])
+def test_tube_tilings_match_oracle(oracle, R, staged, groups):
     """Shared-memory window (TMA-staged) and L1 SpMM variants on a dipole tube,
     whose couplings reach ~3 rings (bandwidth ~60 sites)."""
     import dynaquant_b200 as dq
@@ -156,7 +158,7 @@ def test_tube_tilings_match_oracle(oracle, R, staged):
     rp, col, val, diag = s.off_diagonal()
     S = oracle.System(rp, col, val, diag, m=12, dt=0.5, dot_mode=1, noise=2, sigma=250.0, tau=50.0,
                       sigma_static=150.0, seed=4)
-    B, T = 16, 12
+    B, T = 32, 12
     psi0 = s.bright_state()
     ref = S.run(B, T, psi0, pop_every=4, threads=4)
     p = dq.Propagator(s.n, m=12, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=4, dot=1,
@@ -164,7 +166,9 @@ def test_tube_tilings_match_oracle(oracle, R, staged):
     p.set_system(s)
     p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
     p.set_initial_state(psi0)
-    p.set_tiling(16, 2, 2, R, staged)
+    # 16 trajectories per chunk, 2 per thread: 32 row blocks per step, so
+    # R * 32 rows per staged step stays within one 256-row TMA box
+    p.set_tiling(16, 2, 2, R, staged, groups)
     p.run(T)
     assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
     p.close()
