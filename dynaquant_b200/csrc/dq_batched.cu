@@ -44,6 +44,7 @@ namespace dq {
 constexpr int kBThreads = 256;
 constexpr int kMaxTC = 64;
 constexpr int kMaxCtasPerChunk = 4096;
+constexpr int kStreamCtasPerSm = 8;
 
 // ---- vector access of TPT consecutive complex values ----------------------
 template <typename Real, int TPT> struct VL;
@@ -1221,7 +1222,8 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (groups < 1 || chunks % groups) return DQ_ERR_ARG;
     const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
-    int gx = std::max(1, (bs->sms * ctas_per_sm) / cpg);
+    // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide
+    int gx = std::max(1, (bs->sms * kStreamCtasPerSm) / cpg);
     int rpc = (n + gx - 1) / gx;
     rpc = ((rpc + RPC - 1) / RPC) * RPC;
     gx = (n + rpc - 1) / rpc;
