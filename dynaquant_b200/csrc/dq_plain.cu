@@ -16,6 +16,7 @@
 // Cross-block reductions use the last-block ticket, so every reduction is
 // deterministic and costs no extra launch.
 #include <cstdio>
+#include <mutex>
 
 #include "dq_internal.h"
 #include "dq_rng.cuh"
@@ -351,3 +352,165 @@ dq_status plain_observe_initial(dq_ctx* c) {
 }
 
 }  // namespace dq
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the plain step (dq_krylov_step_static).
+//
+// Some callers cannot allocate device memory at the point where they step a
+// wavefunction: a host application that owns all device memory through its
+// own pool and forbids cudaMalloc/cudaFree once its time loop runs (they can
+// synchronise the device and fragment the pool), or code embedded in a
+// framework that hands out only the buffers it manages.  This entry point
+// needs no context and allocates nothing: its Krylov basis, residual,
+// reduction partials and scalars live in one file-scope __device__ array of
+// kStaticScratchBytes (16 MiB), which every GPU that loads the library holds
+// until the process exits.  The caller passes the Hamiltonian (off-diagonal
+// CSR + this step's diagonal) and the states, all in device memory.
+//
+// The array's host-side name is only a stand-in for a device address: on its
+// first call on a device the entry point, with that device current, asks the
+// runtime for the array's device address (cudaGetSymbolAddress) and raises
+// the Padé kernel's shared-memory limit; that first call should come before
+// any stream capture.  Every call on a device shares the one array and leaves
+// the last call's contents in it (each call clears what must start at zero),
+// so calls that overlap on the GPU (different streams, or host threads
+// without ordering) race and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+namespace dq {
+constexpr size_t kStaticScratchBytes = size_t(16) << 20;
+}  // namespace dq
+
+static __device__ __align__(256) unsigned char g_dq_static_scratch[dq::kStaticScratchBytes];
+
+namespace {
+
+struct StaticScratch {
+    bool init = false;
+    unsigned char* ptr = nullptr;
+};
+constexpr int kMaxDevices = 64;
+StaticScratch g_static_scratch[kMaxDevices];
+std::mutex g_static_mu;
+
+void write_err(char* buf, int len, const char* msg) {
+    if (buf && len > 0) snprintf(buf, (size_t)len, "%s", msg);
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+namespace dq {
+
+// clears what a step expects at zero and starts the recurrence at q_1 = psi_in
+__global__ void k_static_begin(PlainScalars* ps) {
+    if (threadIdx.x == 0) {
+        ps->sc[1] = 1.0;
+        ps->beta[0] = cmk(0.0, 0.0);
+        ps->status = 0;
+        for (int k = 0; k < 4; ++k) ps->ticket[k] = 0;
+    }
+}
+
+}  // namespace dq
+
+extern "C" dq_status dq_krylov_step_static(int n, const int* rowptr, const int* col, const double* val,
+                                           const double* diag, const dq_cdouble* psi_in, dq_cdouble* psi_out, int m,
+                                           double dt, double hbar, int dot_mode, int norm_mode, void* stream,
+                                           double* err_est, char* errbuf, int errbuf_len) {
+    using namespace dq;
+    if (n < 2 || m < 2 || m > kMaxM || m > n || !(dt > 0) || !rowptr || !col || !val || !diag || !psi_in ||
+        !psi_out || psi_in == psi_out || (dot_mode != DQ_DOT_BILINEAR && dot_mode != DQ_DOT_HERMITIAN) ||
+        (norm_mode != DQ_NORM_REAL_ONLY && norm_mode != DQ_NORM_COMPLEX)) {
+        write_err(errbuf, errbuf_len, "krylov_step_static: invalid argument");
+        return DQ_ERR_ARG;
+    }
+    const int T = kPlainThreads;
+    const int G = (n + T - 1) / T;
+    const size_t off_partial = align256(sizeof(PlainScalars));
+    const size_t off_w = off_partial + align256(sizeof(double) * 2 * kMaxPartials);
+    const size_t off_q = off_w + align256(sizeof(cd) * (size_t)n);
+    const size_t need = off_q + sizeof(cd) * (size_t)n * (size_t)(m + 2);
+    if (G > kMaxPartials || need > kStaticScratchBytes) {
+        char msg[200];
+        snprintf(msg, sizeof msg,
+                 "krylov_step_static: n=%d, m=%d needs %zu bytes of scratch, above the %zu-byte static limit "
+                 "((m+3)*n*16 bytes plus ~70 KB)",
+                 n, m, need, kStaticScratchBytes);
+        write_err(errbuf, errbuf_len, msg);
+        return DQ_ERR_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        write_err(errbuf, errbuf_len, "krylov_step_static: no current CUDA device");
+        return DQ_ERR_CUDA;
+    }
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        StaticScratch& sc = g_static_scratch[dev];
+        if (!sc.init) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_dq_static_scratch);
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k_pade_plain, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)pade_smem_bytes(kMaxL));
+            if (e != cudaSuccess) {
+                write_err(errbuf, errbuf_len, cudaGetErrorString(e));
+                return DQ_ERR_CUDA;
+            }
+            sc.ptr = static_cast<unsigned char*>(p);
+            sc.init = true;
+        }
+        base = sc.ptr;
+    }
+    PlainScalars* ps = reinterpret_cast<PlainScalars*>(base);
+    double* partial = reinterpret_cast<double*>(base + off_partial);
+    cd* w = reinterpret_cast<cd*>(base + off_w);
+    cd* Q = reinterpret_cast<cd*>(base + off_q);
+    const cd* pin = reinterpret_cast<const cd*>(psi_in);
+    cd* pout = reinterpret_cast<cd*>(psi_out);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!(hbar > 0)) {
+        const double pi = atan(1.0) * 4.0;
+        hbar = (1 / 100.) * (1e15) * 1. / (299792548. * 2 * pi);   // cppUtility.cpp:19-22
+    }
+    const double tau_im = -dt / hbar;
+    k_static_begin<<<1, 32, 0, st>>>(ps);
+    for (int j = 1; j <= m; ++j) {
+        const cd* rj = (j == 1) ? pin : Q + (size_t)j * n;
+        const cd* rjm = (j <= 1) ? nullptr : (j == 2 ? pin : Q + (size_t)(j - 1) * n);
+        cd* rjp = Q + (size_t)(j + 1) * n;
+        if (dot_mode == DQ_DOT_BILINEAR)
+            k_spmv_alpha<true><<<G, T, 0, st>>>(n, j, rowptr, col, val, diag, rj, w, partial, ps);
+        else
+            k_spmv_alpha<false><<<G, T, 0, st>>>(n, j, rowptr, col, val, diag, rj, w, partial, ps);
+        k_axpy_norm<<<G, T, 0, st>>>(n, j, w, rj, rjm, rjp, partial, ps);
+    }
+    k_spmv_norm<<<G, T, 0, st>>>(n, m + 1, rowptr, col, val, diag, Q + (size_t)(m + 1) * n, partial, ps);
+    k_pade_plain<<<1, 256, pade_smem_bytes(m + 2), st>>>(m, tau_im, norm_mode, ps, nullptr, 0);
+    k_combine<<<G, T, 0, st>>>(n, m, pin, Q, pout, partial, ps);
+    k_renorm<<<G, T, 0, st>>>(n, pout, nullptr, nullptr, nullptr, partial, ps);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        write_err(errbuf, errbuf_len, cudaGetErrorString(e));
+        return DQ_ERR_CUDA;
+    }
+    if (err_est) {
+        double hv[2] = {0.0, 0.0};
+        int status = 0;
+        e = cudaMemcpyAsync(&hv[0], &ps->err, sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &ps->status, sizeof(int), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            write_err(errbuf, errbuf_len, cudaGetErrorString(e));
+            return DQ_ERR_CUDA;
+        }
+        *err_est = hv[0];
+        if (status) {
+            write_err(errbuf, errbuf_len, "krylov_step_static: device reported an error (breakdown/NaN/Padé)");
+            return status;
+        }
+    }
+    return DQ_OK;
+}

@@ -133,6 +133,29 @@ DQ_API dq_status dq_prop_step(dq_ctx *ctx, int traj, int step, const dq_cdouble 
  * n_steps, accumulating populations / correlation / error on the device. */
 DQ_API dq_status dq_run_plain(dq_ctx *ctx, int n_steps);
 
+/* Allocation-free Krylov step; this entry point has no counterpart in the
+ * reference.  For callers that cannot allocate device memory while they step
+ * (an application whose own pool owns all device memory and forbids
+ * cudaMalloc/cudaFree inside its time loop, or a framework that only hands
+ * out buffers it manages): it needs no dq_ctx and allocates nothing.  One
+ * step psi_out = exp(-i H dt/hbar) psi_in by m-step Lanczos + Padé + renorm
+ * for H = diag + offdiag, where rowptr/col/val is the OFF-DIAGONAL CSR and
+ * diag this step's diagonal; every pointer is DEVICE memory owned by the
+ * caller (psi_in and psi_out may not alias).  Work is ordered on `stream`
+ * (a cudaStream_t, NULL = legacy default stream).  Scratch is one static
+ * 16 MiB device array per GPU (held until process exit), so it accepts
+ * (m+3)*n*16 bytes + ~70 KB <= 16 MiB (about 55,000 sites at m = 16) and
+ * returns DQ_ERR_ARG with the reason in errbuf beyond that.  The first call
+ * on a device looks up the array's device address and should come before
+ * any stream capture.  All calls on a device share the array (each clears
+ * what must start at zero): calls that overlap on the GPU race.  If err_est
+ * is non-NULL the call synchronises `stream` and writes the EXPOKIT error
+ * estimate.  errbuf (may be NULL) receives a message on failure. */
+DQ_API dq_status dq_krylov_step_static(int n, const int *rowptr, const int *col, const double *val,
+                                       const double *diag, const dq_cdouble *psi_in, dq_cdouble *psi_out, int m,
+                                       double dt, double hbar, int dot_mode, int norm_mode, void *stream,
+                                       double *err_est, char *errbuf, int errbuf_len);
+
 /* ---- batched ensemble form ---- */
 /* Advances all trajectories by n_steps with the configured precision
  * (shared-structure SpMM Lanczos over all trajectories, batched FP64 Padé,
