@@ -123,6 +123,19 @@ def spmm_bytes(s, B):
     return 20.0 * s.n * B + 8.0 * nnz_off + 4.0 * (s.n + 1)
 
 
+def measured_traffic():
+    """DRAM bytes per launch of the SpMM kernel from the committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of one capture), or None."""
+    p = os.path.join(ROOT, "profiles", "k_spmm_blk_tube60x500.md")
+    try:
+        for line in open(p):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline_sample(s, threads, target_s=12.0):
     """Times the FP64 oracle (C, OpenMP over trajectories) on a bounded
     sample of the same workload; returns traj-steps/s and the sample."""
@@ -289,7 +302,9 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(kernels_per_step * K),
         "roofline": {"bound": "hbm", "kernel": "k_spmm (SpMM + alpha)", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": bytes_spmm, "ms_per_launch": spmm_ms, "traffic": None},
+                     "algorithmic_bytes_per_launch": bytes_spmm, "ms_per_launch": spmm_ms,
+                     "traffic": measured_traffic(),
+                     "traffic_source": "profiles/k_spmm_blk_tube60x500.md (ncu dram bytes, one launch)"},
         "kernels_ms_per_launch": {k: v[0] for k, v in prof.items()},
         "eager_step_ms": step_ms_eager,
         "plain_fp64": {"value": plain, "unit": "traj-steps/s", "speedup_batched_mixed": value / world / plain,
