@@ -585,3 +585,147 @@ void dqo_ifft(int n, double *xd) {
         free(y);
     }
 }
+
+/* ------------------------------------------------------------------ */
+/* Spectrum loss and its adjoint gradient (FP64 host reference).       */
+/* This capability has no reference counterpart; it restates the        */
+/* adjoint of psi(k+1) = exp(tau H_k) psi(k), tau = -i dt/hbar:          */
+/*   lambda(T) = s_T,  lambda(k) = s_k + exp(tau H_k)^dagger lambda(k+1) */
+/*   dL/dp = Re sum_k int_0^1 <e^{(1-s)A^+}lambda(k+1)| tau dH/dp e^{sA} psi(k)> ds */
+/* with both exponentials in their Krylov bases and the s-integral from   */
+/* the block-triangular exponential exp([[tau T_W, e1 e1^T],[0, tau T_V]]) */
+/* (Van Loan 1978).  Needs the Hermitian Lanczos product.               */
+/* ------------------------------------------------------------------ */
+static void tridiag_m(int m, const cx *alpha, const cx *beta, cx *T) {
+    memset(T, 0, sizeof(cx) * m * m);
+    for (int i = 0; i < m; ++i) {
+        T[i * m + i] = alpha[i + 1];
+        if (i + 1 < m) { T[i * m + i + 1] = beta[i + 1]; T[(i + 1) * m + i] = beta[i + 1]; }
+    }
+}
+
+double dqo_spectrum_loss_grad(const dqo_system *sys, const double *val_base, const int *cls, int n_classes,
+                              int n_traj, int n_steps, const double *psi0d, int len, double scale,
+                              const double *target, double *grad, int n_threads) {
+    (void)n_threads;
+    const int n = sys->n, m = sys->m, T = n_steps;
+    const cx *psi0 = (const cx *)psi0d;
+    const cx tau = {0.0, -sys->dt / sys->hbar};
+    /* forward: store psi(k) and the diagonal of every step */
+    cx *psi_all = (cx *)malloc(sizeof(cx) * (size_t)n_traj * (T + 1) * n);
+    double *diag_all = (double *)malloc(sizeof(double) * (size_t)n_traj * T * n);
+    cx *C = (cx *)calloc((size_t)(T + 1), sizeof(cx));
+    double *eps = (double *)malloc(sizeof(double) * n * 2);
+    double *deps = eps + n;
+    for (int b = 0; b < n_traj; ++b) {
+        dqo_traj_init(sys, b, eps, deps);
+        cx *ps = psi_all + (size_t)b * (T + 1) * n;
+        memcpy(ps, psi0, sizeof(cx) * n);
+        for (int k = 0; k < T; ++k) {
+            double *d = diag_all + ((size_t)b * T + k) * n;
+            dqo_noise_update(sys, b, k, eps, deps, d);
+            dqo_krylov_step(sys, d, (const double *)(ps + (size_t)k * n), (double *)(ps + (size_t)(k + 1) * n), NULL,
+                            NULL, NULL);
+        }
+        for (int k = 0; k <= T; ++k) {
+            cx acc = {0, 0};
+            for (int i = 0; i < n; ++i) acc = cadd(acc, cmul(cconj(psi0[i]), ps[(size_t)k * n + i]));
+            C[k].re += acc.re / n_traj;
+            C[k].im += acc.im / n_traj;
+        }
+    }
+    /* spectrum, loss, G = IDFT(g) */
+    cx *S = (cx *)calloc((size_t)len, sizeof(cx));
+    for (int k = 0; k <= T && k < len; ++k) S[k] = C[k];
+    dqo_ifft(len, (double *)S);
+    double loss = 0.0;
+    cx *Gv = (cx *)calloc((size_t)len, sizeof(cx));
+    for (int j = 0; j < len; ++j) {
+        double a = scale * S[j].re - target[j];
+        loss += a * a;
+        Gv[j].re = 2.0 * scale * a;
+    }
+    if (!grad) {
+        free(psi_all); free(diag_all); free(C); free(eps); free(S); free(Gv);
+        return loss;
+    }
+    dqo_ifft(len, (double *)Gv);
+    memset(grad, 0, sizeof(double) * (n + n_classes));
+    cx *V = (cx *)malloc(sizeof(cx) * (size_t)n * (m + 2));
+    cx *W = (cx *)malloc(sizeof(cx) * (size_t)n * (m + 2));
+    cx *aV = (cx *)malloc(sizeof(cx) * (m + 2) * 4);
+    cx *bV = aV + (m + 2), *aW = bV + (m + 2), *bW = aW + (m + 2);
+    cx *lam = (cx *)malloc(sizeof(cx) * n * 3);
+    cx *qw = lam + n, *tvec = lam + 2 * n;
+    const int L2 = 2 * m;
+    cx *Z = (cx *)malloc(sizeof(cx) * L2 * L2 * 2);
+    cx *EZ = Z + L2 * L2;
+    cx *TW = (cx *)malloc(sizeof(cx) * m * m * 3);
+    cx *TV = TW + m * m, *EW = TV + m * m;
+    cx *tb = (cx *)malloc(sizeof(cx) * m);
+    for (int b = 0; b < n_traj; ++b) {
+        const cx *ps = psi_all + (size_t)b * (T + 1) * n;
+        for (int i = 0; i < n; ++i) lam[i] = cscale(cmul(cconj(Gv[T]), psi0[i]), 1.0 / n_traj);
+        for (int t = T - 1; t >= 0; --t) {
+            const double *d = diag_all + ((size_t)b * T + t) * n;
+            dqo_lanczos(sys, d, (const double *)(ps + (size_t)t * n), (double *)V, (double *)aV, (double *)bV);
+            double ln = 0.0;
+            for (int i = 0; i < n; ++i) ln += cabs2(lam[i]);
+            ln = sqrt(ln);
+            cx *Ul = tvec;
+            memset(Ul, 0, sizeof(cx) * n);
+            if (ln > 0.0) {
+                for (int i = 0; i < n; ++i) qw[i] = cscale(lam[i], 1.0 / ln);
+                dqo_lanczos(sys, d, (const double *)qw, (double *)W, (double *)aW, (double *)bW);
+                tridiag_m(m, aW, bW, TW);
+                tridiag_m(m, aV, bV, TV);
+                /* U^dagger lam = ||lam|| W exp(-tau T_W) e1 */
+                const cx mtau = cscale(tau, -1.0);
+                for (int x = 0; x < m * m; ++x) EZ[x] = cmul(mtau, TW[x]);
+                dqo_pade_exp(m, (const double *)EZ, (double *)EW, DQO_NORM_COMPLEX);
+                for (int i = 0; i < n; ++i) {
+                    cx acc = {0, 0};
+                    for (int a = 0; a < m; ++a) acc = cadd(acc, cmul(W[(size_t)(a + 1) * n + i], EW[a * m]));
+                    Ul[i] = cscale(acc, ln);
+                }
+                /* Van Loan: Z = [[tau T_W, E11], [0, tau T_V]] */
+                memset(Z, 0, sizeof(cx) * L2 * L2);
+                for (int i = 0; i < m; ++i)
+                    for (int j = 0; j < m; ++j) {
+                        Z[i * L2 + j] = cmul(tau, TW[i * m + j]);
+                        Z[(m + i) * L2 + m + j] = cmul(tau, TV[i * m + j]);
+                    }
+                Z[0 * L2 + m].re = 1.0;
+                dqo_pade_exp(L2, (const double *)Z, (double *)EZ, DQO_NORM_COMPLEX);
+                /* rho_ik = tau ||lam|| sum_ab conj(W_ia) N_ab V_kb, N = EZ[0:m, m:2m] */
+                cx coef = cscale(tau, ln);
+                for (int i = 0; i < n; ++i) {
+                    for (int bb = 0; bb < m; ++bb) {
+                        cx acc = {0, 0};
+                        for (int a = 0; a < m; ++a)
+                            acc = cadd(acc, cmul(cconj(W[(size_t)(a + 1) * n + i]), EZ[a * L2 + m + bb]));
+                        tb[bb] = cmul(coef, acc);
+                    }
+                    /* diagonal: site energy i */
+                    cx rho = {0, 0};
+                    for (int bb = 0; bb < m; ++bb) rho = cadd(rho, cmul(tb[bb], V[(size_t)(bb + 1) * n + i]));
+                    grad[i] += rho.re;
+                    /* off-diagonal: coupling classes */
+                    if (n_classes > 0) {
+                        for (int p = sys->rowptr[i]; p < sys->rowptr[i + 1]; ++p) {
+                            int k = sys->col[p];
+                            cx r2 = {0, 0};
+                            for (int bb = 0; bb < m; ++bb) r2 = cadd(r2, cmul(tb[bb], V[(size_t)(bb + 1) * n + k]));
+                            grad[n + cls[p]] += val_base[p] * r2.re;
+                        }
+                    }
+                }
+            }
+            for (int i = 0; i < n; ++i)
+                lam[i] = cadd(cscale(cmul(cconj(Gv[t]), psi0[i]), 1.0 / n_traj), Ul[i]);
+        }
+    }
+    free(psi_all); free(diag_all); free(C); free(eps); free(S); free(Gv);
+    free(V); free(W); free(aV); free(lam); free(Z); free(TW); free(tb);
+    return loss;
+}

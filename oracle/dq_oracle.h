@@ -96,6 +96,16 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
  * n complex values; radix-2 when n is a power of two, direct sum otherwise. */
 void dqo_ifft(int n, double *x);
 
+/* ---- adjoint (no reference counterpart) ---- */
+/* Loss L = sum_j (scale * Re(IDFT_len(Cbar)_j) - target_j)^2 with Cbar(k) the
+ * trajectory mean of <psi0|psi(k)>, k = 0..n_steps, zero-padded to len.  The
+ * site energies are sys->static_eps; val (in sys) must equal sum over classes
+ * of scale_c * val_base.  grad (n + n_classes, may be NULL) receives dL/deps_i
+ * and dL/dscale_c.  Hermitian dot only.  Returns L. */
+double dqo_spectrum_loss_grad(const dqo_system *sys, const double *val_base, const int *cls, int n_classes,
+                              int n_traj, int n_steps, const double *psi0, int len, double scale,
+                              const double *target, double *grad, int n_threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,6 +80,10 @@ def lib():
         L.dqo_run.argtypes = [sp, C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_int]
         L.dqo_run.restype = C.c_int
         L.dqo_ifft.argtypes = [C.c_int, dp]
+        ip = C.POINTER(C.c_int)
+        L.dqo_spectrum_loss_grad.argtypes = [sp, dp, ip, C.c_int, C.c_int, C.c_int, dp, C.c_int, C.c_double,
+                                             dp, dp, C.c_int]
+        L.dqo_spectrum_loss_grad.restype = C.c_double
         _lib = L
     return _lib
 
@@ -218,3 +222,30 @@ class System:
         if rc != 0:
             raise RuntimeError(f"oracle run failed ({rc})")
         return {"pops": pops, "corr": corr, "psi_final": fin, "err": err}
+
+
+def spectrum_loss_grad(rowptr, col, val_base, cls, scales, static_eps, m, dt, psi0, n_traj, n_steps,
+                       length, scale, target, want_grad=True, hbar=None, noise=NOISE_NONE, ka_substeps=1,
+                       sigma=None, tau=None, seed=0):
+    """Loss sum_j (scale*Re(IDFT_length(Cbar)_j) - target_j)^2 and its gradient with respect to the
+    site energies (static_eps, n) and the coupling-class scales (len(scales)).
+
+    The off-diagonal couplings are val[p] = scales[cls[p]] * val_base[p]; Hermitian Lanczos dot,
+    complex Padé norm.  Returns (loss, grad) with grad None when want_grad is False."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+    col = np.ascontiguousarray(col, dtype=np.int32)
+    val_base = np.ascontiguousarray(val_base, dtype=np.float64)
+    cls = np.ascontiguousarray(cls, dtype=np.int32)
+    scales = np.asarray(scales, dtype=np.float64)
+    val = scales[cls] * val_base if len(cls) else val_base.copy()
+    eps = np.ascontiguousarray(static_eps, dtype=np.float64)
+    sysm = System(rowptr, col, val, eps, m, dt, hbar=hbar, dot_mode=DOT_HERMITIAN, norm_mode=NORM_COMPLEX,
+                  noise=noise, ka_substeps=ka_substeps, sigma=sigma, tau=tau, static_eps=eps, seed=seed)
+    psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
+    target = np.ascontiguousarray(target, dtype=np.float64)
+    assert target.shape == (length,)
+    grad = np.zeros(sysm.n + len(scales)) if want_grad else None
+    loss = lib().dqo_spectrum_loss_grad(C.byref(sysm.s), _dp(val_base), cls.ctypes.data_as(C.POINTER(C.c_int)),
+                                        len(scales), n_traj, n_steps, _dp(psi0.view(np.float64)), length,
+                                        float(scale), _dp(target), _dp(grad), 0)
+    return loss, grad
