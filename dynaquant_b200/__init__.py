@@ -89,6 +89,7 @@ class Propagator:
         cls = np.ascontiguousarray(cls, dtype=np.int32)
         scales = np.ascontiguousarray(scales, dtype=np.float64)
         self._check(self.L.dq_set_coupling_classes(self.h, _lib.iptr(cls), len(scales), _lib.dptr(scales)))
+        self._n_classes = len(scales)
 
     def set_noise_params(self, sigma, tau=None):
         sigma = np.ascontiguousarray(np.broadcast_to(sigma, (self.n,)), dtype=np.float64)
@@ -188,6 +189,29 @@ class Propagator:
         deps = np.zeros(self.n)
         self._check(self.L.dq_get_noise_state(self.h, traj, _lib.dptr(eps), _lib.dptr(deps)))
         return eps, deps
+
+    # -- adjoint -------------------------------------------------------------------
+    def adjoint_setup(self, n_steps, fft_len, scale, target, checkpoint_every=0):
+        """Fixes the spectrum-fitting loss sum_j (scale*Re(S_j) - target_j)^2 (S: inverse DFT of the
+        ensemble-mean correlation over n_steps, zero-padded to fft_len) for forward()/backward()."""
+        self._target = np.ascontiguousarray(target, dtype=np.float64)
+        if self._target.shape != (fft_len,):
+            raise ValueError("target must hold fft_len values")
+        self._check(self.L.dq_adjoint_setup(self.h, n_steps, fft_len, float(scale), _lib.dptr(self._target),
+                                            checkpoint_every))
+
+    def forward(self) -> float:
+        loss = C.c_double()
+        self._check(self.L.dq_forward(self.h, C.byref(loss)))
+        return loss.value
+
+    def backward(self):
+        """Returns (dL/d site energies (N,), dL/d coupling-class scales (n_classes,), one entry for
+        the implicit class when none were set)."""
+        gs = np.zeros(self.n)
+        gc = np.zeros(getattr(self, "_n_classes", 1))
+        self._check(self.L.dq_backward(self.h, _lib.dptr(gs), _lib.dptr(gc)))
+        return gs, gc
 
     @property
     def steps_done(self) -> int:

@@ -28,7 +28,7 @@ EXPORTS = [
     "dq_set_initial_state", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
-    "dq_krylov_step_static",
+    "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward",
 ]
 
 
@@ -106,6 +106,9 @@ def load(path: str = LIB_PATH):
     L.dq_time_iteration.argtypes = [vp, C.c_int, dp]
     L.dq_krylov_step_static.argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, C.c_int, C.c_double, C.c_double, C.c_int,
                                         C.c_int, vp, dp, C.c_char_p, C.c_int]
+    L.dq_adjoint_setup.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp, C.c_int]
+    L.dq_forward.argtypes = [vp, dp]
+    L.dq_backward.argtypes = [vp, dp, dp]
     for name in EXPORTS:
         if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done"):
             getattr(L, name).restype = C.c_int

@@ -47,8 +47,9 @@ dq_status upload_couplings(dq_ctx* c) {
         c->val[k] = s * c->val_base[k];
     }
     std::vector<float> vf(c->val.begin(), c->val.end());
-    batched_invalidate_blocks(c);
-    dq_status st = upload(c, &c->d_val, c->val.data(), c->val.size());
+    dq_status st = batched_invalidate_blocks(c);
+    if (st) return st;
+    st = upload(c, &c->d_val, c->val.data(), c->val.size());
     if (st) return st;
     return upload(c, &c->d_valf, vf.data(), vf.size());
 }
@@ -113,6 +114,7 @@ void dq_destroy(dq_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->cfg.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    adjoint_free(c);
     batched_free(c);
     plain_free(c);
     cudaFree(c->d_rowptr); cudaFree(c->d_col); cudaFree(c->d_val); cudaFree(c->d_valf); cudaFree(c->d_h0);

@@ -856,12 +856,6 @@ static void free_fmt(BlockFmt& f) {
     f = BlockFmt();
 }
 
-void batched_invalidate_blocks(dq_ctx* c) {
-    if (!c->bat) return;
-    for (auto& f : c->bat->fmt) free_fmt(f);
-    drop_graph(c->bat);
-}
-
 static inline float __int_as_float_host(int v) {
     float f;
     std::memcpy(&f, &v, sizeof f);
@@ -1093,6 +1087,47 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     return DQ_OK;
 }
 
+// The couplings changed: drop every block format and rebuild the one the
+// current tiling uses (falling back to the unstaged SpMM when the new
+// matrix's bandwidth no longer fits the staged window).
+dq_status batched_invalidate_blocks(dq_ctx* c) {
+    BatchedState* bs = c->bat;
+    if (!bs) return DQ_OK;
+    for (auto& f : bs->fmt) free_fmt(f);
+    drop_graph(bs);
+    if (!bs->TC) return DQ_OK;
+    dq_status st = batched_set_tiling(c, bs->TC, bs->TPT, bs->ctas_per_sm, bs->R, bs->staged, bs->groups);
+    if (st && bs->staged) st = batched_set_tiling(c, bs->TC, bs->TPT, bs->ctas_per_sm, bs->R, 0, bs->groups);
+    if (st) c->err = "batched: could not rebuild the coupling blocks";
+    return st;
+}
+
+// Gives dst (a second workspace of the same B and precision) the tiling of
+// c->bat.  The block formats are shared (dst does not own them); the staged
+// SpMM's tensor maps are built on dst's own slabs.
+dq_status batched_mirror_tiling(dq_ctx* c, BatchedState* dst) {
+    BatchedState* src = c->bat;
+    if (!src || !dst || dst->B != src->B || dst->mixed != src->mixed) return DQ_ERR_STATE;
+    drop_graph(dst);
+    if (!dst->fmt_borrowed)
+        for (auto& f : dst->fmt) free_fmt(f);
+    for (int k = 0; k < 5; ++k) dst->fmt[k] = src->fmt[k];
+    dst->fmt_borrowed = true;
+    dst->TC = src->TC; dst->TPT = src->TPT; dst->chunks = src->chunks; dst->gx = src->gx; dst->rpc = src->rpc;
+    dst->ctas_per_sm = src->ctas_per_sm; dst->R = src->R; dst->gxs = src->gxs; dst->bpc = src->bpc;
+    dst->staged = src->staged; dst->groups = src->groups; dst->halo = src->halo; dst->wmask = src->wmask;
+    dst->rpc_win = src->rpc_win; dst->gxw = src->gxw; dst->bw = src->bw; dst->win_smem = src->win_smem;
+    dst->tmaps.clear();
+    if (src->staged) {
+        const int SR = (kBThreads / (src->TC / src->TPT)) * src->R;
+        c->bat = dst;
+        dq_status st = build_tmaps(c, src->TC, SR);
+        c->bat = src;
+        if (st) return st;
+    }
+    return DQ_OK;
+}
+
 // Allocates and initialises one workspace of B trajectories and attaches it
 // to c->bat (the caller restores c->bat when the workspace is a second one).
 static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed) {
@@ -1173,7 +1208,8 @@ void batched_free(dq_ctx* c) {
 void batched_free_ws(BatchedState* bs) {
     if (!bs) return;
     drop_graph(bs);
-    for (auto& f : bs->fmt) free_fmt(f);
+    if (!bs->fmt_borrowed)
+        for (auto& f : bs->fmt) free_fmt(f);
     cudaFree(bs->slabs); cudaFree(bs->diag); cudaFree(bs->eps); cudaFree(bs->deps);
     cudaFree(bs->scal_mem); cudaFree(bs->s.tickets); cudaFree(bs->s.status);
     delete bs;

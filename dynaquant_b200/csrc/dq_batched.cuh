@@ -126,6 +126,7 @@ struct dq::BatchedState {
     size_t win_smem = 0;
     std::vector<CUtensorMap> tmaps;       // one per slab (window variant)
     ::BlockFmt fmt[5];                    // R = 1, 2, 3, 4, 8 (built on demand)
+    bool fmt_borrowed = false;            // fmt belongs to another workspace
     int sms = 148;
     bool mixed = true;
     void* slabs = nullptr;      // (m+2) slabs (slab 0 = w)
@@ -209,5 +210,6 @@ namespace dq {
 BatchedState* batched_alloc_ws(dq_ctx* c, int B, bool mixed, dq_status* st);
 void batched_free_ws(BatchedState* bs);
 dq_status batched_iteration(dq_ctx* c, BatchedState* ws, int j);
+dq_status batched_mirror_tiling(dq_ctx* c, BatchedState* dst);
 dq_status batched_step_eager(dq_ctx* c, const std::function<void()>* after_noise, bool skip_pop);
 }  // namespace dq

@@ -33,12 +33,16 @@ __global__ void k_fft_pass(int len, int half, cd* __restrict__ x) {
     }
 }
 
-dq_status spectrum(dq_ctx* c, int len, cd* d_out) {
-    const int np = c->steps_done + 1;
+// out = IDFT_len(scale * in[0..n_in), zero-padded); len a power of two.
+dq_status fft_inverse(dq_ctx* c, int len, const cd* in, int n_in, double scale, cd* out) {
     int blocks = std::max(1, std::min(148 * 4, (len + 255) / 256));
-    k_fft_load<<<blocks, 256, 0, c->stream>>>(std::min(np, len), len, 1.0 / c->cfg.n_traj, c->d_corr, d_out);
-    for (int half = 1; half < len; half <<= 1) k_fft_pass<<<blocks, 256, 0, c->stream>>>(len, half, d_out);
-    return check_cuda(c, cudaGetLastError(), "spectrum");
+    k_fft_load<<<blocks, 256, 0, c->stream>>>(std::min(n_in, len), len, scale, in, out);
+    for (int half = 1; half < len; half <<= 1) k_fft_pass<<<blocks, 256, 0, c->stream>>>(len, half, out);
+    return check_cuda(c, cudaGetLastError(), "inverse DFT");
+}
+
+dq_status spectrum(dq_ctx* c, int len, cd* d_out) {
+    return fft_inverse(c, len, c->d_corr, c->steps_done + 1, 1.0 / c->cfg.n_traj, d_out);
 }
 
 }  // namespace dq

@@ -30,6 +30,7 @@ constexpr int kPlainThreads = 256;
 constexpr int kMaxPartials = 4096;
 
 struct BatchedState;   // dq_batched.cu
+struct AdjointState;   // dq_adjoint.cu
 
 }  // namespace dq
 
@@ -86,6 +87,7 @@ struct dq_ctx {
     int last_path = 0;            // 0: observables from dq_run_plain, 1: from dq_run
 
     dq::BatchedState* bat = nullptr;
+    dq::AdjointState* adj = nullptr;
 };
 
 namespace dq {
@@ -108,7 +110,11 @@ dq_status batched_collect_corr(dq_ctx* c);
 dq_status batched_profile(dq_ctx* c, int n_steps, double* ms, int* cnt, int nk);
 dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R, int staged, int groups);
 void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged, int* groups);
-void batched_invalidate_blocks(dq_ctx* c);
+dq_status batched_invalidate_blocks(dq_ctx* c);
 dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms);
 void batched_noise_arrays(dq_ctx* c, const double** eps, const double** deps);
+// implemented in dq_fft.cu
+dq_status fft_inverse(dq_ctx* c, int len, const cd* in, int n_in, double scale, cd* out);
+// implemented in dq_adjoint.cu
+void adjoint_free(dq_ctx* c);
 }  // namespace dq

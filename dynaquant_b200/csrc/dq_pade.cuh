@@ -52,13 +52,14 @@ struct PadeOut {
     cd e_m1_mp1;    // E(m-1, m+1)
 };
 
-// Computes E = exp(tau * Tbar) for Tbar built from alpha[1..m], beta[1..m]
-// (complex, shared or global), writes y[j] = E(j, 0) for j = 0..m-1 when
-// y != nullptr.  norm_mode 0: reference |Re|-only row sums; 1: |.|.
-// Returns in every thread.
-__device__ inline PadeOut pade_exp_tbar(int m, const cd* alpha, const cd* beta, cd tau, int norm_mode,
-                                        cd* y, unsigned char* smem_raw) {
-    const int L = m + 2;
+// E = exp(A) for the L x L complex matrix A held in the first L*L entries of
+// smem_raw (6 L^2 complex + 64 doubles of shared memory): Padé(6,6) in the
+// odd/even form with scaling by the row-sum infinity norm (norm_mode 0:
+// |Re|-only sums as padeClass.cu:585-706; 1: complex modulus) and repeated
+// squaring.  Returns the number of squarings s (or -1 when s would reach 50,
+// -2 for a singular quotient) and sets *E_out to the result (A itself or the
+// second buffer).  All threads of the CTA call it and all return s.
+__device__ inline int pade_exp_sm(int L, int norm_mode, unsigned char* smem_raw, cd** E_out) {
     const int LL = L * L;
     cd* A = reinterpret_cast<cd*>(smem_raw);
     cd* A2 = A + LL;
@@ -66,27 +67,11 @@ __device__ inline PadeOut pade_exp_tbar(int m, const cd* alpha, const cd* beta, 
     cd* A6 = A4 + LL;
     cd* U = A6 + LL;
     cd* D = U + LL;
-    double* red = reinterpret_cast<double*>(D + LL);   // 64 doubles
     __shared__ int s_sh;
     __shared__ int piv_sh;
     __shared__ int fail_sh;
 
     const PadeCoeffs P = pade_coeffs();
-
-    // tau * Tbar (gpuLanczosHelper.cu:14-60, padeClass.cu:240-246)
-    for (int e = threadIdx.x; e < LL; e += blockDim.x) {
-        int i = e / L, j = e - i * L;
-        cd t = cmk(0, 0);
-        if (i < m && j < m) {
-            if (i == j) t = alpha[i + 1];
-            else if (j == i + 1) t = beta[i + 1];
-            else if (i == j + 1) t = beta[j + 1];
-        } else {
-            if (i == 0 && j == m) t = cmk(1.0, 0.0);
-            else if (i >= m && j >= m && i == j - 1) t = cmk(1.0, 0.0);
-        }
-        A[e] = cmul(tau, t);
-    }
     if (threadIdx.x == 0) fail_sh = 0;
     __syncthreads();
 
@@ -112,13 +97,8 @@ __device__ inline PadeOut pade_exp_tbar(int m, const cd* alpha, const cd* beta, 
     }
     __syncthreads();
     const int s = s_sh;
-    PadeOut out;
-    if (s >= 50) {
-        out.s = -1;
-        out.e_m1_m = cmk(0, 0);
-        out.e_m1_mp1 = cmk(0, 0);
-        return out;
-    }
+    *E_out = A;
+    if (s >= 50) return -1;
     if (s > 0) {
         double sc = ldexp(1.0, -s);
         for (int e = threadIdx.x; e < LL; e += blockDim.x) A[e] = cscale(A[e], sc);
@@ -189,12 +169,7 @@ __device__ inline PadeOut pade_exp_tbar(int m, const cd* alpha, const cd* beta, 
         }
         __syncthreads();
     }
-    if (fail_sh) {
-        out.s = -2;
-        out.e_m1_m = cmk(0, 0);
-        out.e_m1_mp1 = cmk(0, 0);
-        return out;
-    }
+    if (fail_sh) return -2;
     for (int k = L - 1; k >= 0; --k) {
         const cd inv = cdiv(cmk(1.0, 0.0), D[k * L + k]);
         for (int j = threadIdx.x; j < L; j += blockDim.x) {
@@ -218,12 +193,46 @@ __device__ inline PadeOut pade_exp_tbar(int m, const cd* alpha, const cd* beta, 
         sm_matmul(L, E, E, Tmp);
         cd* sw = E; E = Tmp; Tmp = sw;
     }
+    *E_out = E;
+    return s;
+}
+
+// Computes E = exp(tau * Tbar) for Tbar built from alpha[1..m], beta[1..m]
+// (complex, shared or global), writes y[j] = E(j, 0) for j = 0..m-1 when
+// y != nullptr.  norm_mode 0: reference |Re|-only row sums; 1: |.|.
+// Returns in every thread.
+__device__ inline PadeOut pade_exp_tbar(int m, const cd* alpha, const cd* beta, cd tau, int norm_mode,
+                                        cd* y, unsigned char* smem_raw) {
+    const int L = m + 2;
+    const int LL = L * L;
+    cd* A = reinterpret_cast<cd*>(smem_raw);
+    // tau * Tbar (gpuLanczosHelper.cu:14-60, padeClass.cu:240-246)
+    for (int e = threadIdx.x; e < LL; e += blockDim.x) {
+        int i = e / L, j = e - i * L;
+        cd t = cmk(0, 0);
+        if (i < m && j < m) {
+            if (i == j) t = alpha[i + 1];
+            else if (j == i + 1) t = beta[i + 1];
+            else if (i == j + 1) t = beta[j + 1];
+        } else {
+            if (i == 0 && j == m) t = cmk(1.0, 0.0);
+            else if (i >= m && j >= m && i == j - 1) t = cmk(1.0, 0.0);
+        }
+        A[e] = cmul(tau, t);
+    }
+    __syncthreads();
+    cd* E = nullptr;
+    PadeOut out;
+    out.s = pade_exp_sm(L, norm_mode, smem_raw, &E);
+    if (out.s < 0) {
+        out.e_m1_m = cmk(0, 0);
+        out.e_m1_mp1 = cmk(0, 0);
+        return out;
+    }
     if (y) for (int j = threadIdx.x; j < m; j += blockDim.x) y[j] = E[j * L];
-    out.s = s;
     out.e_m1_m = E[(m - 1) * L + m];
     out.e_m1_mp1 = E[(m - 1) * L + m + 1];
     __syncthreads();
-    (void)red;
     return out;
 }
 

@@ -226,6 +226,38 @@ DQ_API dq_status dq_get_noise_state(dq_ctx *ctx, int traj, double *eps, double *
  * Replaces spectraClass::singleSpectraCalc's cufftExecZ2Z (spectraClass.cu:621). */
 DQ_API dq_status dq_get_spectrum(dq_ctx *ctx, int len, dq_cdouble *out);
 
+/* ---- adjoint: gradient of a spectrum-fitting loss ----
+ * No counterpart in the reference (it has no gradients).  The loss is
+ *   L = sum_j (scale * Re(S_j) - target_j)^2,  j = 0..fft_len-1,
+ * with S the unnormalised inverse DFT (dq_get_spectrum's convention) of the
+ * ensemble-mean correlation Cbar(k) = <psi0|psi(k)>, k = 0..n_steps,
+ * zero-padded to fft_len (a power of two).  The gradient is taken with
+ * respect to the site energies (the diagonal of the input Hamiltonian, or the
+ * explicit static energies; N values) and the coupling-class scales of
+ * dq_set_coupling_classes (one implicit class of scale 1 when none are set).
+ * The backward pass runs the adjoint recursion lambda(k) = s_k +
+ * exp(-i dt H_k/hbar) lambda(k+1) with its own Lanczos basis per step and the
+ * exponential's Fréchet derivative from the block-triangular exponential of
+ * the two tridiagonal matrices (Van Loan).  Requires dot_mode
+ * DQ_DOT_HERMITIAN, m <= 24, n_traj a multiple of 8, at most 8 coupling
+ * classes and a normalised initial state. */
+/* Fixes the loss.  target: fft_len host doubles.  checkpoint_every: steps per
+ * recomputed segment (0 = automatic: keep every step's state and diagonal
+ * resident when they fit in about half of the free device memory, else about
+ * sqrt(n_steps)); states at segment starts are kept, the rest is recomputed
+ * by the backward pass. */
+DQ_API dq_status dq_adjoint_setup(dq_ctx *ctx, int n_steps, int fft_len, double scale, const double *target,
+                                  int checkpoint_every);
+/* Resets the ensemble and runs the n_steps of dq_adjoint_setup, keeping what
+ * the backward pass needs; *loss (may be NULL) receives L.  Populations and
+ * correlation are recorded as by dq_run. */
+DQ_API dq_status dq_forward(dq_ctx *ctx, double *loss);
+/* Gradient of the last dq_forward's loss: grad_sites (N host doubles) and
+ * grad_classes (one per coupling class, or one for the implicit class; may
+ * be NULL).  Overwrites the
+ * ensemble's current states (the next dq_run starts from dq_reset). */
+DQ_API dq_status dq_backward(dq_ctx *ctx, double *grad_sites, double *grad_classes);
+
 #ifdef __cplusplus
 }
 #endif
