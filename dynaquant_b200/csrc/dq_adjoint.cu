@@ -1,11 +1,15 @@
 // dq_adjoint.cu — gradient of a spectrum-fitting loss by the adjoint method.
 //
 // No counterpart in the reference (it computes no gradients).  Forward: the
-// ensemble step of dq_batched.cu, unchanged, with each step's state and
-// diagonal kept (or only segment starts, then recomputed).  Backward, per
-// step t from the last one down, for every trajectory at once:
+// ensemble step of dq_batched.cu, unchanged.  The states at segment starts
+// are kept; each segment is recomputed before its backward pass, and its
+// steps' Krylov bases (psi(t), r_2..r_{m+1}), Lanczos scalars and diagonals
+// stay resident in HBM while it is processed (the last segment's are kept by
+// the forward pass itself), so the backward pass never repeats the forward
+// Lanczos.  Backward, per step t from the last one down, for every
+// trajectory at once:
 //
-//   V, T_V  = Lanczos(H_t, psi(t))             (the forward step's basis)
+//   V, T_V  = the forward step's basis and tridiagonal (kept)
 //   W, T_W  = Lanczos(H_t, lambda(t+1)/|lambda|)
 //   E       = exp([[tau T_W, e1 e1^T], [0, tau T_V]])          (2m x 2m)
 //   N       = E[0:m, m:2m]    (Fréchet derivative of the exponential,
@@ -35,6 +39,10 @@ constexpr int kAdjTraj = 8;       // trajectories per CTA of the gradient kernel
 constexpr int kAdjThreads = 256;  // 32 row lanes x 8 trajectory lanes
 constexpr int kAdjMaxClasses = 8; // coupling classes with a gradient of their own
 
+// alpha (2 LB), beta (LB) and sc (LB) of one step, LB = kMaxL * B: the
+// contiguous head of a workspace's scalar block
+inline size_t scal_block(int B) { return (size_t)4 * kMaxL * B; }
+
 template <typename Real> struct R2;
 template <> struct R2<float> { using T = float2; };
 template <> struct R2<double> { using T = double2; };
@@ -49,8 +57,10 @@ struct AdjointState {
     cd* d_g = nullptr;
     cd* d_G = nullptr;
     double* d_loss = nullptr;
-    unsigned char* seg_psi = nullptr;    // K states (unnormalised, as slab 1 holds them)
-    double* seg_n2 = nullptr;            // K x B
+    // segment slots: (m+1) slabs each (psi(t) as slab 1 held it, then
+    // r_2..r_{m+1}), the step's alpha/beta/sc block and its diagonal
+    unsigned char* seg_V = nullptr;
+    double* seg_sc = nullptr;            // K x kScalBlock(B)
     unsigned char* seg_diag = nullptr;   // K diagonals
     unsigned char* ck_psi = nullptr;     // states at the starts of segments 0..n_seg-2
     double* ck_n2 = nullptr;
@@ -256,7 +266,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_grad(int n, int B, int m, i
 #pragma unroll
         for (int c = 0; c <= MM; ++c) {
             if (c <= m) {
-                const T2 v = *reinterpret_cast<const T2*>(sV + (size_t)(c + 1) * slab_reals + 2 * x);
+                const T2 v = *reinterpret_cast<const T2*>(sV + (size_t)c * slab_reals + 2 * x);
                 vr[c] = v.x;
                 vi[c] = v.y;
             } else {
@@ -374,7 +384,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_cls(int n, int B, int m, in
 #pragma unroll
                 for (int c = 0; c < MM; ++c) {
                     if (c < m) {
-                        const T2 v = *reinterpret_cast<const T2*>(sV + (size_t)(c + 1) * slab_reals + 2 * xk);
+                        const T2 v = *reinterpret_cast<const T2*>(sV + (size_t)c * slab_reals + 2 * xk);
                         rr = fma(tr[c], v.x, fma(-ti[c], v.y, rr));   // Re(t v)
                     }
                 }
@@ -440,7 +450,7 @@ __global__ void k_grad_final(int n, int G, const double* __restrict__ gsite, con
 
 static void free_adj_buffers(AdjointState* a) {
     cudaFree(a->d_target); cudaFree(a->d_spec); cudaFree(a->d_g); cudaFree(a->d_G); cudaFree(a->d_loss);
-    cudaFree(a->seg_psi); cudaFree(a->seg_n2); cudaFree(a->seg_diag);
+    cudaFree(a->seg_V); cudaFree(a->seg_sc); cudaFree(a->seg_diag);
     cudaFree(a->ck_psi); cudaFree(a->ck_n2); cudaFree(a->ck_deps);
     cudaFree(a->d_coef); cudaFree(a->d_lpart); cudaFree(a->d_gsite); cudaFree(a->d_gcpl); cudaFree(a->d_gout);
     cudaFree(a->d_erracc_save);
@@ -464,8 +474,12 @@ static cudaError_t grad_attr(int bytes) {
     return cudaFuncSetAttribute(k_adj_cls<Real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
+static unsigned char* slot_V(AdjointState* a, int m, int slot) {
+    return a->seg_V + (size_t)slot * (m + 1) * a->slab_bytes;
+}
+
 template <typename Real>
-static void launch_grad(dq_ctx* c, AdjointState* a, int t, int write_lam) {
+static void launch_grad(dq_ctx* c, AdjointState* a, int t, int slot, int write_lam) {
     BatchedState* bs = c->bat;
     const int n = c->n, B = bs->B, m = c->cfg.m, G = B / kAdjTraj;
     const size_t slab_reals = (size_t)n * B * 2;
@@ -475,7 +489,8 @@ static void launch_grad(dq_ctx* c, AdjointState* a, int t, int write_lam) {
     using T2 = typename R2<Real>::T;
 #define DQ_GRAD(MMV)                                                                                               \
     k_adj_grad<Real, MMV><<<grid, kAdjThreads, smem, c->stream>>>(                                                  \
-        n, B, m, a->rows_per_cta, G, (const Real*)bs->slabs, (Real*)a->ws2->slabs, slab_reals, (const Real*)bs->diag, \
+        n, B, m, a->rows_per_cta, G, (const Real*)slot_V(a, m, slot), (Real*)a->ws2->slabs, slab_reals,          \
+        (const Real*)(a->seg_diag + (size_t)slot * a->diag_bytes),                                                 \
         c->d_psi0, a->d_G + t, 1.0 / B, write_lam, (const T2*)a->d_coef, a->d_lpart, a->d_gsite, a->d_gcpl)
     switch (mm_bucket(m)) {
         case 8: DQ_GRAD(8); break;
@@ -486,7 +501,7 @@ static void launch_grad(dq_ctx* c, AdjointState* a, int t, int write_lam) {
 }
 
 template <typename Real>
-static void launch_cls(dq_ctx* c, AdjointState* a) {
+static void launch_cls(dq_ctx* c, AdjointState* a, int slot) {
     BatchedState* bs = c->bat;
     const int n = c->n, B = bs->B, m = c->cfg.m, G = B / kAdjTraj;
     const size_t slab_reals = (size_t)n * B * 2;
@@ -495,7 +510,8 @@ static void launch_cls(dq_ctx* c, AdjointState* a) {
     using T2 = typename R2<Real>::T;
 #define DQ_CLS(MMV)                                                                                                  \
     k_adj_cls<Real, MMV><<<grid, kAdjThreads, smem, c->stream>>>(n, B, m, a->rows_per_cta, G, a->n_cls,                \
-                                                               (const Real*)bs->slabs, (const Real*)a->ws2->slabs,    \
+                                                               (const Real*)slot_V(a, m, slot),                      \
+                                                               (const Real*)a->ws2->slabs,                           \
                                                                slab_reals, c->d_rowptr, c->d_col, a->d_cls,           \
                                                                a->d_vbase, (const T2*)a->d_coef, a->d_gcls)
     switch (mm_bucket(m)) {
@@ -529,22 +545,39 @@ static dq_status save_state(dq_ctx* c, AdjointState* a, unsigned char* psi_dst, 
     return DQ_OK;
 }
 
-// Runs steps [s0, s1) from the current ensemble state, storing each step's
-// state and diagonal in the segment buffers (slot k - s0).
+// Runs steps [s0, s1) from the current ensemble state and keeps, in slot
+// k - s0, the step's starting state, diagonal, Krylov residuals r_2..r_{m+1}
+// and Lanczos scalars.
 static dq_status run_segment(dq_ctx* c, AdjointState* a, int s0, int s1, bool record_pops) {
     BatchedState* bs = c->bat;
+    const int m = c->cfg.m;
     dq_status hook_st = DQ_OK;
     for (int k = s0; k < s1; ++k) {
         const int slot = k - s0;
-        dq_status st = save_state(c, a, a->seg_psi + (size_t)slot * a->slab_bytes, a->seg_n2 + (size_t)slot * bs->B);
-        if (st) return st;
+        unsigned char* V = slot_V(a, m, slot);
+        double* scb = a->seg_sc + (size_t)slot * scal_block(bs->B);
+        const size_t LB = (size_t)kMaxL * bs->B;
+        DQ_CU(cudaMemcpyAsync(V, (unsigned char*)bs->slabs + a->slab_bytes, a->slab_bytes, cudaMemcpyDeviceToDevice,
+                              c->stream));
+        // sc_1 = 1/|psi(k)| now; the step's combine replaces it with the next state's
+        DQ_CU(cudaMemcpyAsync(scb + 3 * LB + bs->B, bs->s.sc + bs->B, sizeof(double) * bs->B, cudaMemcpyDeviceToDevice,
+                              c->stream));
         std::function<void()> hook = [&]() {
             cudaError_t e = cudaMemcpyAsync(a->seg_diag + (size_t)slot * a->diag_bytes, bs->diag, a->diag_bytes,
                                             cudaMemcpyDeviceToDevice, c->stream);
             if (e != cudaSuccess) hook_st = check_cuda(c, e, "adjoint diagonal copy");
         };
+        dq_status st;
         if ((st = batched_step_eager(c, &hook, !record_pops))) return st;
         if (hook_st) return hook_st;
+        // the combine replaced slab 1; slabs 2..m+1 still hold this step's basis
+        DQ_CU(cudaMemcpyAsync(V + a->slab_bytes, (unsigned char*)bs->slabs + 2 * a->slab_bytes, m * a->slab_bytes,
+                              cudaMemcpyDeviceToDevice, c->stream));
+        // alpha, beta and sc_0, then sc_2.. (sc_1 was kept before the step)
+        DQ_CU(cudaMemcpyAsync(scb, bs->s.alpha, sizeof(double) * (3 * LB + bs->B), cudaMemcpyDeviceToDevice,
+                              c->stream));
+        DQ_CU(cudaMemcpyAsync(scb + 3 * LB + 2 * bs->B, bs->s.sc + 2 * bs->B, sizeof(double) * (LB - 2 * bs->B),
+                              cudaMemcpyDeviceToDevice, c->stream));
     }
     return DQ_OK;
 }
@@ -598,7 +631,7 @@ dq_status dq_adjoint_setup(dq_ctx* c, int n_steps, int fft_len, double scale, co
     a->scale = scale;
     a->slab_bytes = (size_t)n * B * 2 * rsz;
     a->diag_bytes = (size_t)n * B * rsz;
-    const size_t per_step = a->slab_bytes + a->diag_bytes + sizeof(double) * B;
+    const size_t per_step = a->slab_bytes * (m + 1) + a->diag_bytes + sizeof(double) * scal_block(B);
     const size_t per_ck = a->slab_bytes + sizeof(double) * B + sizeof(double) * (size_t)n * B;
     size_t free_b = 0, total_b = 0;
     DQ_CU(cudaMemGetInfo(&free_b, &total_b));
@@ -626,8 +659,8 @@ dq_status dq_adjoint_setup(dq_ctx* c, int n_steps, int fft_len, double scale, co
         if ((st = check_cuda(c, cudaMalloc(&a->d_g, sizeof(cd) * fft_len), "adjoint alloc"))) break;
         if ((st = check_cuda(c, cudaMalloc(&a->d_G, sizeof(cd) * fft_len), "adjoint alloc"))) break;
         if ((st = check_cuda(c, cudaMalloc(&a->d_loss, sizeof(double)), "adjoint alloc"))) break;
-        if ((st = check_cuda(c, cudaMalloc(&a->seg_psi, a->slab_bytes * K), "adjoint states"))) break;
-        if ((st = check_cuda(c, cudaMalloc(&a->seg_n2, sizeof(double) * B * K), "adjoint alloc"))) break;
+        if ((st = check_cuda(c, cudaMalloc(&a->seg_V, a->slab_bytes * (m + 1) * K), "adjoint Krylov bases"))) break;
+        if ((st = check_cuda(c, cudaMalloc(&a->seg_sc, sizeof(double) * scal_block(B) * K), "adjoint alloc"))) break;
         if ((st = check_cuda(c, cudaMalloc(&a->seg_diag, a->diag_bytes * K), "adjoint diagonals"))) break;
         if (n_seg > 1) {
             if ((st = check_cuda(c, cudaMalloc(&a->ck_psi, a->slab_bytes * (n_seg - 1)), "adjoint checkpoints"))) break;
@@ -751,29 +784,24 @@ dq_status dq_backward(dq_ctx* c, double* grad_sites, double* grad_classes) {
         }
         for (int t = s1 - 1; t >= s0; --t) {
             const int slot = t - s0;
-            DQ_CU(cudaMemcpyAsync((unsigned char*)bs->slabs + a->slab_bytes, a->seg_psi + (size_t)slot * a->slab_bytes,
-                                  a->slab_bytes, cudaMemcpyDeviceToDevice, c->stream));
-            DQ_CU(cudaMemcpyAsync(bs->s.norm2, a->seg_n2 + (size_t)slot * B, sizeof(double) * B,
-                                  cudaMemcpyDeviceToDevice, c->stream));
-            DQ_CU(cudaMemcpyAsync(bs->diag, a->seg_diag + (size_t)slot * a->diag_bytes, a->diag_bytes,
-                                  cudaMemcpyDeviceToDevice, c->stream));
             DQ_CU(cudaMemcpyAsync(w2->diag, a->seg_diag + (size_t)slot * a->diag_bytes, a->diag_bytes,
                                   cudaMemcpyDeviceToDevice, c->stream));
-            k_set_sc1<<<sc_blocks, 256, 0, c->stream>>>(B, bs->s);
-            for (int j = 1; j <= m; ++j)
-                if ((st = batched_iteration(c, bs, j))) return st;
             for (int j = 1; j <= m; ++j)
                 if ((st = batched_iteration(c, w2, j))) return st;
+            // the kept step's tridiagonal and scales, in the workspace layout
+            BatchedScalars SV = bs->s;
+            SV.alpha = a->seg_sc + (size_t)slot * scal_block(B);
+            SV.beta = SV.alpha + 2 * (size_t)kMaxL * B;
+            SV.sc = SV.beta + (size_t)kMaxL * B;
             if (bs->mixed) {
-                k_adj_small<float><<<B, 256, small_smem, c->stream>>>(m, B, c->tau_im, bs->s, w2->s,
-                                                                      (float2*)a->d_coef);
-                if (a->n_cls) launch_cls<float>(c, a);   // reads lambda(t+1) before k_adj_grad replaces it
-                launch_grad<float>(c, a, t, t > 0);
+                k_adj_small<float><<<B, 256, small_smem, c->stream>>>(m, B, c->tau_im, SV, w2->s, (float2*)a->d_coef);
+                if (a->n_cls) launch_cls<float>(c, a, slot);   // reads lambda(t+1) before k_adj_grad replaces it
+                launch_grad<float>(c, a, t, slot, t > 0);
             } else {
-                k_adj_small<double><<<B, 256, small_smem, c->stream>>>(m, B, c->tau_im, bs->s, w2->s,
+                k_adj_small<double><<<B, 256, small_smem, c->stream>>>(m, B, c->tau_im, SV, w2->s,
                                                                        (double2*)a->d_coef);
-                if (a->n_cls) launch_cls<double>(c, a);
-                launch_grad<double>(c, a, t, t > 0);
+                if (a->n_cls) launch_cls<double>(c, a, slot);
+                launch_grad<double>(c, a, t, slot, t > 0);
             }
             if (t > 0) k_lam_norm<<<sc_blocks, 256, 0, c->stream>>>(B, a->row_ctas, a->d_lpart, w2->s);
             DQ_CU(cudaGetLastError());
