@@ -192,33 +192,87 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def adjoint_leg(s, B, seed, tiling, run_ms_per_step, n_steps=16, fft_len=32):
-    """Forward (states kept) and backward pass of the spectrum-loss gradient on the same workload."""
+ADJ = dict(name="lattice64x64_B128_T2000_m16", L=64, J_nn=-250.0, J_nnn=40.0, B=128, dt=1.0, steps=2000, m=16,
+           checkpoint_every=50, fft_len=4096, sigma=200.0, tau=100.0, eps_sigma=100.0, target_shift=30.0, seed=77)
+
+
+def adjoint_leg():
+    """Spectrum-loss gradient on the 64x64 lattice (4096 site energies + 2 coupling scales, 128
+    trajectories, 2000 steps, checkpoints every 50): backward/forward time ratio in mixed precision,
+    and the FP64 gradient against central finite differences on a few parameters."""
     import torch
     import dynaquant_b200 as dq
-    w = WORKLOAD
-    p = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=n_steps)
-    p.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
-                 tiling["staged"], tiling["groups"])
-    target = np.random.default_rng(1).normal(0.0, 0.05, fft_len)
-    p.adjoint_setup(n_steps, fft_len, 1.0 / fft_len, target, checkpoint_every=n_steps)
-    p.forward()
-    p.backward()            # warm-up: attributes, first-touch of the stored states
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    loss = p.forward()
-    t1 = time.perf_counter()
-    gs, gc = p.backward()
-    t2 = time.perf_counter()
-    p.close()
-    fwd = (t1 - t0) * 1e3 / n_steps
-    bwd = (t2 - t1) * 1e3 / n_steps
-    return {"steps": n_steps, "trajectories": B, "precision": "mixed", "m": w["m"], "fft_len": fft_len,
-            "forward_ms_per_step": fwd, "backward_ms_per_step": bwd, "backward_over_forward": bwd / fwd,
-            "backward_over_graph_step": bwd / run_ms_per_step, "loss": loss,
-            "grad_finite": bool(np.isfinite(gs).all() and np.isfinite(gc).all()),
-            "note": "host wall clock around dq_forward / dq_backward (each ends in a device sync); forward "
-                    "keeps every step's state and diagonal; graph step = the timed dq_run step"}
+    from dynaquant_b200 import systems
+    a = ADJ
+    lat = systems.lattice2d(a["L"], J_nn=a["J_nn"], J_nnn=a["J_nnn"], seed=0)
+    n, T, L = lat.n, a["steps"], a["fft_len"]
+    eps = np.random.default_rng(0).normal(0.0, a["eps_sigma"], n)
+    eps_t = eps + np.random.default_rng(1).normal(0.0, a["target_shift"], n)
+
+    def make(prec, e, scales=(1.0, 1.0)):
+        p = dq.Propagator(n, m=a["m"], n_traj=a["B"], dt=a["dt"], noise=dq.NOISE_OU, seed=a["seed"],
+                          dot=dq.DOT_HERMITIAN, precision=prec, max_steps=T)
+        p.set_system(lat)
+        p.set_coupling_classes(lat.cls_off, list(scales))
+        p.set_noise_params(np.full(n, a["sigma"]), np.full(n, a["tau"]))
+        p.set_static_energies(e)
+        p.set_initial_state(lat.bright_state((1.0, 0.0, 0.0)))
+        return p
+
+    out = {"workload": a["name"], "params": n + 2, "loss": "L2 between scale*Re(IDFT_4096(Cbar)) and the same "
+           "spectrum from site energies shifted by N(0, 30 cm^-1)"}
+    for prec, tag in ((dq.PREC_MIXED, "mixed"), (dq.PREC_FP64, "fp64")):
+        p = make(prec, eps_t)
+        tiling = p.autotune(use_cache=False)
+        p.reset()
+        p.run(T)
+        target = (1.0 / T) * p.spectrum(L).real
+        p.close()
+        p = make(prec, eps)
+        p.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
+                     tiling["staged"], tiling["groups"])
+        p.adjoint_setup(T, L, 1.0 / T, target, checkpoint_every=a["checkpoint_every"])
+        p.forward()
+        p.backward()             # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss = p.forward()
+        t1 = time.perf_counter()
+        gs, gc = p.backward()
+        t2 = time.perf_counter()
+        r = {"forward_s": t1 - t0, "backward_s": t2 - t1, "backward_over_forward": (t2 - t1) / (t1 - t0),
+             "loss": loss, "grad_scales": [float(v) for v in gc]}
+        if tag == "fp64":
+            # central differences, h = 1e-3 cm^-1 on the two largest site gradients, 1e-5 on the scales
+            fd = []
+            for i in np.argsort(-np.abs(gs))[:2]:
+                e1, e2 = eps.copy(), eps.copy()
+                e1[i] += 1e-3
+                e2[i] -= 1e-3
+                p.set_static_energies(e1)
+                f1 = p.forward()
+                p.set_static_energies(e2)
+                f2 = p.forward()
+                d = (f1 - f2) / 2e-3
+                fd.append({"param": f"eps[{int(i)}]", "adjoint": float(gs[i]), "fd": d,
+                           "rel_err": abs(gs[i] - d) / abs(d)})
+            p.set_static_energies(eps)
+            for q in range(2):
+                vals = []
+                for sgn in (1, -1):
+                    sc = [1.0, 1.0]
+                    sc[q] += sgn * 1e-5
+                    p.set_coupling_classes(lat.cls_off, sc)
+                    vals.append(p.forward())
+                d = (vals[0] - vals[1]) / 2e-5
+                fd.append({"param": f"scale[{q}]", "adjoint": float(gc[q]), "fd": d, "rel_err": abs(gc[q] - d) / abs(d)})
+            r["finite_differences"] = fd
+            r["fd_max_rel_err"] = max(f["rel_err"] for f in fd)
+        p.close()
+        out[tag] = r
+    out["note"] = ("host wall clock around dq_forward / dq_backward (each ends in a device sync), after one "
+                   "warm-up pair; the backward recomputes every 50-step segment from its checkpoint")
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -315,7 +369,7 @@ def run_ours(args, rank, world, local_rank):
         pm.close()
     except Exception as e:  # pragma: no cover - reported, not hidden
         pop_err = f"unavailable: {e}"
-    adjoint = adjoint_leg(s, B, seed, tiling, ms / K)
+    adjoint = adjoint_leg()
     cpu_v, cpu_sample = cpu_baseline_sample(s, os.cpu_count() or 1)
     clocks = clk.summary()
     line = {
