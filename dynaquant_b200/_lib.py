@@ -19,7 +19,7 @@ NOISE_NONE, NOISE_GAUSS, NOISE_OU = 0, 1, 2
 DOT_BILINEAR, DOT_HERMITIAN = 0, 1
 NORM_REAL_ONLY, NORM_COMPLEX = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
-KIND_NAMES = ["noise", "spmm_alpha", "axpy_beta", "spmm_norm", "pade", "combine", "pop"]
+KIND_NAMES = ["noise", "spmm_alpha", "axpy_beta", "spmm_norm", "pade", "combine", "pop", "fused_iter"]
 
 # every symbol include/dq.h declares
 EXPORTS = [

@@ -556,6 +556,246 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
     }
 }
 
+// One whole Lanczos iteration in one kernel (staged = 2).  Produces
+//   r_j = cw w - (alpha_{j-1} sc_{j-1}) r_{j-1} - (beta_{j-2} sc_{j-2}) r_{j-2}
+// (cw = 1 when w holds sc_{j-1} H r_{j-1}, sc_{j-1} when it holds H r_{j-1})
+// from TMA-streamed boxes of w, r_{j-1} and r_{j-2} straight into a
+// shared-memory ring, writes r_j for the CTA's own rows, and gathers
+// H r_j from the ring: w_out = H r_j (unscaled) and <r_j, H r_j>, or, for the
+// last iteration (kLast), only ||H r_j||.  One pass of the chunk reductions
+// gives beta_{j-1} = ||r_j||, sc_j, alpha_j (or nav).
+//
+// The CTA owns rows [r0, r1) of one trajectory chunk.  Production blocks of
+// SR rows start at y0 = r0 - halo (halo = hb SR >= the matrix bandwidth);
+// SpMM step s (rows r0 + s SR ..) needs production blocks s .. s + 2hb, so the
+// ring holds 2hb + 1 blocks and block p = s + 2hb is produced right before
+// step s.  Input boxes run D production blocks ahead in D stages (one
+// mbarrier each, every wait bounded).  Halo rows are produced by both
+// neighbouring CTAs (identical values); each row is written and reduced by
+// its owner only.  Rows outside [0, n) arrive as zeros.
+struct FusedMaps {
+    CUtensorMap w, r1, r2;
+};
+
+template <typename Real, int TPT, int R, bool kBilinear, bool kLast>
+__global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int TC, int rows_per_cta, int hb, int D,
+                                                            int j, int w_scaled, const int* __restrict__ bptr,
+                                                            const int* __restrict__ bcol,
+                                                            const Real* __restrict__ bcoef,
+                                                            const Real* __restrict__ d, Real* __restrict__ r_out,
+                                                            Real* __restrict__ w_out, BatchedScalars S, int nch,
+                                                            const __grid_constant__ FusedMaps maps) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bars[4];
+    __shared__ double cf[kMaxTC][5];   // cw, Re/Im(alpha sc), beta sc, per trajectory of the chunk
+    const int TPR = TC / TPT;
+    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int BPS = blockDim.x / TPR;
+    const int SR = BPS * R;
+    const int W = (2 * hb + 1) * SR;                 // ring rows
+    const int halo = hb * SR;
+    const int tl = tr * TPT;
+    const int chunk = blockIdx.y;
+    const int b0 = chunk * TC + tl;
+    const int r0 = blockIdx.x * rows_per_cta;
+    const int r1 = min(n, r0 + rows_per_cta);
+    const int nsteps = r1 > r0 ? (r1 - r0 + SR - 1) / SR : 0;
+    const int NP = nsteps > 0 ? nsteps + 2 * hb : 0;  // production blocks
+    const int y0 = r0 - halo;
+    const int xc = chunk * TC * 2;
+    const bool has2 = j > 2;                          // r_{j-2} exists
+    const int nbox = has2 ? 3 : 2;
+    const size_t row_reals = (size_t)TC * 2;
+    // ring [W][TC], then D stages of 3 boxes [SR][TC], every box 128-byte aligned
+    Real* ring = reinterpret_cast<Real*>(smem_raw);
+    const size_t box_reals = (size_t)SR * row_reals;
+    const uint32_t box_bytes = (uint32_t)(box_reals * sizeof(Real));
+    const size_t stage_off = ((size_t)W * row_reals * sizeof(Real) + 127) & ~(size_t)127;
+    const size_t bstride = (((size_t)box_bytes + 127) & ~(size_t)127) / sizeof(Real);
+    Real* stage = reinterpret_cast<Real*>(smem_raw + stage_off);
+    auto ring_row = [&](int row) { return ring + (size_t)((row - y0) % W) * row_reals; };
+    auto issue = [&](int p) {
+        const int st = p % D;
+        uint64_t* bar = &bars[st];
+        Real* dst = stage + (size_t)st * 3 * bstride;
+        const int y = y0 + p * SR;
+        mbar_arrive_expect_tx(bar, box_bytes * nbox);
+        tma_load_2d(dst, &maps.w, bar, xc, y);
+        tma_load_2d(dst + bstride, &maps.r1, bar, xc, y);
+        if (has2) tma_load_2d(dst + 2 * bstride, &maps.r2, bar, xc, y);
+    };
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < D; ++q) mbar_init(&bars[q], 1);
+        fence_barrier_init();
+    }
+    for (int t = threadIdx.x; t < TC; t += blockDim.x) {
+        const int b = chunk * TC + t;
+        const size_t k1 = (size_t)(j - 1) * B + b;
+        const double s1 = S.sc[k1];
+        cf[t][0] = w_scaled ? 1.0 : s1;
+        cf[t][1] = S.alpha[2 * k1] * s1;
+        cf[t][2] = S.alpha[2 * k1 + 1] * s1;
+        cf[t][3] = has2 ? S.beta[(size_t)(j - 2) * B + b] * S.sc[(size_t)(j - 2) * B + b] : 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int p = 0; p < min(D, NP); ++p) issue(p);
+    double cw[TPT], car[TPT], cai[TPT], cb[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        cw[t] = cf[tl + t][0];
+        car[t] = cf[tl + t][1];
+        cai[t] = cf[tl + t][2];
+        cb[t] = cf[tl + t][3];
+    }
+    double nn[TPT], ar[TPT], ai[TPT], zero[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) { nn[t] = 0.0; ar[t] = 0.0; ai[t] = 0.0; zero[t] = 0.0; }
+    int issued = min(D, NP) - 1;
+    constexpr bool kPk = sizeof(Real) == 4 && R <= 3;
+    const float4* rec = reinterpret_cast<const float4*>(bcoef);
+    for (int p = 0; p < NP; ++p) {
+        const int st = p % D;
+        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
+                for (int q = p + 1; q <= issued; ++q) mbar_wait_bounded(&bars[q % D], (uint32_t)((q / D) & 1));
+            }
+            return;
+        }
+        // ---- produce r_j for rows y0 + p SR + rl R + i ----
+        {
+            const Real* sw = stage + (size_t)st * 3 * bstride;
+            const Real* s1 = sw + bstride;
+            const Real* s2 = sw + 2 * bstride;
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const int lr = rl * R + i;                // row within the block
+                const int row = y0 + p * SR + lr;
+                const size_t off = (size_t)lr * row_reals + tl * 2;
+                const CV<Real, TPT> u = ldv<Real, TPT, false>(sw + off, 0);
+                const CV<Real, TPT> x1 = ldv<Real, TPT, false>(s1 + off, 0);
+                CV<Real, TPT> x2;
+                if (has2) x2 = ldv<Real, TPT, false>(s2 + off, 0);
+                CV<Real, TPT> o;
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    const double xr = x1.v[2 * t], xi = x1.v[2 * t + 1];
+                    double rr = cw[t] * (double)u.v[2 * t] - (car[t] * xr - cai[t] * xi);
+                    double ri = cw[t] * (double)u.v[2 * t + 1] - (car[t] * xi + cai[t] * xr);
+                    if (has2) {
+                        rr -= cb[t] * (double)x2.v[2 * t];
+                        ri -= cb[t] * (double)x2.v[2 * t + 1];
+                    }
+                    o.v[2 * t] = (Real)rr;
+                    o.v[2 * t + 1] = (Real)ri;
+                }
+                stv<Real, TPT>(ring_row(row) + tl * 2, 0, o);
+                if (row >= r0 && row < r1) {
+                    stv<Real, TPT>(r_out, (size_t)row * B + b0, o);
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t)
+                        nn[t] += (double)o.v[2 * t] * o.v[2 * t] + (double)o.v[2 * t + 1] * o.v[2 * t + 1];
+                }
+            }
+        }
+        __syncthreads();   // block p is in the ring; its stage is free
+        if (threadIdx.x == 0 && p + D < NP) {
+            issue(p + D);
+            issued = p + D;
+        }
+        const int s = p - 2 * hb;
+        if (s >= 0) {
+            // ---- SpMM step s: rows a + rl R .. ----
+            const int a = r0 + s * SR;
+            const int k = a / R + rl;
+            const int row0 = k * R;
+            if (row0 < r1) {
+                CV<Real, TPT> acc[R];
+                Real dd[R][TPT];
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const int row = row0 + i;
+                    const size_t base = (size_t)min(row, n - 1) * B + b0;
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) {
+                        dd[i][t] = row < r1 ? __ldg(d + base + t) : Real(0);
+                        acc[i].v[2 * t] = 0;
+                        acc[i].v[2 * t + 1] = 0;
+                    }
+                }
+                auto gather = [&](int c) { return ldv<Real, TPT, false>(ring_row(c) + tl * 2, 0); };
+                if constexpr (kPk) {
+                    BlkPre P;
+                    blk_prefetch(P, true, k, bptr, rec);
+                    union_loop_pre<TPT, R>(P, rec, acc, gather);
+                } else {
+                    union_any<Real, TPT, R>(__ldg(bptr + k), __ldg(bptr + k + 1), bcol, bcoef, acc, gather);
+                }
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const int row = row0 + i;
+                    if (row >= r1) break;
+                    const CV<Real, TPT> x = ldv<Real, TPT, false>(ring_row(row) + tl * 2, 0);
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) {
+                        acc[i].v[2 * t] = fma(dd[i][t], x.v[2 * t], acc[i].v[2 * t]);
+                        acc[i].v[2 * t + 1] = fma(dd[i][t], x.v[2 * t + 1], acc[i].v[2 * t + 1]);
+                    }
+                    if constexpr (kLast) {
+#pragma unroll
+                        for (int t = 0; t < TPT; ++t)
+                            ar[t] += (double)acc[i].v[2 * t] * acc[i].v[2 * t] +
+                                     (double)acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
+                    } else {
+                        stv<Real, TPT>(w_out, (size_t)row * B + b0, acc[i]);
+#pragma unroll
+                        for (int t = 0; t < TPT; ++t) {
+                            const double xr = x.v[2 * t], xi = x.v[2 * t + 1];
+                            const double ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
+                            if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
+                            else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();   // step s done: the next production may overwrite block s
+    }
+    // beta_{j-1} = ||r_j||, sc_j; then alpha_j = sc_j^2 <r_j, H r_j> (or nav).
+    // The ring is free now (the loop ended on a barrier): it is the scratch.
+    __shared__ double2 red[kMaxTC];
+    double2* scratch = reinterpret_cast<double2*>(smem_raw);
+    if (chunk_reduce_s<TPT>(nn, zero, TC, S.partial, S.tickets + 5 * nch, red, chunk, scratch)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            double bt = sqrt(red[threadIdx.x].x);
+            if (!isfinite(bt)) atomicCAS(S.status, 0, DQ_ERR_NAN);
+            const size_t km = (size_t)(j - 1) * B + b;
+            const double scale = sqrt(S.alpha[2 * km] * S.alpha[2 * km] + S.alpha[2 * km + 1] * S.alpha[2 * km + 1]) +
+                                 (j > 2 ? S.beta[(size_t)(j - 2) * B + b] : 0.0);
+            if (bt <= kBreakdownRel * scale) bt = 0.0;
+            S.beta[km] = bt;
+            S.sc[(size_t)j * B + b] = bt > 0.0 ? 1.0 / bt : 0.0;
+        }
+    }
+    double* part2 = S.partial + (size_t)gridDim.y * gridDim.x * TC * 2;
+    if (chunk_reduce_s<TPT>(ar, ai, TC, part2, S.tickets + 6 * nch, red, chunk, scratch)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            const double sj = __ldcg(&S.sc[(size_t)j * B + b]);
+            const double2 v = red[threadIdx.x];
+            if constexpr (kLast) {
+                S.nav[b] = sqrt(v.x) * sj;
+            } else {
+                S.alpha[2 * ((size_t)j * B + b)] = v.x * sj * sj;
+                S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * sj * sj;
+            }
+        }
+    }
+}
+
 // r_{j+1} = w - alpha_j q_j - beta_{j-1} q_{j-1};  beta_j = ||r_{j+1}||
 template <typename Real, int TPT>
 __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, int rpc, int j,
@@ -957,32 +1197,56 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// One 2-D tensor map per slab: rows of 2B reals, boxes of SR rows x 2TC reals.
-static dq_status build_tmaps(dq_ctx* c, int tc, int sr) {
+// 2-D tensor map over one slab-shaped buffer (n rows of 2B reals), boxes of
+// sr rows x 2tc reals.
+static dq_status encode_slab_map(dq_ctx* c, void* base, int tc, int sr, CUtensorMap* map) {
     BatchedState* bs = c->bat;
     auto enc = tensor_map_encoder();
     if (!enc) {
         c->err = "cuTensorMapEncodeTiled unavailable";
         return DQ_ERR_CUDA;
     }
-    const int n = c->n, B = bs->B, m = c->cfg.m;
+    const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
+    cuuint64_t dims[2] = {(cuuint64_t)(2 * bs->B), (cuuint64_t)c->n};
+    cuuint64_t strides[1] = {(cuuint64_t)(2 * bs->B * rsz)};
+    cuuint32_t box[2] = {(cuuint32_t)(2 * tc), (cuuint32_t)sr};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, bs->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        c->err = "cuTensorMapEncodeTiled failed";
+        return DQ_ERR_CUDA;
+    }
+    return DQ_OK;
+}
+
+// One tensor map per slab (window SpMM).
+static dq_status build_tmaps(dq_ctx* c, int tc, int sr) {
+    BatchedState* bs = c->bat;
+    const int m = c->cfg.m;
     const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
     bs->tmaps.assign(m + 2, CUtensorMap{});
     for (int j = 0; j <= m + 1; ++j) {
-        void* base = (char*)bs->slabs + (size_t)j * n * B * 2 * rsz;
-        cuuint64_t dims[2] = {(cuuint64_t)(2 * B), (cuuint64_t)n};
-        cuuint64_t strides[1] = {(cuuint64_t)(2 * B * rsz)};
-        cuuint32_t box[2] = {(cuuint32_t)(2 * tc), (cuuint32_t)sr};
-        cuuint32_t estr[2] = {1, 1};
-        CUresult r = enc(&bs->tmaps[j], bs->mixed ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                         2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) {
-            c->err = "cuTensorMapEncodeTiled failed";
-            return DQ_ERR_CUDA;
-        }
+        dq_status st = encode_slab_map(c, (char*)bs->slabs + (size_t)j * c->n * bs->B * 2 * rsz, tc, sr, &bs->tmaps[j]);
+        if (st) return st;
     }
     return DQ_OK;
+}
+
+// Fused iteration: maps of slabs 0..m (w and the residuals it reads) and of wB.
+static dq_status build_fmaps(dq_ctx* c, int tc, int sr) {
+    BatchedState* bs = c->bat;
+    const int m = c->cfg.m;
+    const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
+    const size_t slab = (size_t)c->n * bs->B * 2 * rsz;
+    if (!bs->wB) DQ_CU(cudaMalloc(&bs->wB, slab));
+    bs->fmaps.assign(m + 2, CUtensorMap{});
+    for (int j = 0; j <= m; ++j) {
+        dq_status st = encode_slab_map(c, (char*)bs->slabs + (size_t)j * slab, tc, sr, &bs->fmaps[j]);
+        if (st) return st;
+    }
+    return encode_slab_map(c, bs->wB, tc, sr, &bs->fmaps[m + 1]);
 }
 
 template <typename Real, int TPT, int R>
@@ -1010,6 +1274,42 @@ static cudaError_t win_attr_r(int R, int bytes) {
 
 constexpr size_t kWinSmemMax = 200 * 1024;
 
+template <typename Real, int TPT, int R>
+static cudaError_t fused_attr(int bytes) {
+    cudaError_t e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, false, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, true, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, true, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
+
+template <typename Real, int TPT>
+static cudaError_t fused_attr_r(int R, int bytes) {
+    switch (R) {
+        case 1: return fused_attr<Real, TPT, 1>(bytes);
+        case 2: return fused_attr<Real, TPT, 2>(bytes);
+        case 3: return sizeof(Real) == 4 ? fused_attr<Real, TPT, 3>(bytes) : cudaErrorInvalidValue;
+        case 4: return fused_attr<Real, TPT, 4>(bytes);
+        default: return fused_attr<Real, TPT, 8>(bytes);
+    }
+}
+
+// Shared memory of the fused iteration: ring of (2hb+1) SR rows, D stages of
+// three 128-byte-aligned boxes of SR rows.
+static size_t fused_smem(int tc, int sr, int hb, int D, size_t rsz) {
+    const size_t row = (size_t)tc * 2 * rsz;
+    const size_t ring = (((size_t)(2 * hb + 1) * sr * row) + 127) & ~(size_t)127;
+    const size_t box = ((size_t)sr * row + 127) & ~(size_t)127;
+    return ring + (size_t)D * 3 * box;
+}
+
 // Tiling: TC trajectories per chunk, TPT per thread, ~ctas_per_sm CTAs per
 // SM, R rows per SpMM block, staged: TMA shared-memory window SpMM.
 dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R, int staged, int groups) {
@@ -1019,7 +1319,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
-    if (staged != 0 && staged != 1) return DQ_ERR_ARG;
+    if (staged < 0 || staged > 2) return DQ_ERR_ARG;
     const int ri = r_index(R);
     if (ri < 0) return DQ_ERR_ARG;
     const int chunks = B / tc;
@@ -1044,7 +1344,44 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     }
     int halo = 0, wmask = 0, rpc_win = 0, gxw = 0;
     size_t smem = 0;
-    if (staged) {
+    int f_sr = 0, f_hb = 0, f_D = 0, f_rpc = 0, f_gx = 0;
+    size_t f_smem = 0;
+    if (staged == 2) {
+        // fused iteration: one launch covers every chunk, no trajectory groups
+        const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
+        const int SR = RPC * R;
+        if (groups != 1 || c->cfg.m < 2 || SR > 256 || 2 * tc > 256 || (tc * 2 * rsz) % 16) return DQ_ERR_ARG;
+        f_sr = SR;
+        f_hb = (bs->bw + SR - 1) / SR;
+        // static shared memory (coefficient table, reduction slots, barriers)
+        // plus the 1 KB the SM reserves per CTA; the per-SM pool is 228 KB
+        constexpr size_t kStatic = 6 * 1024;
+        f_D = 0;
+        for (int D = 4; D >= 2; --D) {
+            const size_t sm = fused_smem(tc, SR, f_hb, D, rsz);
+            if (sm <= kWinSmemMax && (size_t)ctas_per_sm * (sm + kStatic) <= 228 * 1024) {
+                f_D = D;
+                f_smem = sm;
+                break;
+            }
+        }
+        if (!f_D) return DQ_ERR_ARG;
+        f_gx = std::max(1, (bs->sms * ctas_per_sm) / chunks);
+        f_rpc = (n + f_gx - 1) / f_gx;
+        f_rpc = ((f_rpc + SR - 1) / SR) * SR;
+        f_gx = (n + f_rpc - 1) / f_rpc;
+        if (f_gx > kMaxCtasPerChunk || (size_t)f_gx * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
+        cudaError_t e = bs->mixed ? (tpt == 2 ? fused_attr_r<float, 2>(R, (int)f_smem)
+                                              : fused_attr_r<float, 1>(R, (int)f_smem))
+                                  : fused_attr_r<double, 1>(R, (int)f_smem);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return DQ_ERR_ARG;
+        }
+        dq_status st = build_fmaps(c, tc, SR);
+        if (st) return st;
+    }
+    if (staged == 1) {
         const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
         const int SR = RPC * R;
         // boxes of SR rows tile the power-of-two ring without wrapping
@@ -1083,6 +1420,12 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     bs->rpc_win = rpc_win;
     bs->gxw = gxw;
     bs->win_smem = smem;
+    bs->f_sr = f_sr;
+    bs->f_hb = f_hb;
+    bs->f_D = f_D;
+    bs->f_rpc = f_rpc;
+    bs->f_gx = f_gx;
+    bs->f_smem = f_smem;
     drop_graph(bs);
     return DQ_OK;
 }
@@ -1117,8 +1460,17 @@ dq_status batched_mirror_tiling(dq_ctx* c, BatchedState* dst) {
     dst->ctas_per_sm = src->ctas_per_sm; dst->R = src->R; dst->gxs = src->gxs; dst->bpc = src->bpc;
     dst->staged = src->staged; dst->groups = src->groups; dst->halo = src->halo; dst->wmask = src->wmask;
     dst->rpc_win = src->rpc_win; dst->gxw = src->gxw; dst->bw = src->bw; dst->win_smem = src->win_smem;
+    dst->f_sr = src->f_sr; dst->f_hb = src->f_hb; dst->f_D = src->f_D; dst->f_rpc = src->f_rpc;
+    dst->f_gx = src->f_gx; dst->f_smem = src->f_smem;
     dst->tmaps.clear();
-    if (src->staged) {
+    dst->fmaps.clear();
+    if (src->staged == 2) {
+        c->bat = dst;
+        dq_status st = build_fmaps(c, src->TC, src->f_sr);
+        c->bat = src;
+        if (st) return st;
+    }
+    if (src->staged == 1) {
         const int SR = (kBThreads / (src->TC / src->TPT)) * src->R;
         c->bat = dst;
         dq_status st = build_tmaps(c, src->TC, SR);
@@ -1210,6 +1562,7 @@ void batched_free_ws(BatchedState* bs) {
     drop_graph(bs);
     if (!bs->fmt_borrowed)
         for (auto& f : bs->fmt) free_fmt(f);
+    cudaFree(bs->wB);
     cudaFree(bs->slabs); cudaFree(bs->diag); cudaFree(bs->eps); cudaFree(bs->deps);
     cudaFree(bs->scal_mem); cudaFree(bs->s.tickets); cudaFree(bs->s.status);
     delete bs;
@@ -1268,7 +1621,7 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w, int cy0, int 
     const int n = c->n, B = bs->B, TC = bs->TC;
     const Real* cf = (const Real*)f.bcoef;
     const Real* d = (const Real*)bs->diag;
-    if (bs->staged) {
+    if (bs->staged == 1) {
         const dim3 grid(bs->gxw, ncy);
         const CUtensorMap& tm = bs->tmaps[j];
 #define DQ_WIN_R(RR)                                                                                       \
@@ -1299,6 +1652,43 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w, int cy0, int 
 #undef DQ_SPMM_R
 }
 
+// Fused iteration producing r_j (2 <= j <= m+1; j = m+1 is the last one,
+// which also gives ||H q_{m+1}||).  w ping-pongs between slab 0 and wB:
+// the SpMM of r_j writes wB for even j and slab 0 for odd j.
+template <typename Real, int TPT, bool kBil, bool kLast>
+static void launch_fused(dq_ctx* c, int j) {
+    BatchedState* bs = c->bat;
+    const BlockFmt& f = bs->fmt[r_index(bs->R)];
+    const int n = c->n, B = bs->B, m = c->cfg.m;
+    const size_t se = (size_t)n * B;
+    Real* slabs = (Real*)bs->slabs;
+    FusedMaps maps;
+    maps.w = (j % 2 == 0) ? bs->fmaps[0] : bs->fmaps[m + 1];
+    maps.r1 = bs->fmaps[j - 1];
+    maps.r2 = bs->fmaps[j >= 3 ? j - 2 : j - 1];
+    Real* r_out = slabs + 2 * se * j;
+    Real* w_out = kLast ? nullptr : ((j % 2 == 0) ? (Real*)bs->wB : slabs);
+    const dim3 grid(bs->f_gx, bs->chunks);
+#define DQ_FUSED_R(RR)                                                                                           \
+    k_lanczos_fused<Real, TPT, RR, kBil, kLast><<<grid, kBThreads, bs->f_smem, c->stream>>>(                      \
+        n, B, bs->TC, bs->f_rpc, bs->f_hb, bs->f_D, j, j == 2, f.bptr, f.bcol, (const Real*)f.bcoef,             \
+        (const Real*)bs->diag, r_out, w_out, bs->s, bs->chunks, maps)
+    switch (bs->R) {
+        case 1: DQ_FUSED_R(1); break;
+        case 2: DQ_FUSED_R(2); break;
+        case 3: if constexpr (sizeof(Real) == 4) DQ_FUSED_R(3); break;
+        case 4: DQ_FUSED_R(4); break;
+        default: DQ_FUSED_R(8); break;
+    }
+#undef DQ_FUSED_R
+}
+
+template <typename Real, int TPT, bool kLast>
+static void launch_fused_any(dq_ctx* c, int j) {
+    if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_fused<Real, TPT, true, kLast>(c, j);
+    else launch_fused<Real, TPT, false, kLast>(c, j);
+}
+
 template <typename Real, int TPT>
 static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int ncy) {
     BatchedState* bs = c->bat;
@@ -1308,9 +1698,27 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
     Real* slabs = (Real*)bs->slabs;
     auto slab = [&](int k) { return slabs + 2 * se * k; };
     const dim3 grid(bs->gx, ncy);
+    if (bs->staged == 2 && j >= 2) {
+        // iteration j of the fused form produces r_j; the last one also r_{m+1}
+        if (tm) tm->mark(DQ_KIND_FUSED, st);
+        launch_fused_any<Real, TPT, false>(c, j);
+        if (j == c->cfg.m) {
+            if (tm) tm->mark(DQ_KIND_FUSED, st);
+            launch_fused_any<Real, TPT, true>(c, j + 1);
+        }
+        return DQ_OK;
+    }
     if (tm) tm->mark(DQ_KIND_SPMM, st);
     if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_spmm<Real, TPT, true, true>(c, j, slab(j), slab(0), cy0, ncy);
     else launch_spmm<Real, TPT, false, true>(c, j, slab(j), slab(0), cy0, ncy);
+    if (bs->staged == 2) {
+        // fused form: the first SpMM only; r_2 comes from the next fused launch
+        if (j == c->cfg.m) {
+            if (tm) tm->mark(DQ_KIND_FUSED, st);
+            launch_fused_any<Real, TPT, true>(c, j + 1);
+        }
+        return DQ_OK;
+    }
     if (tm) tm->mark(DQ_KIND_AXPY, st);
     k_axpy_beta<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slab(0), slab(j), slab(j - 1),
                                                        slab(j + 1), bs->s, cy0, bs->chunks);
@@ -1346,8 +1754,10 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
     const int cpg = bs->chunks / bs->groups;
     for (int g = 0; g < bs->groups; ++g) {
         for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm, g * cpg, cpg);
-        mark(DQ_KIND_SPMM_NORM);
-        launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, g * cpg, cpg);
+        if (bs->staged != 2) {   // the fused form's last launch already gave ||H q_{m+1}||
+            mark(DQ_KIND_SPMM_NORM);
+            launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, g * cpg, cpg);
+        }
     }
     mark(DQ_KIND_PADE);
     k_pade_b<<<B, 128, pade_smem_bytes(m + 2), st>>>(m, B, c->tau_im, c->cfg.norm_mode, bs->s, c->d_erracc);
@@ -1434,13 +1844,33 @@ dq_status batched_profile(dq_ctx* c, int n_steps, double* ms, int* cnt, int nk) 
 
 // Mean device time of one Lanczos iteration (SpMM + axpy) under the current
 // tiling: reps launches of iteration 1 between two events.
+static void fused_iteration_any(dq_ctx* c, int j) {
+    BatchedState* bs = c->bat;
+    if (!bs->mixed) launch_fused_any<double, 1, false>(c, j);
+    else if (bs->TPT == 2) launch_fused_any<float, 2, false>(c, j);
+    else launch_fused_any<float, 1, false>(c, j);
+}
+
+// Device time of one Lanczos iteration: SpMM + axpy of iteration 1, or, in
+// the fused form, one fused launch of iteration min(3, m) (after iterations
+// 1 and 2 have filled its inputs).
 dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
     cudaEvent_t e0, e1;
     DQ_CU(cudaEventCreate(&e0));
     DQ_CU(cudaEventCreate(&e1));
-    enqueue_iteration_any(c, 1);   // warm-up
+    const bool fused = c->bat->staged == 2;
+    const int jt = std::min(3, c->cfg.m);
+    auto one = [&]() {
+        if (fused) fused_iteration_any(c, jt);
+        else enqueue_iteration_any(c, 1);
+    };
+    if (fused) {
+        enqueue_iteration_any(c, 1);
+        if (jt == 3) fused_iteration_any(c, 2);
+    }
+    one();   // warm-up
     DQ_CU(cudaEventRecord(e0, c->stream));
-    for (int r = 0; r < reps; ++r) enqueue_iteration_any(c, 1);
+    for (int r = 0; r < reps; ++r) one();
     DQ_CU(cudaEventRecord(e1, c->stream));
     DQ_CU(cudaEventSynchronize(e1));
     float t = 0.f;

@@ -125,6 +125,12 @@ struct dq::BatchedState {
     int halo = 0, wmask = 0, rpc_win = 0, gxw = 0, bw = 0;   // window geometry, matrix bandwidth
     size_t win_smem = 0;
     std::vector<CUtensorMap> tmaps;       // one per slab (window variant)
+    // fused iteration (staged = 2): second SpMM output buffer, tensor maps of
+    // slabs 0..m and of wB (boxes of f_sr rows), halo blocks, stages, grid
+    void* wB = nullptr;
+    std::vector<CUtensorMap> fmaps;
+    int f_sr = 0, f_hb = 0, f_D = 2, f_rpc = 0, f_gx = 0;
+    size_t f_smem = 0;
     ::BlockFmt fmt[5];                    // R = 1, 2, 3, 4, 8 (built on demand)
     bool fmt_borrowed = false;            // fmt belongs to another workspace
     int sms = 148;
@@ -150,10 +156,12 @@ namespace dq {
 // partial[chunk][blockIdx.x][TC]; the last block of the chunk sums the
 // gridDim.x partials in block order.  Returns true in that block, with the
 // chunk's totals in red_out[0..TC).
+// chunk_reduce_s takes its shared scratch (kBThreads * 2 double2) from the
+// caller; chunk_reduce declares it.
 template <int TPT>
-__device__ __forceinline__ bool chunk_reduce(const double (&ar)[TPT], const double (&ai)[TPT], int TC,
-                                             double* partial, unsigned int* ticket, double2* red_out, int chunk) {
-    __shared__ double2 sm[kBThreads * 2];
+__device__ __forceinline__ bool chunk_reduce_s(const double (&ar)[TPT], const double (&ai)[TPT], int TC,
+                                               double* partial, unsigned int* ticket, double2* red_out, int chunk,
+                                               double2* sm) {
     const int TPR = TC / TPT;
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int RPC = blockDim.x / TPR;
@@ -201,6 +209,13 @@ __device__ __forceinline__ bool chunk_reduce(const double (&ar)[TPT], const doub
         __syncthreads();
     }
     return last;
+}
+
+template <int TPT>
+__device__ __forceinline__ bool chunk_reduce(const double (&ar)[TPT], const double (&ai)[TPT], int TC,
+                                             double* partial, unsigned int* ticket, double2* red_out, int chunk) {
+    __shared__ double2 sm[kBThreads * 2];
+    return chunk_reduce_s<TPT>(ar, ai, TC, partial, ticket, red_out, chunk, sm);
 }
 
 }  // namespace dq

@@ -169,7 +169,9 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * rows computed together by the SpMM over the union of their neighbour
  * columns.  staged = 1 stages the gathered trajectory rows in a shared-memory
  * window filled by TMA (needs the matrix bandwidth to fit the window; the
- * call fails otherwise), 0 gathers through L1.  groups splits the
+ * call fails otherwise), 0 gathers through L1, 2 runs each Lanczos iteration
+ * as one fused kernel (TMA-streamed w, r_j, r_{j-1}; r_{j+1} formed in a
+ * shared-memory ring and gathered from there; groups must be 1).  groups splits the
  * trajectory chunks into groups whose m Lanczos iterations run one group
  * after another, so a group's Krylov slabs stay resident in L2 (must divide
  * n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run
@@ -195,7 +197,8 @@ enum {
     DQ_KIND_PADE = 4,       /* batched Padé exponential */
     DQ_KIND_COMBINE = 5,    /* psi = V y, norms, correlation */
     DQ_KIND_POP = 6,        /* population record */
-    DQ_KIND_COUNT = 7
+    DQ_KIND_FUSED = 7,      /* fused iteration: r_j, SpMM H r_j, beta_{j-1}, alpha_j (staged = 2) */
+    DQ_KIND_COUNT = 8
 };
 /* Advances all trajectories by n_steps exactly like dq_run, but launches the
  * step's kernels eagerly with CUDA events between them; ms_per_launch[k]

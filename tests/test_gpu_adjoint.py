@@ -49,11 +49,13 @@ def _oracle(oracle, s, eps0, psi0, target, scale_c=1.0, noise=True):
                                 target, seed=SEED, **kw)
 
 
-@pytest.mark.parametrize("noise", [True, False])
-def test_adjoint_fp64_matches_oracle(oracle, noise):
+@pytest.mark.parametrize("noise,tiling", [(True, None), (False, None), (True, (8, 1, 2, 2, 2, 1))])
+def test_adjoint_fp64_matches_oracle(oracle, noise, tiling):
     import dynaquant_b200 as dq
     s, eps0, psi0, target = _problem()
     p = _prop(dq.PREC_FP64, s, eps0, psi0, target, noise=noise)
+    if tiling:   # one-kernel Lanczos iterations in both the forward and the adjoint Lanczos
+        p.set_tiling(*tiling)
     loss = p.forward()
     gs, gc = p.backward()
     lo, go = _oracle(oracle, s, eps0, psi0, target, noise=noise)

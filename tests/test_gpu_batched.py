@@ -46,6 +46,22 @@ def test_batched_fp64_matches_golden(tag, dot):
     p.close()
 
 
+@pytest.mark.parametrize("tag,dot", [("herm", 1), ("bil", 0)])
+@pytest.mark.parametrize("R", [1, 2, 4])
+def test_fused_iteration_fp64_matches_golden(tag, dot, R):
+    """One-kernel Lanczos iterations (staged = 2) in complex128 reproduce the golden run."""
+    import dynaquant_b200 as dq
+    g = _golden()
+    p = _chain_prop(dq.PREC_FP64, dot)
+    p.set_tiling(4, 1, 1, R, 2, 1)
+    assert p.get_tiling() == (4, 1, 1, R, 2, 1)
+    p.run(G.CHAIN["n_steps"])
+    assert np.abs(p.populations() - g[f"{tag}_pops"]).max() < POP_TOL_FP64
+    assert np.abs(p.correlation() - g[f"{tag}_corr"]).max() < POP_TOL_FP64
+    assert np.allclose(p.error_accum(), g[f"{tag}_err"], rtol=1e-3, atol=1e-14)
+    p.close()
+
+
 def test_batched_fp64_incremental_equals_single_call():
     import dynaquant_b200 as dq
     g = _golden()
@@ -116,7 +132,8 @@ def test_spectrum_matches_numpy():
 
 @pytest.mark.parametrize("tiling", [(2, 2, 1, 1, 0, 1), (4, 1, 2, 2, 0, 1), (4, 2, 8, 4, 0, 1), (2, 1, 4, 8, 0, 2),
                                     (4, 2, 2, 8, 0, 1), (4, 2, 1, 1, 1, 1), (2, 2, 2, 1, 1, 2), (4, 1, 1, 4, 1, 1),
-                                    (1, 1, 2, 4, 0, 4)])
+                                    (1, 1, 2, 4, 0, 4), (4, 2, 1, 2, 2, 1), (2, 2, 2, 1, 2, 1), (4, 1, 2, 1, 2, 1),
+                                    (4, 1, 1, 3, 2, 1)])
 def test_every_tiling_matches_oracle(tiling):
     """Tilings only change the schedule: each must reproduce the oracle."""
     import dynaquant_b200 as dq
@@ -171,4 +188,31 @@ def test_tube_tilings_match_oracle(oracle, R, staged, groups):
     p.set_tiling(16, 2, 2, R, staged, groups)
     p.run(T)
     assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
+    p.close()
+
+
+@pytest.mark.parametrize("tiling", [(16, 2, 2, 1, 2, 1), (16, 2, 2, 2, 2, 1), (16, 2, 2, 3, 2, 1), (16, 2, 1, 4, 2, 1),
+                                    (32, 2, 1, 2, 2, 1)])
+def test_tube_fused_iterations_match_oracle(oracle, tiling):
+    """One-kernel Lanczos iterations (staged = 2) on the dipole tube: r_{j+1} formed from TMA-streamed
+    boxes in a shared-memory ring whose halo covers the ~3-ring coupling reach."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 40)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=12, dt=0.5, dot_mode=1, noise=2, sigma=250.0, tau=50.0,
+                      sigma_static=150.0, seed=4)
+    B, T = 32, 12
+    psi0 = s.bright_state()
+    ref = S.run(B, T, psi0, pop_every=4, threads=4)
+    p = dq.Propagator(s.n, m=12, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=4, dot=1,
+                      pop_every=4, max_steps=T, precision=dq.PREC_MIXED)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    p.set_initial_state(psi0)
+    p.set_tiling(*tiling)
+    assert p.get_tiling() == tiling
+    p.run(T)
+    assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
+    assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
     p.close()
