@@ -311,8 +311,8 @@ __device__ __forceinline__ void union_any(int pb, int pe, const int* __restrict_
 
 // Row-blocked SpMM: w = H q_j for all trajectories of the chunk, R rows per
 // block.  kWrite: also alpha_j[b] = <q_j, w>_b; !kWrite: ||H q_j||_b only.
-template <typename Real, int TPT, int R, bool kBilinear, bool kWrite>
-__global__ void __launch_bounds__(kBThreads) k_spmm_blk(int n, int B, int TC, int bpc, int nb, int j,
+template <typename Real, int TPT, int R, bool kBilinear, bool kWrite, int NT = kBThreads>
+__global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, int nb, int j,
                                                        const int* __restrict__ bptr, const int* __restrict__ bcol,
                                                        const Real* __restrict__ bcoef, const Real* __restrict__ d,
                                                        const Real* __restrict__ rj, Real* __restrict__ w,
@@ -392,7 +392,8 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_blk(int n, int B, int TC, in
         }
     }
     __shared__ double2 red[kMaxTC];
-    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk)) {
+    __shared__ double2 rscratch[NT * 2];
+    if (chunk_reduce_s<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk, rscratch)) {
         if (threadIdx.x < TC) {
             const int b = chunk * TC + threadIdx.x;
             const double s = S.sc[(size_t)j * B + b];
@@ -402,6 +403,350 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_blk(int n, int B, int TC, in
                 S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s * s;
             } else {
                 S.nav[b] = sqrt(v.x) * s;
+            }
+        }
+    }
+}
+
+// Warp-per-block SpMM (staged = 3; complex64, packed records, R <= 3).  All
+// 32 lanes of a warp work on one block of R rows for TC = 32 TPT
+// trajectories, so the block's column-union records are one warp-uniform
+// stream: the warp fetches 32 records at a time with one coalesced 16-byte
+// load per lane (the next batch, or the next block's first one, in flight
+// while the current batch is used) and keeps them in a per-warp shared
+// buffer that every lane reads back by broadcast.  The next block's header
+// is fetched one block ahead, its own rows and diagonal at its start, so no
+// index load sits on the gathers' dependency chain.
+template <int TPT, int R, bool kBilinear, bool kWrite>
+__global__ void __launch_bounds__(kBThreads) k_spmm_warp(int n, int B, int bpc, int nb, int j,
+                                                        const int* __restrict__ bptr,
+                                                        const float4* __restrict__ rec,
+                                                        const float* __restrict__ d, const float* __restrict__ rj,
+                                                        float* __restrict__ w, BatchedScalars S, int cy0, int nch) {
+    constexpr int TC = 32 * TPT;
+    constexpr int kWarps = kBThreads / 32;
+    __shared__ float4 rbuf[kWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int chunk = blockIdx.y + cy0;
+    const int b0 = chunk * TC + lane * TPT;
+    const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
+    double sc[TPT], ar[TPT], ai[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        sc[t] = S.sc[(size_t)j * B + b0 + t];
+        ar[t] = 0.0;
+        ai[t] = 0.0;
+    }
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    int k = k0 + warp;
+    int pb = 0, pe = 0;
+    if (k < k1) {
+        pb = __ldg(bptr + k);
+        pe = __ldg(bptr + k + 1);
+    }
+    float4 nxt = (k < k1 && lane < pe - pb) ? __ldg(rec + pb + lane) : zero4;
+    while (k < k1) {
+        const int kn = k + kWarps;
+        int pbn = 0, pen = 0;
+        if (kn < k1) {
+            pbn = __ldg(bptr + kn);
+            pen = __ldg(bptr + kn + 1);
+        }
+        const int row0 = k * R;
+        CV<float, TPT> acc[R], xo[R];
+        float dd[R][TPT];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const size_t base = (size_t)min(row0 + i, n - 1) * B + b0;
+            xo[i] = ldv<float, TPT, true>(rj, base);
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                dd[i][t] = row0 + i < n ? __ldg(d + base + t) : 0.f;
+                acc[i].v[2 * t] = 0.f;
+                acc[i].v[2 * t + 1] = 0.f;
+            }
+        }
+        for (int e0 = pb; e0 < pe; e0 += 32) {
+            __syncwarp();
+            rbuf[warp][lane] = nxt;
+            __syncwarp();
+            if (e0 + 32 < pe) nxt = (e0 + 32 + lane < pe) ? __ldg(rec + e0 + 32 + lane) : zero4;
+            else nxt = (kn < k1 && lane < pen - pbn) ? __ldg(rec + pbn + lane) : zero4;
+            const int cnt = min(32, pe - e0);   // a multiple of 4
+            for (int e = 0; e < cnt; e += 4) {
+                float4 r[4];
+                CV<float, TPT> y[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) r[q] = rbuf[warp][e + q];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) y[q] = ldv<float, TPT, true>(rj, (size_t)__float_as_int(r[q].x) * B + b0);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    cfma<float, TPT>(acc[0], r[q].y, y[q]);
+                    if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], r[q].z, y[q]);
+                    if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], r[q].w, y[q]);
+                }
+            }
+        }
+        if (pe <= pb) nxt = (kn < k1 && lane < pen - pbn) ? __ldg(rec + pbn + lane) : zero4;
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int row = row0 + i;
+            if (row >= n) break;
+            const size_t base = (size_t)row * B + b0;
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                acc[i].v[2 * t] = fmaf(dd[i][t], xo[i].v[2 * t], acc[i].v[2 * t]);
+                acc[i].v[2 * t + 1] = fmaf(dd[i][t], xo[i].v[2 * t + 1], acc[i].v[2 * t + 1]);
+            }
+            if (kWrite) {
+                CV<float, TPT> o;
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    o.v[2 * t] = (float)(sc[t] * (double)acc[i].v[2 * t]);
+                    o.v[2 * t + 1] = (float)(sc[t] * (double)acc[i].v[2 * t + 1]);
+                    const double xr = xo[i].v[2 * t], xi = xo[i].v[2 * t + 1];
+                    const double ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
+                    if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
+                    else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+                }
+                stv<float, TPT>(w, base, o);
+            } else {
+#pragma unroll
+                for (int t = 0; t < TPT; ++t)
+                    ar[t] += (double)acc[i].v[2 * t] * acc[i].v[2 * t] + (double)acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
+            }
+        }
+        k = kn;
+        pb = pbn;
+        pe = pen;
+    }
+    __shared__ double2 red[kMaxTC];
+    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            const double s2 = S.sc[(size_t)j * B + b];
+            const double2 v = red[threadIdx.x];
+            if (kWrite) {
+                S.alpha[2 * ((size_t)j * B + b)] = v.x * s2 * s2;
+                S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s2 * s2;
+            } else {
+                S.nav[b] = sqrt(v.x) * s2;
+            }
+        }
+    }
+}
+
+// SpMM over a TMA-fed shared-memory ring (staged = 6; complex64, packed
+// records, R <= 3, TC = 32 trajectories, 2 per lane; one 512-thread CTA per
+// SM).  The CTA owns rows [r0, r1) of one chunk.  Ring block b holds rows
+// y0 + b SR .. (y0 = r0 - halo, SR = 16 R rows: one block of R rows per
+// warp per step); the ring has NB = 2hb + D + 1 blocks, so while step s
+// gathers from blocks s .. s + 2hb the boxes of the next D blocks are in
+// flight, and block s + NB is issued into block s's place once step s is
+// done.  Warp w owns row block (r0 + s SR)/R + w: its records arrive 32 at a
+// time (one coalesced 16-byte load per lane, the next batch in flight) into
+// a per-warp buffer; lanes 0-15 take the even records and lanes 16-31 the
+// odd ones of every batch for the same 32 trajectories, and one shuffle
+// adds the halves.  Every gather is a 16-byte shared load; no global load
+// sits on the gathers' dependency chain.  Each mbarrier wait is bounded.
+constexpr int kRingThreads = 512;
+
+template <int R, bool kBilinear, bool kWrite>
+__global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int rows_per_cta, int hb, int D, int j,
+                                                              const int* __restrict__ bptr,
+                                                              const float4* __restrict__ rec,
+                                                              const float* __restrict__ d, float* __restrict__ w,
+                                                              BatchedScalars S, int nch,
+                                                              const __grid_constant__ CUtensorMap tmap) {
+    constexpr int TPT = 2, TC = 32;
+    constexpr int kWarps = kRingThreads / 32;
+    constexpr int SR = kWarps * R;
+    constexpr size_t row_reals = TC * 2;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bars[32];
+    __shared__ float4 rbuf[kWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int half = lane >> 4, hl = lane & 15;
+    const int NB = 2 * hb + D + 1;
+    const int W = NB * SR;
+    const int halo = hb * SR;
+    const int chunk = blockIdx.y;
+    const int b0 = chunk * TC + hl * TPT;
+    const int r0 = blockIdx.x * rows_per_cta;
+    const int r1 = min(n, r0 + rows_per_cta);
+    const int nsteps = r1 > r0 ? (r1 - r0 + SR - 1) / SR : 0;
+    const int nbox = nsteps > 0 ? nsteps + 2 * hb : 0;
+    const int y0 = r0 - halo;
+    const int xc = chunk * TC * 2;
+    float* ring = reinterpret_cast<float*>(smem_raw);
+    const uint32_t box_bytes = (uint32_t)(SR * row_reals * sizeof(float));
+    auto issue = [&](int b) {
+        uint64_t* bar = &bars[b % NB];
+        mbar_arrive_expect_tx(bar, box_bytes);
+        tma_load_2d(ring + (size_t)(b % NB) * SR * row_reals, &tmap, bar, xc, y0 + b * SR);
+    };
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < NB; ++q) mbar_init(&bars[q], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int b = 0; b < min(NB, nbox); ++b) issue(b);
+    int issued = min(NB, nbox) - 1;
+    double sc[TPT], ar[TPT], ai[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        sc[t] = S.sc[(size_t)j * B + b0 + t];
+        ar[t] = 0.0;
+        ai[t] = 0.0;
+    }
+    // records past a block's end read as its first row with zero
+    // coefficients, so every slot of a batch is a valid gather
+    auto pad = [](int blk) { return make_float4(__int_as_float(blk * R), 0.f, 0.f, 0.f); };
+    // this warp's block of step 0, its header and first record batch
+    int k = r0 / R + warp;
+    int pb = 0, pe = 0;
+    if (nsteps > 0 && k * R < r1) {
+        pb = __ldg(bptr + k);
+        pe = __ldg(bptr + k + 1);
+    }
+    float4 nxt = lane < pe - pb ? __ldg(rec + pb + lane) : pad(k);
+    for (int s = 0; s < nsteps; ++s) {
+        const int row0 = k * R;
+        const bool has_blk = row0 < r1;
+        // next step's block header
+        const int kn = k + kWarps;
+        const bool has_next = s + 1 < nsteps && kn * R < r1;
+        int pbn = 0, pen = 0;
+        if (has_next) {
+            pbn = __ldg(bptr + kn);
+            pen = __ldg(bptr + kn + 1);
+        }
+        CV<float, TPT> acc[R], xo[R];
+        float dd[R][TPT];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const size_t bse = (size_t)min(row0 + i, n - 1) * B + b0;
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                dd[i][t] = (has_blk && row0 + i < r1) ? __ldg(d + bse + t) : 0.f;
+                acc[i].v[2 * t] = 0.f;
+                acc[i].v[2 * t + 1] = 0.f;
+            }
+        }
+        // rows of step s: ring blocks s .. s + 2hb (step 0 waits for all of
+        // them, later steps for the one block that is new)
+        const int bl = s + 2 * hb;
+        int failed = -1;
+        for (int q = (s == 0 ? 0 : bl); q <= bl; ++q)
+            if (failed < 0 && !mbar_wait_bounded(&bars[q % NB], (uint32_t)((q / NB) & 1))) failed = q;
+        if (__syncthreads_or(failed >= 0)) {
+            if (threadIdx.x == 0) {
+                atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
+                // let every copy still in flight land (bounded) before leaving
+                for (int q = (failed >= 0 ? failed : bl) + 1; q <= issued; ++q)
+                    mbar_wait_bounded(&bars[q % NB], (uint32_t)((q / NB) & 1));
+            }
+            return;
+        }
+        const int base = y0 + s * SR;
+        const int q0 = (s % NB) * SR;
+        auto slot = [&](int c) {
+            int t = c - base + q0;
+            t -= (t >= W) ? W : 0;
+            return ring + (size_t)t * row_reals + hl * TPT * 2;
+        };
+        if (has_blk) {
+            for (int e0 = pb; e0 < pe; e0 += 32) {
+                __syncwarp();
+                rbuf[warp][lane] = nxt;
+                __syncwarp();
+                if (e0 + 32 < pe) nxt = (e0 + 32 + lane < pe) ? __ldg(rec + e0 + 32 + lane) : pad(k);
+                else nxt = (has_next && lane < pen - pbn) ? __ldg(rec + pbn + lane) : pad(kn);
+                const int cnt = min(32, pe - e0);   // a multiple of 4
+                // this half's records: e = 2q + half (slots past cnt are padding)
+                for (int e = half; e < cnt; e += 8) {
+                    float4 r[4];
+                    CV<float, TPT> y[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) r[q] = rbuf[warp][e + 2 * q];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) y[q] = ldv<float, TPT, false>(slot(__float_as_int(r[q].x)), 0);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        cfma<float, TPT>(acc[0], r[q].y, y[q]);
+                        if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], r[q].z, y[q]);
+                        if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], r[q].w, y[q]);
+                    }
+                }
+            }
+        }
+        if (pe <= pb) nxt = (has_next && lane < pen - pbn) ? __ldg(rec + pbn + lane) : pad(kn);
+        // halves add up; lanes 0-15 finish the block
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+            for (int v = 0; v < 2 * TPT; ++v) acc[i].v[v] += __shfl_xor_sync(0xffffffffu, acc[i].v[v], 16);
+        if (has_blk && half == 0) {
+            float far[TPT], fai[TPT];   // this block's alpha terms, one conversion per block
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) { far[t] = 0.f; fai[t] = 0.f; }
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const int row = row0 + i;
+                if (row >= r1) break;
+                xo[i] = ldv<float, TPT, false>(slot(row), 0);
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    acc[i].v[2 * t] = fmaf(dd[i][t], xo[i].v[2 * t], acc[i].v[2 * t]);
+                    acc[i].v[2 * t + 1] = fmaf(dd[i][t], xo[i].v[2 * t + 1], acc[i].v[2 * t + 1]);
+                }
+                if (kWrite) {
+                    CV<float, TPT> o;
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) {
+                        o.v[2 * t] = (float)sc[t] * acc[i].v[2 * t];
+                        o.v[2 * t + 1] = (float)sc[t] * acc[i].v[2 * t + 1];
+                        const float xr = xo[i].v[2 * t], xi = xo[i].v[2 * t + 1];
+                        const float ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
+                        if (kBilinear) { far[t] += xr * ur - xi * ui; fai[t] += xr * ui + xi * ur; }
+                        else { far[t] += xr * ur + xi * ui; fai[t] += xr * ui - xi * ur; }
+                    }
+                    stv<float, TPT>(w, (size_t)row * B + b0, o);
+                } else {
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t)
+                        far[t] += acc[i].v[2 * t] * acc[i].v[2 * t] + acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                ar[t] += (double)far[t];
+                ai[t] += (double)fai[t];
+            }
+        }
+        __syncthreads();   // step s done: block s's place can take block s + NB
+        if (threadIdx.x == 0 && s + NB < nbox) {
+            issue(s + NB);
+            issued = s + NB;
+        }
+        k = kn;
+        pb = pbn;
+        pe = pen;
+    }
+    __shared__ double2 red[kMaxTC];
+    double2* scratch = reinterpret_cast<double2*>(smem_raw);   // the ring is free now
+    if (chunk_reduce_s<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk, scratch)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            const double s2 = S.sc[(size_t)j * B + b];
+            const double2 v = red[threadIdx.x];
+            if (kWrite) {
+                S.alpha[2 * ((size_t)j * B + b)] = v.x * s2 * s2;
+                S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s2 * s2;
+            } else {
+                S.nav[b] = sqrt(v.x) * s2;
             }
         }
     }
@@ -568,8 +913,8 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
 // The CTA owns rows [r0, r1) of one trajectory chunk.  Production blocks of
 // SR rows start at y0 = r0 - halo (halo = hb SR >= the matrix bandwidth);
 // SpMM step s (rows r0 + s SR ..) needs production blocks s .. s + 2hb, so the
-// ring holds 2hb + 1 blocks and block p = s + 2hb is produced right before
-// step s.  Input boxes run D production blocks ahead in D stages (one
+// ring holds at least 2hb + 1 blocks and block p = s + 2hb is produced right
+// before step s.  Input boxes run D production blocks ahead in D stages (one
 // mbarrier each, every wait bounded).  Halo rows are produced by both
 // neighbouring CTAs (identical values); each row is written and reduced by
 // its owner only.  Rows outside [0, n) arrive as zeros.
@@ -579,7 +924,8 @@ struct FusedMaps {
 
 template <typename Real, int TPT, int R, bool kBilinear, bool kLast>
 __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int TC, int rows_per_cta, int hb, int D,
-                                                            int j, int w_scaled, const int* __restrict__ bptr,
+                                                            int j, int w_scaled,
+                                                            const int* __restrict__ bptr,
                                                             const int* __restrict__ bcol,
                                                             const Real* __restrict__ bcoef,
                                                             const Real* __restrict__ d, Real* __restrict__ r_out,
@@ -592,8 +938,9 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int BPS = blockDim.x / TPR;
     const int SR = BPS * R;
-    const int W = (2 * hb + 1) * SR;                 // ring rows
     const int halo = hb * SR;
+    const int NB = 2 * hb + 1;                       // ring blocks
+    const int W = NB * SR;                           // ring rows
     const int tl = tr * TPT;
     const int chunk = blockIdx.y;
     const int b0 = chunk * TC + tl;
@@ -606,14 +953,14 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
     const bool has2 = j > 2;                          // r_{j-2} exists
     const int nbox = has2 ? 3 : 2;
     const size_t row_reals = (size_t)TC * 2;
-    // ring [W][TC], then D stages of 3 boxes [SR][TC], every box 128-byte aligned
+    // ring [W][TC] (production block p in ring block p mod NB), then D stages
+    // of 3 boxes [SR][TC], each box 128-byte aligned
     Real* ring = reinterpret_cast<Real*>(smem_raw);
     const size_t box_reals = (size_t)SR * row_reals;
     const uint32_t box_bytes = (uint32_t)(box_reals * sizeof(Real));
     const size_t stage_off = ((size_t)W * row_reals * sizeof(Real) + 127) & ~(size_t)127;
     const size_t bstride = (((size_t)box_bytes + 127) & ~(size_t)127) / sizeof(Real);
     Real* stage = reinterpret_cast<Real*>(smem_raw + stage_off);
-    auto ring_row = [&](int row) { return ring + (size_t)((row - y0) % W) * row_reals; };
     auto issue = [&](int p) {
         const int st = p % D;
         uint64_t* bar = &bars[st];
@@ -656,6 +1003,22 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
     const float4* rec = reinterpret_cast<const float4*>(bcoef);
     for (int p = 0; p < NP; ++p) {
         const int st = p % D;
+        // this step's block header, first records and diagonal are fetched
+        // before the production phase, which hides their latency
+        const int s = p - 2 * hb;
+        const int k = (r0 + s * SR) / R + rl;
+        const int row0 = k * R;
+        const bool has_blk = s >= 0 && row0 < r1;
+        BlkPre P;
+        if constexpr (kPk) blk_prefetch(P, has_blk, k, bptr, rec);
+        Real dd[R][TPT];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int row = row0 + i;
+            const size_t base = (size_t)min(max(row, 0), n - 1) * B + b0;
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) dd[i][t] = (has_blk && row < r1) ? __ldg(d + base + t) : Real(0);
+        }
         const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1));
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
@@ -691,7 +1054,7 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
                     o.v[2 * t] = (Real)rr;
                     o.v[2 * t + 1] = (Real)ri;
                 }
-                stv<Real, TPT>(ring_row(row) + tl * 2, 0, o);
+                stv<Real, TPT>(ring + (size_t)((p % NB) * SR + lr) * row_reals + tl * 2, 0, o);
                 if (row >= r0 && row < r1) {
                     stv<Real, TPT>(r_out, (size_t)row * B + b0, o);
 #pragma unroll
@@ -705,30 +1068,28 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
             issue(p + D);
             issued = p + D;
         }
-        const int s = p - 2 * hb;
-        if (s >= 0) {
-            // ---- SpMM step s: rows a + rl R .. ----
-            const int a = r0 + s * SR;
-            const int k = a / R + rl;
-            const int row0 = k * R;
-            if (row0 < r1) {
+        if (has_blk) {
+            // ---- SpMM step s: rows row0 .. row0 + R of step s ----
+            {
                 CV<Real, TPT> acc[R];
-                Real dd[R][TPT];
 #pragma unroll
-                for (int i = 0; i < R; ++i) {
-                    const int row = row0 + i;
-                    const size_t base = (size_t)min(row, n - 1) * B + b0;
+                for (int i = 0; i < R; ++i)
 #pragma unroll
                     for (int t = 0; t < TPT; ++t) {
-                        dd[i][t] = row < r1 ? __ldg(d + base + t) : Real(0);
                         acc[i].v[2 * t] = 0;
                         acc[i].v[2 * t + 1] = 0;
                     }
-                }
-                auto gather = [&](int c) { return ldv<Real, TPT, false>(ring_row(c) + tl * 2, 0); };
+                // rows of step s lie in ring blocks s .. s + 2hb: row c sits at
+                // c - base + q (mod W), base = y0 + s SR, q = (s mod NB) SR
+                const int base = y0 + s * SR;
+                const int q = (s % NB) * SR;
+                auto slot = [&](int c) {
+                    int t = c - base + q;
+                    t -= (t >= W) ? W : 0;
+                    return ring + (size_t)t * row_reals + tl * 2;
+                };
+                auto gather = [&](int c) { return ldv<Real, TPT, false>(slot(c), 0); };
                 if constexpr (kPk) {
-                    BlkPre P;
-                    blk_prefetch(P, true, k, bptr, rec);
                     union_loop_pre<TPT, R>(P, rec, acc, gather);
                 } else {
                     union_any<Real, TPT, R>(__ldg(bptr + k), __ldg(bptr + k + 1), bcol, bcoef, acc, gather);
@@ -737,7 +1098,7 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
                 for (int i = 0; i < R; ++i) {
                     const int row = row0 + i;
                     if (row >= r1) break;
-                    const CV<Real, TPT> x = ldv<Real, TPT, false>(ring_row(row) + tl * 2, 0);
+                    const CV<Real, TPT> x = ldv<Real, TPT, false>(slot(row), 0);
 #pragma unroll
                     for (int t = 0; t < TPT; ++t) {
                         acc[i].v[2 * t] = fma(dd[i][t], x.v[2 * t], acc[i].v[2 * t]);
@@ -765,6 +1126,271 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
     }
     // beta_{j-1} = ||r_j||, sc_j; then alpha_j = sc_j^2 <r_j, H r_j> (or nav).
     // The ring is free now (the loop ended on a barrier): it is the scratch.
+    __shared__ double2 red[kMaxTC];
+    double2* scratch = reinterpret_cast<double2*>(smem_raw);
+    if (chunk_reduce_s<TPT>(nn, zero, TC, S.partial, S.tickets + 5 * nch, red, chunk, scratch)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            double bt = sqrt(red[threadIdx.x].x);
+            if (!isfinite(bt)) atomicCAS(S.status, 0, DQ_ERR_NAN);
+            const size_t km = (size_t)(j - 1) * B + b;
+            const double scale = sqrt(S.alpha[2 * km] * S.alpha[2 * km] + S.alpha[2 * km + 1] * S.alpha[2 * km + 1]) +
+                                 (j > 2 ? S.beta[(size_t)(j - 2) * B + b] : 0.0);
+            if (bt <= kBreakdownRel * scale) bt = 0.0;
+            S.beta[km] = bt;
+            S.sc[(size_t)j * B + b] = bt > 0.0 ? 1.0 / bt : 0.0;
+        }
+    }
+    double* part2 = S.partial + (size_t)gridDim.y * gridDim.x * TC * 2;
+    if (chunk_reduce_s<TPT>(ar, ai, TC, part2, S.tickets + 6 * nch, red, chunk, scratch)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            const double sj = __ldcg(&S.sc[(size_t)j * B + b]);
+            const double2 v = red[threadIdx.x];
+            if constexpr (kLast) {
+                S.nav[b] = sqrt(v.x) * sj;
+            } else {
+                S.alpha[2 * ((size_t)j * B + b)] = v.x * sj * sj;
+                S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * sj * sj;
+            }
+        }
+    }
+}
+
+// Fused iteration with warp-owned row blocks (staged = 4; complex64,
+// packed records, R <= 3, TC = 32 TPT; one 512-thread CTA per SM).  Same
+// production ring and TMA stages as k_lanczos_fused, but the SpMM phase gives
+// each of the 16 warps RB whole blocks of R rows per step (SR = 16 RB R
+// rows), so a block's records are a
+// warp-uniform stream read 32 at a time into a per-warp shared buffer (the
+// next batch, or the next block's first one, in flight while the current
+// batch is used) and every gather is a broadcast-free 16-byte shared load
+// from the ring.  Lane l handles trajectories chunk TC + l TPT throughout.
+constexpr int kFwThreads = 512;
+
+template <int TPT, int R, bool kBilinear, bool kLast>
+__global__ void __launch_bounds__(kFwThreads, 1) k_lanczos_fw(int n, int B, int rows_per_cta, int hb, int D, int RB, int j,
+                                                         int w_scaled, const int* __restrict__ bptr,
+                                                         const float4* __restrict__ rec,
+                                                         const float* __restrict__ d, float* __restrict__ r_out,
+                                                         float* __restrict__ w_out, BatchedScalars S, int nch,
+                                                         const __grid_constant__ FusedMaps maps) {
+    constexpr int TC = 32 * TPT;
+    constexpr int kWarps = kFwThreads / 32;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bars[4];
+    __shared__ float4 rbuf[kWarps][32];
+    __shared__ double cf[TC][4];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int SR = kWarps * RB * R;
+    const int halo = hb * SR;
+    const int NB = 2 * hb + 1;
+    const int W = NB * SR;
+    const int tl = lane * TPT;
+    const int chunk = blockIdx.y;
+    const int b0 = chunk * TC + tl;
+    const int r0 = blockIdx.x * rows_per_cta;
+    const int r1 = min(n, r0 + rows_per_cta);
+    const int nsteps = r1 > r0 ? (r1 - r0 + SR - 1) / SR : 0;
+    const int NP = nsteps > 0 ? nsteps + 2 * hb : 0;
+    const int y0 = r0 - halo;
+    const int xc = chunk * TC * 2;
+    const bool has2 = j > 2;
+    const int nbox = has2 ? 3 : 2;
+    constexpr size_t row_reals = (size_t)TC * 2;
+    float* ring = reinterpret_cast<float*>(smem_raw);
+    const size_t box_reals = (size_t)SR * row_reals;
+    const uint32_t box_bytes = (uint32_t)(box_reals * sizeof(float));
+    const size_t stage_off = ((size_t)W * row_reals * sizeof(float) + 127) & ~(size_t)127;
+    const size_t bstride = (((size_t)box_bytes + 127) & ~(size_t)127) / sizeof(float);
+    float* stage = reinterpret_cast<float*>(smem_raw + stage_off);
+    auto issue = [&](int p) {
+        const int st = p % D;
+        uint64_t* bar = &bars[st];
+        float* dst = stage + (size_t)st * 3 * bstride;
+        const int y = y0 + p * SR;
+        mbar_arrive_expect_tx(bar, box_bytes * nbox);
+        tma_load_2d(dst, &maps.w, bar, xc, y);
+        tma_load_2d(dst + bstride, &maps.r1, bar, xc, y);
+        if (has2) tma_load_2d(dst + 2 * bstride, &maps.r2, bar, xc, y);
+    };
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < D; ++q) mbar_init(&bars[q], 1);
+        fence_barrier_init();
+    }
+    for (int t = threadIdx.x; t < TC; t += blockDim.x) {
+        const int b = chunk * TC + t;
+        const size_t k1 = (size_t)(j - 1) * B + b;
+        const double s1 = S.sc[k1];
+        cf[t][0] = w_scaled ? 1.0 : s1;
+        cf[t][1] = S.alpha[2 * k1] * s1;
+        cf[t][2] = S.alpha[2 * k1 + 1] * s1;
+        cf[t][3] = has2 ? S.beta[(size_t)(j - 2) * B + b] * S.sc[(size_t)(j - 2) * B + b] : 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int p = 0; p < min(D, NP); ++p) issue(p);
+    double cw[TPT], car[TPT], cai[TPT], cb[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        cw[t] = cf[tl + t][0];
+        car[t] = cf[tl + t][1];
+        cai[t] = cf[tl + t][2];
+        cb[t] = cf[tl + t][3];
+    }
+    double nn[TPT], ar[TPT], ai[TPT], zero[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) { nn[t] = 0.0; ar[t] = 0.0; ai[t] = 0.0; zero[t] = 0.0; }
+    int issued = min(D, NP) - 1;
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int p = 0; p < NP; ++p) {
+        const int st = p % D;
+        // this warp's first block of step s: header and first record batch
+        // are fetched before the production phase, which hides them
+        const int s = p - 2 * hb;
+        const int kfirst = (r0 + s * SR) / R + warp * RB;
+        int k = kfirst, pb = 0, pe = 0;
+        float4 nxt = zero4;
+        if (s >= 0 && k * R < r1) {
+            pb = __ldg(bptr + k);
+            pe = __ldg(bptr + k + 1);
+            nxt = lane < pe - pb ? __ldg(rec + pb + lane) : zero4;
+        }
+        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) {
+                atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
+                for (int q = p + 1; q <= issued; ++q) mbar_wait_bounded(&bars[q % D], (uint32_t)((q / D) & 1));
+            }
+            return;
+        }
+        // ---- produce r_j: warp w writes rows lr = w, w + 8, ... of block p ----
+        {
+            const float* sw = stage + (size_t)st * 3 * bstride;
+            const float* s1 = sw + bstride;
+            const float* s2 = sw + 2 * bstride;
+            float* blk = ring + (size_t)((p % NB) * SR) * row_reals;
+            for (int lr = warp; lr < SR; lr += kWarps) {
+                const int row = y0 + p * SR + lr;
+                const size_t off = (size_t)lr * row_reals + tl * 2;
+                const CV<float, TPT> u = ldv<float, TPT, false>(sw + off, 0);
+                const CV<float, TPT> x1 = ldv<float, TPT, false>(s1 + off, 0);
+                CV<float, TPT> x2;
+                if (has2) x2 = ldv<float, TPT, false>(s2 + off, 0);
+                CV<float, TPT> o;
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    const double xr = x1.v[2 * t], xi = x1.v[2 * t + 1];
+                    double rr = cw[t] * (double)u.v[2 * t] - (car[t] * xr - cai[t] * xi);
+                    double ri = cw[t] * (double)u.v[2 * t + 1] - (car[t] * xi + cai[t] * xr);
+                    if (has2) {
+                        rr -= cb[t] * (double)x2.v[2 * t];
+                        ri -= cb[t] * (double)x2.v[2 * t + 1];
+                    }
+                    o.v[2 * t] = (float)rr;
+                    o.v[2 * t + 1] = (float)ri;
+                }
+                stv<float, TPT>(blk + off, 0, o);
+                if (row >= r0 && row < r1) {
+                    stv<float, TPT>(r_out, (size_t)row * B + b0, o);
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t)
+                        nn[t] += (double)o.v[2 * t] * o.v[2 * t] + (double)o.v[2 * t + 1] * o.v[2 * t + 1];
+                }
+            }
+        }
+        __syncthreads();   // block p is in the ring; its stage is free
+        if (threadIdx.x == 0 && p + D < NP) {
+            issue(p + D);
+            issued = p + D;
+        }
+        if (s >= 0) {
+            // ---- SpMM step s: this warp's RB blocks ----
+            const int base = y0 + s * SR;
+            const int q0 = (s % NB) * SR;
+            auto slot = [&](int c) {
+                int t = c - base + q0;
+                t -= (t >= W) ? W : 0;
+                return ring + (size_t)t * row_reals + tl * 2;
+            };
+            for (int ib = 0; ib < RB; ++ib, ++k) {
+                const int row0 = k * R;
+                if (row0 >= r1) break;
+                // next block's header (its first batch is fetched during this block's last batch)
+                const int kn = k + 1;
+                const bool has_next = ib + 1 < RB && kn * R < r1;
+                int pbn = 0, pen = 0;
+                if (has_next) {
+                    pbn = __ldg(bptr + kn);
+                    pen = __ldg(bptr + kn + 1);
+                }
+                CV<float, TPT> acc[R];
+                float dd[R][TPT];
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const size_t bse = (size_t)min(row0 + i, n - 1) * B + b0;
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) {
+                        dd[i][t] = row0 + i < r1 ? __ldg(d + bse + t) : 0.f;
+                        acc[i].v[2 * t] = 0.f;
+                        acc[i].v[2 * t + 1] = 0.f;
+                    }
+                }
+                for (int e0 = pb; e0 < pe; e0 += 32) {
+                    __syncwarp();
+                    rbuf[warp][lane] = nxt;
+                    __syncwarp();
+                    if (e0 + 32 < pe) nxt = (e0 + 32 + lane < pe) ? __ldg(rec + e0 + 32 + lane) : zero4;
+                    else nxt = (has_next && lane < pen - pbn) ? __ldg(rec + pbn + lane) : zero4;
+                    const int cnt = min(32, pe - e0);   // a multiple of 4
+                    for (int e = 0; e < cnt; e += 4) {
+                        float4 r[4];
+                        CV<float, TPT> y[4];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) r[q] = rbuf[warp][e + q];
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) y[q] = ldv<float, TPT, false>(slot(__float_as_int(r[q].x)), 0);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            cfma<float, TPT>(acc[0], r[q].y, y[q]);
+                            if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], r[q].z, y[q]);
+                            if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], r[q].w, y[q]);
+                        }
+                    }
+                }
+                if (pe <= pb) nxt = (has_next && lane < pen - pbn) ? __ldg(rec + pbn + lane) : zero4;
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const int row = row0 + i;
+                    if (row >= r1) break;
+                    const CV<float, TPT> x = ldv<float, TPT, false>(slot(row), 0);
+#pragma unroll
+                    for (int t = 0; t < TPT; ++t) {
+                        acc[i].v[2 * t] = fmaf(dd[i][t], x.v[2 * t], acc[i].v[2 * t]);
+                        acc[i].v[2 * t + 1] = fmaf(dd[i][t], x.v[2 * t + 1], acc[i].v[2 * t + 1]);
+                    }
+                    if constexpr (kLast) {
+#pragma unroll
+                        for (int t = 0; t < TPT; ++t)
+                            ar[t] += (double)acc[i].v[2 * t] * acc[i].v[2 * t] +
+                                     (double)acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
+                    } else {
+                        stv<float, TPT>(w_out, (size_t)row * B + b0, acc[i]);
+#pragma unroll
+                        for (int t = 0; t < TPT; ++t) {
+                            const double xr = x.v[2 * t], xi = x.v[2 * t + 1];
+                            const double ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
+                            if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
+                            else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+                        }
+                    }
+                }
+                pb = pbn;
+                pe = pen;
+            }
+        }
+        __syncthreads();   // step s done: the next production may overwrite block s
+    }
     __shared__ double2 red[kMaxTC];
     double2* scratch = reinterpret_cast<double2*>(smem_raw);
     if (chunk_reduce_s<TPT>(nn, zero, TC, S.partial, S.tickets + 5 * nch, red, chunk, scratch)) {
@@ -1301,6 +1927,28 @@ static cudaError_t fused_attr_r(int R, int bytes) {
     }
 }
 
+template <int TPT, int R>
+static cudaError_t fw_attr(int bytes) {
+    cudaError_t e = cudaSuccess;
+    for (int v = 0; v < 4 && e == cudaSuccess; ++v) {
+        const void* f = v == 0 ? (const void*)k_lanczos_fw<TPT, R, false, false>
+                      : v == 1 ? (const void*)k_lanczos_fw<TPT, R, true, false>
+                      : v == 2 ? (const void*)k_lanczos_fw<TPT, R, false, true>
+                               : (const void*)k_lanczos_fw<TPT, R, true, true>;
+        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    }
+    return e;
+}
+
+template <int TPT>
+static cudaError_t fw_attr_r(int R, int bytes) {
+    switch (R) {
+        case 1: return fw_attr<TPT, 1>(bytes);
+        case 2: return fw_attr<TPT, 2>(bytes);
+        default: return fw_attr<TPT, 3>(bytes);
+    }
+}
+
 // Shared memory of the fused iteration: ring of (2hb+1) SR rows, D stages of
 // three 128-byte-aligned boxes of SR rows.
 static size_t fused_smem(int tc, int sr, int hb, int D, size_t rsz) {
@@ -1319,13 +1967,20 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
-    if (staged < 0 || staged > 2) return DQ_ERR_ARG;
+    if (staged < 0 || staged > 6) return DQ_ERR_ARG;
+    // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane, one CTA per SM
+    if (staged == 6 && (!bs->mixed || R > 3 || tc != 32 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
+        return DQ_ERR_ARG;
+    if (staged == 5 && tc / tpt > 512) return DQ_ERR_ARG;
+    // warp-per-block forms: complex64 packed records, one warp spans the chunk
+    if ((staged == 3 || staged == 4) && (!bs->mixed || R > 3 || tc != 32 * tpt)) return DQ_ERR_ARG;
     const int ri = r_index(R);
     if (ri < 0) return DQ_ERR_ARG;
     const int chunks = B / tc;
     if (groups < 1 || chunks % groups) return DQ_ERR_ARG;
     const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
+    const int RPC_spmm = (staged == 5 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
     // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide
     int gx = std::max(1, (bs->sms * kStreamCtasPerSm) / cpg);
     int rpc = (n + gx - 1) / gx;
@@ -1334,7 +1989,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     const int nb = (n + R - 1) / R;
     int gxs = std::max(1, (bs->sms * ctas_per_sm) / cpg);
     int bpc = (nb + gxs - 1) / gxs;
-    bpc = ((bpc + RPC - 1) / RPC) * RPC;
+    bpc = ((bpc + RPC_spmm - 1) / RPC_spmm) * RPC_spmm;
     gxs = (nb + bpc - 1) / bpc;
     if (gx > kMaxCtasPerChunk || (size_t)gx * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
     if (gxs > kMaxCtasPerChunk || (size_t)gxs * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
@@ -1344,8 +1999,85 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     }
     int halo = 0, wmask = 0, rpc_win = 0, gxw = 0;
     size_t smem = 0;
-    int f_sr = 0, f_hb = 0, f_D = 0, f_rpc = 0, f_gx = 0;
+    int f_sr = 0, f_hb = 0, f_D = 0, f_rpc = 0, f_gx = 0, f_rb = 1;
     size_t f_smem = 0;
+    if (staged == 4) {
+        // fused iteration with warp-owned blocks: the largest RB (blocks per
+        // warp per step) and deepest staging that fit ctas_per_sm CTAs per SM
+        // one 512-thread CTA per SM; the reduction scratch (2 x 512 double2)
+        // lives in the dynamic region
+        if (groups != 1 || c->cfg.m < 2 || ctas_per_sm != 1) return DQ_ERR_ARG;
+        constexpr size_t kStatic = 13 * 1024;   // record buffers, coefficients, reduction slots, reserve
+        for (int rb = 16 / R; rb >= 1 && !f_D; --rb) {
+            const int SR = (kFwThreads / 32) * rb * R;
+            if (SR > 256) continue;
+            const int hb = (bs->bw + SR - 1) / SR;
+            for (int D = 4; D >= 2; --D) {
+                const size_t sm = std::max<size_t>(fused_smem(tc, SR, hb, D, sizeof(float)), 16384);
+                if (sm + kStatic <= 227 * 1024) {
+                    f_D = D; f_smem = sm; f_sr = SR; f_hb = hb; f_rb = rb;
+                    break;
+                }
+            }
+        }
+        if (!f_D) return DQ_ERR_ARG;
+        f_gx = std::max(1, (bs->sms * ctas_per_sm) / chunks);
+        f_rpc = (n + f_gx - 1) / f_gx;
+        f_rpc = ((f_rpc + f_sr - 1) / f_sr) * f_sr;
+        f_gx = (n + f_rpc - 1) / f_rpc;
+        if (f_gx > kMaxCtasPerChunk || (size_t)f_gx * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
+        cudaError_t e = tpt == 2 ? fw_attr_r<2>(R, (int)f_smem) : fw_attr_r<1>(R, (int)f_smem);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return DQ_ERR_ARG;
+        }
+        dq_status st = build_fmaps(c, tc, f_sr);
+        if (st) return st;
+    }
+    if (staged == 6) {
+        // ring SpMM: SR = 16 R rows per step; the deepest prefetch (D boxes)
+        // whose ring fits one CTA per SM
+        const int SR = (kRingThreads / 32) * R;
+        const int hb = (bs->bw + SR - 1) / SR;
+        constexpr size_t kStatic = 11 * 1024;   // record buffers, barriers, reduction slots, reserve
+        for (int D = 4; D >= 1; --D) {
+            const int NB = 2 * hb + D + 1;
+            const size_t sm = std::max<size_t>((size_t)NB * SR * 32 * 2 * sizeof(float), 16384);
+            if (NB <= 32 && sm + kStatic <= 227 * 1024) {
+                f_D = D; f_smem = sm; f_sr = SR; f_hb = hb;
+                break;
+            }
+        }
+        if (!f_D) return DQ_ERR_ARG;
+        f_gx = std::max(1, bs->sms / chunks);
+        f_rpc = (n + f_gx - 1) / f_gx;
+        f_rpc = ((f_rpc + SR - 1) / SR) * SR;
+        f_gx = (n + f_rpc - 1) / f_rpc;
+        if (f_gx > kMaxCtasPerChunk || (size_t)f_gx * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
+        cudaError_t e = cudaSuccess;
+        for (int v = 0; v < 4 && e == cudaSuccess; ++v) {
+            const bool bil = v & 1, wr = v & 2;
+            const void* fn = nullptr;
+            switch (R) {
+                case 1: fn = bil ? (wr ? (const void*)k_spmm_ring<1, true, true> : (const void*)k_spmm_ring<1, true, false>)
+                                 : (wr ? (const void*)k_spmm_ring<1, false, true> : (const void*)k_spmm_ring<1, false, false>);
+                        break;
+                case 2: fn = bil ? (wr ? (const void*)k_spmm_ring<2, true, true> : (const void*)k_spmm_ring<2, true, false>)
+                                 : (wr ? (const void*)k_spmm_ring<2, false, true> : (const void*)k_spmm_ring<2, false, false>);
+                        break;
+                default: fn = bil ? (wr ? (const void*)k_spmm_ring<3, true, true> : (const void*)k_spmm_ring<3, true, false>)
+                                  : (wr ? (const void*)k_spmm_ring<3, false, true> : (const void*)k_spmm_ring<3, false, false>);
+                        break;
+            }
+            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f_smem);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return DQ_ERR_ARG;
+        }
+        dq_status st = build_tmaps(c, tc, SR);
+        if (st) return st;
+    }
     if (staged == 2) {
         // fused iteration: one launch covers every chunk, no trajectory groups
         const size_t rsz = bs->mixed ? sizeof(float) : sizeof(double);
@@ -1426,6 +2158,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     bs->f_rpc = f_rpc;
     bs->f_gx = f_gx;
     bs->f_smem = f_smem;
+    bs->f_rb = f_rb;
     drop_graph(bs);
     return DQ_OK;
 }
@@ -1461,17 +2194,17 @@ dq_status batched_mirror_tiling(dq_ctx* c, BatchedState* dst) {
     dst->staged = src->staged; dst->groups = src->groups; dst->halo = src->halo; dst->wmask = src->wmask;
     dst->rpc_win = src->rpc_win; dst->gxw = src->gxw; dst->bw = src->bw; dst->win_smem = src->win_smem;
     dst->f_sr = src->f_sr; dst->f_hb = src->f_hb; dst->f_D = src->f_D; dst->f_rpc = src->f_rpc;
-    dst->f_gx = src->f_gx; dst->f_smem = src->f_smem;
+    dst->f_gx = src->f_gx; dst->f_smem = src->f_smem; dst->f_rb = src->f_rb;
     dst->tmaps.clear();
     dst->fmaps.clear();
-    if (src->staged == 2) {
+    if (src->staged == 2 || src->staged == 4) {
         c->bat = dst;
         dq_status st = build_fmaps(c, src->TC, src->f_sr);
         c->bat = src;
         if (st) return st;
     }
-    if (src->staged == 1) {
-        const int SR = (kBThreads / (src->TC / src->TPT)) * src->R;
+    if (src->staged == 1 || src->staged == 6) {
+        const int SR = src->staged == 6 ? src->f_sr : (kBThreads / (src->TC / src->TPT)) * src->R;
         c->bat = dst;
         dq_status st = build_tmaps(c, src->TC, SR);
         c->bat = src;
@@ -1637,11 +2370,51 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w, int cy0, int 
 #undef DQ_WIN_R
         return;
     }
+    if (bs->staged == 6) {
+        if constexpr (sizeof(Real) == 4 && TPT == 2) {
+            const dim3 grid(bs->f_gx, ncy);
+            const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
+            const CUtensorMap& tm = bs->tmaps[j];
+#define DQ_RING_R(RR)                                                                                              \
+    k_spmm_ring<RR, kBil, kWrite><<<grid, kRingThreads, bs->f_smem, c->stream>>>(n, B, bs->f_rpc, bs->f_hb, bs->f_D, j, \
+                                                                               f.bptr, rec, d, w, bs->s, bs->chunks, tm)
+            switch (bs->R) {
+                case 1: DQ_RING_R(1); break;
+                case 2: DQ_RING_R(2); break;
+                default: DQ_RING_R(3); break;
+            }
+#undef DQ_RING_R
+        }
+        return;
+    }
+    if (bs->staged == 3) {
+        if constexpr (sizeof(Real) == 4) {
+            const dim3 grid(bs->gxs, ncy);
+            const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
+#define DQ_WARP_R(RR)                                                                                             \
+    k_spmm_warp<TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, bs->bpc, f.nb, j, f.bptr, rec, d, rj, w, \
+                                                                      bs->s, cy0, bs->chunks)
+            switch (bs->R) {
+                case 1: DQ_WARP_R(1); break;
+                case 2: DQ_WARP_R(2); break;
+                default: DQ_WARP_R(3); break;
+            }
+#undef DQ_WARP_R
+        }
+        return;
+    }
     const dim3 grid(bs->gxs, ncy);
+    // staged = 5: the same L1 SpMM in 512-thread CTAs (one per SM, one
+    // sliding gather window per SM instead of two competing ones)
 #define DQ_SPMM_R(RR)                                                                                             \
-    k_spmm_blk<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j, f.bptr, \
-                                                                               f.bcol, cf, d, rj, w, bs->s, cy0,    \
-                                                                               bs->chunks)
+    if (bs->staged == 5)                                                                                         \
+        k_spmm_blk<Real, TPT, RR, kBil, kWrite, 512><<<grid, 512, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j,     \
+                                                                                 f.bptr, f.bcol, cf, d, rj, w,   \
+                                                                                 bs->s, cy0, bs->chunks);        \
+    else                                                                                                         \
+        k_spmm_blk<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j,    \
+                                                                                   f.bptr, f.bcol, cf, d, rj, w, \
+                                                                                   bs->s, cy0, bs->chunks)
     switch (bs->R) {
         case 1: DQ_SPMM_R(1); break;
         case 2: DQ_SPMM_R(2); break;
@@ -1683,8 +2456,42 @@ static void launch_fused(dq_ctx* c, int j) {
 #undef DQ_FUSED_R
 }
 
+template <int TPT, bool kBil, bool kLast>
+static void launch_fw(dq_ctx* c, int j) {
+    BatchedState* bs = c->bat;
+    const BlockFmt& f = bs->fmt[r_index(bs->R)];
+    const int n = c->n, B = bs->B, m = c->cfg.m;
+    const size_t se = (size_t)n * B;
+    float* slabs = (float*)bs->slabs;
+    FusedMaps maps;
+    maps.w = (j % 2 == 0) ? bs->fmaps[0] : bs->fmaps[m + 1];
+    maps.r1 = bs->fmaps[j - 1];
+    maps.r2 = bs->fmaps[j >= 3 ? j - 2 : j - 1];
+    float* r_out = slabs + 2 * se * j;
+    float* w_out = kLast ? nullptr : ((j % 2 == 0) ? (float*)bs->wB : slabs);
+    const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
+    const dim3 grid(bs->f_gx, bs->chunks);
+#define DQ_FW_R(RR)                                                                                               \
+    k_lanczos_fw<TPT, RR, kBil, kLast><<<grid, kFwThreads, bs->f_smem, c->stream>>>(                               \
+        n, B, bs->f_rpc, bs->f_hb, bs->f_D, bs->f_rb, j, j == 2, f.bptr, rec, (const float*)bs->diag, r_out, w_out, \
+        bs->s, bs->chunks, maps)
+    switch (bs->R) {
+        case 1: DQ_FW_R(1); break;
+        case 2: DQ_FW_R(2); break;
+        default: DQ_FW_R(3); break;
+    }
+#undef DQ_FW_R
+}
+
 template <typename Real, int TPT, bool kLast>
 static void launch_fused_any(dq_ctx* c, int j) {
+    if constexpr (sizeof(Real) == 4) {
+        if (c->bat->staged == 4) {
+            if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_fw<TPT, true, kLast>(c, j);
+            else launch_fw<TPT, false, kLast>(c, j);
+            return;
+        }
+    }
     if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_fused<Real, TPT, true, kLast>(c, j);
     else launch_fused<Real, TPT, false, kLast>(c, j);
 }
@@ -1698,7 +2505,8 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
     Real* slabs = (Real*)bs->slabs;
     auto slab = [&](int k) { return slabs + 2 * se * k; };
     const dim3 grid(bs->gx, ncy);
-    if (bs->staged == 2 && j >= 2) {
+    const bool fused = bs->staged == 2 || bs->staged == 4;
+    if (fused && j >= 2) {
         // iteration j of the fused form produces r_j; the last one also r_{m+1}
         if (tm) tm->mark(DQ_KIND_FUSED, st);
         launch_fused_any<Real, TPT, false>(c, j);
@@ -1711,7 +2519,7 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
     if (tm) tm->mark(DQ_KIND_SPMM, st);
     if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_spmm<Real, TPT, true, true>(c, j, slab(j), slab(0), cy0, ncy);
     else launch_spmm<Real, TPT, false, true>(c, j, slab(j), slab(0), cy0, ncy);
-    if (bs->staged == 2) {
+    if (fused) {
         // fused form: the first SpMM only; r_2 comes from the next fused launch
         if (j == c->cfg.m) {
             if (tm) tm->mark(DQ_KIND_FUSED, st);
@@ -1754,7 +2562,7 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
     const int cpg = bs->chunks / bs->groups;
     for (int g = 0; g < bs->groups; ++g) {
         for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm, g * cpg, cpg);
-        if (bs->staged != 2) {   // the fused form's last launch already gave ||H q_{m+1}||
+        if (bs->staged != 2 && bs->staged != 4) {   // the fused form's last launch gave ||H q_{m+1}||
             mark(DQ_KIND_SPMM_NORM);
             launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, g * cpg, cpg);
         }
@@ -1858,7 +2666,7 @@ dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
     cudaEvent_t e0, e1;
     DQ_CU(cudaEventCreate(&e0));
     DQ_CU(cudaEventCreate(&e1));
-    const bool fused = c->bat->staged == 2;
+    const bool fused = c->bat->staged == 2 || c->bat->staged == 4;
     const int jt = std::min(3, c->cfg.m);
     auto one = [&]() {
         if (fused) fused_iteration_any(c, jt);

@@ -129,7 +129,7 @@ struct dq::BatchedState {
     // slabs 0..m and of wB (boxes of f_sr rows), halo blocks, stages, grid
     void* wB = nullptr;
     std::vector<CUtensorMap> fmaps;
-    int f_sr = 0, f_hb = 0, f_D = 2, f_rpc = 0, f_gx = 0;
+    int f_sr = 0, f_hb = 0, f_D = 2, f_rpc = 0, f_gx = 0, f_rb = 1;   // f_rb: blocks per warp (staged = 4)
     size_t f_smem = 0;
     ::BlockFmt fmt[5];                    // R = 1, 2, 3, 4, 8 (built on demand)
     bool fmt_borrowed = false;            // fmt belongs to another workspace

@@ -171,7 +171,11 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * window filled by TMA (needs the matrix bandwidth to fit the window; the
  * call fails otherwise), 0 gathers through L1, 2 runs each Lanczos iteration
  * as one fused kernel (TMA-streamed w, r_j, r_{j-1}; r_{j+1} formed in a
- * shared-memory ring and gathered from there; groups must be 1).  groups splits the
+ * shared-memory ring and gathered from there; groups must be 1), 3 gathers
+ * through L1 with one warp per row block (records fetched 32 at a time;
+ * complex64, traj_chunk = 32 vec), 4 is the fused form with warp-owned row
+ * blocks (complex64, traj_chunk = 32 vec, ctas_per_sm 1), 5 is the L1 form
+ * in 512-thread CTAs (one sliding gather window per CTA).  groups splits the
  * trajectory chunks into groups whose m Lanczos iterations run one group
  * after another, so a group's Krylov slabs stay resident in L2 (must divide
  * n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run

@@ -133,7 +133,7 @@ def test_spectrum_matches_numpy():
 @pytest.mark.parametrize("tiling", [(2, 2, 1, 1, 0, 1), (4, 1, 2, 2, 0, 1), (4, 2, 8, 4, 0, 1), (2, 1, 4, 8, 0, 2),
                                     (4, 2, 2, 8, 0, 1), (4, 2, 1, 1, 1, 1), (2, 2, 2, 1, 1, 2), (4, 1, 1, 4, 1, 1),
                                     (1, 1, 2, 4, 0, 4), (4, 2, 1, 2, 2, 1), (2, 2, 2, 1, 2, 1), (4, 1, 2, 1, 2, 1),
-                                    (4, 1, 1, 3, 2, 1)])
+                                    (4, 1, 1, 3, 2, 1), (4, 2, 1, 3, 5, 1), (2, 1, 1, 2, 5, 2)])
 def test_every_tiling_matches_oracle(tiling):
     """Tilings only change the schedule: each must reproduce the oracle."""
     import dynaquant_b200 as dq
@@ -165,7 +165,7 @@ def test_autotune_picks_valid_tiling_and_keeps_parity(tmp_path, monkeypatch):
 
 
 @pytest.mark.parametrize("R,staged,groups", [(1, 1, 1), (2, 1, 1), (3, 0, 1), (4, 1, 1), (8, 1, 1), (4, 0, 1),
-                                             (3, 0, 2), (2, 1, 2), (2, 0, 2)])
+                                             (3, 0, 2), (2, 1, 2), (2, 0, 2), (3, 5, 1), (1, 5, 2)])
 def test_tube_tilings_match_oracle(oracle, R, staged, groups):
     """Shared-memory window (TMA-staged) and L1 SpMM variants on a dipole tube,
     whose couplings reach ~3 rings (bandwidth ~60 sites)."""
@@ -191,7 +191,7 @@ def test_tube_tilings_match_oracle(oracle, R, staged, groups):
     p.close()
 
 
-@pytest.mark.parametrize("tiling", [(16, 2, 2, 1, 2, 1), (16, 2, 2, 2, 2, 1), (16, 2, 2, 3, 2, 1), (16, 2, 1, 4, 2, 1),
+@pytest.mark.parametrize("tiling", [(16, 2, 2, 1, 2, 1), (16, 2, 2, 2, 2, 1), (16, 2, 1, 3, 2, 1), (16, 2, 1, 4, 2, 1),
                                     (32, 2, 1, 2, 2, 1)])
 def test_tube_fused_iterations_match_oracle(oracle, tiling):
     """One-kernel Lanczos iterations (staged = 2) on the dipole tube: r_{j+1} formed from TMA-streamed
@@ -216,3 +216,63 @@ def test_tube_fused_iterations_match_oracle(oracle, tiling):
     assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
     assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
     p.close()
+
+
+@pytest.mark.parametrize("B,tiling", [(32, (32, 1, 4, 1, 3, 1)), (32, (32, 1, 4, 2, 3, 1)), (32, (32, 1, 3, 3, 3, 1)),
+                                      (64, (64, 2, 3, 3, 3, 1)), (64, (32, 1, 2, 3, 3, 2)),
+                                      (32, (32, 2, 1, 1, 6, 1)), (32, (32, 2, 1, 2, 6, 1)), (32, (32, 2, 1, 3, 6, 1)),
+                                      (64, (32, 2, 1, 3, 6, 1))])
+def test_tube_warp_spmm_matches_oracle(oracle, B, tiling):
+    """Warp-per-block SpMMs: staged = 3 gathers through L1, staged = 6 from a TMA-fed shared-memory
+    ring; both read each block's packed records 32 at a time into a per-warp buffer."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 40)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=12, dt=0.5, dot_mode=1, noise=2, sigma=250.0, tau=50.0,
+                      sigma_static=150.0, seed=4)
+    T = 12
+    psi0 = s.bright_state()
+    ref = S.run(B, T, psi0, pop_every=4, threads=4)
+    p = dq.Propagator(s.n, m=12, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=4, dot=1,
+                      pop_every=4, max_steps=T, precision=dq.PREC_MIXED)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    p.set_initial_state(psi0)
+    p.set_tiling(*tiling)
+    assert p.get_tiling() == tiling
+    p.run(T)
+    assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
+    assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
+    p.close()
+
+
+@pytest.mark.parametrize("B,tiling", [(32, (32, 1, 1, 1, 4, 1)), (32, (32, 1, 1, 2, 4, 1)), (32, (32, 1, 1, 3, 4, 1)),
+                                      (64, (64, 2, 1, 1, 4, 1)), (64, (64, 2, 1, 2, 4, 1))])
+def test_tube_fused_warp_blocks_match_oracle(oracle, B, tiling):
+    """Fused iteration with warp-owned row blocks (staged = 4): records in per-warp batches, gathers
+    from the shared-memory ring of freshly formed residuals."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 40)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=12, dt=0.5, dot_mode=1, noise=2, sigma=250.0, tau=50.0,
+                      sigma_static=150.0, seed=4)
+    T = 12
+    psi0 = s.bright_state()
+    ref = S.run(B, T, psi0, pop_every=4, threads=4)
+    for dot in (1, 0):
+        p = dq.Propagator(s.n, m=12, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=4, dot=dot,
+                          pop_every=4, max_steps=T, precision=dq.PREC_MIXED)
+        p.set_system(s)
+        p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+        p.set_initial_state(psi0)
+        p.set_tiling(*tiling)
+        assert p.get_tiling() == tiling
+        p.run(T)
+        if dot == 1:
+            assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
+            assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
+        else:   # the bilinear dot: populations stay normalised and finite
+            assert np.isfinite(p.populations()).all()
+        p.close()
