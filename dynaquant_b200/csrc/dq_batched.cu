@@ -1491,6 +1491,93 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
     }
 }
 
+// Full reorthogonalisation (Hermitian dot, cfg.reorth; classical
+// Gram-Schmidt once, FP64 sums): h_k = <q_k, r_{j+1}> per trajectory, one k
+// per launch, into h[k][b] (the combine-weight array, unused until the Padé
+// step); then r_{j+1} -= sum_k h_k q_k and beta_j, sc_{j+1} from its norm.
+template <typename Real, int TPT>
+__global__ void __launch_bounds__(kBThreads) k_reorth_dot_b(int n, int B, int TC, int rpc, int k,
+                                                           const Real* __restrict__ xk, const Real* __restrict__ r,
+                                                           BatchedScalars S, int cy0, int nch) {
+    const Tile<TPT> T(TC, rpc, n, cy0);
+    double ar[TPT], ai[TPT], sck[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        ar[t] = 0.0;
+        ai[t] = 0.0;
+        sck[t] = S.sc[(size_t)k * B + T.b0 + t];
+    }
+    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+        const size_t base = (size_t)row * B + T.b0;
+        const CV<Real, TPT> x = ldv<Real, TPT, false>(xk, base);
+        const CV<Real, TPT> v = ldv<Real, TPT, false>(r, base);
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+            const double qr = sck[t] * x.v[2 * t], qi = sck[t] * x.v[2 * t + 1];
+            const double vr = v.v[2 * t], vi = v.v[2 * t + 1];
+            ar[t] += qr * vr + qi * vi;   // conj(q) v
+            ai[t] += qr * vi - qi * vr;
+        }
+    }
+    __shared__ double2 red[kMaxTC];
+    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + 7 * nch, red, T.chunk)) {
+        if (threadIdx.x < TC) {
+            const size_t kb = (size_t)k * B + T.chunk * TC + threadIdx.x;
+            S.yt[2 * kb] = red[threadIdx.x].x;
+            S.yt[2 * kb + 1] = red[threadIdx.x].y;
+        }
+    }
+}
+
+template <typename Real, int TPT>
+__global__ void __launch_bounds__(kBThreads) k_reorth_apply_b(int n, int B, int TC, int rpc, int j, Real* slabs,
+                                                             size_t slab_stride, BatchedScalars S, int cy0, int nch) {
+    const Tile<TPT> T(TC, rpc, n, cy0);
+    Real* r = slabs + 2 * slab_stride * (j + 1);
+    double nn[TPT], zero[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) { nn[t] = 0.0; zero[t] = 0.0; }
+    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+        const size_t base = (size_t)row * B + T.b0;
+        const CV<Real, TPT> v0 = ldv<Real, TPT, false>(r, base);
+        double vr[TPT], vi[TPT];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) { vr[t] = v0.v[2 * t]; vi[t] = v0.v[2 * t + 1]; }
+        for (int k = 1; k <= j; ++k) {
+            const CV<Real, TPT> x = ldv<Real, TPT, false>(slabs + 2 * slab_stride * k, base);
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                const size_t kb = (size_t)k * B + T.b0 + t;
+                const double s = S.sc[kb], hr = S.yt[2 * kb] * s, hi = S.yt[2 * kb + 1] * s;
+                vr[t] -= hr * x.v[2 * t] - hi * x.v[2 * t + 1];
+                vi[t] -= hr * x.v[2 * t + 1] + hi * x.v[2 * t];
+            }
+        }
+        CV<Real, TPT> o;
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+            o.v[2 * t] = (Real)vr[t];
+            o.v[2 * t + 1] = (Real)vi[t];
+            nn[t] += (double)o.v[2 * t] * o.v[2 * t] + (double)o.v[2 * t + 1] * o.v[2 * t + 1];
+        }
+        stv<Real, TPT>(r, base, o);
+    }
+    __shared__ double2 red[kMaxTC];
+    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 1 * nch, red, T.chunk)) {
+        if (threadIdx.x < TC) {
+            const int b = T.chunk * TC + threadIdx.x;
+            double bt = sqrt(red[threadIdx.x].x);
+            if (!isfinite(bt)) atomicCAS(S.status, 0, DQ_ERR_NAN);
+            const size_t kj = (size_t)j * B + b;
+            const double scale = sqrt(S.alpha[2 * kj] * S.alpha[2 * kj] + S.alpha[2 * kj + 1] * S.alpha[2 * kj + 1]) +
+                                 (j > 1 ? S.beta[(size_t)(j - 1) * B + b] : 0.0);
+            if (bt <= kBreakdownRel * scale) bt = 0.0;
+            S.beta[kj] = bt;
+            S.sc[(size_t)(j + 1) * B + b] = bt > 0.0 ? 1.0 / bt : 0.0;
+        }
+    }
+}
+
 // one CTA per trajectory: exp(tau Tbar), combine weights, error estimate
 __global__ void k_pade_b(int m, int B, double tau_im, int norm_mode, BatchedScalars S, double* erracc) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1968,6 +2055,8 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
     if (staged < 0 || staged > 6) return DQ_ERR_ARG;
+    // reorthogonalisation runs between the axpy and the next SpMM: not in the fused forms
+    if (c->cfg.reorth && (staged == 2 || staged == 4)) return DQ_ERR_ARG;
     // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane, one CTA per SM
     if (staged == 6 && (!bs->mixed || R > 3 || tc != 32 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
         return DQ_ERR_ARG;
@@ -2530,6 +2619,13 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
     if (tm) tm->mark(DQ_KIND_AXPY, st);
     k_axpy_beta<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slab(0), slab(j), slab(j - 1),
                                                        slab(j + 1), bs->s, cy0, bs->chunks);
+    if (c->cfg.reorth) {
+        if (tm) tm->mark(DQ_KIND_AXPY, st);
+        for (int k = 1; k <= j; ++k)
+            k_reorth_dot_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, k, slab(k), slab(j + 1), bs->s,
+                                                                  cy0, bs->chunks);
+        k_reorth_apply_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slabs, se, bs->s, cy0, bs->chunks);
+    }
     return DQ_OK;
 }
 

@@ -24,6 +24,8 @@ struct PlainScalars {
     int s;                // Padé squarings of the last step
     int status;           // DQ_OK or a DQ_ERR_* code raised on the device
     unsigned int ticket[4];
+    cd h[kMaxL];          // full reorthogonalisation: <q_k, r_{j+1}>
+    unsigned int ticket_r[2];
 };
 
 constexpr int kPlainThreads = 256;

@@ -139,6 +139,48 @@ __global__ void __launch_bounds__(kPlainThreads) k_axpy_norm(int n, int j, const
     }
 }
 
+// Full reorthogonalisation (Hermitian dot, cfg.reorth): h_k = <q_k, r_{j+1}>
+// for one k per launch, then r_{j+1} -= sum_k h_k q_k and beta_j, sc_{j+1}
+// from the new norm (classical Gram-Schmidt once, FP64).
+__global__ void __launch_bounds__(kPlainThreads) k_reorth_dot(int n, int k, const cd* __restrict__ xk,
+                                                             const cd* __restrict__ r, double* partial,
+                                                             PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ar = 0.0, ai = 0.0;
+    if (i < n) {
+        const cd p = cmul(cconj(cscale(xk[i], ps->sc[k])), r[i]);
+        ar = p.x;
+        ai = p.y;
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(ar, ai, partial, &ps->ticket_r[0], out2) && threadIdx.x == 0) ps->h[k] = cmk(out2[0], out2[1]);
+}
+
+__global__ void __launch_bounds__(kPlainThreads) k_reorth_apply(int n, int j, const cd* __restrict__ x1,
+                                                               const cd* __restrict__ Q, cd* r, double* partial,
+                                                               PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double nn = 0.0;
+    if (i < n) {
+        cd v = r[i];
+        for (int k = 1; k <= j; ++k) {
+            const cd x = k == 1 ? x1[i] : Q[(size_t)k * n + i];
+            v = csub(v, cmul(ps->h[k], cscale(x, ps->sc[k])));
+        }
+        r[i] = v;
+        nn = cabs2(v);
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(nn, 0.0, partial, &ps->ticket_r[1], out2) && threadIdx.x == 0) {
+        double b = sqrt(out2[0]);
+        if (!isfinite(b)) atomicCAS(&ps->status, 0, DQ_ERR_NAN);
+        const double scale = sqrt(cabs2(ps->alpha[j])) + (j > 1 ? ps->beta[j - 1].x : 0.0);
+        if (b <= kBreakdownRel * scale) b = 0.0;
+        ps->beta[j] = cmk(b, 0.0);
+        ps->sc[j + 1] = b > 0.0 ? 1.0 / b : 0.0;
+    }
+}
+
 // ||H q_{m+1}||
 __global__ void __launch_bounds__(kPlainThreads) k_spmv_norm(int n, int j, const int* __restrict__ rowptr,
                                                             const int* __restrict__ col,
@@ -330,6 +372,12 @@ dq_status plain_step(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_ou
             k_spmv_alpha<false><<<G, T, 0, st>>>(n, j, c->d_rowptr, c->d_col, c->d_val, c->d_diag, rj, c->d_w,
                                                  c->d_partial, c->d_ps);
         k_axpy_norm<<<G, T, 0, st>>>(n, j, c->d_w, rj, rjm, rjp, c->d_partial, c->d_ps);
+        if (c->cfg.reorth) {
+            for (int k = 1; k <= j; ++k)
+                k_reorth_dot<<<G, T, 0, st>>>(n, k, k == 1 ? psi_in : c->d_Q + (size_t)k * n, rjp, c->d_partial,
+                                              c->d_ps);
+            k_reorth_apply<<<G, T, 0, st>>>(n, j, psi_in, c->d_Q, rjp, c->d_partial, c->d_ps);
+        }
     }
     k_spmv_norm<<<G, T, 0, st>>>(n, m + 1, c->d_rowptr, c->d_col, c->d_val, c->d_diag, c->d_Q + (size_t)(m + 1) * n,
                                  c->d_partial, c->d_ps);

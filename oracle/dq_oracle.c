@@ -384,6 +384,22 @@ double dqo_lanczos(const dqo_system *sys, const double *diag, const double *q1, 
             w[i] = csub(w[i], cmul(a, qj[i]));
             w[i] = csub(w[i], cmul(beta[j - 1], qjm[i]));
         }
+        if (sys->reorth) {
+            /* full reorthogonalisation: h_k = <q_k, w> for k = 1..j from the
+             * same w, then w -= sum_k h_k q_k (classical Gram-Schmidt, once) */
+            cx h[64];
+            for (int k = 1; k <= j; ++k) {
+                const cx *qk = Q + (size_t)k * n;
+                cx acc = {0, 0};
+                for (int i = 0; i < n; ++i) acc = cadd(acc, cmul(cconj(qk[i]), w[i]));
+                h[k] = acc;
+            }
+            for (int i = 0; i < n; ++i) {
+                cx acc = {0, 0};
+                for (int k = 1; k <= j; ++k) acc = cadd(acc, cmul(h[k], Q[(size_t)k * n + i]));
+                w[i] = csub(w[i], acc);
+            }
+        }
         double nn = 0.0;
         for (int i = 0; i < n; ++i) nn += cabs2(w[i]);
         double b = sqrt(nn);

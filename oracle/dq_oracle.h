@@ -49,6 +49,7 @@ typedef struct {
     double sigma_static;   /* static disorder sigma, redrawn per trajectory */
     const double *static_eps; /* optional explicit static energies (n), replaces h0diag+disorder */
     uint64_t seed;
+    int reorth;            /* 1: full reorthogonalisation (classical Gram-Schmidt, once) */
 } dqo_system;
 
 /* ---- building blocks ---- */

@@ -46,6 +46,7 @@ class _System(C.Structure):
         ("sigma_static", C.c_double),
         ("static_eps", C.POINTER(C.c_double)),
         ("seed", C.c_uint64),
+        ("reorth", C.c_int),
     ]
 
 
@@ -145,7 +146,7 @@ class System:
 
     def __init__(self, rowptr, col, val, h0diag, m, dt, hbar=None, dot_mode=DOT_BILINEAR,
                  norm_mode=NORM_COMPLEX, noise=NOISE_NONE, ka_substeps=1, sigma=None, tau=None,
-                 sigma_static=0.0, static_eps=None, seed=0):
+                 sigma_static=0.0, static_eps=None, seed=0, reorth=0):
         self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
         self.col = np.ascontiguousarray(col, dtype=np.int32)
         self.val = np.ascontiguousarray(val, dtype=np.float64)
@@ -164,7 +165,7 @@ class System:
             _dp(self.val),
             _dp(self.h0diag),
             m, dt, self.hbar, dot_mode, norm_mode, noise, ka_substeps,
-            _dp(self.sigma), _dp(self.tau), float(sigma_static), _dp(self.static_eps), seed,
+            _dp(self.sigma), _dp(self.tau), float(sigma_static), _dp(self.static_eps), seed, int(reorth),
         )
 
     def dense(self, diag=None):

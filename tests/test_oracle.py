@@ -120,6 +120,31 @@ def test_lanczos_relation(oracle):
     assert nav == pytest.approx(np.linalg.norm(H @ Q[m + 1]), rel=1e-12)
 
 
+def test_full_reorthogonalisation_keeps_the_basis_orthonormal(oracle):
+    """reorth = 1 (Hermitian dot): classical Gram-Schmidt against q_1..q_j after every step of the
+    recurrence keeps Q orthonormal to rounding where plain Lanczos drifts, and the step still equals
+    the dense exponential."""
+    import scipy.linalg as sl2
+    n = 200
+    rng = np.random.default_rng(4)
+    d = rng.normal(0, 400, n)
+    q1 = rng.normal(size=n) + 1j * rng.normal(size=n)
+    q1 /= np.linalg.norm(q1)
+    orth = {}
+    for reorth in (0, 1):
+        S = _chain_sys(oracle, n, 1, reorth=reorth)
+        S.m = 32
+        S.s.m = 32
+        Q, al, be, nav = S.lanczos(d, q1)
+        Qm = Q[1:33].T
+        orth[reorth] = np.abs(Qm.conj().T @ Qm - np.eye(32)).max()
+        out, err, nrm, s = S.krylov_step(d, q1)
+        ex = sl2.expm(-1j * S.dt / S.hbar * S.dense(d)) @ q1
+        assert np.abs(out - ex).max() < 1e-10
+    assert orth[1] < 1e-13
+    assert orth[1] <= orth[0]
+
+
 def test_ifft_matches_numpy(oracle):
     rng = np.random.default_rng(2)
     for n in (8, 64, 1024, 7, 30):
