@@ -102,12 +102,12 @@ def build_system():
     return systems.tube(w["around"], w["along"], cutoff=w["cutoff"])
 
 
-def make_prop(s, B, precision, seed, max_steps, pop_every=16):
+def make_prop(s, B, precision, seed, max_steps, pop_every=16, reorth=0):
     import dynaquant_b200 as dq
     w = WORKLOAD
     p = dq.Propagator(s.n, m=w["m"], n_traj=B, dt=w["dt"], noise=dq.NOISE_OU, sigma_static=w["sigma_static"],
                       seed=seed, dot=dq.DOT_HERMITIAN, precision=precision, pop_every=pop_every,
-                      max_steps=max_steps)
+                      max_steps=max_steps, reorth=reorth)
     p.set_system(s)
     p.set_noise_params(np.full(s.n, w["sigma"]), np.full(s.n, w["tau"]))
     p.set_initial_state(s.bright_state())
@@ -123,17 +123,29 @@ def spmm_bytes(s, B):
     return 20.0 * s.n * B + 8.0 * nnz_off + 4.0 * (s.n + 1)
 
 
-def measured_traffic():
-    """DRAM bytes per launch of the SpMM kernel from the committed ncu summary
-    (dram__bytes_read.sum + dram__bytes_write.sum of one capture), or None."""
-    p = os.path.join(ROOT, "profiles", "k_spmm_blk_tube60x500.md")
+# SpMM form per tiling `staged` value: kernel name and the committed ncu summary of it
+SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha)", "k_spmm_blk_tube60x500.md"),
+              2: ("k_lanczos_fused (r_{j+1} + SpMM + alpha, beta)", None),
+              3: ("k_spmm_warp (L1 gathers, warp per block + alpha)", None),
+              4: ("k_lanczos_fw (fused, warp-owned blocks)", None),
+              5: ("k_spmm_blk, 512-thread CTAs (L1 gathers + alpha)", None),
+              6: ("k_spmm_ring (TMA ring gathers + alpha)", "k_spmm_ring_tube60x500.md")}
+
+
+def measured_traffic(staged):
+    """DRAM bytes per launch of the chosen SpMM kernel from its committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of one capture), and the file, or (None, None)."""
+    name = SPMM_FORMS.get(staged, (None, None))[1]
+    if not name:
+        return None, None
+    p = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(p):
             if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":")[1])
+                return float(line.split(":")[1]), "profiles/" + name
     except OSError:
         pass
-    return None
+    return None, None
 
 
 def cpu_baseline_sample(s, threads, target_s=12.0):
@@ -311,7 +323,13 @@ def run_ours(args, rank, world, local_rank):
     p.close()
     peak, peak_kind = _peaks()
     spmm_ms = prof["spmm_alpha"][0]
+    if tiling["staged"] in (2, 4):
+        # fused forms: the dominant launch is the whole iteration (reads w, r_j, r_{j-1}, d and the
+        # CSR; writes r_{j+1} and w)
+        spmm_ms = prof["fused_iter"][0]
     bytes_spmm = spmm_bytes(s, B)
+    if tiling["staged"] in (2, 4):
+        bytes_spmm += 24.0 * s.n * B   # + r_j, r_{j-1} reads and the r_{j+1} write
     achieved = bytes_spmm / (spmm_ms / 1e3) / 1e9
     step_ms_eager = sum(v[0] * v[1] for v in prof.values()) / 2
     kernels_per_step = sum(v[1] for v in prof.values()) // 2
@@ -369,7 +387,28 @@ def run_ours(args, rank, world, local_rank):
         pm.close()
     except Exception as e:  # pragma: no cover - reported, not hidden
         pop_err = f"unavailable: {e}"
+    # ---- the same step with full FP64 reorthogonalisation ------------------------
+    pr = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=16, reorth=1)
+    if tiling["staged"] in (2, 4):   # the fused forms cannot reorthogonalise between iterations
+        pr.set_tiling(32, 2, 2, 3, 0, 1)
+    else:
+        pr.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
+                      tiling["staged"], tiling["groups"])
+    pr.reset()
+    pr.run(2)
+    rs = torch.cuda.ExternalStream(pr.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(rs)
+    pr.run(8)
+    e1.record(rs)
+    torch.cuda.synchronize()
+    reorth_ms = e0.elapsed_time(e1) / 8
+    pr.close()
+    with_reorth = {"value": B / (reorth_ms / 1e3), "unit": "traj-steps/s", "ms_per_step": reorth_ms,
+                   "note": "classical Gram-Schmidt against q_1..q_j after every iteration, FP64 sums; 8 steps"}
     adjoint = adjoint_leg()
+    traffic, traffic_src = measured_traffic(tiling["staged"])
     cpu_v, cpu_sample = cpu_baseline_sample(s, os.cpu_count() or 1)
     clocks = clk.summary()
     line = {
@@ -384,16 +423,18 @@ def run_ours(args, rank, world, local_rank):
                                                     "groups", "ms_per_iter")}},
         "e2e": e2e,
         "gpu_launches": int(kernels_per_step * K),
-        "roofline": {"bound": "hbm", "kernel": "k_spmm (SpMM + alpha)", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": SPMM_FORMS.get(tiling["staged"], ("SpMM + alpha",))[0],
+                     "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_spmm, "ms_per_launch": spmm_ms,
-                     "traffic": measured_traffic(),
-                     "traffic_source": "profiles/k_spmm_blk_tube60x500.md (ncu dram bytes, one launch)"},
+                     "traffic": traffic,
+                     "traffic_source": (traffic_src + " (ncu dram bytes, one launch)") if traffic_src else None},
         "kernels_ms_per_launch": {k: v[0] for k, v in prof.items()},
         "eager_step_ms": step_ms_eager,
         "plain_fp64": {"value": plain, "unit": "traj-steps/s", "speedup_batched_mixed": value / world / plain,
                        "sample": f"2 trajectories x {plain_steps} steps, dq_run_plain"},
         "pop_err_vs_fp64_oracle": pop_err,
+        "with_reorth": with_reorth,
         "adjoint": adjoint,
         "cpu_baseline": {"value": cpu_v, "unit": "traj-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
                          "sample": cpu_sample},

@@ -1630,8 +1630,21 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
         double accr[TPT], acci[TPT];
 #pragma unroll
         for (int t = 0; t < TPT; ++t) { accr[t] = 0.0; acci[t] = 0.0; }
-        // four slabs per trip: four independent loads in flight per thread
+        // eight slabs per trip: eight independent loads in flight per thread
         int j = 1;
+        for (; j + 7 <= m; j += 8) {
+            CV<Real, TPT> x[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) x[q] = ldv<Real, TPT, false>(slabs + 2 * slab_stride * (j + q), base);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    const double2 yv = yts[(j + q - 1) * TC + tl + t];
+                    accr[t] += yv.x * x[q].v[2 * t] - yv.y * x[q].v[2 * t + 1];
+                    acci[t] += yv.x * x[q].v[2 * t + 1] + yv.y * x[q].v[2 * t];
+                }
+        }
         for (; j + 3 <= m; j += 4) {
             CV<Real, TPT> x[4];
 #pragma unroll
