@@ -31,7 +31,7 @@ class Propagator:
 
     def __init__(self, n_sites, m=16, n_traj=1, dt=1.0, hbar=0.0, noise=NOISE_NONE, ka_substeps=1,
                  sigma_static=0.0, seed=0, dot=DOT_HERMITIAN, norm=NORM_COMPLEX, precision=PREC_MIXED,
-                 reorth=0, pop_every=1, max_steps=1024, device=0):
+                 reorth=0, pop_every=1, max_steps=1024, device=0, m_min=0, m_tol=0.0):
         self.L = _lib.load()
         cfg = _lib.Config()
         self.L.dq_config_default(C.byref(cfg))
@@ -39,6 +39,7 @@ class Propagator:
         cfg.noise_model, cfg.ka_substeps, cfg.sigma_static, cfg.seed = noise, ka_substeps, sigma_static, seed
         cfg.dot_mode, cfg.norm_mode, cfg.precision, cfg.reorth = dot, norm, precision, reorth
         cfg.pop_every, cfg.max_steps, cfg.device = pop_every, max_steps, device
+        cfg.m_min, cfg.m_tol = m_min, m_tol
         self.cfg = cfg
         self.n = n_sites
         self.n_traj = n_traj

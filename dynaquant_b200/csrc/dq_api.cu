@@ -80,7 +80,8 @@ dq_status dq_create(const dq_config* cfg, dq_ctx** out) {
     if (cfg->n_sites < 2 || cfg->m < 2 || cfg->m > kMaxM || cfg->n_traj < 1 || !(cfg->dt > 0) ||
         cfg->pop_every < 1 || cfg->max_steps < 1 || cfg->ka_substeps < 0 ||
         cfg->noise_model < DQ_NOISE_NONE || cfg->noise_model > DQ_NOISE_OU ||
-        (cfg->reorth && cfg->dot_mode != DQ_DOT_HERMITIAN) || cfg->m > cfg->n_sites)
+        (cfg->reorth && cfg->dot_mode != DQ_DOT_HERMITIAN) || cfg->m > cfg->n_sites ||
+        cfg->m_min < 0 || cfg->m_min > cfg->m || (cfg->m_min > 0 && cfg->m_min < 2) || cfg->m_tol < 0)
         return DQ_ERR_ARG;
     if ((cfg->n_sites + kPlainThreads - 1) / kPlainThreads > kMaxPartials) return DQ_ERR_ARG;
     dq_ctx* c = new (std::nothrow) dq_ctx();

@@ -321,6 +321,7 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int RPC = blockDim.x / TPR;
     const int chunk = blockIdx.y + cy0;
+    if (chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + tr * TPT;
     const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
     double sc[TPT], ar[TPT], ai[TPT];
@@ -428,6 +429,7 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_warp(int n, int B, int bpc, 
     __shared__ float4 rbuf[kWarps][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int chunk = blockIdx.y + cy0;
+    if (chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + lane * TPT;
     const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
     double sc[TPT], ar[TPT], ai[TPT];
@@ -572,6 +574,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
     const int W = NB * SR;
     const int halo = hb * SR;
     const int chunk = blockIdx.y;
+    if (chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + hl * TPT;
     const int r0 = blockIdx.x * rows_per_cta;
     const int r1 = min(n, r0 + rows_per_cta);
@@ -775,6 +778,7 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
     const int SR = BPS * R;             // rows per step
     const int tl = tr * TPT;
     const int chunk = blockIdx.y + cy0;
+    if (chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + tl;
     const int r0 = blockIdx.x * rows_per_cta;
     const int r1 = min(n, r0 + rows_per_cta);
@@ -943,6 +947,7 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
     const int W = NB * SR;                           // ring rows
     const int tl = tr * TPT;
     const int chunk = blockIdx.y;
+    if (chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + tl;
     const int r0 = blockIdx.x * rows_per_cta;
     const int r1 = min(n, r0 + rows_per_cta);
@@ -1188,6 +1193,7 @@ __global__ void __launch_bounds__(kFwThreads, 1) k_lanczos_fw(int n, int B, int 
     const int W = NB * SR;
     const int tl = lane * TPT;
     const int chunk = blockIdx.y;
+    if (chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + tl;
     const int r0 = blockIdx.x * rows_per_cta;
     const int r1 = min(n, r0 + rows_per_cta);
@@ -1429,6 +1435,7 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
                                                         const Real* __restrict__ rjm, Real* __restrict__ rjp,
                                                         BatchedScalars S, int cy0, int nch) {
     const Tile<TPT> T(TC, rpc, n, cy0);
+    if (chunk_converged(S, T.chunk)) return;
     double ajr[TPT], aji[TPT], bm[TPT], nn[TPT], zero[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) {
@@ -1500,6 +1507,7 @@ __global__ void __launch_bounds__(kBThreads) k_reorth_dot_b(int n, int B, int TC
                                                            const Real* __restrict__ xk, const Real* __restrict__ r,
                                                            BatchedScalars S, int cy0, int nch) {
     const Tile<TPT> T(TC, rpc, n, cy0);
+    if (chunk_converged(S, T.chunk)) return;
     double ar[TPT], ai[TPT], sck[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) {
@@ -1533,6 +1541,7 @@ template <typename Real, int TPT>
 __global__ void __launch_bounds__(kBThreads) k_reorth_apply_b(int n, int B, int TC, int rpc, int j, Real* slabs,
                                                              size_t slab_stride, BatchedScalars S, int cy0, int nch) {
     const Tile<TPT> T(TC, rpc, n, cy0);
+    if (chunk_converged(S, T.chunk)) return;
     Real* r = slabs + 2 * slab_stride * (j + 1);
     double nn[TPT], zero[TPT];
 #pragma unroll
@@ -1578,11 +1587,68 @@ __global__ void __launch_bounds__(kBThreads) k_reorth_apply_b(int n, int B, int 
     }
 }
 
+// ---- adaptive Krylov dimension (cfg.m_min > 0) -------------------------------
+__global__ void k_adapt_reset(int B, int chunks, int mmax, BatchedScalars S) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < B; b += gridDim.x * blockDim.x) {
+        S.mtraj[b] = 0;
+        if (b < chunks) {
+            S.cdone[b] = 0;
+            S.mchunk[b] = mmax;
+        }
+    }
+}
+
+// One CTA per undecided trajectory after iteration j: EXPOKIT's first error
+// term beta_j |E(j-1, j)| of exp(tau Tbar_j); the trajectory keeps dimension
+// j when it meets the tolerance.
+__global__ void k_mcheck_b(int j, int B, int TC, double tau_im, int norm_mode, double tol, BatchedScalars S) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ cd al[kMaxL], be[kMaxL];
+    const int b = blockIdx.x;
+    if (S.mtraj[b] != 0 || S.cdone[b / TC]) return;
+    for (int i = threadIdx.x; i <= j + 1; i += blockDim.x) {
+        const size_t k = (size_t)i * B + b;
+        al[i] = (i >= 1 && i <= j) ? cmk(S.alpha[2 * k], S.alpha[2 * k + 1]) : cmk(0, 0);
+        be[i] = (i >= 1 && i <= j) ? cmk(S.beta[k], 0.0) : cmk(0, 0);
+    }
+    __syncthreads();
+    const PadeOut o = pade_exp_tbar(j, al, be, cmk(0.0, tau_im), norm_mode, nullptr, smem);
+    if (threadIdx.x == 0 && o.s >= 0 && fabs(be[j].x) * sqrt(cabs2(o.e_m1_m)) <= tol) S.mtraj[b] = j;
+}
+
+// Per chunk: all trajectories decided -> its remaining iterations are skipped;
+// the largest decided dimension bounds the combine.  final: undecided
+// trajectories take the largest dimension.
+__global__ void k_chunk_flags(int TC, int mmax, int final_pass, BatchedScalars S) {
+    __shared__ int s_all, s_max;
+    if (threadIdx.x == 0) { s_all = 1; s_max = 0; }
+    __syncthreads();
+    const int c = blockIdx.x;
+    for (int t = threadIdx.x; t < TC; t += blockDim.x) {
+        int mb = S.mtraj[c * TC + t];
+        if (mb == 0 && final_pass) {
+            mb = mmax;
+            S.mtraj[c * TC + t] = mb;
+        }
+        if (mb == 0) atomicAnd(&s_all, 0);
+        atomicMax(&s_max, mb);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (s_all) {
+            S.cdone[c] = 1;
+            S.mchunk[c] = s_max;
+        }
+    }
+}
+
 // one CTA per trajectory: exp(tau Tbar), combine weights, error estimate
-__global__ void k_pade_b(int m, int B, double tau_im, int norm_mode, BatchedScalars S, double* erracc) {
+__global__ void k_pade_b(int mmax, int B, double tau_im, int norm_mode, BatchedScalars S, double* erracc) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ cd al[kMaxL], be[kMaxL], y[kMaxM];
     const int b = blockIdx.x;
+    // adaptive dimension: this trajectory's choice; weights past it are zero
+    const int m = S.mtraj ? S.mtraj[b] : mmax;
     for (int j = threadIdx.x; j <= m + 1; j += blockDim.x) {
         const size_t k = (size_t)j * B + b;
         al[j] = (j >= 1 && j <= m) ? cmk(S.alpha[2 * k], S.alpha[2 * k + 1]) : cmk(0, 0);
@@ -1595,13 +1661,17 @@ __global__ void k_pade_b(int m, int B, double tau_im, int norm_mode, BatchedScal
         return;
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    for (int j = threadIdx.x; j < mmax; j += blockDim.x) {
         const size_t k = (size_t)(j + 1) * B + b;
-        const cd v = cscale(y[j], S.sc[k]);
+        const cd v = j < m ? cscale(y[j], S.sc[k]) : cmk(0.0, 0.0);
         S.yt[2 * k] = v.x;
         S.yt[2 * k + 1] = v.y;
     }
-    if (threadIdx.x == 0) erracc[b] += expokit_error(be[m].x, S.nav[b], o.e_m1_m, o.e_m1_mp1);
+    if (threadIdx.x == 0) {
+        // with the adaptive dimension only err1 (||H q_{m+1}|| belongs to the largest m)
+        if (S.mtraj) erracc[b] += fmax(fabs(be[m].x) * sqrt(cabs2(o.e_m1_m)), 1.110223e-16);
+        else erracc[b] += expokit_error(be[m].x, S.nav[b], o.e_m1_m, o.e_m1_mp1);
+    }
 }
 
 // psi = sum_j yt_j r_j written over slab 1; ||psi||^2 and <psi0|psi> per
@@ -1625,6 +1695,7 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
 #pragma unroll
     for (int t = 0; t < TPT; ++t) { nn[t] = 0.0; cr[t] = 0.0; ci[t] = 0.0; }
     Real* r1 = slabs + 2 * slab_stride;
+    if (S.mchunk) m = S.mchunk[blockIdx.y];   // adaptive: the chunk's largest Krylov dimension
     for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
         const size_t base = (size_t)row * B + T.b0;
         double accr[TPT], acci[TPT];
@@ -2069,7 +2140,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
     if (staged < 0 || staged > 6) return DQ_ERR_ARG;
     // reorthogonalisation runs between the axpy and the next SpMM: not in the fused forms
-    if (c->cfg.reorth && (staged == 2 || staged == 4)) return DQ_ERR_ARG;
+    if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4)) return DQ_ERR_ARG;
     // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane, one CTA per SM
     if (staged == 6 && (!bs->mixed || R > 3 || tc != 32 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
         return DQ_ERR_ARG;
@@ -2356,7 +2427,15 @@ static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed) {
     DQ_CU(cudaMalloc(&bs->s.status, sizeof(int) * 2));
     bs->s.step = bs->s.status + 1;
     DQ_CU(cudaMemsetAsync(bs->s.status, 0, sizeof(int) * 2, c->stream));
+    bs->s.mtraj = bs->s.cdone = bs->s.mchunk = nullptr;
+    if (c->cfg.m_min > 0) {
+        DQ_CU(cudaMalloc(&bs->s.mtraj, sizeof(int) * 3 * (size_t)B));
+        DQ_CU(cudaMemsetAsync(bs->s.mtraj, 0, sizeof(int) * 3 * (size_t)B, c->stream));
+        bs->s.cdone = bs->s.mtraj + B;
+        bs->s.mchunk = bs->s.cdone + B;
+    }
     DQ_CU(cudaFuncSetAttribute(k_pade_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pade_smem_bytes(m + 2)));
+    DQ_CU(cudaFuncSetAttribute(k_mcheck_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pade_smem_bytes(m + 2)));
     // default tiling (dq_autotune refines it)
     int tpt = bs->mixed ? 2 : 1;
     int tc = 16;
@@ -2399,7 +2478,7 @@ void batched_free_ws(BatchedState* bs) {
         for (auto& f : bs->fmt) free_fmt(f);
     cudaFree(bs->wB);
     cudaFree(bs->slabs); cudaFree(bs->diag); cudaFree(bs->eps); cudaFree(bs->deps);
-    cudaFree(bs->scal_mem); cudaFree(bs->s.tickets); cudaFree(bs->s.status);
+    cudaFree(bs->scal_mem); cudaFree(bs->s.tickets); cudaFree(bs->s.status); cudaFree(bs->s.mtraj);
     delete bs;
 }
 
@@ -2666,14 +2745,32 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
                                                      c->cfg.seed, c->d_sigma, c->d_invtau, c->d_coeff, bs->eps,
                                                      bs->deps, (Real*)bs->diag, bs->s);
     if (after_noise) (*after_noise)();
-    // trajectory groups one after another: a group's Krylov slabs stay in L2
-    // across its m iterations
-    const int cpg = bs->chunks / bs->groups;
-    for (int g = 0; g < bs->groups; ++g) {
-        for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm, g * cpg, cpg);
-        if (bs->staged != 2 && bs->staged != 4) {   // the fused form's last launch gave ||H q_{m+1}||
-            mark(DQ_KIND_SPMM_NORM);
-            launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, g * cpg, cpg);
+    const bool adaptive = bs->s.mtraj != nullptr;
+    if (adaptive) {
+        // adaptive Krylov dimension: checks after iterations m_min, m_min + 4, ...;
+        // chunks whose trajectories all chose skip their remaining iterations
+        const int m_min = c->cfg.m_min;
+        const double tol = c->cfg.m_tol > 0 ? c->cfg.m_tol : 1e-7;
+        k_adapt_reset<<<(B + 255) / 256, 256, 0, st>>>(B, bs->chunks, m, bs->s);
+        for (int j = 1; j <= m; ++j) {
+            enqueue_iteration<Real, TPT>(c, j, tm, 0, bs->chunks);
+            if (j >= m_min && j < m && (j - m_min) % kMCheckStride == 0) {
+                mark(DQ_KIND_PADE);
+                k_mcheck_b<<<B, 128, pade_smem_bytes(j + 2), st>>>(j, B, TC, c->tau_im, c->cfg.norm_mode, tol, bs->s);
+                k_chunk_flags<<<bs->chunks, 64, 0, st>>>(TC, m, 0, bs->s);
+            }
+        }
+        k_chunk_flags<<<bs->chunks, 64, 0, st>>>(TC, m, 1, bs->s);
+    } else {
+        // trajectory groups one after another: a group's Krylov slabs stay in
+        // L2 across its m iterations
+        const int cpg = bs->chunks / bs->groups;
+        for (int g = 0; g < bs->groups; ++g) {
+            for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm, g * cpg, cpg);
+            if (bs->staged != 2 && bs->staged != 4) {   // the fused form's last launch gave ||H q_{m+1}||
+                mark(DQ_KIND_SPMM_NORM);
+                launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, g * cpg, cpg);
+            }
         }
     }
     mark(DQ_KIND_PADE);

@@ -15,6 +15,7 @@ constexpr int kBThreads = 256;
 constexpr int kMaxTC = 64;
 constexpr int kMaxCtasPerChunk = 4096;
 constexpr int kStreamCtasPerSm = 8;
+constexpr int kMCheckStride = 4;   // adaptive Krylov dimension: checks at m_min, m_min + 4, ... below m
 
 // ---- vector access of TPT consecutive complex values ----------------------
 template <typename Real, int TPT> struct VL;
@@ -84,7 +85,20 @@ struct BatchedScalars {
     int* status;      // [1]
     int* step;        // [1] current step index
     double* corr;     // [(max_steps+1)][chunks][2]
+    // adaptive Krylov dimension (null when the dimension is fixed): the
+    // dimension chosen per trajectory (0 = not yet), per chunk whether every
+    // trajectory has chosen (its remaining iterations exit at once) and the
+    // largest choice
+    int* mtraj;       // [B]
+    int* cdone;       // [chunks]
+    int* mchunk;      // [chunks]
 };
+
+// Iteration kernels return at once for a chunk whose trajectories all chose
+// their Krylov dimension (uniform over the chunk's CTAs, before any barrier).
+__device__ __forceinline__ bool chunk_converged(const BatchedScalars& S, int chunk) {
+    return S.cdone != nullptr && S.cdone[chunk] != 0;
+}
 
 // Thread -> (row lane, trajectory lane) map and the CTA's row range.
 template <int TPT>

@@ -78,8 +78,10 @@ typedef struct dq_config {
     int precision;          /* DQ_PREC_*: ensemble path (dq_run) */
     int reorth;             /* 1: full reorthogonalisation (Hermitian dot only) */
     int pop_every;          /* record ensemble populations every k steps */
-    int m_min;              /* adaptive Krylov dimension: lower bound (0 = fixed m) */
-    double m_tol;           /* adaptive Krylov dimension: EXPOKIT error tolerance */
+    int m_min;              /* adaptive Krylov dimension (ensemble path, dq_run): 0 = fixed m; else each
+                               trajectory takes the first j = m_min, m_min + 4, ... below m whose
+                               EXPOKIT term beta_j |E(j-1, j)| <= m_tol, or m (the plain path keeps m) */
+    double m_tol;           /* adaptive Krylov dimension: tolerance (0 selects 1e-7) */
     int max_steps;          /* capacity of the correlation / population records */
     int device;             /* CUDA device ordinal */
 } dq_config;

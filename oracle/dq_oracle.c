@@ -438,13 +438,48 @@ void dqo_build_tbar(int m, const double *alpha_d, const double *beta_d, double *
 
 int dqo_krylov_step(const dqo_system *sys, const double *diag, const double *psi_in, double *psi_out,
                     double *err_est, double *norm_out, int *s_out) {
-    int n = sys->n, m = sys->m, L = m + 2;
-    double *Q = (double *)malloc(sizeof(cx) * (size_t)n * (m + 2));
-    double *al = (double *)malloc(sizeof(cx) * (m + 2));
-    double *be = (double *)malloc(sizeof(cx) * (m + 2));
+    return dqo_krylov_step_m(sys, diag, psi_in, psi_out, err_est, norm_out, s_out, NULL);
+}
+
+/* EXPOKIT's first error term for a Krylov dimension j: beta_j |E(j-1, j)|,
+ * E = exp(tau Tbar_j) of the augmented (j+2) matrix. */
+static double err1_at(int j, const double *al, const double *be, cx tau, int norm_mode) {
+    const int L = j + 2;
     double *T = (double *)malloc(sizeof(cx) * L * L);
     double *E = (double *)malloc(sizeof(cx) * L * L);
+    dqo_build_tbar(j, al, be, T);
+    cx *Tc = (cx *)T;
+    for (int i = 0; i < L * L; ++i) Tc[i] = cmul(tau, Tc[i]);
+    const int s = dqo_pade_exp(L, T, E, norm_mode);
+    const cx *Ec = (const cx *)E;
+    const double r = s < 0 ? INFINITY : sqrt(cabs2(((const cx *)be)[j])) * sqrt(cabs2(Ec[(j - 1) * L + j]));
+    free(T);
+    free(E);
+    return r;
+}
+
+int dqo_krylov_step_m(const dqo_system *sys, const double *diag, const double *psi_in, double *psi_out,
+                      double *err_est, double *norm_out, int *s_out, int *m_used) {
+    int n = sys->n, mmax = sys->m;
+    double *Q = (double *)malloc(sizeof(cx) * (size_t)n * (mmax + 2));
+    double *al = (double *)malloc(sizeof(cx) * (mmax + 2));
+    double *be = (double *)malloc(sizeof(cx) * (mmax + 2));
     double nrm_av = dqo_lanczos(sys, diag, psi_in, Q, al, be);
+    const cx tau0 = {0.0, -sys->dt / sys->hbar};
+    int m = mmax;
+    if (sys->m_min > 0) {
+        /* adaptive dimension: the first checked j whose EXPOKIT err1 meets the tolerance */
+        for (int j = sys->m_min; j < mmax; j += DQO_M_CHECK_STRIDE) {
+            if (err1_at(j, al, be, tau0, sys->norm_mode) <= sys->m_tol) {
+                m = j;
+                break;
+            }
+        }
+    }
+    if (m_used) *m_used = m;
+    const int L = m + 2;
+    double *T = (double *)malloc(sizeof(cx) * L * L);
+    double *E = (double *)malloc(sizeof(cx) * L * L);
     dqo_build_tbar(m, al, be, T);
     cx tau = {0.0, -sys->dt / sys->hbar};
     cx *Tc = (cx *)T;
@@ -464,13 +499,14 @@ int dqo_krylov_step(const dqo_system *sys, const double *diag, const double *psi
     if (norm_out) *norm_out = nrm;
     double inv = 1. / nrm;
     for (int i = 0; i < n; ++i) out[i] = cscale(out[i], inv);
-    /* EXPOKIT Alg. 3.2 (padeClass.cu:750-782; systemClass.cu:2075-2077) */
+    /* EXPOKIT Alg. 3.2 (padeClass.cu:750-782; systemClass.cu:2075-2077); with
+     * the adaptive dimension only err1 (||H q_{m+1}|| belongs to the largest m) */
     if (err_est) {
         cx *bec = (cx *)be;
         double hm = sqrt(cabs2(bec[m]));
         double err1 = hm * sqrt(cabs2(Ec[(m - 1) * L + m]));
         double err2 = hm * nrm_av * sqrt(cabs2(Ec[(m - 1) * L + m + 1]));
-        double est = (err1 > err2) ? err2 / (1 - err2 / err1) : err1;
+        double est = (sys->m_min > 0) ? err1 : (err1 > err2) ? err2 / (1 - err2 / err1) : err1;
         if (est < 1.110223e-16) est = 1.110223e-16;
         *err_est = est;
     }

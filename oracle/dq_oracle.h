@@ -50,7 +50,13 @@ typedef struct {
     const double *static_eps; /* optional explicit static energies (n), replaces h0diag+disorder */
     uint64_t seed;
     int reorth;            /* 1: full reorthogonalisation (classical Gram-Schmidt, once) */
+    int m_min;             /* adaptive Krylov dimension: first check (0 = fixed m) */
+    double m_tol;          /* adaptive: accept the first checked j with beta_j |E(j-1, j)| <= m_tol */
 } dqo_system;
+
+/* Checks of the adaptive Krylov dimension happen at j = m_min, m_min + 4,
+ * ... below m; a trajectory that passes none uses m. */
+enum { DQO_M_CHECK_STRIDE = 4 };
 
 /* ---- building blocks ---- */
 void dqo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
@@ -76,6 +82,10 @@ void dqo_noise_update(const dqo_system *sys, int traj, int step, const double *e
  * norm_out the pre-renormalisation norm, s_out the Padé scaling. */
 int dqo_krylov_step(const dqo_system *sys, const double *diag, const double *psi_in,
                     double *psi_out, double *err_est, double *norm_out, int *s_out);
+/* As dqo_krylov_step, also returning the Krylov dimension used (m, or the
+ * adaptive choice when sys->m_min > 0). */
+int dqo_krylov_step_m(const dqo_system *sys, const double *diag, const double *psi_in,
+                      double *psi_out, double *err_est, double *norm_out, int *s_out, int *m_used);
 /* Lanczos only: Q (m+2) columns of n complex each (column 0 zero), alpha and
  * beta (m+2 complex each), returns ||H q_{m+1}||. */
 double dqo_lanczos(const dqo_system *sys, const double *diag, const double *q1,

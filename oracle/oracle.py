@@ -47,6 +47,8 @@ class _System(C.Structure):
         ("static_eps", C.POINTER(C.c_double)),
         ("seed", C.c_uint64),
         ("reorth", C.c_int),
+        ("m_min", C.c_int),
+        ("m_tol", C.c_double),
     ]
 
 
@@ -75,6 +77,8 @@ def lib():
         L.dqo_noise_update.argtypes = [sp, C.c_int, C.c_int, dp, dp, dp]
         L.dqo_krylov_step.argtypes = [sp, dp, dp, dp, dp, dp, C.POINTER(C.c_int)]
         L.dqo_krylov_step.restype = C.c_int
+        L.dqo_krylov_step_m.argtypes = [sp, dp, dp, dp, dp, dp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.dqo_krylov_step_m.restype = C.c_int
         L.dqo_lanczos.argtypes = [sp, dp, dp, dp, dp, dp]
         L.dqo_lanczos.restype = C.c_double
         L.dqo_build_tbar.argtypes = [C.c_int, dp, dp, dp]
@@ -146,7 +150,7 @@ class System:
 
     def __init__(self, rowptr, col, val, h0diag, m, dt, hbar=None, dot_mode=DOT_BILINEAR,
                  norm_mode=NORM_COMPLEX, noise=NOISE_NONE, ka_substeps=1, sigma=None, tau=None,
-                 sigma_static=0.0, static_eps=None, seed=0, reorth=0):
+                 sigma_static=0.0, static_eps=None, seed=0, reorth=0, m_min=0, m_tol=1e-7):
         self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
         self.col = np.ascontiguousarray(col, dtype=np.int32)
         self.val = np.ascontiguousarray(val, dtype=np.float64)
@@ -166,6 +170,7 @@ class System:
             _dp(self.h0diag),
             m, dt, self.hbar, dot_mode, norm_mode, noise, ka_substeps,
             _dp(self.sigma), _dp(self.tau), float(sigma_static), _dp(self.static_eps), seed, int(reorth),
+            int(m_min), float(m_tol),
         )
 
     def dense(self, diag=None):
@@ -197,6 +202,18 @@ class System:
         if rc != 0:
             raise RuntimeError(f"oracle krylov step failed ({rc})")
         return out, err.value, nrm.value, s.value
+
+    def krylov_step_m(self, diag, psi):
+        """One step; also returns the Krylov dimension used (adaptive when m_min > 0)."""
+        psi = np.ascontiguousarray(psi, dtype=np.complex128)
+        out = np.zeros_like(psi)
+        err, nrm, s, mu = C.c_double(), C.c_double(), C.c_int(), C.c_int()
+        rc = lib().dqo_krylov_step_m(C.byref(self.s), _dp(np.ascontiguousarray(diag, dtype=np.float64)),
+                                     _dp(psi.view(np.float64)), _dp(out.view(np.float64)),
+                                     C.byref(err), C.byref(nrm), C.byref(s), C.byref(mu))
+        if rc != 0:
+            raise RuntimeError(f"oracle krylov step failed ({rc})")
+        return out, err.value, mu.value
 
     def lanczos(self, diag, q1):
         n, m = self.n, self.m
