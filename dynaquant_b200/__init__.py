@@ -16,7 +16,7 @@ from . import _lib
 from ._lib import (DOT_BILINEAR, DOT_HERMITIAN, NOISE_GAUSS, NOISE_NONE, NOISE_OU, NORM_COMPLEX,
                    NORM_REAL_ONLY, PREC_FP64, PREC_MIXED, DQError)
 
-__all__ = ["Propagator", "DQError", "NOISE_NONE", "NOISE_GAUSS", "NOISE_OU", "DOT_BILINEAR", "DOT_HERMITIAN",
+__all__ = ["Propagator", "Group", "DQError", "NOISE_NONE", "NOISE_GAUSS", "NOISE_OU", "DOT_BILINEAR", "DOT_HERMITIAN",
            "NORM_REAL_ONLY", "NORM_COMPLEX", "PREC_FP64", "PREC_MIXED", "reference_hbar"]
 
 
@@ -217,3 +217,34 @@ class Propagator:
     @property
     def steps_done(self) -> int:
         return self.L.dq_steps_done(self.h)
+
+
+class Group:
+    """Several Propagators (aggregates of any size and trajectory count, one device) advanced together:
+    each step is one CUDA graph with a concurrent branch per member (dq_group_*)."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        self.L = _lib.load()
+        arr = (C.c_void_p * len(self.members))(*[m.h for m in self.members])
+        h = C.c_void_p()
+        rc = self.L.dq_group_create(arr, len(self.members), C.byref(h))
+        if rc != 0:
+            raise DQError(rc, "dq_group_create failed (members on one device, each once)")
+        self.h = h
+
+    def run(self, n_steps):
+        rc = self.L.dq_group_run(self.h, n_steps)
+        if rc != 0:
+            raise DQError(rc, self.L.dq_group_last_error(self.h).decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.dq_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -29,6 +29,7 @@ EXPORTS = [
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
     "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward",
+    "dq_group_create", "dq_group_destroy", "dq_group_last_error", "dq_group_run",
 ]
 
 
@@ -109,8 +110,15 @@ def load(path: str = LIB_PATH):
     L.dq_adjoint_setup.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp, C.c_int]
     L.dq_forward.argtypes = [vp, dp]
     L.dq_backward.argtypes = [vp, dp, dp]
+    L.dq_group_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
+    L.dq_group_destroy.argtypes = [vp]
+    L.dq_group_destroy.restype = None
+    L.dq_group_last_error.argtypes = [vp]
+    L.dq_group_last_error.restype = C.c_char_p
+    L.dq_group_run.argtypes = [vp, C.c_int]
     for name in EXPORTS:
-        if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done"):
+        if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done",
+                        "dq_group_destroy", "dq_group_last_error"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -2795,6 +2795,9 @@ static dq_status enqueue_step_any(dq_ctx* c, StepTimer* tm, const std::function<
                         : enqueue_step<float, 1>(c, tm, after_noise, skip_pop);
 }
 
+// One ensemble step of c enqueued on c's stream (stream capture by a group).
+dq_status batched_enqueue_step(dq_ctx* c) { return enqueue_step_any(c, nullptr); }
+
 dq_status batched_step_eager(dq_ctx* c, const std::function<void()>* after_noise, bool skip_pop) {
     return enqueue_step_any(c, nullptr, after_noise, skip_pop);
 }
@@ -2836,6 +2839,14 @@ dq_status batched_run(dq_ctx* c, int n_steps) {
     int status = 0;
     DQ_CU(cudaMemcpy(&status, bs->s.status, sizeof(int), cudaMemcpyDeviceToHost));
     c->steps_done += n_steps;
+    if (status) return read_status(c, status, "run");
+    return DQ_OK;
+}
+
+// Device status word of the ensemble (after a synchronisation).
+dq_status batched_read_status(dq_ctx* c) {
+    int status = 0;
+    DQ_CU(cudaMemcpy(&status, c->bat->s.status, sizeof(int), cudaMemcpyDeviceToHost));
     if (status) return read_status(c, status, "run");
     return DQ_OK;
 }

@@ -107,6 +107,8 @@ dq_status batched_alloc(dq_ctx* c);
 void batched_free(dq_ctx* c);
 dq_status batched_reset(dq_ctx* c);
 dq_status batched_run(dq_ctx* c, int n_steps);
+dq_status batched_enqueue_step(dq_ctx* c);
+dq_status batched_read_status(dq_ctx* c);
 dq_status batched_get_states(dq_ctx* c, dq_cdouble* out);
 dq_status batched_collect_corr(dq_ctx* c);
 dq_status batched_profile(dq_ctx* c, int n_steps, double* ms, int* cnt, int nk);

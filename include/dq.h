@@ -235,6 +235,19 @@ DQ_API dq_status dq_get_noise_state(dq_ctx *ctx, int traj, double *eps, double *
  * Replaces spectraClass::singleSpectraCalc's cufftExecZ2Z (spectraClass.cu:621). */
 DQ_API dq_status dq_get_spectrum(dq_ctx *ctx, int len, dq_cdouble *out);
 
+/* ---- several aggregates together (no reference counterpart) ----
+ * A group advances the ensembles of several contexts (aggregates of any
+ * size and trajectory count, on one device) by the same number of steps:
+ * each group step is one CUDA graph with one concurrent branch per member,
+ * so small aggregates run beside large ones.  Members keep their own
+ * settings (tiling, adaptive Krylov dimension, noise) and observables. */
+typedef struct dq_group dq_group;
+DQ_API dq_status dq_group_create(dq_ctx *const *members, int n_members, dq_group **out);
+DQ_API void dq_group_destroy(dq_group *group);
+DQ_API const char *dq_group_last_error(const dq_group *group);
+/* Advances every member by n_steps (as dq_run does for one context). */
+DQ_API dq_status dq_group_run(dq_group *group, int n_steps);
+
 /* ---- adjoint: gradient of a spectrum-fitting loss ----
  * No counterpart in the reference (it has no gradients).  The loss is
  *   L = sum_j (scale * Re(S_j) - target_j)^2,  j = 0..fft_len-1,
