@@ -204,6 +204,63 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+AGG = dict(name="tubes60xL_8aggregates_B512_adaptive_m8-32", around=60, Ls=(34, 68, 135, 270, 405, 540, 810, 1000),
+           B=(240, 120, 64, 32, 24, 16, 8, 8), m=32, m_min=8, m_tol=1e-7, dt=0.5, steps=2000)
+
+
+def aggregates_leg():
+    """Eight tubes 60 x L with 512 trajectories split about as 1/L (multiples of 8), adaptive Krylov
+    dimension 8..32 at tolerance 1e-7, dt 0.5 fs, 2000 steps: all aggregates in one graph per step
+    (dq_group_run) against the same aggregates run one after another (dq_run each)."""
+    import torch
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    a = AGG
+    w = WORKLOAD
+
+    def members(seed0):
+        out = []
+        for i, (L, B) in enumerate(zip(a["Ls"], a["B"])):
+            s = systems.tube(a["around"], L, cutoff=w["cutoff"])
+            p = dq.Propagator(s.n, m=a["m"], n_traj=B, dt=a["dt"], noise=dq.NOISE_OU, sigma_static=w["sigma_static"],
+                              seed=seed0 + i, dot=dq.DOT_HERMITIAN, precision=dq.PREC_MIXED, pop_every=50,
+                              max_steps=a["steps"] + 8, m_min=a["m_min"], m_tol=a["m_tol"])
+            p.set_system(s)
+            p.set_noise_params(np.full(s.n, w["sigma"]), np.full(s.n, w["tau"]))
+            p.set_initial_state(s.bright_state())
+            out.append(p)
+        return out
+
+    ms = members(500)
+    g = dq.Group(ms)
+    g.run(4)                       # warm-up (allocation, first capture)
+    for p in ms:
+        p.reset()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g.run(a["steps"])
+    torch.cuda.synchronize()
+    t_group = time.perf_counter() - t0
+    g.close()
+    for p in ms:
+        p.reset()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for p in ms:
+        p.run(a["steps"])
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    n_sites = [p.n for p in ms]
+    for p in ms:
+        p.close()
+    total = sum(a["B"]) * a["steps"]
+    return {"workload": a["name"], "sites": n_sites, "trajectories": list(a["B"]), "steps": a["steps"],
+            "value": total / t_group, "unit": "traj-steps/s", "sequential_value": total / t_seq,
+            "group_over_sequential": t_seq / t_group,
+            "note": "host wall clock around dq_group_run (one graph per step, a branch per aggregate) and around "
+                    "the eight dq_run calls; default tilings"}
+
+
 ADJ = dict(name="lattice64x64_B128_T2000_m16", L=64, J_nn=-250.0, J_nnn=40.0, B=128, dt=1.0, steps=2000, m=16,
            checkpoint_every=50, fft_len=4096, sigma=200.0, tau=100.0, eps_sigma=100.0, target_shift=30.0, seed=77)
 
@@ -408,6 +465,7 @@ def run_ours(args, rank, world, local_rank):
     with_reorth = {"value": B / (reorth_ms / 1e3), "unit": "traj-steps/s", "ms_per_step": reorth_ms,
                    "note": "classical Gram-Schmidt against q_1..q_j after every iteration, FP64 sums; 8 steps"}
     adjoint = adjoint_leg()
+    aggregates = aggregates_leg()
     traffic, traffic_src = measured_traffic(tiling["staged"])
     cpu_v, cpu_sample = cpu_baseline_sample(s, os.cpu_count() or 1)
     clocks = clk.summary()
@@ -436,6 +494,7 @@ def run_ours(args, rank, world, local_rank):
         "pop_err_vs_fp64_oracle": pop_err,
         "with_reorth": with_reorth,
         "adjoint": adjoint,
+        "aggregates": aggregates,
         "cpu_baseline": {"value": cpu_v, "unit": "traj-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
                          "sample": cpu_sample},
         "clocks": clocks,

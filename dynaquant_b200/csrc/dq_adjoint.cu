@@ -277,8 +277,15 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_grad(int n, int B, int m, i
         Real site = 0, cpl = 0;
         const cd p0 = psi0[valid ? row : r0];
         Real lr = (Real)(sr * p0.x - si * p0.y), li = (Real)(sr * p0.y + si * p0.x);
-        for (int a = 0; a < m; ++a) {
-            const T2 w = *reinterpret_cast<const T2*>(sW + (size_t)(a + 1) * slab_reals + 2 * x);
+        // W column streamed four entries ahead (a register pipeline), so its
+        // loads overlap the products
+        auto ldw = [&](int a) {
+            T2 v;
+            if (a < m) v = *reinterpret_cast<const T2*>(sW + (size_t)(a + 1) * slab_reals + 2 * x);
+            else { v.x = 0; v.y = 0; }
+            return v;
+        };
+        auto body = [&](int a, const T2& w) {
             Real Xr = 0, Xi = 0, Yr = 0, Yi = 0;
 #pragma unroll
             for (int c = 0; c < MM; ++c) {
@@ -301,6 +308,18 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_grad(int n, int B, int m, i
             const T2 y = Yc[a * kAdjTraj + tl];
             lr = fma(y.x, w.x, fma(-y.y, w.y, lr));
             li = fma(y.x, w.y, fma(y.y, w.x, li));
+        };
+        T2 w0 = ldw(0), w1 = ldw(1), w2 = ldw(2), w3 = ldw(3);
+        for (int a = 0; a < m; a += 4) {
+            const T2 n0 = ldw(a + 4), n1 = ldw(a + 5), n2 = ldw(a + 6), n3 = ldw(a + 7);
+            body(a, w0);
+            if (a + 1 < m) body(a + 1, w1);
+            if (a + 2 < m) body(a + 2, w2);
+            if (a + 3 < m) body(a + 3, w3);
+            w0 = n0;
+            w1 = n1;
+            w2 = n2;
+            w3 = n3;
         }
         double s_d = valid ? (double)site : 0.0;
         double c_d = valid ? (double)cpl - (double)d[x] * (double)site : 0.0;
@@ -334,7 +353,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_grad(int n, int B, int m, i
 // Coupling-class gradients when there are several classes:
 //   dL/dscale_c += sum_{p in c} vbase_p Re sum_b t_b(i) rV_b(col_p),
 //   t_b(i) = sum_a M_ab conj(rW_a(i)),
-// gathering the V basis at every neighbour column (m loads per entry).
+// gathering the V basis at every neighbour column (m loads per entry).  With
+// skip0, class-0 entries are left out: their sum follows on the host from the
+// total off-diagonal form (free from the Lanczos relation in k_adj_grad).
 template <typename Real, int MM>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_cls(int n, int B, int m, int rows_per_cta, int G, int C,
                                                         const Real* __restrict__ sV, const Real* __restrict__ sW,
@@ -342,7 +363,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_cls(int n, int B, int m, in
                                                         const int* __restrict__ col, const int* __restrict__ cls,
                                                         const double* __restrict__ vbase,
                                                         const typename R2<Real>::T* __restrict__ coef,
-                                                        double* __restrict__ gcls) {
+                                                        double* __restrict__ gcls, int skip0) {
     using T2 = typename R2<Real>::T;
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T2* Mc = reinterpret_cast<T2*>(sm_raw);
@@ -379,6 +400,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_cls(int n, int B, int m, in
         for (int q = 0; q < kAdjMaxClasses; ++q) acc[q] = 0.0;
         if (valid) {
             for (int p = rowptr[row]; p < rowptr[row + 1]; ++p) {
+                if (skip0 && cls[p] == 0) continue;
                 const size_t xk = (size_t)col[p] * B + b;
                 Real rr = 0;
 #pragma unroll
@@ -513,7 +535,8 @@ static void launch_cls(dq_ctx* c, AdjointState* a, int slot) {
                                                                (const Real*)slot_V(a, m, slot),                      \
                                                                (const Real*)a->ws2->slabs,                           \
                                                                slab_reals, c->d_rowptr, c->d_col, a->d_cls,           \
-                                                               a->d_vbase, (const T2*)a->d_coef, a->d_gcls)
+                                                               a->d_vbase, (const T2*)a->d_coef, a->d_gcls,    \
+                                                               c->scales[0] != 0.0)
     switch (mm_bucket(m)) {
         case 8: DQ_CLS(8); break;
         case 16: DQ_CLS(16); break;
@@ -831,6 +854,14 @@ dq_status dq_backward(dq_ctx* c, double* grad_sites, double* grad_classes) {
             double tot = 0.0;
             for (int k = 0; k < a->fin_blocks; ++k) tot += part[(size_t)k * a->n_cls + q];
             grad_classes[q] = tot;
+        }
+        if (c->scales[0] != 0.0) {
+            // class 0 from the total: sum_p val_p rho_p = sum_c scale_c grad_c
+            double total = 0.0;
+            for (int k = 0; k < a->fin_blocks; ++k) total += out[n + k];
+            double rest = 0.0;
+            for (int q = 1; q < a->n_cls; ++q) rest += c->scales[q] * grad_classes[q];
+            grad_classes[0] = (total - rest) / c->scales[0];
         }
     } else if (grad_classes) {
         double tot = 0.0;
