@@ -191,6 +191,20 @@ class Propagator:
         self._check(self.L.dq_get_noise_state(self.h, traj, _lib.dptr(eps), _lib.dptr(deps)))
         return eps, deps
 
+    # -- the reference's output files ---------------------------------------------
+    def write_populations(self, path, binary=False, continuation=False):
+        """pops.dat (popPrintClass format): population sums over trajectories per recorded step."""
+        self._check(self.L.dq_write_populations(self.h, str(path).encode(), int(binary), int(continuation)))
+
+    def write_states(self, folder):
+        """folder/_states_<t>.dat (statePrintClass format) for the current step."""
+        self._check(self.L.dq_write_states(self.h, str(folder).encode()))
+
+    def write_spectrum(self, corr_path, spec_path, scaling=1.0):
+        """Correlation and spectrum text files (spectraClass format), transform length steps + 1."""
+        self._check(self.L.dq_write_spectrum(self.h, str(corr_path).encode(), str(spec_path).encode(),
+                                             float(scaling)))
+
     # -- adjoint -------------------------------------------------------------------
     def adjoint_setup(self, n_steps, fft_len, scale, target, checkpoint_every=0):
         """Fixes the spectrum-fitting loss sum_j (scale*Re(S_j) - target_j)^2 (S: inverse DFT of the

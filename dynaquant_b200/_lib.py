@@ -30,6 +30,7 @@ EXPORTS = [
     "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
     "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward",
     "dq_group_create", "dq_group_destroy", "dq_group_last_error", "dq_group_run",
+    "dq_write_populations", "dq_write_states", "dq_write_spectrum",
 ]
 
 
@@ -116,6 +117,9 @@ def load(path: str = LIB_PATH):
     L.dq_group_last_error.argtypes = [vp]
     L.dq_group_last_error.restype = C.c_char_p
     L.dq_group_run.argtypes = [vp, C.c_int]
+    L.dq_write_populations.argtypes = [vp, C.c_char_p, C.c_int, C.c_int]
+    L.dq_write_states.argtypes = [vp, C.c_char_p]
+    L.dq_write_spectrum.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_double]
     for name in EXPORTS:
         if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done",
                         "dq_group_destroy", "dq_group_last_error"):

@@ -235,6 +235,28 @@ DQ_API dq_status dq_get_noise_state(dq_ctx *ctx, int traj, double *eps, double *
  * Replaces spectraClass::singleSpectraCalc's cufftExecZ2Z (spectraClass.cu:621). */
 DQ_API dq_status dq_get_spectrum(dq_ctx *ctx, int len, dq_cdouble *out);
 
+/* ---- the reference's output files ---- */
+/* pops.dat of popPrintClass (popPrintClass.cu:160-522): header numsims / dt /
+ * totalsteps / numprintedsites (text lines, or int/double/int/int in binary),
+ * then for every recorded step s >= 1 ("STEP s" in text) each site's SUM of
+ * |psi|^2 over the runs (text "%25.17g (site)").  numsims is the number of
+ * trajectories summed.  continuation = 1 adds the sums of the existing file
+ * at path (same dt, totalsteps, sites; numsims accumulates); the file is
+ * written as temp_<name> beside it and renamed over it.  With pop_every = 1
+ * the step lines are the reference's every step. */
+DQ_API dq_status dq_write_populations(dq_ctx *ctx, const char *path, int binary, int continuation);
+/* folder/_states_<t>.dat of statePrintClass (statePrintClass.cu:82-199) for
+ * the current step: float t = dt * steps done, int N, int n_traj, then every
+ * trajectory's normalised state (N complex128). */
+DQ_API dq_status dq_write_states(dq_ctx *ctx, const char *folder);
+/* The correlation and spectrum text files of spectraClass (spectraClass.cu:
+ * 621-690) for the ensemble-mean correlation of the steps done: transform
+ * length steps + 1, frequency index wrapped above steps/2, rev/fs and cm^-1
+ * axes (c = 299792458 m/s), values scaled by `scaling` held as a float (the
+ * caller passes mu_tot^2 for absorption or (pi/2) 1e-7 mu_tot RD_tot for CD),
+ * the transform also divided by the step count. */
+DQ_API dq_status dq_write_spectrum(dq_ctx *ctx, const char *corr_path, const char *spec_path, double scaling);
+
 /* ---- several aggregates together (no reference counterpart) ----
  * A group advances the ensembles of several contexts (aggregates of any
  * size and trajectory count, on one device) by the same number of steps:
