@@ -13,10 +13,10 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import (DOT_BILINEAR, DOT_HERMITIAN, NOISE_GAUSS, NOISE_NONE, NOISE_OU, NORM_COMPLEX,
+from ._lib import (DOT_BILINEAR, DOT_HERMITIAN, NOISE_GAUSS, NOISE_NONE, NOISE_OU, NOISE_ZZ, NORM_COMPLEX,
                    NORM_REAL_ONLY, PREC_FP64, PREC_MIXED, DQError)
 
-__all__ = ["Propagator", "Group", "DQError", "NOISE_NONE", "NOISE_GAUSS", "NOISE_OU", "DOT_BILINEAR", "DOT_HERMITIAN",
+__all__ = ["Propagator", "Group", "DQError", "NOISE_NONE", "NOISE_GAUSS", "NOISE_OU", "NOISE_ZZ", "DOT_BILINEAR", "DOT_HERMITIAN",
            "NORM_REAL_ONLY", "NORM_COMPLEX", "PREC_FP64", "PREC_MIXED", "reference_hbar"]
 
 
@@ -96,6 +96,15 @@ class Propagator:
         sigma = np.ascontiguousarray(np.broadcast_to(sigma, (self.n,)), dtype=np.float64)
         tau = None if tau is None else np.ascontiguousarray(np.broadcast_to(tau, (self.n,)), dtype=np.float64)
         self._check(self.L.dq_set_noise_params(self.h, _lib.dptr(sigma), _lib.dptr(tau)))
+
+    def set_zz_spectral_density(self, omega, J, d_omega, temperature):
+        """Spectral density of the ZZ real noise: omega and J in cm^-1 at spacing d_omega, temperature in K."""
+        omega = np.ascontiguousarray(omega, dtype=np.float64)
+        J = np.ascontiguousarray(J, dtype=np.float64)
+        if omega.shape != J.shape or omega.ndim != 1:
+            raise ValueError("omega and J must be 1-D arrays of one length")
+        self._check(self.L.dq_set_zz_spectral_density(self.h, len(omega), _lib.dptr(omega), _lib.dptr(J),
+                                                      float(d_omega), float(temperature)))
 
     def set_static_energies(self, eps):
         eps = None if eps is None else np.ascontiguousarray(eps, dtype=np.float64)

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libdq.so")
 
 DQ_OK, DQ_ERR_ARG, DQ_ERR_CUDA, DQ_ERR_BREAKDOWN, DQ_ERR_NAN, DQ_ERR_TIMEOUT, DQ_ERR_SCALING, DQ_ERR_STATE, \
     DQ_ERR_SINGULAR = range(9)
-NOISE_NONE, NOISE_GAUSS, NOISE_OU = 0, 1, 2
+NOISE_NONE, NOISE_GAUSS, NOISE_OU, NOISE_ZZ = 0, 1, 2, 3
 DOT_BILINEAR, DOT_HERMITIAN = 0, 1
 NORM_REAL_ONLY, NORM_COMPLEX = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
@@ -25,6 +25,7 @@ KIND_NAMES = ["noise", "spmm_alpha", "axpy_beta", "spmm_norm", "pade", "combine"
 EXPORTS = [
     "dq_config_default", "dq_create", "dq_destroy", "dq_last_error", "dq_get_stream",
     "dq_set_hamiltonian_csr", "dq_set_coupling_classes", "dq_set_noise_params", "dq_set_static_energies",
+    "dq_set_zz_spectral_density",
     "dq_set_initial_state", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
@@ -87,6 +88,7 @@ def load(path: str = LIB_PATH):
     L.dq_set_hamiltonian_csr.argtypes = [vp, C.c_int, ip, ip, dp]
     L.dq_set_coupling_classes.argtypes = [vp, ip, C.c_int, dp]
     L.dq_set_noise_params.argtypes = [vp, dp, dp]
+    L.dq_set_zz_spectral_density.argtypes = [vp, C.c_int, dp, dp, C.c_double, C.c_double]
     L.dq_set_static_energies.argtypes = [vp, dp]
     L.dq_set_initial_state.argtypes = [vp, dp]
     L.dq_reset.argtypes = [vp]

@@ -79,7 +79,7 @@ dq_status dq_create(const dq_config* cfg, dq_ctx** out) {
     *out = nullptr;
     if (cfg->n_sites < 2 || cfg->m < 2 || cfg->m > kMaxM || cfg->n_traj < 1 || !(cfg->dt > 0) ||
         cfg->pop_every < 1 || cfg->max_steps < 1 || cfg->ka_substeps < 0 ||
-        cfg->noise_model < DQ_NOISE_NONE || cfg->noise_model > DQ_NOISE_OU ||
+        cfg->noise_model < DQ_NOISE_NONE || cfg->noise_model > DQ_NOISE_ZZ ||
         (cfg->reorth && cfg->dot_mode != DQ_DOT_HERMITIAN) || cfg->m > cfg->n_sites ||
         cfg->m_min < 0 || cfg->m_min > cfg->m || (cfg->m_min > 0 && cfg->m_min < 2) || cfg->m_tol < 0)
         return DQ_ERR_ARG;
@@ -121,6 +121,7 @@ void dq_destroy(dq_ctx* c) {
     cudaFree(c->d_rowptr); cudaFree(c->d_col); cudaFree(c->d_val); cudaFree(c->d_valf); cudaFree(c->d_h0);
     cudaFree(c->d_static); cudaFree(c->d_sigma); cudaFree(c->d_invtau); cudaFree(c->d_coeff);
     cudaFree(c->d_psi0); cudaFree(c->d_pops); cudaFree(c->d_corr); cudaFree(c->d_erracc);
+    cudaFree(c->d_zz_omega); cudaFree(c->d_zz_coeff); cudaFree(c->d_zz_u);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -212,6 +213,32 @@ dq_status dq_set_noise_params(dq_ctx* c, const double* sigma, const double* tau)
     return DQ_OK;
 }
 
+dq_status dq_set_zz_spectral_density(dq_ctx* c, int n_osc, const double* omega, const double* J, double d_omega,
+                                     double temperature) {
+    if (!c) return DQ_ERR_ARG;
+    if (n_osc < 1 || n_osc > kMaxZZOsc || !omega || !J || !(temperature > 0) || !(d_omega > 0))
+        return fail(c, DQ_ERR_ARG, "zz: 1..1024 oscillators, positive spacing and temperature");
+    // systemClass.cu:1128-1139: hbar = 1, k_B = 0.695035 cm^-1/K, 1/cm -> 1/fs by 5308.84
+    const double pi = 3.14159265358979323846;
+    c->zz_omega.resize(n_osc);
+    c->zz_coeff.resize(n_osc);
+    for (int o = 0; o < n_osc; ++o) {
+        const double G = J[o] / (1 - exp(-1. / (0.695035 * temperature) * 1.0 * omega[o]));
+        c->zz_coeff[o] = sqrt(2.) * sqrt(G * d_omega / pi);
+        c->zz_omega[o] = omega[o] / 5308.84;
+        if (!std::isfinite(c->zz_coeff[o])) return fail(c, DQ_ERR_ARG, "zz: non-finite amplitude (omega <= 0?)");
+    }
+    c->zz_n_osc = n_osc;
+    dq_status st;
+    if ((st = upload(c, &c->d_zz_omega, c->zz_omega.data(), (size_t)n_osc))) return st;
+    if ((st = upload(c, &c->d_zz_coeff, c->zz_coeff.data(), (size_t)n_osc))) return st;
+    cudaFree(c->d_zz_u);
+    c->d_zz_u = nullptr;
+    DQ_CU(cudaMalloc(&c->d_zz_u, sizeof(float) * (size_t)c->cfg.n_traj * n_osc * c->n));
+    c->ready = false;   // the ensemble's phase buffer follows at the next reset
+    return DQ_OK;
+}
+
 dq_status dq_set_static_energies(dq_ctx* c, const double* eps) {
     if (!c) return DQ_ERR_ARG;
     if (!eps) {
@@ -236,7 +263,9 @@ dq_status dq_set_initial_state(dq_ctx* c, const dq_cdouble* psi0) {
 
 static dq_status check_ready(dq_ctx* c) {
     if (!c->have_ham) return fail(c, DQ_ERR_STATE, "no Hamiltonian set");
-    if (c->cfg.noise_model != DQ_NOISE_NONE && !c->have_noise) return fail(c, DQ_ERR_STATE, "no noise parameters set");
+    if ((c->cfg.noise_model == DQ_NOISE_GAUSS || c->cfg.noise_model == DQ_NOISE_OU) && !c->have_noise)
+        return fail(c, DQ_ERR_STATE, "no noise parameters set");
+    if (c->cfg.noise_model == DQ_NOISE_ZZ && c->zz_n_osc == 0) return fail(c, DQ_ERR_STATE, "no ZZ spectral density set");
     if (!c->have_psi0) return fail(c, DQ_ERR_STATE, "no initial state set");
     return DQ_OK;
 }

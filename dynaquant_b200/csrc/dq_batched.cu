@@ -59,6 +59,17 @@ __global__ void k_traj_init_b(int n, int B, uint64_t seed, const double* __restr
     }
 }
 
+// ZZ phase fractions of every (oscillator, site, trajectory), [osc][site][traj]
+__global__ void k_zz_phases_b(int n, int B, int n_osc, uint64_t seed, float* __restrict__ u) {
+    const size_t total = (size_t)n * B * n_osc;
+    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(x % B);
+        const size_t r = x / B;
+        const int i = (int)(r % n), o = (int)(r / n);
+        u[x] = zz_phase(seed, (uint32_t)b, (uint32_t)i, (uint32_t)o);
+    }
+}
+
 template <typename Real>
 __global__ void k_set_psi0_b(int n, int B, const cd* __restrict__ psi0, Real* __restrict__ r1) {
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
@@ -80,9 +91,31 @@ __global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int TC, int
                                                       const double* __restrict__ invtau,
                                                       const double* __restrict__ coeff,
                                                       const double* __restrict__ eps, double* __restrict__ deps,
-                                                      Real* __restrict__ d, BatchedScalars S) {
+                                                      Real* __restrict__ d, BatchedScalars S, ZZParams zz) {
     const Tile<TPT> T(TC, rpc, n);
     const int step = *S.step;
+    if (noise == DQ_NOISE_ZZ) {
+        // sum_osc c cos(omega t + phi) + eps (gpuSysHelper.cu:134-177), frac(omega t / 2 pi) shared
+        __shared__ double w[kMaxZZOsc];
+        for (int o = threadIdx.x; o < zz.n_osc; o += blockDim.x) w[o] = zz_wfrac(zz.omega[o], step, zz.dt);
+        __syncthreads();
+        const size_t stride = (size_t)n * B;
+        for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
+            const size_t x = (size_t)row * B + T.b0;
+            double acc[TPT];
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) acc[t] = 0.0;
+            const float* u = zz.u + x;
+            for (int o = 0; o < zz.n_osc; ++o) {
+                const double wo = w[o], co = __ldg(zz.coeff + o);
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) acc[t] = __dadd_rn(acc[t], zz_term(wo, co, __ldg(u + (size_t)o * stride + t)));
+            }
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) d[x + t] = (Real)__dadd_rn(acc[t], eps[x + t]);
+        }
+        return;
+    }
     for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
         if constexpr (TPT == 2) {
             // trajectories b0, b0+1 form one Philox pair (b0 is even)
@@ -2487,8 +2520,17 @@ dq_status batched_reset(dq_ctx* c) {
     const int n = c->n, B = bs->B;
     const int blocks = std::min(n, bs->sms * 8);
     const int thr = std::min(256, ((B + 31) / 32) * 32);
+    // a setter may have re-allocated a parameter array the captured step reads
+    drop_graph(bs);
     k_traj_init_b<<<blocks, thr, 0, c->stream>>>(n, B, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
                                                  c->d_sigma, c->cfg.noise_model, bs->eps, bs->deps);
+    if (c->cfg.noise_model == DQ_NOISE_ZZ) {
+        if (B != c->cfg.n_traj) {
+            c->err = "batched: ZZ phases are laid out for n_traj trajectories";
+            return DQ_ERR_STATE;
+        }
+        k_zz_phases_b<<<bs->sms * 16, 256, 0, c->stream>>>(n, B, c->zz_n_osc, c->cfg.seed, c->d_zz_u);
+    }
     const size_t real_sz = bs->mixed ? sizeof(float) : sizeof(double);
     const size_t slab = (size_t)n * B * 2 * real_sz;
     if (bs->mixed)
@@ -2721,6 +2763,18 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
     return DQ_OK;
 }
 
+static ZZParams zz_params(const dq_ctx* c) {
+    ZZParams zz;
+    if (c->cfg.noise_model == DQ_NOISE_ZZ) {
+        zz.n_osc = c->zz_n_osc;
+        zz.omega = c->d_zz_omega;
+        zz.coeff = c->d_zz_coeff;
+        zz.u = c->d_zz_u;
+        zz.dt = c->cfg.dt;
+    }
+    return zz;
+}
+
 // Advances the device step counter when a recomputed step records nothing.
 __global__ void k_advance_step(BatchedScalars S) {
     if (threadIdx.x == 0) *S.step = *S.step + 1;
@@ -2743,7 +2797,7 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
     mark(DQ_KIND_NOISE);
     k_noise_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, c->cfg.noise_model, ns, subdt, sqrt_subdt,
                                                      c->cfg.seed, c->d_sigma, c->d_invtau, c->d_coeff, bs->eps,
-                                                     bs->deps, (Real*)bs->diag, bs->s);
+                                                     bs->deps, (Real*)bs->diag, bs->s, zz_params(c));
     if (after_noise) (*after_noise)();
     const bool adaptive = bs->s.mtraj != nullptr;
     if (adaptive) {

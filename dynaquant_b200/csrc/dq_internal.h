@@ -30,6 +30,7 @@ struct PlainScalars {
 
 constexpr int kPlainThreads = 256;
 constexpr int kMaxPartials = 4096;
+constexpr int kMaxZZOsc = 1024;   // oscillators of one ZZ spectral density
 
 struct BatchedState;   // dq_batched.cu
 struct AdjointState;   // dq_adjoint.cu
@@ -67,6 +68,13 @@ struct dq_ctx {
     double* d_coeff = nullptr;
     dq::cd* d_psi0 = nullptr;
     int nnz_off = 0;
+    // ZZ real noise: oscillators (angular frequency rad/fs, amplitude) and
+    // the plain path's phase fractions [traj][osc][site]
+    int zz_n_osc = 0;
+    std::vector<double> zz_omega, zz_coeff;
+    double* d_zz_omega = nullptr;
+    double* d_zz_coeff = nullptr;
+    float* d_zz_u = nullptr;   // ensemble phase fractions [osc][site][traj]
 
     // plain path: per trajectory state [traj][site], work buffers
     double* d_eps_p = nullptr;

@@ -18,6 +18,8 @@
 #include <cstdio>
 #include <mutex>
 
+#include <algorithm>
+
 #include "dq_internal.h"
 #include "dq_rng.cuh"
 
@@ -36,6 +38,21 @@ __global__ void k_traj_init_plain(int n, int n_traj, uint64_t seed, const double
         eps[x] = e;
         deps[x] = (noise == DQ_NOISE_OU) ? __dmul_rn(sigma[i], normal(seed, P_OU_INIT, t, 0, i, 0)) : 0.0;
     }
+}
+
+// ZZ diagonal of one trajectory at step: sum_osc c cos(omega t + phi) + eps
+// (gpuSysHelper.cu:134-177); the phases are drawn from Philox here, one per (site, osc)
+__global__ void k_noise_zz(int n, int traj, int step, uint64_t seed, ZZParams zz, const double* __restrict__ eps,
+                           double* __restrict__ diag) {
+    __shared__ double w[kMaxZZOsc];
+    for (int o = threadIdx.x; o < zz.n_osc; o += blockDim.x) w[o] = zz_wfrac(zz.omega[o], step, zz.dt);
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc = 0.0;
+    for (int o = 0; o < zz.n_osc; ++o)
+        acc = __dadd_rn(acc, zz_term(w[o], zz.coeff[o], zz_phase(seed, (uint32_t)traj, (uint32_t)i, (uint32_t)o)));
+    diag[i] = __dadd_rn(acc, eps[i]);
 }
 
 __global__ void k_noise(int n, int traj, int step, int noise, int ns, double subdt, double sqrt_subdt,
@@ -359,8 +376,17 @@ dq_status plain_step(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_ou
     const double sqrt_subdt = sqrt(subdt);
     const double* eps = c->d_eps_p + (size_t)traj * n;
     double* deps = c->d_deps_p + (size_t)traj * n;
-    k_noise<<<G, T, 0, st>>>(n, traj, step, c->cfg.noise_model, ns, subdt, sqrt_subdt, c->cfg.seed, c->d_sigma,
-                             c->d_invtau, c->d_coeff, eps, deps, c->d_diag, c->d_ps);
+    if (c->cfg.noise_model == DQ_NOISE_ZZ) {
+        ZZParams zz;
+        zz.n_osc = c->zz_n_osc;
+        zz.omega = c->d_zz_omega;
+        zz.coeff = c->d_zz_coeff;
+        zz.dt = c->cfg.dt;
+        k_noise_zz<<<G, T, 0, st>>>(n, traj, step, c->cfg.seed, zz, eps, c->d_diag);
+    } else {
+        k_noise<<<G, T, 0, st>>>(n, traj, step, c->cfg.noise_model, ns, subdt, sqrt_subdt, c->cfg.seed, c->d_sigma,
+                                 c->d_invtau, c->d_coeff, eps, deps, c->d_diag, c->d_ps);
+    }
     for (int j = 1; j <= m; ++j) {
         const cd* rj = (j == 1) ? psi_in : c->d_Q + (size_t)j * n;
         const cd* rjm = (j <= 1) ? nullptr : (j == 2 ? psi_in : c->d_Q + (size_t)(j - 1) * n);

@@ -17,7 +17,7 @@
 
 namespace dq {
 
-enum : uint32_t { P_OU = 1, P_GAUSS = 2, P_OU_INIT = 3, P_STATIC = 4 };
+enum : uint32_t { P_OU = 1, P_GAUSS = 2, P_OU_INIT = 3, P_STATIC = 4, P_ZZPHASE = 5 };
 
 __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 #pragma unroll
@@ -158,4 +158,43 @@ __device__ __forceinline__ void ou_update_pair(double& c0, double& c1, double in
     }
 }
 
+// ---- ZZ real noise (gpuSysHelper.cu:134-177) ------------------------------
+// Phase fraction phi / 2 pi of oscillator osc at site for a trajectory, as a
+// float: one Philox block per trajectory pair (even: first 64 bits).
+__device__ __forceinline__ float zz_phase(uint64_t seed, uint32_t traj, uint32_t site, uint32_t osc) {
+    uint32_t c[4] = {site, osc, traj >> 1, P_ZZPHASE << 24};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t a = (traj & 1) ? (((uint64_t)c[3] << 32) | c[2]) : (((uint64_t)c[1] << 32) | c[0]);
+    float u = __double2float_rn(__dmul_rn((double)(a >> 11), 0x1.0p-53));
+    if (u >= 1.0f) u = 0.0f;
+    return u;
+}
+
+constexpr double kZZInv2Pi = 0x1.45f306dc9c883p-3;   // 1 / (2 pi)
+
+// frac(omega t / 2 pi) for one oscillator at t = step dt
+__device__ __forceinline__ double zz_wfrac(double omega, int step, double dt) {
+    const double t = __dmul_rn((double)step, dt);
+    const double w = __dmul_rn(__dmul_rn(omega, t), kZZInv2Pi);
+    return __dsub_rn(w, floor(w));
+}
+
+// coeff cos(2 pi frac(w + u)) of one oscillator
+__device__ __forceinline__ double zz_term(double w, double coeff, float u) {
+    double x = __dadd_rn(w, (double)u);
+    if (x >= 1.0) x = __dsub_rn(x, 1.0);
+    double sn, cs;
+    own_sincos_2pi(x, sn, cs);
+    return __dmul_rn(coeff, cs);
+}
+
+struct ZZParams {
+    int n_osc = 0;
+    const double* omega = nullptr;   // rad/fs
+    const double* coeff = nullptr;   // cm^-1
+    const float* u = nullptr;        // phase fractions
+    double dt = 0.0;
+};
+
 }  // namespace dq
+

@@ -52,7 +52,8 @@ enum {
 };
 
 /* Noise on the diagonal site energies (includeFiles.cu:19-25). */
-enum { DQ_NOISE_NONE = 0, DQ_NOISE_GAUSS = 1 /* SIM_TYPE_HSR */, DQ_NOISE_OU = 2 /* SIM_TYPE_KUBO_ANDERSON */ };
+enum { DQ_NOISE_NONE = 0, DQ_NOISE_GAUSS = 1 /* SIM_TYPE_HSR */, DQ_NOISE_OU = 2 /* SIM_TYPE_KUBO_ANDERSON */,
+       DQ_NOISE_ZZ = 3 /* SIM_TYPE_ZZ_REAL_NOISE */ };
 /* Lanczos alpha: DQ_DOT_BILINEAR is the reference's unconjugated cublasZdotu
  * (lanczosClass.cu:421); DQ_DOT_HERMITIAN the Hermitian inner product. */
 enum { DQ_DOT_BILINEAR = 0, DQ_DOT_HERMITIAN = 1 };
@@ -111,6 +112,15 @@ DQ_API dq_status dq_set_coupling_classes(dq_ctx *ctx, const int *cls, int n_clas
 /* Per-site noise parameters: sigma (cm^-1) and, for OU, tau (fs).
  * Replaces prepForKA / prepForHsr (systemClass.cu:912-1071). */
 DQ_API dq_status dq_set_noise_params(dq_ctx *ctx, const double *sigma, const double *tau);
+/* ZZ real noise (SIM_TYPE_ZZ_REAL_NOISE; prepForZZReal, systemClass.cu:1077-1207):
+ * the spectral density's n_osc points omega (cm^-1) and J (cm^-1), spacing
+ * d_omega and temperature (K).  Each site's diagonal at t = step dt is its
+ * static energy plus sum_osc c cos(omega_fs t + phi), c = sqrt(2) sqrt(G d_omega
+ * / pi), G = J / (1 - exp(-omega / (k_B T))), omega_fs = omega / 5308.84, with
+ * phases drawn per trajectory, site and oscillator (Philox; the reference
+ * redraws them per run, systemClass.cu:1212-1234). */
+DQ_API dq_status dq_set_zz_spectral_density(dq_ctx *ctx, int n_osc, const double *omega, const double *J,
+                                            double d_omega, double temperature);
 /* Explicit static site energies shared by all trajectories (replaces the
  * Hamiltonian diagonal plus static disorder); NULL restores them. */
 DQ_API dq_status dq_set_static_energies(dq_ctx *ctx, const double *eps);

@@ -353,6 +353,52 @@ void dqo_noise_update(const dqo_system *sys, int traj, int step, const double *e
 }
 
 /* ------------------------------------------------------------------ */
+/* ZZ real noise                                                       */
+/* ------------------------------------------------------------------ */
+static const double ZZ_INV_2PI = 0x1.45f306dc9c883p-3; /* 1 / (2 pi) */
+
+void dqo_zz_coefficients(int n_osc, const double *omega_invcm, const double *J, double d_omega, double temperature,
+                         double *omega_fs, double *coeff) {
+    /* systemClass.cu:1128-1139 with hbar = 1, k_B = 0.695035 cm^-1/K,
+     * pi = 3.14159265358979323846 and the 1/cm -> 1/fs factor 5308.84 */
+    const double pi = 3.14159265358979323846;
+    for (int o = 0; o < n_osc; ++o) {
+        const double G = J[o] / (1 - exp(-1. / (0.695035 * temperature) * 1.0 * omega_invcm[o]));
+        coeff[o] = sqrt(2.) * sqrt(G * d_omega / pi);
+        omega_fs[o] = omega_invcm[o] / 5308.84;
+    }
+}
+
+float dqo_zz_phase(uint64_t seed, uint32_t traj, uint32_t site, uint32_t osc) {
+    uint32_t ctr[4] = {site, osc, traj >> 1, (uint32_t)DQO_P_ZZPHASE << 24};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t o[4];
+    dqo_philox4x32_10(ctr, key, o);
+    const uint64_t a = (traj & 1) ? (((uint64_t)o[3] << 32) | o[2]) : (((uint64_t)o[1] << 32) | o[0]);
+    float u = (float)((double)(a >> 11) * 0x1.0p-53);
+    if (u >= 1.0f) u = 0.0f; /* the same phase */
+    return u;
+}
+
+void dqo_noise_update_zz(const dqo_system *sys, int step, const double *eps, const float *u, double *diag) {
+    const int n = sys->n;
+    const double t = (double)step * sys->dt;
+    for (int i = 0; i < n; ++i) {
+        double acc = 0.0;
+        for (int o = 0; o < sys->n_osc; ++o) {
+            double w = (sys->zz_omega[o] * t) * ZZ_INV_2PI;
+            w = w - floor(w);
+            double x = w + (double)u[(size_t)o * n + i];
+            if (x >= 1.0) x = x - 1.0;
+            double sn, cs;
+            dqo_sincos_2pi(x, &sn, &cs);
+            acc = acc + sys->zz_coeff[o] * cs;
+        }
+        diag[i] = acc + eps[i];
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* Lanczos                                                             */
 /* ------------------------------------------------------------------ */
 static void spmv(const dqo_system *sys, const double *diag, const cx *x, cx *y) {
@@ -543,6 +589,7 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
         double *myc = cacc + (size_t)tid * (n_steps + 1) * 2;
         double *eps = (double *)malloc(sizeof(double) * n * 3);
         double *deps = eps + n, *diag = deps + n;
+        float *zzu = sys->noise == DQO_NOISE_ZZ ? (float *)malloc(sizeof(float) * (size_t)sys->n_osc * n) : NULL;
         cx *psi = (cx *)malloc(sizeof(cx) * n * 2);
         cx *tmp = psi + n;
 #ifdef _OPENMP
@@ -551,6 +598,10 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
         for (int t = 0; t < n_traj; ++t) {
             int traj = traj0 + t;
             dqo_traj_init(sys, traj, eps, deps);
+            if (zzu)
+                for (int o = 0; o < sys->n_osc; ++o)
+                    for (int i = 0; i < n; ++i)
+                        zzu[(size_t)o * n + i] = dqo_zz_phase(sys->seed, (uint32_t)traj, (uint32_t)i, (uint32_t)o);
             memcpy(psi, psi0, sizeof(cx) * n);
             double errsum = 0.0;
             cx c = {0, 0};
@@ -558,7 +609,8 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
             myc[0] += c.re; myc[1] += c.im;
             for (int i = 0; i < n; ++i) myp[i] += cabs2(psi[i]);
             for (int k = 0; k < n_steps; ++k) {
-                dqo_noise_update(sys, traj, k, eps, deps, diag);
+                if (zzu) dqo_noise_update_zz(sys, k, eps, zzu, diag);
+                else dqo_noise_update(sys, traj, k, eps, deps, diag);
                 double est;
                 int rc = dqo_krylov_step(sys, diag, (const double *)psi, (double *)tmp, &est, NULL, NULL);
                 if (rc != 0) { status = rc; break; }
@@ -576,6 +628,7 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
             if (err_acc) err_acc[t] = errsum;
         }
         free(eps);
+        free(zzu);
         free(psi);
     }
     double inv = 1.0 / n_traj;
@@ -669,13 +722,19 @@ double dqo_spectrum_loss_grad(const dqo_system *sys, const double *val_base, con
     cx *C = (cx *)calloc((size_t)(T + 1), sizeof(cx));
     double *eps = (double *)malloc(sizeof(double) * n * 2);
     double *deps = eps + n;
+    float *zzu = sys->noise == DQO_NOISE_ZZ ? (float *)malloc(sizeof(float) * (size_t)sys->n_osc * n) : NULL;
     for (int b = 0; b < n_traj; ++b) {
         dqo_traj_init(sys, b, eps, deps);
+        if (zzu)
+            for (int o = 0; o < sys->n_osc; ++o)
+                for (int i = 0; i < n; ++i)
+                    zzu[(size_t)o * n + i] = dqo_zz_phase(sys->seed, (uint32_t)b, (uint32_t)i, (uint32_t)o);
         cx *ps = psi_all + (size_t)b * (T + 1) * n;
         memcpy(ps, psi0, sizeof(cx) * n);
         for (int k = 0; k < T; ++k) {
             double *d = diag_all + ((size_t)b * T + k) * n;
-            dqo_noise_update(sys, b, k, eps, deps, d);
+            if (zzu) dqo_noise_update_zz(sys, k, eps, zzu, d);
+            else dqo_noise_update(sys, b, k, eps, deps, d);
             dqo_krylov_step(sys, d, (const double *)(ps + (size_t)k * n), (double *)(ps + (size_t)(k + 1) * n), NULL,
                             NULL, NULL);
         }
@@ -698,7 +757,7 @@ double dqo_spectrum_loss_grad(const dqo_system *sys, const double *val_base, con
         Gv[j].re = 2.0 * scale * a;
     }
     if (!grad) {
-        free(psi_all); free(diag_all); free(C); free(eps); free(S); free(Gv);
+        free(psi_all); free(diag_all); free(C); free(eps); free(zzu); free(S); free(Gv);
         return loss;
     }
     dqo_ifft(len, (double *)Gv);
@@ -777,7 +836,7 @@ double dqo_spectrum_loss_grad(const dqo_system *sys, const double *val_base, con
                 lam[i] = cadd(cscale(cmul(cconj(Gv[t]), psi0[i]), 1.0 / n_traj), Ul[i]);
         }
     }
-    free(psi_all); free(diag_all); free(C); free(eps); free(S); free(Gv);
+    free(psi_all); free(diag_all); free(C); free(eps); free(zzu); free(S); free(Gv);
     free(V); free(W); free(aV); free(lam); free(Z); free(TW); free(tb);
     return loss;
 }

@@ -21,7 +21,7 @@ extern "C" {
 #endif
 
 /* Noise models (reference enum simulationType, includeFiles.cu:19-25). */
-enum { DQO_NOISE_NONE = 0, DQO_NOISE_GAUSS = 1, DQO_NOISE_OU = 2 };
+enum { DQO_NOISE_NONE = 0, DQO_NOISE_GAUSS = 1, DQO_NOISE_OU = 2, DQO_NOISE_ZZ = 3 };
 /* Lanczos alpha: reference-exact unconjugated dot (lanczosClass.cu:421,
  * cublasZdotu) or the Hermitian inner product. */
 enum { DQO_DOT_BILINEAR = 0, DQO_DOT_HERMITIAN = 1 };
@@ -29,7 +29,7 @@ enum { DQO_DOT_BILINEAR = 0, DQO_DOT_HERMITIAN = 1 };
  * the complex-modulus infinity norm. */
 enum { DQO_NORM_REAL_ONLY = 0, DQO_NORM_COMPLEX = 1 };
 /* Philox purposes (the fourth counter word's top byte). */
-enum { DQO_P_OU = 1, DQO_P_GAUSS = 2, DQO_P_OU_INIT = 3, DQO_P_STATIC = 4 };
+enum { DQO_P_OU = 1, DQO_P_GAUSS = 2, DQO_P_OU_INIT = 3, DQO_P_STATIC = 4, DQO_P_ZZPHASE = 5 };
 
 typedef struct {
     int n;                 /* sites */
@@ -52,6 +52,9 @@ typedef struct {
     int reorth;            /* 1: full reorthogonalisation (classical Gram-Schmidt, once) */
     int m_min;             /* adaptive Krylov dimension: first check (0 = fixed m) */
     double m_tol;          /* adaptive: accept the first checked j with beta_j |E(j-1, j)| <= m_tol */
+    int n_osc;             /* ZZ real noise: oscillators per site */
+    const double *zz_omega; /* ZZ: angular frequencies (rad/fs), n_osc */
+    const double *zz_coeff; /* ZZ: amplitudes (cm^-1), n_osc */
 } dqo_system;
 
 /* Checks of the adaptive Krylov dimension happen at j = m_min, m_min + 4,
@@ -91,6 +94,19 @@ int dqo_krylov_step_m(const dqo_system *sys, const double *diag, const double *p
 double dqo_lanczos(const dqo_system *sys, const double *diag, const double *q1,
                    double *Q, double *alpha, double *beta);
 void dqo_build_tbar(int m, const double *alpha, const double *beta, double *T);
+
+/* ---- ZZ real noise (gpuSysHelper.cu:134-177, systemClass.cu:1077-1240) ---- */
+/* Amplitude and angular frequency of one oscillator of the spectral density:
+ * G = J / (1 - exp(-omega / (k_B T))), coeff = sqrt(2) sqrt(G d_omega / pi),
+ * omega_fs = omega / 5308.84 (omega, J, d_omega in cm^-1, T in K). */
+void dqo_zz_coefficients(int n_osc, const double *omega_invcm, const double *J, double d_omega, double temperature,
+                         double *omega_fs, double *coeff);
+/* Phase fraction (phi / 2 pi, float) of oscillator osc at site for a
+ * trajectory: Philox keyed (seed, ZZPHASE, trajectory pair, osc, site). */
+float dqo_zz_phase(uint64_t seed, uint32_t traj, uint32_t site, uint32_t osc);
+/* diag_i = sum_osc coeff cos(2 pi frac(omega t / 2 pi + u_osc,i)) + eps_i at
+ * t = step dt; u is [osc][site]. */
+void dqo_noise_update_zz(const dqo_system *sys, int step, const double *eps, const float *u, double *diag);
 
 /* ---- ensemble run ---- */
 /* Runs trajectories traj0..traj0+n_traj-1 for n_steps from psi0 (n complex).

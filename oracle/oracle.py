@@ -15,10 +15,10 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liboracle.so")
 
-NOISE_NONE, NOISE_GAUSS, NOISE_OU = 0, 1, 2
+NOISE_NONE, NOISE_GAUSS, NOISE_OU, NOISE_ZZ = 0, 1, 2, 3
 DOT_BILINEAR, DOT_HERMITIAN = 0, 1
 NORM_REAL_ONLY, NORM_COMPLEX = 0, 1
-P_OU, P_GAUSS, P_OU_INIT, P_STATIC = 1, 2, 3, 4
+P_OU, P_GAUSS, P_OU_INIT, P_STATIC, P_ZZPHASE = 1, 2, 3, 4, 5
 
 
 def build() -> str:
@@ -49,6 +49,9 @@ class _System(C.Structure):
         ("reorth", C.c_int),
         ("m_min", C.c_int),
         ("m_tol", C.c_double),
+        ("n_osc", C.c_int),
+        ("zz_omega", C.POINTER(C.c_double)),
+        ("zz_coeff", C.POINTER(C.c_double)),
     ]
 
 
@@ -85,6 +88,10 @@ def lib():
         L.dqo_run.argtypes = [sp, C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_int]
         L.dqo_run.restype = C.c_int
         L.dqo_ifft.argtypes = [C.c_int, dp]
+        L.dqo_zz_coefficients.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, dp, dp]
+        L.dqo_zz_phase.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.dqo_zz_phase.restype = C.c_float
+        L.dqo_noise_update_zz.argtypes = [sp, C.c_int, dp, C.POINTER(C.c_float), dp]
         ip = C.POINTER(C.c_int)
         L.dqo_spectrum_loss_grad.argtypes = [sp, dp, ip, C.c_int, C.c_int, C.c_int, dp, C.c_int, C.c_double,
                                              dp, dp, C.c_int]
@@ -150,7 +157,8 @@ class System:
 
     def __init__(self, rowptr, col, val, h0diag, m, dt, hbar=None, dot_mode=DOT_BILINEAR,
                  norm_mode=NORM_COMPLEX, noise=NOISE_NONE, ka_substeps=1, sigma=None, tau=None,
-                 sigma_static=0.0, static_eps=None, seed=0, reorth=0, m_min=0, m_tol=1e-7):
+                 sigma_static=0.0, static_eps=None, seed=0, reorth=0, m_min=0, m_tol=1e-7, zz_omega=None,
+                 zz_coeff=None):
         self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
         self.col = np.ascontiguousarray(col, dtype=np.int32)
         self.val = np.ascontiguousarray(val, dtype=np.float64)
@@ -159,6 +167,9 @@ class System:
         self.sigma = None if sigma is None else np.ascontiguousarray(np.broadcast_to(sigma, (self.n,)), dtype=np.float64)
         self.tau = None if tau is None else np.ascontiguousarray(np.broadcast_to(tau, (self.n,)), dtype=np.float64)
         self.static_eps = None if static_eps is None else np.ascontiguousarray(static_eps, dtype=np.float64)
+        self.zz_omega = None if zz_omega is None else np.ascontiguousarray(zz_omega, dtype=np.float64)
+        self.zz_coeff = None if zz_coeff is None else np.ascontiguousarray(zz_coeff, dtype=np.float64)
+        self.n_osc = 0 if self.zz_omega is None else len(self.zz_omega)
         self.m = m
         self.dt = dt
         self.hbar = hbar_reference() if hbar is None else hbar
@@ -170,7 +181,7 @@ class System:
             _dp(self.h0diag),
             m, dt, self.hbar, dot_mode, norm_mode, noise, ka_substeps,
             _dp(self.sigma), _dp(self.tau), float(sigma_static), _dp(self.static_eps), seed, int(reorth),
-            int(m_min), float(m_tol),
+            int(m_min), float(m_tol), self.n_osc, _dp(self.zz_omega), _dp(self.zz_coeff),
         )
 
     def dense(self, diag=None):
@@ -186,6 +197,21 @@ class System:
         deps = np.zeros(self.n)
         lib().dqo_traj_init(C.byref(self.s), traj, _dp(eps), _dp(deps))
         return eps, deps
+
+    def zz_phases(self, traj):
+        """[osc][site] phase fractions of one trajectory."""
+        u = np.zeros((self.n_osc, self.n), dtype=np.float32)
+        for o in range(self.n_osc):
+            for i in range(self.n):
+                u[o, i] = lib().dqo_zz_phase(self.s.seed, traj, i, o)
+        return u
+
+    def noise_update_zz(self, step, eps, u):
+        diag = np.zeros(self.n)
+        u = np.ascontiguousarray(u, dtype=np.float32)
+        lib().dqo_noise_update_zz(C.byref(self.s), step, _dp(np.ascontiguousarray(eps, dtype=np.float64)),
+                                  u.ctypes.data_as(C.POINTER(C.c_float)), _dp(diag))
+        return diag
 
     def noise_update(self, traj, step, eps, deps):
         diag = np.zeros(self.n)
@@ -244,7 +270,7 @@ class System:
 
 def spectrum_loss_grad(rowptr, col, val_base, cls, scales, static_eps, m, dt, psi0, n_traj, n_steps,
                        length, scale, target, want_grad=True, hbar=None, noise=NOISE_NONE, ka_substeps=1,
-                       sigma=None, tau=None, seed=0):
+                       sigma=None, tau=None, seed=0, zz_omega=None, zz_coeff=None):
     """Loss sum_j (scale*Re(IDFT_length(Cbar)_j) - target_j)^2 and its gradient with respect to the
     site energies (static_eps, n) and the coupling-class scales (len(scales)).
 
@@ -258,7 +284,8 @@ def spectrum_loss_grad(rowptr, col, val_base, cls, scales, static_eps, m, dt, ps
     val = scales[cls] * val_base if len(cls) else val_base.copy()
     eps = np.ascontiguousarray(static_eps, dtype=np.float64)
     sysm = System(rowptr, col, val, eps, m, dt, hbar=hbar, dot_mode=DOT_HERMITIAN, norm_mode=NORM_COMPLEX,
-                  noise=noise, ka_substeps=ka_substeps, sigma=sigma, tau=tau, static_eps=eps, seed=seed)
+                  noise=noise, ka_substeps=ka_substeps, sigma=sigma, tau=tau, static_eps=eps, seed=seed,
+                  zz_omega=zz_omega, zz_coeff=zz_coeff)
     psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
     target = np.ascontiguousarray(target, dtype=np.float64)
     assert target.shape == (length,)
@@ -267,3 +294,21 @@ def spectrum_loss_grad(rowptr, col, val_base, cls, scales, static_eps, m, dt, ps
                                         len(scales), n_traj, n_steps, _dp(psi0.view(np.float64)), length,
                                         float(scale), _dp(target), _dp(grad), 0)
     return loss, grad
+
+
+def zz_coefficients(omega_invcm, J, d_omega, temperature):
+    """(angular frequencies in rad/fs, amplitudes in cm^-1) of a ZZ spectral density."""
+    omega_invcm = np.ascontiguousarray(omega_invcm, dtype=np.float64)
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    w = np.zeros_like(omega_invcm)
+    c = np.zeros_like(omega_invcm)
+    lib().dqo_zz_coefficients(len(w), _dp(omega_invcm), _dp(J), float(d_omega), float(temperature), _dp(w), _dp(c))
+    return w, c
+
+
+def read_spectral_density(path):
+    """A ZZ spectral-density file: first line "dOmega nOsc", then nOsc lines "omega J" (cm^-1)."""
+    lines = [ln.split() for ln in open(path).read().splitlines() if ln.strip()]
+    d_omega, n_osc = float(lines[0][0]), int(lines[0][1])
+    rows = np.array([[float(a), float(b)] for a, b in lines[1:1 + n_osc]])
+    return d_omega, rows[:, 0], rows[:, 1]
