@@ -214,6 +214,34 @@ class Propagator:
         self._check(self.L.dq_write_spectrum(self.h, str(corr_path).encode(), str(spec_path).encode(),
                                              float(scaling)))
 
+    def write_ipr(self, path):
+        """invParticRat.dat: the ensemble-mean inverse participation ratio of steps 0..steps-1."""
+        self._check(self.L.dq_write_ipr(self.h, str(path).encode()))
+
+    # -- Taylor-Krylov mode and the inverse participation ratio ---------------------
+    def set_taylor_krylov(self, p, m_b=None, rowptr=None, col=None, val=None):
+        """Taylor-Krylov propagation of order p with m_b Lanczos iterations on the auxiliary matrix B
+        (full CSR over the sites, diagonal included); p = 0 returns to Lanczos mode."""
+        if p == 0:
+            self._check(self.L.dq_set_taylor_krylov(self.h, 0, 0, None, None, None))
+            return
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        col = np.ascontiguousarray(col, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        self._check(self.L.dq_set_taylor_krylov(self.h, int(p), int(m_b), _lib.iptr(rowptr), _lib.iptr(col),
+                                                _lib.dptr(val)))
+
+    def set_ipr(self, enable=True):
+        self._check(self.L.dq_set_ipr(self.h, int(bool(enable))))
+
+    def ipr(self):
+        """Ensemble mean of 1 / sum_i |psi_i|^4 after 0..steps_done steps."""
+        nv = C.c_int()
+        self._check(self.L.dq_get_ipr(self.h, None, C.byref(nv)))
+        out = np.zeros(nv.value)
+        self._check(self.L.dq_get_ipr(self.h, _lib.dptr(out), C.byref(nv)))
+        return out
+
     # -- adjoint -------------------------------------------------------------------
     def adjoint_setup(self, n_steps, fft_len, scale, target, checkpoint_every=0):
         """Fixes the spectrum-fitting loss sum_j (scale*Re(S_j) - target_j)^2 (S: inverse DFT of the

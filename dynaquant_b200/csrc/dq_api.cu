@@ -111,6 +111,16 @@ dq_status dq_create(const dq_config* cfg, dq_ctx** out) {
     return DQ_OK;
 }
 
+static void tk_free(dq_ctx* c) {
+    cudaFree(c->d_tk_rowptr); cudaFree(c->d_tk_col); cudaFree(c->d_tk_val); cudaFree(c->d_tk_diag);
+    cudaFree(c->d_tk_Q); cudaFree(c->d_tk_x); cudaFree(c->d_tk_acc);
+    c->d_tk_rowptr = c->d_tk_col = nullptr;
+    c->d_tk_val = c->d_tk_diag = nullptr;
+    c->d_tk_Q = c->d_tk_x = c->d_tk_acc = nullptr;
+    c->tk_p = c->tk_m = 0;
+    c->tk_coef.clear();
+}
+
 void dq_destroy(dq_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->cfg.device);
@@ -122,6 +132,8 @@ void dq_destroy(dq_ctx* c) {
     cudaFree(c->d_static); cudaFree(c->d_sigma); cudaFree(c->d_invtau); cudaFree(c->d_coeff);
     cudaFree(c->d_psi0); cudaFree(c->d_pops); cudaFree(c->d_corr); cudaFree(c->d_erracc);
     cudaFree(c->d_zz_omega); cudaFree(c->d_zz_coeff); cudaFree(c->d_zz_u);
+    tk_free(c);
+    cudaFree(c->d_ipr); cudaFree(c->d_ipr_partial); cudaFree(c->d_ipr_ticket);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -239,6 +251,88 @@ dq_status dq_set_zz_spectral_density(dq_ctx* c, int n_osc, const double* omega, 
     return DQ_OK;
 }
 
+dq_status dq_set_taylor_krylov(dq_ctx* c, int p, int m_b, const int* rowptr, const int* col, const double* val) {
+    if (!c) return DQ_ERR_ARG;
+    if (p == 0) {
+        tk_free(c);
+        c->ready = false;
+        return DQ_OK;
+    }
+    if (p < 2 || m_b < 1 || m_b > kMaxM || m_b + p > kMaxL || !rowptr || !col || !val)
+        return fail(c, DQ_ERR_ARG, "taylor_krylov: need 2 <= p, 1 <= m_b <= 32, m_b + p <= 34 and a CSR matrix B");
+    if (c->cfg.m_min > 0) return fail(c, DQ_ERR_ARG, "taylor_krylov: needs a fixed Krylov dimension (m_min = 0)");
+    const int n = c->n;
+    if (rowptr[0] != 0) return fail(c, DQ_ERR_ARG, "taylor_krylov: rowptr[0] != 0");
+    for (int i = 0; i < n; ++i)
+        if (rowptr[i + 1] < rowptr[i]) return fail(c, DQ_ERR_ARG, "taylor_krylov: rowptr not monotone");
+    // split B into its diagonal and off-diagonal CSR like the Hamiltonian
+    std::vector<int> rp(n + 1, 0), cl;
+    std::vector<double> vb, dg(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+            const int j = col[q];
+            if (j < 0 || j >= n) return fail(c, DQ_ERR_ARG, "taylor_krylov: column index out of range");
+            if (!std::isfinite(val[q])) return fail(c, DQ_ERR_ARG, "taylor_krylov: non-finite value");
+            if (j == i) dg[i] += val[q];
+            else { cl.push_back(j); vb.push_back(val[q]); }
+        }
+        rp[i + 1] = (int)cl.size();
+    }
+    if (cl.empty()) { cl.push_back(0); vb.push_back(0.0); }   // valid pointers for the kernels
+    tk_free(c);
+    dq_status st;
+    if ((st = upload(c, &c->d_tk_rowptr, rp.data(), rp.size()))) return st;
+    if ((st = upload(c, &c->d_tk_col, cl.data(), cl.size()))) return st;
+    if ((st = upload(c, &c->d_tk_val, vb.data(), vb.size()))) return st;
+    if ((st = upload(c, &c->d_tk_diag, dg.data(), dg.size()))) return st;
+    DQ_CU(cudaMalloc(&c->d_tk_Q, sizeof(cd) * (size_t)n * (m_b + 2)));
+    DQ_CU(cudaMemsetAsync(c->d_tk_Q, 0, sizeof(cd) * (size_t)n * (m_b + 2), c->stream));
+    DQ_CU(cudaMalloc(&c->d_tk_x, sizeof(cd) * (size_t)n * 2));
+    DQ_CU(cudaMalloc(&c->d_tk_acc, sizeof(cd) * (size_t)n));
+    // tau^k / k! with tau = -i dt / hbar (taylorKrylovClass.cu:196-206)
+    const cd tau = cmk(0.0, c->tau_im);
+    cd pw = cmk(1.0, 0.0);
+    double fact = 1.0;
+    c->tk_coef.assign(p, cmk(0.0, 0.0));
+    c->tk_coef[0] = pw;
+    for (int k = 1; k < p; ++k) {
+        pw = cmk(pw.x * tau.x - pw.y * tau.y, pw.x * tau.y + pw.y * tau.x);
+        fact *= k;
+        c->tk_coef[k] = cmk(pw.x / fact, pw.y / fact);
+    }
+    c->tk_p = p;
+    c->tk_m = m_b;
+    c->ready = false;
+    return DQ_OK;
+}
+
+dq_status dq_set_ipr(dq_ctx* c, int enable) {
+    if (!c) return DQ_ERR_ARG;
+    if (enable && !c->d_ipr) {
+        DQ_CU(cudaMalloc(&c->d_ipr, sizeof(double) * (size_t)(c->cfg.max_steps + 1)));
+        DQ_CU(cudaMemsetAsync(c->d_ipr, 0, sizeof(double) * (size_t)(c->cfg.max_steps + 1), c->stream));
+        DQ_CU(cudaMalloc(&c->d_ipr_partial, sizeof(double) * (size_t)kIprRowGroups * c->cfg.n_traj));
+        DQ_CU(cudaMalloc(&c->d_ipr_ticket, sizeof(unsigned int)));
+        DQ_CU(cudaMemsetAsync(c->d_ipr_ticket, 0, sizeof(unsigned int), c->stream));
+    }
+    c->ipr_on = enable != 0;
+    c->ready = false;
+    return DQ_OK;
+}
+
+dq_status dq_get_ipr(dq_ctx* c, double* out, int* n_values) {
+    if (!c) return DQ_ERR_ARG;
+    if (!c->ipr_on) return fail(c, DQ_ERR_STATE, "get_ipr: the inverse participation ratio is not enabled");
+    const int nv = c->steps_done + 1;
+    if (n_values) *n_values = nv;
+    if (!out) return DQ_OK;
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    DQ_CU(cudaMemcpy(out, c->d_ipr, sizeof(double) * nv, cudaMemcpyDeviceToHost));
+    const double inv = 1.0 / c->cfg.n_traj;
+    for (int k = 0; k < nv; ++k) out[k] *= inv;
+    return DQ_OK;
+}
+
 dq_status dq_set_static_energies(dq_ctx* c, const double* eps) {
     if (!c) return DQ_ERR_ARG;
     if (!eps) {
@@ -314,6 +408,8 @@ dq_status dq_run_plain(dq_ctx* c, int n_steps) {
     if (n_steps < 0 || n_steps > c->cfg.max_steps) return fail(c, DQ_ERR_ARG, "run_plain: n_steps out of range");
     dq_status st;
     if ((st = dq_reset(c))) return st;
+    // the ensemble's initial record (added at its reset) belongs to dq_run
+    if ((st = plain_clear_observables(c))) return st;
     const int n = c->n, pe = c->cfg.pop_every;
     for (int t = 0; t < c->cfg.n_traj; ++t) {
         if ((st = plain_observe_initial(c))) return st;
@@ -341,6 +437,8 @@ dq_status dq_run(dq_ctx* c, int n_steps) {
     if (!c) return DQ_ERR_ARG;
     if (n_steps < 0 || c->steps_done + n_steps > c->cfg.max_steps)
         return fail(c, DQ_ERR_ARG, "run: steps exceed max_steps");
+    if (c->tk_p > 0)
+        return fail(c, DQ_ERR_STATE, "run: Taylor-Krylov mode runs on the per-trajectory path (dq_run_plain)");
     dq_status st;
     if (!c->bat) {
         if ((st = batched_alloc(c))) return st;

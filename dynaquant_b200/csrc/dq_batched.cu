@@ -1848,6 +1848,52 @@ __global__ void k_pop_b(int n, int B, int pop_every, const Real* __restrict__ r1
     }
 }
 
+// ipr[step + 1] += sum_b 1 / sum_i (|r1_ib|^2 / ||r1_b||^2)^2 (systemClass.cu:2219-2257):
+// one thread per trajectory sums a strided share of the rows (coalesced over
+// trajectories); the last block adds the row-group partials in a fixed order.
+template <typename Real>
+__global__ void k_ipr_b(int n, int B, const Real* __restrict__ r1, BatchedScalars S, double* partial,
+                        unsigned int* ticket, double* ipr) {
+    const int b = blockIdx.y * blockDim.x + threadIdx.x;
+    if (b < B) {
+        const double inv = 1.0 / S.norm2[b];
+        double s = 0.0;
+        for (int row = blockIdx.x; row < n; row += gridDim.x) {
+            const size_t x = (size_t)row * B + b;
+            const double vr = r1[2 * x], vi = r1[2 * x + 1];
+            const double a = (vr * vr + vi * vi) * inv;
+            s += a * a;
+        }
+        partial[(size_t)blockIdx.x * B + b] = s;
+    }
+    if (last_block_ticket(ticket, gridDim.x * gridDim.y)) {
+        __shared__ double scratch[32];
+        double acc = 0.0;
+        for (int bb = threadIdx.x; bb < B; bb += blockDim.x) {
+            double q = 0.0;
+            for (unsigned int g = 0; g < gridDim.x; ++g) q += __ldcg(&partial[(size_t)g * B + bb]);
+            acc += 1.0 / q;
+        }
+        acc = block_sum(acc, scratch);
+        if (threadIdx.x == 0) {
+            ipr[*S.step + 1] += acc;
+            *ticket = 0;
+        }
+    }
+}
+
+// ipr[0] += B / sum_i |psi0_i|^4
+__global__ void k_ipr_init_b(int n, int B, const cd* __restrict__ psi0, double* ipr) {
+    __shared__ double scratch[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double a = cabs2(psi0[i]);
+        s += a * a;
+    }
+    s = block_sum(s, scratch);
+    if (threadIdx.x == 0) ipr[0] += (double)B / s;
+}
+
 // initial record: pops[0] += B |psi0|^2, corr[0] = B <psi0|psi0>
 __global__ void k_init_obs_b(int n, int B, const cd* __restrict__ psi0, double* pops, BatchedScalars S,
                              int chunks) {
@@ -2541,6 +2587,7 @@ dq_status batched_reset(dq_ctx* c) {
     k_set_norms_b<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, bs->s);
     k_init_obs_b<<<std::max(1, std::min(bs->sms, (n + 255) / 256)), 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops,
                                                                                         bs->s, bs->chunks);
+    if (c->ipr_on) k_ipr_init_b<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_ipr);
     DQ_CU(cudaGetLastError());
     return DQ_OK;
 }
@@ -2833,6 +2880,9 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
     k_combine_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, m, slabs, se, c->d_psi0, bs->s);
     const int pblocks = std::max(1, std::min(bs->sms * 4, (n + 7) / 8));
     mark(DQ_KIND_POP);
+    if (c->ipr_on && !skip_pop)
+        k_ipr_b<Real><<<dim3(std::min(n, kIprRowGroups), (B + 127) / 128), 128, 0, st>>>(
+            n, B, slab(1), bs->s, c->d_ipr_partial, c->d_ipr_ticket, c->d_ipr);
     if (skip_pop) k_advance_step<<<1, 32, 0, st>>>(bs->s);
     else
         k_pop_b<Real><<<pblocks, 256, 0, st>>>(n, B, c->cfg.pop_every, slab(1), c->d_pops, bs->s,

@@ -8,7 +8,7 @@ namespace dq {
 
 struct cd { double x, y; };   // complex128, same layout as dq_cdouble / cuDoubleComplex
 
-__device__ __forceinline__ cd cmk(double x, double y) { cd r; r.x = x; r.y = y; return r; }
+__host__ __device__ __forceinline__ cd cmk(double x, double y) { cd r; r.x = x; r.y = y; return r; }
 __device__ __forceinline__ cd cadd(cd a, cd b) { return cmk(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ cd csub(cd a, cd b) { return cmk(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ cd cmul(cd a, cd b) { return cmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }

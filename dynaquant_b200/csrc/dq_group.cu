@@ -84,6 +84,7 @@ dq_status dq_group_run(dq_group* g, int n_steps) {
         if (c->steps_done + n_steps > c->cfg.max_steps)
             return gfail(g, DQ_ERR_ARG, "group run: a member's steps exceed its max_steps");
         dq_status st = DQ_OK;
+        if (c->tk_p > 0) return gfail(g, DQ_ERR_STATE, "group run: Taylor-Krylov members run on their own");
         if (!c->bat) {
             if ((st = dq::batched_alloc(c))) return gfail(g, st, c->err);
             c->ready = false;

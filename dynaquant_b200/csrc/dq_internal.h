@@ -26,11 +26,14 @@ struct PlainScalars {
     unsigned int ticket[4];
     cd h[kMaxL];          // full reorthogonalisation: <q_k, r_{j+1}>
     unsigned int ticket_r[2];
+    double tk_beta0;      // Taylor-Krylov: ||A^p psi_in||
+    double tk_kerr;       // Taylor-Krylov: EXPOKIT estimate of the B part
 };
 
 constexpr int kPlainThreads = 256;
 constexpr int kMaxPartials = 4096;
 constexpr int kMaxZZOsc = 1024;   // oscillators of one ZZ spectral density
+constexpr int kIprRowGroups = 296; // row groups of the ensemble IPR reduction (2 per SM)
 
 struct BatchedState;   // dq_batched.cu
 struct AdjointState;   // dq_adjoint.cu
@@ -69,7 +72,7 @@ struct dq_ctx {
     dq::cd* d_psi0 = nullptr;
     int nnz_off = 0;
     // ZZ real noise: oscillators (angular frequency rad/fs, amplitude) and
-    // the plain path's phase fractions [traj][osc][site]
+    // the ensemble's phase fractions (the plain path draws them per step)
     int zz_n_osc = 0;
     std::vector<double> zz_omega, zz_coeff;
     double* d_zz_omega = nullptr;
@@ -95,6 +98,24 @@ struct dq_ctx {
     int steps_done = 0;
     int plain_traj_done = 0;      // trajectories completed by dq_run_plain
     int last_path = 0;            // 0: observables from dq_run_plain, 1: from dq_run
+
+    // Taylor-Krylov mode (tk_p > 0): the auxiliary matrix B (off-diagonal
+    // CSR + diagonal), its Krylov basis and the Taylor work vectors
+    int tk_p = 0, tk_m = 0;
+    int* d_tk_rowptr = nullptr;
+    int* d_tk_col = nullptr;
+    double* d_tk_val = nullptr;
+    double* d_tk_diag = nullptr;
+    dq::cd* d_tk_Q = nullptr;     // (tk_m + 2) slabs of n; slab 1 holds A^p psi
+    dq::cd* d_tk_x = nullptr;     // 2 slabs: A^k psi ping-pong
+    dq::cd* d_tk_acc = nullptr;   // Taylor sum
+    std::vector<dq::cd> tk_coef;  // tau^k / k!, k < p
+
+    // inverse participation ratio (sums over trajectories of 1 / sum |psi|^4)
+    bool ipr_on = false;
+    double* d_ipr = nullptr;            // max_steps + 1
+    double* d_ipr_partial = nullptr;    // kIprRowGroups x n_traj
+    unsigned int* d_ipr_ticket = nullptr;
 
     dq::BatchedState* bat = nullptr;
     dq::AdjointState* adj = nullptr;

@@ -171,6 +171,24 @@ dq_status dq_write_states(dq_ctx* c, const char* folder) {
     return ok ? DQ_OK : ofail(c, DQ_ERR_ARG, "write_states: write failed");
 }
 
+// invParticRat.dat (systemClass.cu:1735-1750): a two-line header, then one
+// line "k  IPR_k" per step k = 0..steps-1 with the ensemble mean of
+// 1 / sum_i |psi_i(k)|^4 printed like an ostream at its default precision.
+dq_status dq_write_ipr(dq_ctx* c, const char* path) {
+    if (!c || !path) return DQ_ERR_ARG;
+    int nv = 0;
+    dq_status st = dq_get_ipr(c, nullptr, &nv);
+    if (st) return st;
+    std::vector<double> v(nv);
+    if ((st = dq_get_ipr(c, v.data(), &nv))) return st;
+    FILE* f = fopen(path, "w");
+    if (!f) return ofail(c, DQ_ERR_ARG, std::string("write_ipr: cannot open ") + path);
+    fprintf(f, "# Inverse Particle Ratios\n# {timestep} {IPR}}\n");
+    for (int k = 0; k + 1 < nv; ++k) fprintf(f, "%d  %g\n", k, v[k]);
+    fclose(f);
+    return DQ_OK;
+}
+
 dq_status dq_write_spectrum(dq_ctx* c, const char* corr_path, const char* spec_path, double scaling) {
     if (!c || !corr_path || !spec_path) return DQ_ERR_ARG;
     if (c->last_path == 1 && c->bat) {

@@ -43,8 +43,9 @@ __global__ void k_traj_init_plain(int n, int n_traj, uint64_t seed, const double
 // ZZ diagonal of one trajectory at step: sum_osc c cos(omega t + phi) + eps
 // (gpuSysHelper.cu:134-177); the phases are drawn from Philox here, one per (site, osc)
 __global__ void k_noise_zz(int n, int traj, int step, uint64_t seed, ZZParams zz, const double* __restrict__ eps,
-                           double* __restrict__ diag) {
+                           double* __restrict__ diag, PlainScalars* ps) {
     __shared__ double w[kMaxZZOsc];
+    if (blockIdx.x == 0 && threadIdx.x == 0) ps->sc[1] = 1.0;   // q_1 = psi_in
     for (int o = threadIdx.x; o < zz.n_osc; o += blockDim.x) w[o] = zz_wfrac(zz.omega[o], step, zz.dt);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -298,6 +299,114 @@ __global__ void k_observe_initial(int n, const cd* __restrict__ psi0, double* po
     }
 }
 
+// ---- Taylor-Krylov mode (taylorKrylovClass.cu:223-434) --------------------
+// y = A x (A: the step's Hamiltonian); k < p: acc += c_k y (acc starts at
+// psi_in for k = 1); k = p: tk_beta0 = ||y|| and sc_1 = 1 / tk_beta0, so the
+// B Lanczos starts from q_1 = y / ||y||.
+__global__ void __launch_bounds__(kPlainThreads) k_tk_power(int n, int k, int p, const int* __restrict__ rowptr,
+                                                           const int* __restrict__ col,
+                                                           const double* __restrict__ val,
+                                                           const double* __restrict__ diag, const cd* x,
+                                                           cd* __restrict__ y, cd* acc, cd coef, double* partial,
+                                                           PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double nn = 0.0;
+    if (i < n) {
+        cd a = cscale(x[i], diag[i]);
+        for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) a = cadd(a, cscale(x[col[q]], val[q]));
+        y[i] = a;
+        if (k < p) acc[i] = cadd(k == 1 ? x[i] : acc[i], cmul(coef, a));
+        nn = cabs2(a);
+    }
+    if (k < p) return;   // uniform over the grid
+    __shared__ double out2[2];
+    if (reduce2_last(nn, 0.0, partial, &ps->ticket[2], out2) && threadIdx.x == 0) {
+        const double b = sqrt(out2[0]);
+        if (!(b > 0.0) || !isfinite(b)) atomicCAS(&ps->status, 0, DQ_ERR_NAN);
+        ps->tk_beta0 = b;
+        ps->sc[1] = 1.0 / b;
+    }
+}
+
+// exp(tau Tbar_B) of the (mB + p) augmented matrix (ones at (0, mB) and
+// (mB+k, mB+k+1), gpuLanczosHelper.cu:14-60); combine weights from its last
+// column scaled by ||A^p psi||; the EXPOKIT estimate of the B part.
+__global__ void k_pade_tk(int mb, int p, double tau_im, int norm_mode, PlainScalars* ps) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int L = mb + p;
+    cd* A = reinterpret_cast<cd*>(smem);
+    const cd tau = cmk(0.0, tau_im);
+    for (int e = threadIdx.x; e < L * L; e += blockDim.x) {
+        const int i = e / L, j = e % L;
+        cd v = cmk(0.0, 0.0);
+        if (i < mb && j < mb) {
+            if (i == j) v = ps->alpha[i + 1];
+            else if (j == i + 1) v = ps->beta[i + 1];
+            else if (i == j + 1) v = ps->beta[j + 1];
+        } else if ((i == 0 && j == mb) || (i >= mb && j == i + 1)) {
+            v = cmk(1.0, 0.0);
+        }
+        A[e] = cmul(tau, v);
+    }
+    __syncthreads();
+    cd* E = nullptr;
+    const int s = pade_exp_sm(L, norm_mode, smem, &E);
+    if (s < 0) {
+        if (threadIdx.x == 0) atomicCAS(&ps->status, 0, (s == -1) ? DQ_ERR_SCALING : DQ_ERR_SINGULAR);
+        return;
+    }
+    const double b0 = ps->tk_beta0;
+    if (threadIdx.x < mb)
+        ps->yt[threadIdx.x + 1] = cscale(E[threadIdx.x * L + L - 1], b0 * ps->sc[threadIdx.x + 1]);
+    if (threadIdx.x == 0) {
+        ps->s = s;
+        ps->tk_kerr = expokit_error(ps->beta[mb].x, ps->nav, E[(mb - 1) * L + mb], E[(mb - 1) * L + mb + 1]);
+    }
+}
+
+// psi_out = sum_j yt_j r_j (r_1 = A^p psi) + Taylor sum, ||psi_out||^2
+__global__ void __launch_bounds__(kPlainThreads) k_combine_tk(int n, int mb, const cd* __restrict__ Q,
+                                                             const cd* __restrict__ acc, cd* __restrict__ out,
+                                                             double* partial, PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double nn = 0.0;
+    if (i < n) {
+        cd k = cmul(Q[(size_t)n + i], ps->yt[1]);
+        for (int j = 2; j <= mb; ++j) k = cadd(k, cmul(Q[(size_t)j * n + i], ps->yt[j]));
+        const cd v = cadd(k, acc[i]);
+        out[i] = v;
+        nn = cabs2(v);
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(nn, 0.0, partial, &ps->ticket[0], out2) && threadIdx.x == 0) {
+        double nrm = sqrt(out2[0]);
+        ps->norm = nrm;
+        ps->invnorm = 1. / nrm;
+        if (!(nrm > 0.0) || !isfinite(nrm)) atomicCAS(&ps->status, 0, DQ_ERR_NAN);
+        // taylorKrylovClass.cu:417-434: the B part's estimate plus |1 - norm|
+        double est = ps->tk_kerr + fabs(1.0 - nrm);
+        if (est < 1.110223e-16) est = 1.110223e-16;
+        ps->err = est;
+    }
+}
+
+__global__ void k_tk_erracc(PlainScalars* ps, double* erracc, int traj) {
+    if (threadIdx.x == 0) erracc[traj] += ps->err;
+}
+
+// ipr[rec] += 1 / sum_i |psi_i|^4 (systemClass.cu:2219-2257, FP64 sum)
+__global__ void __launch_bounds__(kPlainThreads) k_ipr_plain(int n, const cd* __restrict__ psi, double* ipr_pt,
+                                                            double* partial, PlainScalars* ps) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double q = 0.0;
+    if (i < n) {
+        const double a = cabs2(psi[i]);
+        q = a * a;
+    }
+    __shared__ double out2[2];
+    if (reduce2_last(q, 0.0, partial, &ps->ticket[2], out2) && threadIdx.x == 0) *ipr_pt += 1.0 / out2[0];
+}
+
 // ------------------------------------------------------------------------
 dq_status check_cuda(dq_ctx* c, cudaError_t e, const char* what) {
     if (e == cudaSuccess) return DQ_OK;
@@ -335,6 +444,8 @@ dq_status plain_alloc(dq_ctx* c) {
     DQ_CU(cudaMemsetAsync(c->d_Q, 0, sizeof(cd) * (size_t)n * (m + 2), c->stream));
     size_t smem = pade_smem_bytes(m + 2);
     DQ_CU(cudaFuncSetAttribute(k_pade_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DQ_CU(cudaFuncSetAttribute(k_pade_tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)pade_smem_bytes(kMaxL)));
     return DQ_OK;
 }
 
@@ -361,6 +472,58 @@ dq_status plain_clear_observables(dq_ctx* c) {
     DQ_CU(cudaMemsetAsync(c->d_pops, 0, sizeof(double) * (size_t)c->n_rec_max * c->n, c->stream));
     DQ_CU(cudaMemsetAsync(c->d_corr, 0, sizeof(cd) * (size_t)(c->cfg.max_steps + 1), c->stream));
     DQ_CU(cudaMemsetAsync(c->d_erracc, 0, sizeof(double) * c->cfg.n_traj, c->stream));
+    if (c->d_ipr) DQ_CU(cudaMemsetAsync(c->d_ipr, 0, sizeof(double) * (size_t)(c->cfg.max_steps + 1), c->stream));
+    return DQ_OK;
+}
+
+// m Lanczos iterations on (rowptr, col, val, diag) from r_1 = x1 (q_1 =
+// sc_1 x1), residuals r_2..r_{m+1} in slabs 2..m+1 of Q, then ||H q_{m+1}||.
+static void plain_lanczos(dq_ctx* c, int m, const int* rowptr, const int* col, const double* val,
+                          const double* diag, const cd* x1, cd* Q) {
+    const int n = c->n, T = kPlainThreads, G = (n + T - 1) / T;
+    cudaStream_t st = c->stream;
+    for (int j = 1; j <= m; ++j) {
+        const cd* rj = (j == 1) ? x1 : Q + (size_t)j * n;
+        const cd* rjm = (j <= 1) ? nullptr : (j == 2 ? x1 : Q + (size_t)(j - 1) * n);
+        cd* rjp = Q + (size_t)(j + 1) * n;
+        if (c->cfg.dot_mode == DQ_DOT_BILINEAR)
+            k_spmv_alpha<true><<<G, T, 0, st>>>(n, j, rowptr, col, val, diag, rj, c->d_w, c->d_partial, c->d_ps);
+        else
+            k_spmv_alpha<false><<<G, T, 0, st>>>(n, j, rowptr, col, val, diag, rj, c->d_w, c->d_partial, c->d_ps);
+        k_axpy_norm<<<G, T, 0, st>>>(n, j, c->d_w, rj, rjm, rjp, c->d_partial, c->d_ps);
+        if (c->cfg.reorth) {
+            for (int k = 1; k <= j; ++k)
+                k_reorth_dot<<<G, T, 0, st>>>(n, k, k == 1 ? x1 : Q + (size_t)k * n, rjp, c->d_partial, c->d_ps);
+            k_reorth_apply<<<G, T, 0, st>>>(n, j, x1, Q, rjp, c->d_partial, c->d_ps);
+        }
+    }
+    k_spmv_norm<<<G, T, 0, st>>>(n, m + 1, rowptr, col, val, diag, Q + (size_t)(m + 1) * n, c->d_partial, c->d_ps);
+}
+
+// Taylor-Krylov step after the noise update: p products with A (Taylor sum
+// and A^p psi), mB Lanczos iterations on B from A^p psi, the augmented Padé,
+// combine with the Taylor sum, renormalisation and observables.
+static dq_status plain_tk_tail(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_out, bool observe,
+                               int rec) {
+    const int n = c->n, p = c->tk_p, mb = c->tk_m, T = kPlainThreads, G = (n + T - 1) / T;
+    cudaStream_t st = c->stream;
+    const cd* x = psi_in;
+    for (int k = 1; k <= p; ++k) {
+        // the last product lands in slab 1 of the B basis
+        cd* y = (k == p) ? c->d_tk_Q + n : c->d_tk_x + (size_t)(k & 1) * n;
+        k_tk_power<<<G, T, 0, st>>>(n, k, p, c->d_rowptr, c->d_col, c->d_val, c->d_diag, x, y, c->d_tk_acc,
+                                    k < p ? c->tk_coef[k] : cmk(0.0, 0.0), c->d_partial, c->d_ps);
+        x = y;
+    }
+    plain_lanczos(c, mb, c->d_tk_rowptr, c->d_tk_col, c->d_tk_val, c->d_tk_diag, c->d_tk_Q + n, c->d_tk_Q);
+    k_pade_tk<<<1, 256, pade_smem_bytes(mb + p), st>>>(mb, p, c->tau_im, c->cfg.norm_mode, c->d_ps);
+    k_combine_tk<<<G, T, 0, st>>>(n, mb, c->d_tk_Q, c->d_tk_acc, psi_out, c->d_partial, c->d_ps);
+    if (observe) k_tk_erracc<<<1, 32, 0, st>>>(c->d_ps, c->d_erracc, traj);
+    double* prow = (observe && rec >= 0) ? c->d_pops + (size_t)rec * n : nullptr;
+    cd* cpt = observe ? c->d_corr + (step + 1) : nullptr;
+    k_renorm<<<G, T, 0, st>>>(n, psi_out, c->d_psi0, prow, cpt, c->d_partial, c->d_ps);
+    if (observe && c->ipr_on) k_ipr_plain<<<G, T, 0, st>>>(n, psi_out, c->d_ipr + step + 1, c->d_partial, c->d_ps);
+    DQ_CU(cudaGetLastError());
     return DQ_OK;
 }
 
@@ -382,37 +545,20 @@ dq_status plain_step(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_ou
         zz.omega = c->d_zz_omega;
         zz.coeff = c->d_zz_coeff;
         zz.dt = c->cfg.dt;
-        k_noise_zz<<<G, T, 0, st>>>(n, traj, step, c->cfg.seed, zz, eps, c->d_diag);
+        k_noise_zz<<<G, T, 0, st>>>(n, traj, step, c->cfg.seed, zz, eps, c->d_diag, c->d_ps);
     } else {
         k_noise<<<G, T, 0, st>>>(n, traj, step, c->cfg.noise_model, ns, subdt, sqrt_subdt, c->cfg.seed, c->d_sigma,
                                  c->d_invtau, c->d_coeff, eps, deps, c->d_diag, c->d_ps);
     }
-    for (int j = 1; j <= m; ++j) {
-        const cd* rj = (j == 1) ? psi_in : c->d_Q + (size_t)j * n;
-        const cd* rjm = (j <= 1) ? nullptr : (j == 2 ? psi_in : c->d_Q + (size_t)(j - 1) * n);
-        cd* rjp = c->d_Q + (size_t)(j + 1) * n;
-        if (c->cfg.dot_mode == DQ_DOT_BILINEAR)
-            k_spmv_alpha<true><<<G, T, 0, st>>>(n, j, c->d_rowptr, c->d_col, c->d_val, c->d_diag, rj, c->d_w,
-                                                c->d_partial, c->d_ps);
-        else
-            k_spmv_alpha<false><<<G, T, 0, st>>>(n, j, c->d_rowptr, c->d_col, c->d_val, c->d_diag, rj, c->d_w,
-                                                 c->d_partial, c->d_ps);
-        k_axpy_norm<<<G, T, 0, st>>>(n, j, c->d_w, rj, rjm, rjp, c->d_partial, c->d_ps);
-        if (c->cfg.reorth) {
-            for (int k = 1; k <= j; ++k)
-                k_reorth_dot<<<G, T, 0, st>>>(n, k, k == 1 ? psi_in : c->d_Q + (size_t)k * n, rjp, c->d_partial,
-                                              c->d_ps);
-            k_reorth_apply<<<G, T, 0, st>>>(n, j, psi_in, c->d_Q, rjp, c->d_partial, c->d_ps);
-        }
-    }
-    k_spmv_norm<<<G, T, 0, st>>>(n, m + 1, c->d_rowptr, c->d_col, c->d_val, c->d_diag, c->d_Q + (size_t)(m + 1) * n,
-                                 c->d_partial, c->d_ps);
+    if (c->tk_p > 0) return plain_tk_tail(c, traj, step, psi_in, psi_out, observe, rec);
+    plain_lanczos(c, m, c->d_rowptr, c->d_col, c->d_val, c->d_diag, psi_in, c->d_Q);
     k_pade_plain<<<1, 256, pade_smem_bytes(m + 2), st>>>(m, c->tau_im, c->cfg.norm_mode, c->d_ps,
                                                          observe ? c->d_erracc : nullptr, traj);
     k_combine<<<G, T, 0, st>>>(n, m, psi_in, c->d_Q, psi_out, c->d_partial, c->d_ps);
     double* prow = (observe && rec >= 0) ? c->d_pops + (size_t)rec * n : nullptr;
     cd* cpt = observe ? c->d_corr + (step + 1) : nullptr;
     k_renorm<<<G, T, 0, st>>>(n, psi_out, c->d_psi0, prow, cpt, c->d_partial, c->d_ps);
+    if (observe && c->ipr_on) k_ipr_plain<<<G, T, 0, st>>>(n, psi_out, c->d_ipr + step + 1, c->d_partial, c->d_ps);
     DQ_CU(cudaGetLastError());
     return DQ_OK;
 }
@@ -421,6 +567,7 @@ dq_status plain_observe_initial(dq_ctx* c) {
     const int n = c->n;
     const int G = (n + kPlainThreads - 1) / kPlainThreads;
     k_observe_initial<<<G, kPlainThreads, 0, c->stream>>>(n, c->d_psi0, c->d_pops, c->d_corr, c->d_partial, c->d_ps);
+    if (c->ipr_on) k_ipr_plain<<<G, kPlainThreads, 0, c->stream>>>(n, c->d_psi0, c->d_ipr, c->d_partial, c->d_ps);
     DQ_CU(cudaGetLastError());
     return DQ_OK;
 }

@@ -121,6 +121,27 @@ DQ_API dq_status dq_set_noise_params(dq_ctx *ctx, const double *sigma, const dou
  * redraws them per run, systemClass.cu:1212-1234). */
 DQ_API dq_status dq_set_zz_spectral_density(dq_ctx *ctx, int n_osc, const double *omega, const double *J,
                                             double d_omega, double temperature);
+/* Taylor-Krylov propagation (PROP_MODE_TAYLOR_LANCZOS; taylorKrylovClass.cu:
+ * 135-434, replaces the taylorKrylovClass constructor and the auxiliary
+ * matrix file): each step is psi <- sum_{k<p} tau^k/k! A^k psi +
+ * ||A^p psi|| Q_B [exp(tau Tbar_B)]_{:, L-1}, A the step's Hamiltonian,
+ * Q_B and Tbar_B (size L = m_b + p, EXPOKIT's phi_p augmentation) from m_b
+ * Lanczos iterations on the auxiliary matrix B (full CSR over the N sites,
+ * diagonal included) started from A^p psi, then renormalised; the error
+ * estimate is EXPOKIT's on the B part plus |1 - norm|.  2 <= p, 1 <= m_b <= 32,
+ * m_b + p <= 34; p = 0 returns to Lanczos mode.  Steps run on the
+ * per-trajectory path (dq_prop_step, dq_run_plain); dq_run, groups and the
+ * adjoint refuse this mode. */
+DQ_API dq_status dq_set_taylor_krylov(dq_ctx *ctx, int p, int m_b, const int *rowptr, const int *col,
+                                      const double *val);
+/* Inverse participation ratio (print_partic; systemClass.cu:2219-2257):
+ * when enabled, every path adds 1 / sum_i |psi_i|^4 of each trajectory's
+ * state after every step (and of psi0) into a per-step sum, kept in FP64
+ * (the reference rounds sum |psi|^4 to float).  Takes effect at the next
+ * reset. */
+DQ_API dq_status dq_set_ipr(dq_ctx *ctx, int enable);
+/* steps done + 1 values: the ensemble mean of 1 / sum |psi(k)|^4, k = 0.. */
+DQ_API dq_status dq_get_ipr(dq_ctx *ctx, double *out, int *n_values);
 /* Explicit static site energies shared by all trajectories (replaces the
  * Hamiltonian diagonal plus static disorder); NULL restores them. */
 DQ_API dq_status dq_set_static_energies(dq_ctx *ctx, const double *eps);
@@ -266,6 +287,10 @@ DQ_API dq_status dq_write_states(dq_ctx *ctx, const char *folder);
  * caller passes mu_tot^2 for absorption or (pi/2) 1e-7 mu_tot RD_tot for CD),
  * the transform also divided by the step count. */
 DQ_API dq_status dq_write_spectrum(dq_ctx *ctx, const char *corr_path, const char *spec_path, double scaling);
+/* invParticRat.dat (systemClass.cu:1735-1750): "# Inverse Particle Ratios",
+ * "# {timestep} {IPR}}", then "k  IPR_k" (%g) for k = 0..steps-1, IPR_k the
+ * ensemble mean from dq_get_ipr.  Needs dq_set_ipr(ctx, 1) before the run. */
+DQ_API dq_status dq_write_ipr(dq_ctx *ctx, const char *path);
 
 /* ---- several aggregates together (no reference counterpart) ----
  * A group advances the ensembles of several contexts (aggregates of any

@@ -561,10 +561,112 @@ int dqo_krylov_step_m(const dqo_system *sys, const double *diag, const double *p
 }
 
 /* ------------------------------------------------------------------ */
+/* Taylor-Krylov (taylorKrylovClass.cu:196-434)                        */
+/* ------------------------------------------------------------------ */
+int dqo_tk_step(const dqo_system *sys, const double *diag, const double *psi_in, double *psi_out,
+                double *err_est, double *norm_out) {
+    const int n = sys->n, p = sys->tk_p, mb = sys->tk_m, L = mb + p;
+    const cx tau = {0.0, -sys->dt / sys->hbar};
+    /* Taylor coefficients tau^k / k! (taylorKrylovClass.cu:200-206) */
+    cx ck[DQO_TK_MAX_P];
+    cx pw = {1.0, 0.0};
+    double fact = 1.0;
+    ck[0] = pw;
+    for (int k = 1; k < p; ++k) {
+        pw = cmul(pw, tau);
+        fact *= k;
+        ck[k].re = pw.re / fact;
+        ck[k].im = pw.im / fact;
+    }
+    cx *acc = (cx *)malloc(sizeof(cx) * (size_t)n * 3);
+    cx *x = acc + n, *y = x + n;
+    memcpy(acc, psi_in, sizeof(cx) * n);
+    memcpy(x, psi_in, sizeof(cx) * n);
+    /* acc = sum_{k<p} c_k A^k psi; x ends as A^p psi (:231-300) */
+    for (int k = 1; k <= p; ++k) {
+        spmv(sys, diag, x, y);
+        if (k < p)
+            for (int i = 0; i < n; ++i) acc[i] = cadd(acc[i], cmul(ck[k], y[i]));
+        cx *t = x; x = y; y = t;
+    }
+    /* Krylov part on B from A^p psi (:327-375) */
+    double nn = 0.0;
+    for (int i = 0; i < n; ++i) nn += cabs2(x[i]);
+    const double beta0 = sqrt(nn);
+    const double inv0 = beta0 > 0.0 ? 1.0 / beta0 : 0.0;
+    for (int i = 0; i < n; ++i) y[i] = cscale(x[i], inv0);
+    dqo_system sb = *sys;
+    sb.rowptr = sys->tk_rowptr;
+    sb.col = sys->tk_col;
+    sb.val = sys->tk_val;
+    sb.m = mb;
+    double *Q = (double *)malloc(sizeof(cx) * (size_t)n * (mb + 2));
+    double *al = (double *)malloc(sizeof(cx) * (mb + 2));
+    double *be = (double *)malloc(sizeof(cx) * (mb + 2));
+    const double nrm_bv = dqo_lanczos(&sb, sys->tk_diag, (const double *)y, Q, al, be);
+    /* augmented matrix of size mB + p (gpuLanczosHelper.cu:14-60) */
+    cx *T = (cx *)calloc((size_t)L * L, sizeof(cx));
+    cx *E = (cx *)malloc(sizeof(cx) * (size_t)L * L);
+    const cx *alc = (const cx *)al, *bec = (const cx *)be;
+    for (int i = 0; i < mb; ++i) {
+        T[i * L + i] = alc[i + 1];
+        if (i + 1 < mb) {
+            T[i * L + i + 1] = bec[i + 1];
+            T[(i + 1) * L + i] = bec[i + 1];
+        }
+    }
+    T[0 * L + mb].re = 1.0;
+    for (int k = mb; k + 1 < L; ++k) T[k * L + k + 1].re = 1.0;
+    for (int i = 0; i < L * L; ++i) T[i] = cmul(tau, T[i]);
+    const int s = dqo_pade_exp(L, (const double *)T, (double *)E, sys->norm_mode);
+    int rc = 0;
+    if (s < 0) {
+        rc = s;
+    } else {
+        /* out = ||A^p psi|| Q_B phi + taylor part (:345-396) */
+        const cx *Qc = (const cx *)Q;
+        cx *out = (cx *)psi_out;
+        for (int i = 0; i < n; ++i) {
+            cx k = {0, 0};
+            for (int j = 0; j < mb; ++j) k = cadd(k, cmul(Qc[(size_t)(j + 1) * n + i], E[j * L + L - 1]));
+            out[i] = cadd(cscale(k, beta0), acc[i]);
+        }
+        double on = 0.0;
+        for (int i = 0; i < n; ++i) on += cabs2(out[i]);
+        const double nrm = sqrt(on);
+        if (norm_out) *norm_out = nrm;
+        const double inv = 1.0 / nrm;
+        for (int i = 0; i < n; ++i) out[i] = cscale(out[i], inv);
+        if (err_est) {
+            /* padeClass.cu:750-782 on the B part, plus |1 - norm| (:417-434) */
+            const double hm = sqrt(cabs2(bec[mb]));
+            const double err1 = hm * sqrt(cabs2(E[(mb - 1) * L + mb]));
+            const double err2 = hm * nrm_bv * sqrt(cabs2(E[(mb - 1) * L + mb + 1]));
+            double est = (err1 > err2) ? err2 / (1 - err2 / err1) : err1;
+            est += fabs(1.0 - nrm);
+            if (est < 1.110223e-16) est = 1.110223e-16;
+            *err_est = est;
+        }
+    }
+    free(acc); free(Q); free(al); free(be); free(T); free(E);
+    return rc;
+}
+
+/* ------------------------------------------------------------------ */
 /* ensemble                                                            */
 /* ------------------------------------------------------------------ */
+/* 1 / sum_i |psi_i|^4 (systemClass.cu:2209-2253, accumulated in FP64) */
+static double ipr_of(int n, const cx *psi) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const double a = cabs2(psi[i]);
+        s += a * a;
+    }
+    return 1.0 / s;
+}
+
 int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const double *psi0d, int pop_every,
-            double *pops, double *corr, double *psi_final, double *err_acc, int n_threads) {
+            double *pops, double *corr, double *psi_final, double *err_acc, double *ipr, int n_threads) {
     int n = sys->n;
     int n_rec = n_steps / pop_every + 1;
     int nt = 1;
@@ -575,6 +677,7 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
 #endif
     double *pacc = (double *)calloc((size_t)nt * n_rec * n, sizeof(double));
     double *cacc = (double *)calloc((size_t)nt * (n_steps + 1) * 2, sizeof(double));
+    double *iacc = (double *)calloc((size_t)nt * (n_steps + 1), sizeof(double));
     int status = 0;
     const cx *psi0 = (const cx *)psi0d;
 #ifdef _OPENMP
@@ -587,6 +690,7 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
 #endif
         double *myp = pacc + (size_t)tid * n_rec * n;
         double *myc = cacc + (size_t)tid * (n_steps + 1) * 2;
+        double *myi = iacc + (size_t)tid * (n_steps + 1);
         double *eps = (double *)malloc(sizeof(double) * n * 3);
         double *deps = eps + n, *diag = deps + n;
         float *zzu = sys->noise == DQO_NOISE_ZZ ? (float *)malloc(sizeof(float) * (size_t)sys->n_osc * n) : NULL;
@@ -608,17 +712,20 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
             for (int i = 0; i < n; ++i) c = cadd(c, cmul(cconj(psi0[i]), psi[i]));
             myc[0] += c.re; myc[1] += c.im;
             for (int i = 0; i < n; ++i) myp[i] += cabs2(psi[i]);
+            myi[0] += ipr_of(n, psi);
             for (int k = 0; k < n_steps; ++k) {
                 if (zzu) dqo_noise_update_zz(sys, k, eps, zzu, diag);
                 else dqo_noise_update(sys, traj, k, eps, deps, diag);
                 double est;
-                int rc = dqo_krylov_step(sys, diag, (const double *)psi, (double *)tmp, &est, NULL, NULL);
+                int rc = sys->tk_p > 0 ? dqo_tk_step(sys, diag, (const double *)psi, (double *)tmp, &est, NULL)
+                                       : dqo_krylov_step(sys, diag, (const double *)psi, (double *)tmp, &est, NULL, NULL);
                 if (rc != 0) { status = rc; break; }
                 errsum += est;
                 memcpy(psi, tmp, sizeof(cx) * n);
                 c.re = 0; c.im = 0;
                 for (int i = 0; i < n; ++i) c = cadd(c, cmul(cconj(psi0[i]), psi[i]));
                 myc[2 * (k + 1)] += c.re; myc[2 * (k + 1) + 1] += c.im;
+                myi[k + 1] += ipr_of(n, psi);
                 if ((k + 1) % pop_every == 0) {
                     double *row = myp + (size_t)((k + 1) / pop_every) * n;
                     for (int i = 0; i < n; ++i) row[i] += cabs2(psi[i]);
@@ -646,8 +753,16 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
             corr[x] = s * inv;
         }
     }
+    if (ipr) {
+        for (int k = 0; k <= n_steps; ++k) {
+            double s = 0.0;
+            for (int t = 0; t < nt; ++t) s += iacc[(size_t)t * (n_steps + 1) + k];
+            ipr[k] = s * inv;
+        }
+    }
     free(pacc);
     free(cacc);
+    free(iacc);
     return status;
 }
 

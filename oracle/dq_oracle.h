@@ -55,11 +55,19 @@ typedef struct {
     int n_osc;             /* ZZ real noise: oscillators per site */
     const double *zz_omega; /* ZZ: angular frequencies (rad/fs), n_osc */
     const double *zz_coeff; /* ZZ: amplitudes (cm^-1), n_osc */
+    int tk_p;              /* Taylor-Krylov order p (0 = Lanczos mode) */
+    int tk_m;              /* Taylor-Krylov: Krylov dimension on the auxiliary matrix B */
+    const int *tk_rowptr;  /* B: off-diagonal CSR, n+1 */
+    const int *tk_col;
+    const double *tk_val;
+    const double *tk_diag; /* B: diagonal, n */
 } dqo_system;
 
 /* Checks of the adaptive Krylov dimension happen at j = m_min, m_min + 4,
  * ... below m; a trajectory that passes none uses m. */
 enum { DQO_M_CHECK_STRIDE = 4 };
+/* Taylor-Krylov order limit */
+enum { DQO_TK_MAX_P = 32 };
 
 /* ---- building blocks ---- */
 void dqo_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
@@ -89,6 +97,13 @@ int dqo_krylov_step(const dqo_system *sys, const double *diag, const double *psi
  * adaptive choice when sys->m_min > 0). */
 int dqo_krylov_step_m(const dqo_system *sys, const double *diag, const double *psi_in,
                       double *psi_out, double *err_est, double *norm_out, int *s_out, int *m_used);
+/* Taylor-Krylov step (taylorKrylovClass.cu:223-434): psi_out = sum_{k<p}
+ * tau^k/k! A^k psi_in + ||A^p psi_in|| Q_B [exp(tau Tbar_B)]_{0..mB-1, L-1},
+ * Tbar_B the (mB + p) augmented Lanczos matrix of B from A^p psi_in (ones at
+ * (0, mB) and (mB+k, mB+k+1)), then renormalised.  err_est = EXPOKIT
+ * estimate of the B part + |1 - norm|.  A is H with this step's diagonal. */
+int dqo_tk_step(const dqo_system *sys, const double *diag, const double *psi_in, double *psi_out,
+                double *err_est, double *norm_out);
 /* Lanczos only: Q (m+2) columns of n complex each (column 0 zero), alpha and
  * beta (m+2 complex each), returns ||H q_{m+1}||. */
 double dqo_lanczos(const dqo_system *sys, const double *diag, const double *q1,
@@ -112,11 +127,13 @@ void dqo_noise_update_zz(const dqo_system *sys, int step, const double *eps, con
 /* Runs trajectories traj0..traj0+n_traj-1 for n_steps from psi0 (n complex).
  * pops: (n_steps/pop_every + 1) x n, ensemble-averaged |psi|^2 at steps
  * 0, pop_every, ...; corr: (n_steps+1) complex, averaged <psi0|psi(t)>;
- * psi_final: n_traj x n complex (may be NULL); err_acc: n_traj (may be NULL).
+ * psi_final: n_traj x n complex (may be NULL); err_acc: n_traj (may be NULL);
+ * ipr: n_steps + 1, averaged 1 / sum_i |psi_i(k)|^4 (may be NULL,
+ * systemClass.cu:2219-2257).  Taylor-Krylov steps when sys->tk_p > 0.
  * Returns 0 or a negative error code. */
 int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const double *psi0,
             int pop_every, double *pops, double *corr, double *psi_final, double *err_acc,
-            int n_threads);
+            double *ipr, int n_threads);
 
 /* ---- spectrum ---- */
 /* In-place inverse DFT (sign +1, unnormalised, cuFFT INVERSE convention) of

@@ -52,6 +52,12 @@ class _System(C.Structure):
         ("n_osc", C.c_int),
         ("zz_omega", C.POINTER(C.c_double)),
         ("zz_coeff", C.POINTER(C.c_double)),
+        ("tk_p", C.c_int),
+        ("tk_m", C.c_int),
+        ("tk_rowptr", C.POINTER(C.c_int)),
+        ("tk_col", C.POINTER(C.c_int)),
+        ("tk_val", C.POINTER(C.c_double)),
+        ("tk_diag", C.POINTER(C.c_double)),
     ]
 
 
@@ -85,7 +91,9 @@ def lib():
         L.dqo_lanczos.argtypes = [sp, dp, dp, dp, dp, dp]
         L.dqo_lanczos.restype = C.c_double
         L.dqo_build_tbar.argtypes = [C.c_int, dp, dp, dp]
-        L.dqo_run.argtypes = [sp, C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_int]
+        L.dqo_run.argtypes = [sp, C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, dp, dp, dp, dp, C.c_int]
+        L.dqo_tk_step.argtypes = [sp, dp, dp, dp, dp, dp]
+        L.dqo_tk_step.restype = C.c_int
         L.dqo_run.restype = C.c_int
         L.dqo_ifft.argtypes = [C.c_int, dp]
         L.dqo_zz_coefficients.argtypes = [C.c_int, dp, dp, C.c_double, C.c_double, dp, dp]
@@ -158,7 +166,9 @@ class System:
     def __init__(self, rowptr, col, val, h0diag, m, dt, hbar=None, dot_mode=DOT_BILINEAR,
                  norm_mode=NORM_COMPLEX, noise=NOISE_NONE, ka_substeps=1, sigma=None, tau=None,
                  sigma_static=0.0, static_eps=None, seed=0, reorth=0, m_min=0, m_tol=1e-7, zz_omega=None,
-                 zz_coeff=None):
+                 zz_coeff=None, tk=None):
+        """tk: optional Taylor-Krylov mode (p, m_B, rowptr_B, col_B, val_B, diag_B), B's off-diagonal CSR
+        and diagonal."""
         self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
         self.col = np.ascontiguousarray(col, dtype=np.int32)
         self.val = np.ascontiguousarray(val, dtype=np.float64)
@@ -173,6 +183,14 @@ class System:
         self.m = m
         self.dt = dt
         self.hbar = hbar_reference() if hbar is None else hbar
+        if tk is not None:
+            tp, tm, trp, tcol, tval, tdiag = tk
+            self.tk = (int(tp), int(tm), np.ascontiguousarray(trp, dtype=np.int32),
+                       np.ascontiguousarray(tcol, dtype=np.int32), np.ascontiguousarray(tval, dtype=np.float64),
+                       np.ascontiguousarray(tdiag, dtype=np.float64))
+        else:
+            self.tk = (0, 0, None, None, None, None)
+        _ip = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_int))
         self.s = _System(
             self.n,
             self.rowptr.ctypes.data_as(C.POINTER(C.c_int)),
@@ -182,6 +200,7 @@ class System:
             m, dt, self.hbar, dot_mode, norm_mode, noise, ka_substeps,
             _dp(self.sigma), _dp(self.tau), float(sigma_static), _dp(self.static_eps), seed, int(reorth),
             int(m_min), float(m_tol), self.n_osc, _dp(self.zz_omega), _dp(self.zz_coeff),
+            self.tk[0], self.tk[1], _ip(self.tk[2]), _ip(self.tk[3]), _dp(self.tk[4]), _dp(self.tk[5]),
         )
 
     def dense(self, diag=None):
@@ -229,6 +248,17 @@ class System:
             raise RuntimeError(f"oracle krylov step failed ({rc})")
         return out, err.value, nrm.value, s.value
 
+    def tk_step(self, diag, psi):
+        """One Taylor-Krylov step: (psi_out, error estimate, norm before renormalisation)."""
+        psi = np.ascontiguousarray(psi, dtype=np.complex128)
+        out = np.zeros_like(psi)
+        err, nrm = C.c_double(), C.c_double()
+        rc = lib().dqo_tk_step(C.byref(self.s), _dp(np.ascontiguousarray(diag, dtype=np.float64)),
+                               _dp(psi.view(np.float64)), _dp(out.view(np.float64)), C.byref(err), C.byref(nrm))
+        if rc != 0:
+            raise RuntimeError(f"oracle Taylor-Krylov step failed ({rc})")
+        return out, err.value, nrm.value
+
     def krylov_step_m(self, diag, psi):
         """One step; also returns the Krylov dimension used (adaptive when m_min > 0)."""
         psi = np.ascontiguousarray(psi, dtype=np.complex128)
@@ -260,12 +290,13 @@ class System:
         corr = np.zeros(n_steps + 1, dtype=np.complex128)
         fin = np.zeros((n_traj, n), dtype=np.complex128) if want_final else None
         err = np.zeros(n_traj)
+        ipr = np.zeros(n_steps + 1)
         rc = lib().dqo_run(C.byref(self.s), traj0, n_traj, n_steps, _dp(psi0.view(np.float64)), pop_every,
                            _dp(pops), _dp(corr.view(np.float64)),
-                           _dp(fin.view(np.float64)) if fin is not None else None, _dp(err), threads)
+                           _dp(fin.view(np.float64)) if fin is not None else None, _dp(err), _dp(ipr), threads)
         if rc != 0:
             raise RuntimeError(f"oracle run failed ({rc})")
-        return {"pops": pops, "corr": corr, "psi_final": fin, "err": err}
+        return {"pops": pops, "corr": corr, "psi_final": fin, "err": err, "ipr": ipr}
 
 
 def spectrum_loss_grad(rowptr, col, val_base, cls, scales, static_eps, m, dt, psi0, n_traj, n_steps,
