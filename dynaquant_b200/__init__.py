@@ -43,6 +43,7 @@ class Propagator:
         self.cfg = cfg
         self.n = n_sites
         self.n_traj = n_traj
+        self.ipr_enabled = False
         h = C.c_void_p()
         rc = self.L.dq_create(C.byref(cfg), C.byref(h))
         if rc != 0:
@@ -231,8 +232,32 @@ class Propagator:
         self._check(self.L.dq_set_taylor_krylov(self.h, int(p), int(m_b), _lib.iptr(rowptr), _lib.iptr(col),
                                                 _lib.dptr(val)))
 
+    # -- sharded ensembles ------------------------------------------------------------
+    def set_trajectory_offset(self, traj0):
+        """Index of this context's trajectory 0 in the whole ensemble (even): the random-draw key."""
+        self._check(self.L.dq_set_trajectory_offset(self.h, int(traj0)))
+
+    def observable_sums(self, with_ipr=False):
+        """Raw sums over this context's trajectories: (pops, corr, ipr or None)."""
+        T = self.steps_done
+        pops = np.zeros((T // self.cfg.pop_every + 1, self.n))
+        corr = np.zeros(T + 1, dtype=np.complex128)
+        ipr = np.zeros(T + 1) if with_ipr else None
+        self._check(self.L.dq_get_observable_sums(self.h, _lib.dptr(pops), _lib.dptr(corr.view(np.float64)),
+                                                  _lib.dptr(ipr)))
+        return pops, corr, ipr
+
+    def set_observable_sums(self, pops, corr, ipr, n_traj_total):
+        """Install observable sums reduced over all shards, standing for n_traj_total trajectories."""
+        pops = np.ascontiguousarray(pops, dtype=np.float64)
+        corr = np.ascontiguousarray(corr, dtype=np.complex128)
+        ipr = None if ipr is None else np.ascontiguousarray(ipr, dtype=np.float64)
+        self._check(self.L.dq_set_observable_sums(self.h, _lib.dptr(pops), _lib.dptr(corr.view(np.float64)),
+                                                  _lib.dptr(ipr), int(n_traj_total)))
+
     def set_ipr(self, enable=True):
         self._check(self.L.dq_set_ipr(self.h, int(bool(enable))))
+        self.ipr_enabled = bool(enable)
 
     def ipr(self):
         """Ensemble mean of 1 / sum_i |psi_i|^4 after 0..steps_done steps."""

@@ -26,6 +26,7 @@ EXPORTS = [
     "dq_config_default", "dq_create", "dq_destroy", "dq_last_error", "dq_get_stream",
     "dq_set_hamiltonian_csr", "dq_set_coupling_classes", "dq_set_noise_params", "dq_set_static_energies",
     "dq_set_zz_spectral_density", "dq_set_taylor_krylov", "dq_set_ipr", "dq_get_ipr", "dq_write_ipr",
+    "dq_set_trajectory_offset", "dq_get_observable_sums", "dq_set_observable_sums",
     "dq_set_initial_state", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
@@ -91,6 +92,9 @@ def load(path: str = LIB_PATH):
     L.dq_set_zz_spectral_density.argtypes = [vp, C.c_int, dp, dp, C.c_double, C.c_double]
     L.dq_set_taylor_krylov.argtypes = [vp, C.c_int, C.c_int, ip, ip, dp]
     L.dq_set_ipr.argtypes = [vp, C.c_int]
+    L.dq_set_trajectory_offset.argtypes = [vp, C.c_int]
+    L.dq_get_observable_sums.argtypes = [vp, dp, dp, dp]
+    L.dq_set_observable_sums.argtypes = [vp, dp, dp, dp, C.c_int]
     L.dq_get_ipr.argtypes = [vp, dp, C.POINTER(C.c_int)]
     L.dq_write_ipr.argtypes = [vp, C.c_char_p]
     L.dq_set_static_energies.argtypes = [vp, dp]

@@ -328,8 +328,47 @@ dq_status dq_get_ipr(dq_ctx* c, double* out, int* n_values) {
     if (!out) return DQ_OK;
     DQ_CU(cudaStreamSynchronize(c->stream));
     DQ_CU(cudaMemcpy(out, c->d_ipr, sizeof(double) * nv, cudaMemcpyDeviceToHost));
-    const double inv = 1.0 / c->cfg.n_traj;
+    const double inv = 1.0 / observed_trajectories(c);
     for (int k = 0; k < nv; ++k) out[k] *= inv;
+    return DQ_OK;
+}
+
+dq_status dq_set_trajectory_offset(dq_ctx* c, int traj0) {
+    if (!c) return DQ_ERR_ARG;
+    if (traj0 < 0 || traj0 % 2) return fail(c, DQ_ERR_ARG, "trajectory_offset: must be even and >= 0");
+    c->traj0 = traj0;
+    c->ready = false;
+    return DQ_OK;
+}
+
+dq_status dq_get_observable_sums(dq_ctx* c, double* pops, dq_cdouble* corr, double* ipr) {
+    if (!c) return DQ_ERR_ARG;
+    if (c->last_path == 1 && c->bat) {
+        dq_status st = batched_collect_corr(c);
+        if (st) return st;
+    }
+    const int nrec = c->steps_done / c->cfg.pop_every + 1, np = c->steps_done + 1;
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    if (pops) DQ_CU(cudaMemcpy(pops, c->d_pops, sizeof(double) * (size_t)nrec * c->n, cudaMemcpyDeviceToHost));
+    if (corr) DQ_CU(cudaMemcpy(corr, c->d_corr, sizeof(cd) * np, cudaMemcpyDeviceToHost));
+    if (ipr) {
+        if (!c->ipr_on) return fail(c, DQ_ERR_STATE, "observable_sums: the inverse participation ratio is off");
+        DQ_CU(cudaMemcpy(ipr, c->d_ipr, sizeof(double) * np, cudaMemcpyDeviceToHost));
+    }
+    return DQ_OK;
+}
+
+dq_status dq_set_observable_sums(dq_ctx* c, const double* pops, const dq_cdouble* corr, const double* ipr,
+                                 int n_traj_total) {
+    if (!c || !pops || !corr || n_traj_total < 1) return DQ_ERR_ARG;
+    if (ipr && !c->ipr_on) return fail(c, DQ_ERR_STATE, "observable_sums: the inverse participation ratio is off");
+    const int nrec = c->steps_done / c->cfg.pop_every + 1, np = c->steps_done + 1;
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    DQ_CU(cudaMemcpy(c->d_pops, pops, sizeof(double) * (size_t)nrec * c->n, cudaMemcpyHostToDevice));
+    DQ_CU(cudaMemcpy(c->d_corr, corr, sizeof(cd) * np, cudaMemcpyHostToDevice));
+    if (ipr) DQ_CU(cudaMemcpy(c->d_ipr, ipr, sizeof(double) * np, cudaMemcpyHostToDevice));
+    c->obs_traj = n_traj_total;
+    c->last_path = 2;
     return DQ_OK;
 }
 
@@ -372,6 +411,8 @@ dq_status dq_reset(dq_ctx* c) {
     if ((st = plain_clear_observables(c))) return st;
     c->steps_done = 0;
     c->plain_traj_done = 0;
+    c->obs_traj = 0;
+    if (c->last_path == 2) c->last_path = 0;
     if (c->bat) {
         if ((st = batched_reset(c))) return st;
     }
@@ -439,6 +480,8 @@ dq_status dq_run(dq_ctx* c, int n_steps) {
         return fail(c, DQ_ERR_ARG, "run: steps exceed max_steps");
     if (c->tk_p > 0)
         return fail(c, DQ_ERR_STATE, "run: Taylor-Krylov mode runs on the per-trajectory path (dq_run_plain)");
+    if (c->obs_traj > 0)
+        return fail(c, DQ_ERR_STATE, "run: the observables hold reduced ensemble sums; dq_reset first");
     dq_status st;
     if (!c->bat) {
         if ((st = batched_alloc(c))) return st;
@@ -458,7 +501,7 @@ dq_status dq_get_populations(dq_ctx* c, double* out, int* n_records) {
     if (!out) return DQ_OK;
     DQ_CU(cudaStreamSynchronize(c->stream));
     DQ_CU(cudaMemcpy(out, c->d_pops, sizeof(double) * (size_t)nrec * c->n, cudaMemcpyDeviceToHost));
-    const double inv = 1.0 / c->cfg.n_traj;
+    const double inv = 1.0 / observed_trajectories(c);
     for (size_t x = 0; x < (size_t)nrec * c->n; ++x) out[x] *= inv;
     return DQ_OK;
 }
@@ -474,7 +517,7 @@ dq_status dq_get_correlation(dq_ctx* c, dq_cdouble* out, int* n_points) {
     }
     DQ_CU(cudaStreamSynchronize(c->stream));
     DQ_CU(cudaMemcpy(out, c->d_corr, sizeof(cd) * np, cudaMemcpyDeviceToHost));
-    const double inv = 1.0 / c->cfg.n_traj;
+    const double inv = 1.0 / observed_trajectories(c);
     for (int k = 0; k < np; ++k) { out[k].re *= inv; out[k].im *= inv; }
     return DQ_OK;
 }

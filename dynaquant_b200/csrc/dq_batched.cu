@@ -43,30 +43,31 @@
 namespace dq {
 
 // ---------------------------------------------------------------------------
-__global__ void k_traj_init_b(int n, int B, uint64_t seed, const double* __restrict__ h0,
+__global__ void k_traj_init_b(int n, int B, int traj0, uint64_t seed, const double* __restrict__ h0,
                               const double* __restrict__ static_eps, double sigma_static,
                               const double* __restrict__ sigma, int noise, double* __restrict__ eps,
                               double* __restrict__ deps) {
     for (int i = blockIdx.x; i < n; i += gridDim.x) {
         for (int b = threadIdx.x; b < B; b += blockDim.x) {
             const size_t x = (size_t)i * B + b;
+            const int g = traj0 + b;   // trajectory index of the whole ensemble (Philox key)
             double e;
             if (static_eps) e = static_eps[i];
-            else e = __dadd_rn(__dmul_rn(sigma_static, normal(seed, P_STATIC, b, 0, i, 0)), h0[i]);
+            else e = __dadd_rn(__dmul_rn(sigma_static, normal(seed, P_STATIC, g, 0, i, 0)), h0[i]);
             eps[x] = e;
-            deps[x] = (noise == DQ_NOISE_OU) ? __dmul_rn(sigma[i], normal(seed, P_OU_INIT, b, 0, i, 0)) : 0.0;
+            deps[x] = (noise == DQ_NOISE_OU) ? __dmul_rn(sigma[i], normal(seed, P_OU_INIT, g, 0, i, 0)) : 0.0;
         }
     }
 }
 
 // ZZ phase fractions of every (oscillator, site, trajectory), [osc][site][traj]
-__global__ void k_zz_phases_b(int n, int B, int n_osc, uint64_t seed, float* __restrict__ u) {
+__global__ void k_zz_phases_b(int n, int B, int traj0, int n_osc, uint64_t seed, float* __restrict__ u) {
     const size_t total = (size_t)n * B * n_osc;
     for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
         const int b = (int)(x % B);
         const size_t r = x / B;
         const int i = (int)(r % n), o = (int)(r / n);
-        u[x] = zz_phase(seed, (uint32_t)b, (uint32_t)i, (uint32_t)o);
+        u[x] = zz_phase(seed, (uint32_t)(traj0 + b), (uint32_t)i, (uint32_t)o);
     }
 }
 
@@ -85,7 +86,8 @@ __global__ void k_set_psi0_b(int n, int B, const cd* __restrict__ psi0, Real* __
 // OU / Gaussian update of every trajectory's diagonal for this step
 // (gpuSysHelper.cu:32-128 with Philox keys instead of shared cuRAND states)
 template <typename Real, int TPT>
-__global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int TC, int rpc, int noise, int ns, double subdt,
+__global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int traj0, int TC, int rpc, int noise, int ns,
+                                                      double subdt,
                                                       double sqrt_subdt, uint64_t seed,
                                                       const double* __restrict__ sigma,
                                                       const double* __restrict__ invtau,
@@ -123,14 +125,15 @@ __global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int TC, int
             double v0, v1;
             if (noise == DQ_NOISE_OU) {
                 double c0 = deps[x], c1 = deps[x + 1];
-                ou_update_pair(c0, c1, invtau[row], coeff[row], subdt, sqrt_subdt, ns, seed, T.b0 >> 1, step, row);
+                ou_update_pair(c0, c1, invtau[row], coeff[row], subdt, sqrt_subdt, ns, seed, (traj0 + T.b0) >> 1, step,
+                               row);
                 deps[x] = c0;
                 deps[x + 1] = c1;
                 v0 = __dadd_rn(c0, eps[x]);
                 v1 = __dadd_rn(c1, eps[x + 1]);
             } else if (noise == DQ_NOISE_GAUSS) {
                 double z0, z1;
-                normal_pair(seed, P_GAUSS, T.b0 >> 1, step, row, 0, z0, z1);
+                normal_pair(seed, P_GAUSS, (traj0 + T.b0) >> 1, step, row, 0, z0, z1);
                 v0 = __dadd_rn(__dmul_rn(z0, sigma[row]), eps[x]);
                 v1 = __dadd_rn(__dmul_rn(z1, sigma[row]), eps[x + 1]);
             } else {
@@ -147,11 +150,11 @@ __global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int TC, int
             const size_t x = (size_t)row * B + b;
             double v;
             if (noise == DQ_NOISE_OU) {
-                double cur = ou_update(deps[x], invtau[row], coeff[row], subdt, sqrt_subdt, ns, seed, b, step, row);
+                double cur = ou_update(deps[x], invtau[row], coeff[row], subdt, sqrt_subdt, ns, seed, traj0 + b, step, row);
                 deps[x] = cur;
                 v = __dadd_rn(cur, eps[x]);
             } else if (noise == DQ_NOISE_GAUSS) {
-                double xi = normal(seed, P_GAUSS, b, step, row, 0);
+                double xi = normal(seed, P_GAUSS, traj0 + b, step, row, 0);
                 v = __dadd_rn(__dmul_rn(xi, sigma[row]), eps[x]);
             } else {
                 v = eps[x];
@@ -2568,14 +2571,14 @@ dq_status batched_reset(dq_ctx* c) {
     const int thr = std::min(256, ((B + 31) / 32) * 32);
     // a setter may have re-allocated a parameter array the captured step reads
     drop_graph(bs);
-    k_traj_init_b<<<blocks, thr, 0, c->stream>>>(n, B, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
+    k_traj_init_b<<<blocks, thr, 0, c->stream>>>(n, B, c->traj0, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
                                                  c->d_sigma, c->cfg.noise_model, bs->eps, bs->deps);
     if (c->cfg.noise_model == DQ_NOISE_ZZ) {
         if (B != c->cfg.n_traj) {
             c->err = "batched: ZZ phases are laid out for n_traj trajectories";
             return DQ_ERR_STATE;
         }
-        k_zz_phases_b<<<bs->sms * 16, 256, 0, c->stream>>>(n, B, c->zz_n_osc, c->cfg.seed, c->d_zz_u);
+        k_zz_phases_b<<<bs->sms * 16, 256, 0, c->stream>>>(n, B, c->traj0, c->zz_n_osc, c->cfg.seed, c->d_zz_u);
     }
     const size_t real_sz = bs->mixed ? sizeof(float) : sizeof(double);
     const size_t slab = (size_t)n * B * 2 * real_sz;
@@ -2842,7 +2845,7 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
     const double sqrt_subdt = sqrt(subdt);
     const dim3 grid(bs->gx, bs->chunks);
     mark(DQ_KIND_NOISE);
-    k_noise_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, c->cfg.noise_model, ns, subdt, sqrt_subdt,
+    k_noise_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, c->traj0, TC, rpc, c->cfg.noise_model, ns, subdt, sqrt_subdt,
                                                      c->cfg.seed, c->d_sigma, c->d_invtau, c->d_coeff, bs->eps,
                                                      bs->deps, (Real*)bs->diag, bs->s, zz_params(c));
     if (after_noise) (*after_noise)();

@@ -97,7 +97,9 @@ struct dq_ctx {
     double* d_erracc = nullptr;   // n_traj
     int steps_done = 0;
     int plain_traj_done = 0;      // trajectories completed by dq_run_plain
-    int last_path = 0;            // 0: observables from dq_run_plain, 1: from dq_run
+    int last_path = 0;            // 0: observables from dq_run_plain, 1: from dq_run, 2: reduced sums set
+    int traj0 = 0;                // index of trajectory 0 in the whole (sharded) ensemble: the Philox key
+    int obs_traj = 0;             // trajectories behind the observable sums when set from a reduction
 
     // Taylor-Krylov mode (tk_p > 0): the auxiliary matrix B (off-diagonal
     // CSR + diagonal), its Krylov basis and the Taylor work vectors
@@ -122,6 +124,12 @@ struct dq_ctx {
 };
 
 namespace dq {
+// Trajectories the observable sums stand for (their divisor for means).
+inline int observed_trajectories(const dq_ctx* c) {
+    if (c->obs_traj > 0) return c->obs_traj;
+    return (c->last_path == 0 && c->plain_traj_done > 0) ? c->plain_traj_done : c->cfg.n_traj;
+}
+
 // implemented in dq_plain.cu
 dq_status plain_alloc(dq_ctx* c);
 void plain_free(dq_ctx* c);

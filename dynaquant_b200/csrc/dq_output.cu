@@ -84,7 +84,7 @@ dq_status dq_write_populations(dq_ctx* c, const char* path, int binary, int cont
     const int n = c->n, T = c->steps_done, pe = c->cfg.pop_every;
     const int nsteps_out = nrec - 1;   // records at pop_every, 2 pop_every, ... (step 0 is not printed)
     const double dt = c->cfg.dt;
-    int numsims = c->plain_traj_done > 0 && c->last_path == 0 ? c->plain_traj_done : c->cfg.n_traj;
+    int numsims = observed_trajectories(c);
     std::vector<double> prev;
     if (continuation) {
         // add the sums of an earlier file with the same dt, steps and sites
@@ -206,7 +206,7 @@ dq_status dq_write_spectrum(dq_ctx* c, const char* corr_path, const char* spec_p
     st = check_cuda(c, cudaMemcpyAsync(d, c->d_corr, sizeof(cd) * len, cudaMemcpyDeviceToDevice, c->stream), "copy");
     if (!st) {
         const int blocks = std::max(1, std::min(148 * 4, (len + 127) / 128));
-        k_idft_direct<<<blocks, 128, 0, c->stream>>>(len, d, 1.0 / c->cfg.n_traj, d + len);
+        k_idft_direct<<<blocks, 128, 0, c->stream>>>(len, d, 1.0 / observed_trajectories(c), d + len);
         st = check_cuda(c, cudaGetLastError(), "inverse DFT");
     }
     if (!st) st = check_cuda(c, cudaMemcpyAsync(corr.data(), d, sizeof(cd) * len, cudaMemcpyDeviceToHost, c->stream),
@@ -218,7 +218,7 @@ dq_status dq_write_spectrum(dq_ctx* c, const char* corr_path, const char* spec_p
     if (st) return st;
     // the reference keeps the scaling constant in a float (spectraClass.cu:643-651)
     const float sc = (float)scaling;
-    const double inv_traj = 1.0 / c->cfg.n_traj;
+    const double inv_traj = 1.0 / observed_trajectories(c);
     FILE* f = fopen(corr_path, "w");
     if (!f) return ofail(c, DQ_ERR_ARG, std::string("write_spectrum: cannot create ") + corr_path);
     bool ok = fprintf(f, "{timestep #} {timestamp fs} {M(t) real imag}: \n") > 0;

@@ -25,13 +25,13 @@
 
 namespace dq {
 
-__global__ void k_traj_init_plain(int n, int n_traj, uint64_t seed, const double* __restrict__ h0,
+__global__ void k_traj_init_plain(int n, int n_traj, int traj0, uint64_t seed, const double* __restrict__ h0,
                                   const double* __restrict__ static_eps, double sigma_static,
                                   const double* __restrict__ sigma, int noise, double* __restrict__ eps,
                                   double* __restrict__ deps) {
     size_t total = (size_t)n * n_traj;
     for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-        int t = (int)(x / n), i = (int)(x % n);
+        int t = traj0 + (int)(x / n), i = (int)(x % n);   // t: trajectory index of the whole ensemble
         double e;
         if (static_eps) e = static_eps[i];
         else e = __dadd_rn(__dmul_rn(sigma_static, normal(seed, P_STATIC, t, 0, i, 0)), h0[i]);
@@ -461,7 +461,7 @@ dq_status plain_traj_init(dq_ctx* c) {
     const int n = c->n, B = c->cfg.n_traj;
     size_t total = (size_t)n * B;
     int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
-    k_traj_init_plain<<<blocks, 256, 0, c->stream>>>(n, B, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
+    k_traj_init_plain<<<blocks, 256, 0, c->stream>>>(n, B, c->traj0, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
                                                      c->d_sigma, c->cfg.noise_model, c->d_eps_p, c->d_deps_p);
     DQ_CU(cudaGetLastError());
     DQ_CU(cudaMemsetAsync(&c->d_ps->status, 0, sizeof(int), c->stream));
@@ -545,9 +545,9 @@ dq_status plain_step(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_ou
         zz.omega = c->d_zz_omega;
         zz.coeff = c->d_zz_coeff;
         zz.dt = c->cfg.dt;
-        k_noise_zz<<<G, T, 0, st>>>(n, traj, step, c->cfg.seed, zz, eps, c->d_diag, c->d_ps);
+        k_noise_zz<<<G, T, 0, st>>>(n, c->traj0 + traj, step, c->cfg.seed, zz, eps, c->d_diag, c->d_ps);
     } else {
-        k_noise<<<G, T, 0, st>>>(n, traj, step, c->cfg.noise_model, ns, subdt, sqrt_subdt, c->cfg.seed, c->d_sigma,
+        k_noise<<<G, T, 0, st>>>(n, c->traj0 + traj, step, c->cfg.noise_model, ns, subdt, sqrt_subdt, c->cfg.seed, c->d_sigma,
                                  c->d_invtau, c->d_coeff, eps, deps, c->d_diag, c->d_ps);
     }
     if (c->tk_p > 0) return plain_tk_tail(c, traj, step, psi_in, psi_out, observe, rec);

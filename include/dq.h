@@ -142,6 +142,23 @@ DQ_API dq_status dq_set_taylor_krylov(dq_ctx *ctx, int p, int m_b, const int *ro
 DQ_API dq_status dq_set_ipr(dq_ctx *ctx, int enable);
 /* steps done + 1 values: the ensemble mean of 1 / sum |psi(k)|^4, k = 0.. */
 DQ_API dq_status dq_get_ipr(dq_ctx *ctx, double *out, int *n_values);
+/* ---- ensembles sharded over processes / GPUs (no reference counterpart;
+ * the reference runs numEnsembleRuns one after another, propagate.cu:167-298) ----
+ * Index of this context's trajectory 0 in the whole ensemble (even, >= 0):
+ * every random draw of local trajectory b is keyed by traj0 + b, so shards
+ * [r B, (r+1) B) over ranks r reproduce one ensemble of world x B
+ * trajectories.  Takes effect at the next reset. */
+DQ_API dq_status dq_set_trajectory_offset(dq_ctx *ctx, int traj0);
+/* Raw observable SUMS over this context's trajectories (not divided):
+ * populations (steps/pop_every + 1) x N, correlation steps + 1 complex and,
+ * when enabled, IPR steps + 1 (each pointer may be NULL). */
+DQ_API dq_status dq_get_observable_sums(dq_ctx *ctx, double *pops, dq_cdouble *corr, double *ipr);
+/* Replaces the observable sums by ones reduced over all shards (same
+ * shapes; ipr may be NULL) standing for n_traj_total trajectories: the
+ * getters and file writers then report the whole ensemble.  dq_run refuses
+ * to continue until dq_reset. */
+DQ_API dq_status dq_set_observable_sums(dq_ctx *ctx, const double *pops, const dq_cdouble *corr, const double *ipr,
+                                        int n_traj_total);
 /* Explicit static site energies shared by all trajectories (replaces the
  * Hamiltonian diagonal plus static disorder); NULL restores them. */
 DQ_API dq_status dq_set_static_energies(dq_ctx *ctx, const double *eps);
