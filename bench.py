@@ -9,9 +9,11 @@ reference's Hamiltonian file is not distributed).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints one JSON line on rank 0.  Multi-GPU: one process per GPU (torchrun),
-every rank propagates its own independent trajectories (different Philox
-trajectory keys), no data-path collective ("replicas", weak scaling).
+Prints one JSON line on rank 0.  Multi-GPU: one process per GPU (torchrun);
+rank r propagates trajectories [r B, (r+1) B) of one ensemble of N B (Philox
+keys by global trajectory index), with no exchange while stepping (weak
+scaling); the end-to-end leg ends with one NCCL all-reduce of the observable
+sums, the ensemble average every rank then reports.
 """
 from __future__ import annotations
 
@@ -353,9 +355,11 @@ def run_ours(args, rank, world, local_rank):
     B = w["B"]
     s = build_system()
     K, W = args.steps, args.warmup
-    seed = w["seed"] + 7919 * rank
+    seed = w["seed"]
     # ---- device-resident throughput ----------------------------------------
+    # rank r runs trajectories [r B, (r+1) B) of one ensemble of world x B (no exchange while stepping)
     p = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=W + K + 8)
+    p.set_trajectory_offset(rank * B)
     tiling = p.autotune()
     p.reset()
     p.run(W)
@@ -396,10 +400,15 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     p2 = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=K + 8)
+    p2.set_trajectory_offset(rank * B)
     p2.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
                   tiling["staged"], tiling["groups"])
     p2.reset()
     p2.run(K)
+    if world > 1:
+        # the ensemble's one exchange: observable sums all-reduced over the ranks (NCCL)
+        from dynaquant_b200.ensemble import allreduce_observables
+        allreduce_observables(p2, B * world)
     pops = p2.populations()
     corr = p2.correlation()
     torch.cuda.synchronize()
@@ -414,7 +423,7 @@ def run_ours(args, rank, world, local_rank):
     e2e = {"value": B * K * world / e2e_s, "unit": "traj-steps/s", "h2d_bytes_per_step": h2d / K,
            "d2h_bytes_per_step": d2h / K,
            "note": "whole job through the C ABI from host arrays: CSR/noise/psi0 upload, reset, K steps, "
-                   "populations + correlation download"}
+                   "(N > 1: all-reduce of the observable sums), populations + correlation download"}
     if rank != 0:
         return
     # ---- plain FP64 per-trajectory GPU path on the same workload ---------------
@@ -476,7 +485,8 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": w["name"], "n_sites": s.n, "nnz_per_row": (s.nnz - s.n) / s.n, "m": w["m"],
                    "trajectories_per_gpu": B, "dt_fs": w["dt"], "noise": "OU 250/50 fs + static 150",
                    "l2": "inputs larger than L2 (Krylov slabs %.1f GB)" % (8.0 * s.n * B * (w["m"] + 2) / 1e9),
-                   "parallelism": f"replicas x{world}",
+                   "parallelism": (f"ensemble shards x{world}: trajectory ranges per GPU, one NCCL all-reduce of "
+                                   "the observables at the end of the e2e run") if world > 1 else "1 GPU",
                    "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged",
                                                     "groups", "ms_per_iter")}},
         "e2e": e2e,
