@@ -112,6 +112,7 @@ dq_status dq_create(const dq_config* cfg, dq_ctx** out) {
 }
 
 static void tk_free(dq_ctx* c) {
+    tk_ensemble_free(c);
     cudaFree(c->d_tk_rowptr); cudaFree(c->d_tk_col); cudaFree(c->d_tk_val); cudaFree(c->d_tk_diag);
     cudaFree(c->d_tk_Q); cudaFree(c->d_tk_x); cudaFree(c->d_tk_acc);
     c->d_tk_rowptr = c->d_tk_col = nullptr;
@@ -413,7 +414,9 @@ dq_status dq_reset(dq_ctx* c) {
     c->plain_traj_done = 0;
     c->obs_traj = 0;
     if (c->last_path == 2) c->last_path = 0;
-    if (c->bat) {
+    if (c->tk_p > 0 && c->tke) {
+        if ((st = tk_ensemble_reset(c))) return st;
+    } else if (c->bat) {
         if ((st = batched_reset(c))) return st;
     }
     c->ready = true;
@@ -478,11 +481,23 @@ dq_status dq_run(dq_ctx* c, int n_steps) {
     if (!c) return DQ_ERR_ARG;
     if (n_steps < 0 || c->steps_done + n_steps > c->cfg.max_steps)
         return fail(c, DQ_ERR_ARG, "run: steps exceed max_steps");
-    if (c->tk_p > 0)
-        return fail(c, DQ_ERR_STATE, "run: Taylor-Krylov mode runs on the per-trajectory path (dq_run_plain)");
     if (c->obs_traj > 0)
         return fail(c, DQ_ERR_STATE, "run: the observables hold reduced ensemble sums; dq_reset first");
     dq_status st;
+    if (c->tk_p > 0) {
+        // Taylor-Krylov mode: the FP64 ensemble of dq_tk_ensemble.cu
+        if (c->cfg.reorth) return fail(c, DQ_ERR_ARG, "run: Taylor-Krylov ensemble without reorthogonalisation");
+        if (!c->tke) {
+            if ((st = check_ready(c))) return st;
+            if ((st = tk_ensemble_reset(c))) return st;
+            c->ready = false;
+        }
+        if (!c->ready || c->last_path != 3) {
+            if ((st = dq_reset(c))) return st;
+        }
+        c->last_path = 3;
+        return tk_ensemble_run(c, n_steps);
+    }
     if (!c->bat) {
         if ((st = batched_alloc(c))) return st;
         c->ready = false;
@@ -524,6 +539,7 @@ dq_status dq_get_correlation(dq_ctx* c, dq_cdouble* out, int* n_points) {
 
 dq_status dq_get_states(dq_ctx* c, dq_cdouble* out) {
     if (!c || !out) return DQ_ERR_ARG;
+    if (c->last_path == 3 && c->tke) return tk_ensemble_states(c, out);
     if (!c->bat) return fail(c, DQ_ERR_STATE, "get_states: no ensemble state (run dq_run first)");
     return batched_get_states(c, out);
 }

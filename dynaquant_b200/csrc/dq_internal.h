@@ -36,6 +36,7 @@ constexpr int kMaxZZOsc = 1024;   // oscillators of one ZZ spectral density
 constexpr int kIprRowGroups = 296; // row groups of the ensemble IPR reduction (2 per SM)
 
 struct BatchedState;   // dq_batched.cu
+struct TkEnsemble;     // dq_tk_ensemble.cu
 struct AdjointState;   // dq_adjoint.cu
 
 }  // namespace dq
@@ -97,7 +98,7 @@ struct dq_ctx {
     double* d_erracc = nullptr;   // n_traj
     int steps_done = 0;
     int plain_traj_done = 0;      // trajectories completed by dq_run_plain
-    int last_path = 0;            // 0: observables from dq_run_plain, 1: from dq_run, 2: reduced sums set
+    int last_path = 0;            // 0: dq_run_plain, 1: dq_run, 2: reduced sums set, 3: Taylor-Krylov dq_run
     int traj0 = 0;                // index of trajectory 0 in the whole (sharded) ensemble: the Philox key
     int obs_traj = 0;             // trajectories behind the observable sums when set from a reduction
 
@@ -121,6 +122,7 @@ struct dq_ctx {
 
     dq::BatchedState* bat = nullptr;
     dq::AdjointState* adj = nullptr;
+    dq::TkEnsemble* tke = nullptr;   // ensemble workspace of Taylor-Krylov mode
 };
 
 namespace dq {
@@ -154,6 +156,15 @@ void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* sta
 dq_status batched_invalidate_blocks(dq_ctx* c);
 dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms);
 void batched_noise_arrays(dq_ctx* c, const double** eps, const double** deps);
+// kernels of dq_batched.cu also launched by the Taylor-Krylov ensemble
+__global__ void k_traj_init_b(int n, int B, int traj0, uint64_t seed, const double* h0, const double* static_eps,
+                              double sigma_static, const double* sigma, int noise, double* eps, double* deps);
+__global__ void k_zz_phases_b(int n, int B, int traj0, int n_osc, uint64_t seed, float* u);
+// implemented in dq_tk_ensemble.cu
+dq_status tk_ensemble_reset(dq_ctx* c);
+dq_status tk_ensemble_run(dq_ctx* c, int n_steps);
+dq_status tk_ensemble_states(dq_ctx* c, dq_cdouble* out);
+void tk_ensemble_free(dq_ctx* c);
 // implemented in dq_fft.cu
 dq_status fft_inverse(dq_ctx* c, int len, const cd* in, int n_in, double scale, cd* out);
 // implemented in dq_adjoint.cu

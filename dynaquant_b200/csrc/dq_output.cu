@@ -152,10 +152,10 @@ dq_status dq_write_populations(dq_ctx* c, const char* path, int binary, int cont
 
 dq_status dq_write_states(dq_ctx* c, const char* folder) {
     if (!c || !folder) return DQ_ERR_ARG;
-    if (!c->bat) return ofail(c, DQ_ERR_STATE, "write_states: no ensemble state (run dq_run first)");
+    if (!c->bat && !c->tke) return ofail(c, DQ_ERR_STATE, "write_states: no ensemble state (run dq_run first)");
     const int n = c->n, nr = c->cfg.n_traj;
     std::vector<dq_cdouble> st_host((size_t)nr * n);
-    dq_status st = batched_get_states(c, st_host.data());
+    dq_status st = dq_get_states(c, st_host.data());
     if (st) return st;
     // statePrintClass.cu:112-127: stamp = dt * step as a float, printed by the stream default
     const float stamp = (float)(c->cfg.dt * c->steps_done);

@@ -129,8 +129,9 @@ DQ_API dq_status dq_set_zz_spectral_density(dq_ctx *ctx, int n_osc, const double
  * Lanczos iterations on the auxiliary matrix B (full CSR over the N sites,
  * diagonal included) started from A^p psi, then renormalised; the error
  * estimate is EXPOKIT's on the B part plus |1 - norm|.  2 <= p, 1 <= m_b <= 32,
- * m_b + p <= 34; p = 0 returns to Lanczos mode.  Steps run on the
- * per-trajectory path (dq_prop_step, dq_run_plain); dq_run, groups and the
+ * m_b + p <= 34; p = 0 returns to Lanczos mode.  Steps run in FP64 on the
+ * per-trajectory path (dq_prop_step, dq_run_plain) and, for dq_run, on an
+ * ensemble path that advances all trajectories together; groups and the
  * adjoint refuse this mode. */
 DQ_API dq_status dq_set_taylor_krylov(dq_ctx *ctx, int p, int m_b, const int *rowptr, const int *col,
                                       const double *val);

@@ -82,12 +82,31 @@ def test_taylor_krylov_prop_step_and_modes(oracle):
     ref, ref_err, _ = S.tk_step(S.h0diag, s.bright_state())
     assert np.abs(out.cpu().numpy() - ref).max() <= 1e-12
     assert err == pytest.approx(ref_err, rel=1e-6)
-    with pytest.raises(dq.DQError):
-        prop.run(2)                     # the ensemble path refuses Taylor-Krylov mode
+    # the ensemble path: every (noise-free) trajectory equals two oracle steps
+    prop.run(2)
+    st = prop.states()
+    ref2, _, _ = S.tk_step(S.h0diag, ref)
+    assert np.abs(st - ref2[None, :]).max() <= 1e-12
     with pytest.raises(dq.DQError):
         prop.set_taylor_krylov(1, 8, np.zeros(s.n + 1, np.int32), np.zeros(0, np.int32), np.zeros(0))
     prop.set_taylor_krylov(0)          # back to Lanczos mode
     prop.run(2)
+    prop.close()
+
+
+@pytest.mark.parametrize("noise", [True, False])
+def test_taylor_krylov_ensemble_matches_oracle(oracle, noise):
+    prop, s, tk = _setup(6, 12, noise=noise, B=4)
+    S, ref = _oracle(oracle, s, tk, noise=noise, B=4)
+    prop.run(5)
+    prop.run(7)
+    assert np.abs(prop.populations() - ref["pops"]).max() <= TOL_FP64
+    assert np.abs(prop.correlation() - ref["corr"]).max() <= TOL_FP64
+    assert np.allclose(prop.ipr(), ref["ipr"], rtol=1e-11)
+    assert np.allclose(prop.error_accum(), ref["err"], rtol=1e-6, atol=1e-14)
+    # the per-trajectory path gives the same ensemble
+    prop.run_plain(12)
+    assert np.abs(prop.populations() - ref["pops"]).max() <= TOL_FP64
     prop.close()
 
 
