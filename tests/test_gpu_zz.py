@@ -92,7 +92,7 @@ def test_zz_noise_changes_with_density(oracle):
 def test_zz_adjoint_matches_oracle(oracle):
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
-    N, B, T, LEN = 48, 4, 10, 12
+    N, B, T, LEN = 48, 8, 10, 16
     s = systems.chain(N, -300.0)
     rng = np.random.default_rng(3)
     eps0 = rng.normal(0.0, 80.0, N)
