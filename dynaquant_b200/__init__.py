@@ -232,6 +232,14 @@ class Propagator:
         self._check(self.L.dq_set_taylor_krylov(self.h, int(p), int(m_b), _lib.iptr(rowptr), _lib.iptr(col),
                                                 _lib.dptr(val)))
 
+    def set_correlation_bra(self, bra):
+        """Bra of the correlation M(t) = <bra|psi(t)> (CD spectra); None returns to psi0."""
+        if bra is None:
+            self._check(self.L.dq_set_correlation_bra(self.h, None))
+            return
+        bra = np.ascontiguousarray(bra, dtype=np.complex128)
+        self._check(self.L.dq_set_correlation_bra(self.h, _lib.dptr(bra.view(np.float64))))
+
     # -- sharded ensembles ------------------------------------------------------------
     def set_trajectory_offset(self, traj0):
         """Index of this context's trajectory 0 in the whole ensemble (even): the random-draw key."""

@@ -26,13 +26,13 @@ EXPORTS = [
     "dq_config_default", "dq_create", "dq_destroy", "dq_last_error", "dq_get_stream",
     "dq_set_hamiltonian_csr", "dq_set_coupling_classes", "dq_set_noise_params", "dq_set_static_energies",
     "dq_set_zz_spectral_density", "dq_set_taylor_krylov", "dq_set_ipr", "dq_get_ipr", "dq_write_ipr",
-    "dq_set_trajectory_offset", "dq_get_observable_sums", "dq_set_observable_sums",
+    "dq_set_correlation_bra", "dq_set_trajectory_offset", "dq_get_observable_sums", "dq_set_observable_sums",
     "dq_set_initial_state", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
     "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward",
     "dq_group_create", "dq_group_destroy", "dq_group_last_error", "dq_group_run",
-    "dq_write_populations", "dq_write_states", "dq_write_spectrum",
+    "dq_write_populations", "dq_write_states", "dq_write_spectrum", "dq_write_spectrum_mean",
 ]
 
 
@@ -93,6 +93,7 @@ def load(path: str = LIB_PATH):
     L.dq_set_taylor_krylov.argtypes = [vp, C.c_int, C.c_int, ip, ip, dp]
     L.dq_set_ipr.argtypes = [vp, C.c_int]
     L.dq_set_trajectory_offset.argtypes = [vp, C.c_int]
+    L.dq_set_correlation_bra.argtypes = [vp, dp]
     L.dq_get_observable_sums.argtypes = [vp, dp, dp, dp]
     L.dq_set_observable_sums.argtypes = [vp, dp, dp, dp, C.c_int]
     L.dq_get_ipr.argtypes = [vp, dp, C.POINTER(C.c_int)]
@@ -130,6 +131,7 @@ def load(path: str = LIB_PATH):
     L.dq_write_populations.argtypes = [vp, C.c_char_p, C.c_int, C.c_int]
     L.dq_write_states.argtypes = [vp, C.c_char_p]
     L.dq_write_spectrum.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_double]
+    L.dq_write_spectrum_mean.argtypes = [C.POINTER(vp), C.c_int, dp, C.c_char_p, C.c_char_p]
     for name in EXPORTS:
         if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done",
                         "dq_group_destroy", "dq_group_last_error"):

@@ -633,6 +633,7 @@ dq_status dq_adjoint_setup(dq_ctx* c, int n_steps, int fft_len, double scale, co
     if (c->cfg.reorth) return fail(c, DQ_ERR_ARG, "adjoint: not with reorthogonalisation (the recurrence is used)");
     if (c->cfg.m_min > 0) return fail(c, DQ_ERR_ARG, "adjoint: needs a fixed Krylov dimension (m_min = 0)");
     if (c->tk_p > 0) return fail(c, DQ_ERR_ARG, "adjoint: Lanczos mode only (not Taylor-Krylov)");
+    if (c->d_bra) return fail(c, DQ_ERR_ARG, "adjoint: the loss uses the correlation with psi0 (no separate bra)");
     if (c->cfg.m > kAdjMaxM) return fail(c, DQ_ERR_ARG, "adjoint: m must be <= 24");
     if (n_steps < 1 || n_steps > c->cfg.max_steps) return fail(c, DQ_ERR_ARG, "adjoint: n_steps out of range");
     if (fft_len < n_steps + 1 || (fft_len & (fft_len - 1))) {

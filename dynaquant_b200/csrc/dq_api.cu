@@ -131,7 +131,7 @@ void dq_destroy(dq_ctx* c) {
     plain_free(c);
     cudaFree(c->d_rowptr); cudaFree(c->d_col); cudaFree(c->d_val); cudaFree(c->d_valf); cudaFree(c->d_h0);
     cudaFree(c->d_static); cudaFree(c->d_sigma); cudaFree(c->d_invtau); cudaFree(c->d_coeff);
-    cudaFree(c->d_psi0); cudaFree(c->d_pops); cudaFree(c->d_corr); cudaFree(c->d_erracc);
+    cudaFree(c->d_psi0); cudaFree(c->d_bra); cudaFree(c->d_pops); cudaFree(c->d_corr); cudaFree(c->d_erracc);
     cudaFree(c->d_zz_omega); cudaFree(c->d_zz_coeff); cudaFree(c->d_zz_u);
     tk_free(c);
     cudaFree(c->d_ipr); cudaFree(c->d_ipr_partial); cudaFree(c->d_ipr_ticket);
@@ -331,6 +331,23 @@ dq_status dq_get_ipr(dq_ctx* c, double* out, int* n_values) {
     DQ_CU(cudaMemcpy(out, c->d_ipr, sizeof(double) * nv, cudaMemcpyDeviceToHost));
     const double inv = 1.0 / observed_trajectories(c);
     for (int k = 0; k < nv; ++k) out[k] *= inv;
+    return DQ_OK;
+}
+
+dq_status dq_set_correlation_bra(dq_ctx* c, const dq_cdouble* bra) {
+    if (!c) return DQ_ERR_ARG;
+    if (!bra) {
+        cudaFree(c->d_bra);
+        c->d_bra = nullptr;
+    } else {
+        for (int i = 0; i < c->n; ++i)
+            if (!std::isfinite(bra[i].re) || !std::isfinite(bra[i].im))
+                return fail(c, DQ_ERR_ARG, "correlation_bra: non-finite value");
+        if (!c->d_bra) DQ_CU(cudaMalloc(&c->d_bra, sizeof(cd) * c->n));
+        DQ_CU(cudaMemcpyAsync(c->d_bra, bra, sizeof(cd) * c->n, cudaMemcpyHostToDevice, c->stream));
+        DQ_CU(cudaStreamSynchronize(c->stream));
+    }
+    c->ready = false;
     return DQ_OK;
 }
 

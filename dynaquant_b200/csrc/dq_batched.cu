@@ -1897,9 +1897,10 @@ __global__ void k_ipr_init_b(int n, int B, const cd* __restrict__ psi0, double* 
     if (threadIdx.x == 0) ipr[0] += (double)B / s;
 }
 
-// initial record: pops[0] += B |psi0|^2, corr[0] = B <psi0|psi0>
+// initial record: pops[0] += B |psi0|^2, corr[0] = B <psi0|psi0> (B with a
+// separate correlation bra: the reference stores M(0) = 1, spectraClass.cu:296)
 __global__ void k_init_obs_b(int n, int B, const cd* __restrict__ psi0, double* pops, BatchedScalars S,
-                             int chunks) {
+                             int chunks, int unit0) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         pops[i] += (double)B * cabs2(psi0[i]);
     if (blockIdx.x == 0) {
@@ -1909,7 +1910,7 @@ __global__ void k_init_obs_b(int n, int B, const cd* __restrict__ psi0, double* 
         s = block_sum(s, scratch);
         if (threadIdx.x == 0) {
             for (int ch = 0; ch < chunks; ++ch) {
-                S.corr[2 * ch] = (ch == 0) ? (double)B * s : 0.0;
+                S.corr[2 * ch] = (ch == 0) ? (double)B * (unit0 ? 1.0 : s) : 0.0;
                 S.corr[2 * ch + 1] = 0.0;
             }
         }
@@ -2589,7 +2590,8 @@ dq_status batched_reset(dq_ctx* c) {
     DQ_CU(cudaMemsetAsync(bs->s.tickets, 0, sizeof(unsigned int) * ((size_t)8 * B + 8), c->stream));
     k_set_norms_b<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, bs->s);
     k_init_obs_b<<<std::max(1, std::min(bs->sms, (n + 255) / 256)), 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops,
-                                                                                        bs->s, bs->chunks);
+                                                                                        bs->s, bs->chunks,
+                                                                                        c->d_bra != nullptr);
     if (c->ipr_on) k_ipr_init_b<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_ipr);
     DQ_CU(cudaGetLastError());
     return DQ_OK;
@@ -2880,7 +2882,7 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
     mark(DQ_KIND_PADE);
     k_pade_b<<<B, 128, pade_smem_bytes(m + 2), st>>>(m, B, c->tau_im, c->cfg.norm_mode, bs->s, c->d_erracc);
     mark(DQ_KIND_COMBINE);
-    k_combine_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, m, slabs, se, c->d_psi0, bs->s);
+    k_combine_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, m, slabs, se, corr_bra(c), bs->s);
     const int pblocks = std::max(1, std::min(bs->sms * 4, (n + 7) / 8));
     mark(DQ_KIND_POP);
     if (c->ipr_on && !skip_pop)

@@ -71,6 +71,7 @@ struct dq_ctx {
     double* d_invtau = nullptr;
     double* d_coeff = nullptr;
     dq::cd* d_psi0 = nullptr;
+    dq::cd* d_bra = nullptr;               // correlation bra (null: psi0)
     int nnz_off = 0;
     // ZZ real noise: oscillators (angular frequency rad/fs, amplitude) and
     // the ensemble's phase fractions (the plain path draws them per step)
@@ -126,6 +127,9 @@ struct dq_ctx {
 };
 
 namespace dq {
+// The bra of the correlation M(t) = <bra|psi(t)>: psi0 unless one was set.
+inline const cd* corr_bra(const dq_ctx* c) { return c->d_bra ? c->d_bra : c->d_psi0; }
+
 // Trajectories the observable sums stand for (their divisor for means).
 inline int observed_trajectories(const dq_ctx* c) {
     if (c->obs_traj > 0) return c->obs_traj;

@@ -189,20 +189,21 @@ dq_status dq_write_ipr(dq_ctx* c, const char* path) {
     return DQ_OK;
 }
 
-dq_status dq_write_spectrum(dq_ctx* c, const char* corr_path, const char* spec_path, double scaling) {
-    if (!c || !corr_path || !spec_path) return DQ_ERR_ARG;
+// The ensemble-mean correlation and its inverse DFT of length steps + 1
+// (spectraClass.cu:108, :621-626), scaled as spectraClass.cu:640-687 does
+// before printing: M(t) by the scaling constant (held in a float), the
+// transform by that constant over the step count.
+static dq_status scaled_spectrum(dq_ctx* c, double scaling, std::vector<cd>& corr, std::vector<cd>& spec) {
     if (c->last_path == 1 && c->bat) {
         dq_status st = batched_collect_corr(c);
         if (st) return st;
     }
     const int T = c->steps_done, len = T + 1;
-    const double dt = c->cfg.dt;
-    // ensemble-mean correlation and its inverse DFT of length steps + 1
-    // (spectraClass.cu:108, :621-626)
     cd* d = nullptr;
     dq_status st = check_cuda(c, cudaMalloc(&d, sizeof(cd) * 2 * (size_t)len), "spectrum alloc");
     if (st) return st;
-    std::vector<cd> corr(len), spec(len);
+    corr.assign(len, cd{0.0, 0.0});
+    spec.assign(len, cd{0.0, 0.0});
     st = check_cuda(c, cudaMemcpyAsync(d, c->d_corr, sizeof(cd) * len, cudaMemcpyDeviceToDevice, c->stream), "copy");
     if (!st) {
         const int blocks = std::max(1, std::min(148 * 4, (len + 127) / 128));
@@ -219,11 +220,22 @@ dq_status dq_write_spectrum(dq_ctx* c, const char* corr_path, const char* spec_p
     // the reference keeps the scaling constant in a float (spectraClass.cu:643-651)
     const float sc = (float)scaling;
     const double inv_traj = 1.0 / observed_trajectories(c);
+    for (int i = 0; i < len; ++i) {
+        corr[i].x = corr[i].x * inv_traj * sc;
+        corr[i].y = corr[i].y * inv_traj * sc;
+        spec[i].x = spec[i].x * (sc / T);
+        spec[i].y = spec[i].y * (sc / T);
+    }
+    return DQ_OK;
+}
+
+static dq_status write_spectrum_files(dq_ctx* c, int T, double dt, const std::vector<cd>& corr,
+                                      const std::vector<cd>& spec, const char* corr_path, const char* spec_path) {
+    const int len = T + 1;
     FILE* f = fopen(corr_path, "w");
     if (!f) return ofail(c, DQ_ERR_ARG, std::string("write_spectrum: cannot create ") + corr_path);
     bool ok = fprintf(f, "{timestep #} {timestamp fs} {M(t) real imag}: \n") > 0;
-    for (int i = 0; i < len && ok; ++i)
-        ok = fprintf(f, "%6d%14g%14g%14g\n", i, i * dt, corr[i].x * inv_traj * sc, corr[i].y * inv_traj * sc) > 0;
+    for (int i = 0; i < len && ok; ++i) ok = fprintf(f, "%6d%14g%14g%14g\n", i, i * dt, corr[i].x, corr[i].y) > 0;
     ok = (fclose(f) == 0) && ok;
     if (!ok) return ofail(c, DQ_ERR_ARG, "write_spectrum: correlation write failed");
     // 1 / (c[m/s] 100 [cm/m] 1e-15 [s/fs]) with c = 299792458 (spectraClass.cu:151-154)
@@ -233,11 +245,54 @@ dq_status dq_write_spectrum(dq_ctx* c, const char* corr_path, const char* spec_p
     ok = fprintf(f, "{k #} {freq rev/fs} {freq cm^-1} {Transform real imag}: \n") > 0;
     for (int id = 0; id < len && ok; ++id) {
         const int k = id > T / 2 ? -T + id : id;
-        ok = fprintf(f, "%6d%14g%14g%14g%14g\n", k, (double)k / (T * dt), inv_fs_to_inv_cm * k / (dt * T),
-                     spec[id].x * (sc / T), spec[id].y * (sc / T)) > 0;
+        ok = fprintf(f, "%6d%14g%14g%14g%14g\n", k, (double)k / (T * dt), inv_fs_to_inv_cm * k / (dt * T), spec[id].x,
+                     spec[id].y) > 0;
     }
     ok = (fclose(f) == 0) && ok;
     return ok ? DQ_OK : ofail(c, DQ_ERR_ARG, "write_spectrum: spectrum write failed");
+}
+
+dq_status dq_write_spectrum(dq_ctx* c, const char* corr_path, const char* spec_path, double scaling) {
+    if (!c || !corr_path || !spec_path) return DQ_ERR_ARG;
+    std::vector<cd> corr, spec;
+    dq_status st = scaled_spectrum(c, scaling, corr, spec);
+    if (st) return st;
+    return write_spectrum_files(c, c->steps_done, c->cfg.dt, corr, spec, corr_path, spec_path);
+}
+
+// The overall spectrum files over the polarisation directions (spectraClass.cu:
+// 697-744): the mean of the directions' scaled correlations and transforms.
+dq_status dq_write_spectrum_mean(dq_ctx* const* ctxs, int n_ctx, const double* scalings, const char* corr_path,
+                                 const char* spec_path) {
+    if (!ctxs || n_ctx < 1 || !scalings || !corr_path || !spec_path) return DQ_ERR_ARG;
+    dq_ctx* c0 = ctxs[0];
+    if (!c0) return DQ_ERR_ARG;
+    const int T = c0->steps_done;
+    std::vector<cd> corr(T + 1, cd{0.0, 0.0}), spec(T + 1, cd{0.0, 0.0}), ci, si;
+    for (int k = 0; k < n_ctx; ++k) {
+        dq_ctx* c = ctxs[k];
+        if (!c) return DQ_ERR_ARG;
+        if (c->steps_done != T || c->cfg.dt != c0->cfg.dt)
+            return ofail(c0, DQ_ERR_ARG, "write_spectrum_mean: the contexts differ in steps done or dt");
+        dq_status st = scaled_spectrum(c, scalings[k], ci, si);
+        if (st) {
+            if (c != c0) c0->err = c->err;
+            return st;
+        }
+        for (int i = 0; i <= T; ++i) {
+            corr[i].x += ci[i].x;
+            corr[i].y += ci[i].y;
+            spec[i].x += si[i].x;
+            spec[i].y += si[i].y;
+        }
+    }
+    for (int i = 0; i <= T; ++i) {
+        corr[i].x /= n_ctx;
+        corr[i].y /= n_ctx;
+        spec[i].x /= n_ctx;
+        spec[i].y /= n_ctx;
+    }
+    return write_spectrum_files(c0, T, c0->cfg.dt, corr, spec, corr_path, spec_path);
 }
 
 }  // extern "C"

@@ -281,8 +281,10 @@ __global__ void __launch_bounds__(kPlainThreads) k_renorm(int n, cd* out, const 
     }
 }
 
+// pops_row += |psi0|^2; corr_pt += <psi0|psi0>, or += 1 with a separate bra
+// (the reference stores M(0) = 1, spectraClass.cu:296)
 __global__ void k_observe_initial(int n, const cd* __restrict__ psi0, double* pops_row, cd* corr_pt,
-                                  double* partial, PlainScalars* ps) {
+                                  double* partial, PlainScalars* ps, int unit0) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double cr = 0.0, ci = 0.0;
     if (i < n) {
@@ -294,8 +296,8 @@ __global__ void k_observe_initial(int n, const cd* __restrict__ psi0, double* po
     }
     __shared__ double out2[2];
     if (reduce2_last(cr, ci, partial, &ps->ticket[3], out2) && threadIdx.x == 0) {
-        corr_pt->x += out2[0];
-        corr_pt->y += out2[1];
+        corr_pt->x += unit0 ? 1.0 : out2[0];
+        corr_pt->y += unit0 ? 0.0 : out2[1];
     }
 }
 
@@ -521,7 +523,7 @@ static dq_status plain_tk_tail(dq_ctx* c, int traj, int step, const cd* psi_in, 
     if (observe) k_tk_erracc<<<1, 32, 0, st>>>(c->d_ps, c->d_erracc, traj);
     double* prow = (observe && rec >= 0) ? c->d_pops + (size_t)rec * n : nullptr;
     cd* cpt = observe ? c->d_corr + (step + 1) : nullptr;
-    k_renorm<<<G, T, 0, st>>>(n, psi_out, c->d_psi0, prow, cpt, c->d_partial, c->d_ps);
+    k_renorm<<<G, T, 0, st>>>(n, psi_out, corr_bra(c), prow, cpt, c->d_partial, c->d_ps);
     if (observe && c->ipr_on) k_ipr_plain<<<G, T, 0, st>>>(n, psi_out, c->d_ipr + step + 1, c->d_partial, c->d_ps);
     DQ_CU(cudaGetLastError());
     return DQ_OK;
@@ -557,7 +559,7 @@ dq_status plain_step(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_ou
     k_combine<<<G, T, 0, st>>>(n, m, psi_in, c->d_Q, psi_out, c->d_partial, c->d_ps);
     double* prow = (observe && rec >= 0) ? c->d_pops + (size_t)rec * n : nullptr;
     cd* cpt = observe ? c->d_corr + (step + 1) : nullptr;
-    k_renorm<<<G, T, 0, st>>>(n, psi_out, c->d_psi0, prow, cpt, c->d_partial, c->d_ps);
+    k_renorm<<<G, T, 0, st>>>(n, psi_out, corr_bra(c), prow, cpt, c->d_partial, c->d_ps);
     if (observe && c->ipr_on) k_ipr_plain<<<G, T, 0, st>>>(n, psi_out, c->d_ipr + step + 1, c->d_partial, c->d_ps);
     DQ_CU(cudaGetLastError());
     return DQ_OK;
@@ -566,7 +568,8 @@ dq_status plain_step(dq_ctx* c, int traj, int step, const cd* psi_in, cd* psi_ou
 dq_status plain_observe_initial(dq_ctx* c) {
     const int n = c->n;
     const int G = (n + kPlainThreads - 1) / kPlainThreads;
-    k_observe_initial<<<G, kPlainThreads, 0, c->stream>>>(n, c->d_psi0, c->d_pops, c->d_corr, c->d_partial, c->d_ps);
+    k_observe_initial<<<G, kPlainThreads, 0, c->stream>>>(n, c->d_psi0, c->d_pops, c->d_corr, c->d_partial, c->d_ps,
+                                                          c->d_bra != nullptr);
     if (c->ipr_on) k_ipr_plain<<<G, kPlainThreads, 0, c->stream>>>(n, c->d_psi0, c->d_ipr, c->d_partial, c->d_ps);
     DQ_CU(cudaGetLastError());
     return DQ_OK;

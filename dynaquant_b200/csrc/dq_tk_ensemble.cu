@@ -341,8 +341,10 @@ __global__ void k_tke_set_psi0(int n, int B, const cd* __restrict__ psi0, cd* __
         psi[x] = psi0[x / B];
 }
 
-// initial records: pops[0] += B |psi0|^2, corr[0] += B <psi0|psi0>, ipr[0] += B / sum |psi0|^4
-__global__ void k_tke_init_obs(int n, int B, const cd* __restrict__ psi0, double* pops, cd* corr, double* ipr) {
+// initial records: pops[0] += B |psi0|^2, corr[0] += B <psi0|psi0> (B with a
+// separate bra), ipr[0] += B / sum |psi0|^4
+__global__ void k_tke_init_obs(int n, int B, const cd* __restrict__ psi0, double* pops, cd* corr, double* ipr,
+                               int unit0) {
     __shared__ double scratch[32];
     double s2 = 0.0, s4 = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -354,7 +356,7 @@ __global__ void k_tke_init_obs(int n, int B, const cd* __restrict__ psi0, double
     s2 = block_sum(s2, scratch);
     s4 = block_sum(s4, scratch);
     if (threadIdx.x == 0) {
-        corr[0].x += (double)B * s2;
+        corr[0].x += (double)B * (unit0 ? 1.0 : s2);
         if (ipr) ipr[0] += (double)B / s4;
     }
 }
@@ -430,7 +432,8 @@ dq_status tk_ensemble_reset(dq_ctx* c) {
     if (c->cfg.noise_model == DQ_NOISE_ZZ)
         k_zz_phases_b<<<148 * 16, 256, 0, c->stream>>>(n, B, c->traj0, c->zz_n_osc, c->cfg.seed, c->d_zz_u);
     k_tke_set_psi0<<<148 * 8, 256, 0, c->stream>>>(n, B, c->d_psi0, t->psi);
-    k_tke_init_obs<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops, c->d_corr, c->ipr_on ? c->d_ipr : nullptr);
+    k_tke_init_obs<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops, c->d_corr, c->ipr_on ? c->d_ipr : nullptr,
+                                             c->d_bra != nullptr);
     DQ_CU(cudaMemsetAsync(t->s.status, 0, sizeof(int), c->stream));
     DQ_CU(cudaGetLastError());
     return DQ_OK;
@@ -482,7 +485,7 @@ dq_status tk_ensemble_run(dq_ctx* c, int n_steps) {
                                                t->Q + (size_t)(mb + 1) * se, t->s);
         k_tke_pade<<<B, 256, pade_smem_bytes(mb + p), st>>>(mb, p, B, c->tau_im, c->cfg.norm_mode, t->s);
         k_tke_combine<<<grid, kTkThreads, 0, st>>>(n, B, mb, t->Q, t->acc, t->psi, c->d_erracc, t->s);
-        k_tke_observe<<<grid, kTkThreads, 0, st>>>(n, B, c->d_psi0, t->psi, c->d_corr + step + 1,
+        k_tke_observe<<<grid, kTkThreads, 0, st>>>(n, B, corr_bra(c), t->psi, c->d_corr + step + 1,
                                                    c->ipr_on ? c->d_ipr + step + 1 : nullptr, t->s);
         if ((step + 1) % pe == 0)
             k_tke_pops<<<std::max(1, std::min(148 * 4, (n + 7) / 8)), 256, 0, st>>>(

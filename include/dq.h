@@ -143,6 +143,13 @@ DQ_API dq_status dq_set_taylor_krylov(dq_ctx *ctx, int p, int m_b, const int *ro
 DQ_API dq_status dq_set_ipr(dq_ctx *ctx, int enable);
 /* steps done + 1 values: the ensemble mean of 1 / sum |psi(k)|^4, k = 0.. */
 DQ_API dq_status dq_get_ipr(dq_ctx *ctx, double *out, int *n_values);
+/* The bra of the correlation M(t) = sum_i conj(bra_i) psi_i(t) (N complex,
+ * host), replacing psi0: the CD spectrum's transition-dipole bra with the
+ * R x mu initial state (spectraClass.cu:464-496, calcCorrFunc :505-571).  As
+ * in the reference, M(0) is then recorded as 1 for every trajectory
+ * (spectraClass.cu:296).  NULL returns to <psi0|psi(t)>.  The adjoint refuses
+ * a separate bra.  Takes effect at the next reset. */
+DQ_API dq_status dq_set_correlation_bra(dq_ctx *ctx, const dq_cdouble *bra);
 /* ---- ensembles sharded over processes / GPUs (no reference counterpart;
  * the reference runs numEnsembleRuns one after another, propagate.cu:167-298) ----
  * Index of this context's trajectory 0 in the whole ensemble (even, >= 0):
@@ -305,6 +312,12 @@ DQ_API dq_status dq_write_states(dq_ctx *ctx, const char *folder);
  * caller passes mu_tot^2 for absorption or (pi/2) 1e-7 mu_tot RD_tot for CD),
  * the transform also divided by the step count. */
 DQ_API dq_status dq_write_spectrum(dq_ctx *ctx, const char *corr_path, const char *spec_path, double scaling);
+/* The overall files over polarisation directions (spectraClass.cu:697-744):
+ * the mean of n_ctx contexts' scaled correlations and transforms (one
+ * context per direction, scalings[k] as for dq_write_spectrum); the contexts
+ * must have the same steps done and dt. */
+DQ_API dq_status dq_write_spectrum_mean(dq_ctx *const *ctxs, int n_ctx, const double *scalings, const char *corr_path,
+                                        const char *spec_path);
 /* invParticRat.dat (systemClass.cu:1735-1750): "# Inverse Particle Ratios",
  * "# {timestep} {IPR}}", then "k  IPR_k" (%g) for k = 0..steps-1, IPR_k the
  * ensemble mean from dq_get_ipr.  Needs dq_set_ipr(ctx, 1) before the run. */

@@ -708,8 +708,10 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
                         zzu[(size_t)o * n + i] = dqo_zz_phase(sys->seed, (uint32_t)traj, (uint32_t)i, (uint32_t)o);
             memcpy(psi, psi0, sizeof(cx) * n);
             double errsum = 0.0;
+            const cx *bra = sys->corr_bra ? (const cx *)sys->corr_bra : psi0;
             cx c = {0, 0};
-            for (int i = 0; i < n; ++i) c = cadd(c, cmul(cconj(psi0[i]), psi[i]));
+            if (sys->corr_bra) c.re = 1.0;
+            else for (int i = 0; i < n; ++i) c = cadd(c, cmul(cconj(psi0[i]), psi[i]));
             myc[0] += c.re; myc[1] += c.im;
             for (int i = 0; i < n; ++i) myp[i] += cabs2(psi[i]);
             myi[0] += ipr_of(n, psi);
@@ -723,7 +725,7 @@ int dqo_run(const dqo_system *sys, int traj0, int n_traj, int n_steps, const dou
                 errsum += est;
                 memcpy(psi, tmp, sizeof(cx) * n);
                 c.re = 0; c.im = 0;
-                for (int i = 0; i < n; ++i) c = cadd(c, cmul(cconj(psi0[i]), psi[i]));
+                for (int i = 0; i < n; ++i) c = cadd(c, cmul(cconj(bra[i]), psi[i]));
                 myc[2 * (k + 1)] += c.re; myc[2 * (k + 1) + 1] += c.im;
                 myi[k + 1] += ipr_of(n, psi);
                 if ((k + 1) % pop_every == 0) {

@@ -61,6 +61,7 @@ typedef struct {
     const int *tk_col;
     const double *tk_val;
     const double *tk_diag; /* B: diagonal, n */
+    const double *corr_bra; /* optional correlation bra (n complex); M(0) is then 1 (spectraClass.cu:296) */
 } dqo_system;
 
 /* Checks of the adaptive Krylov dimension happen at j = m_min, m_min + 4,

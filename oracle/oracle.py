@@ -58,6 +58,7 @@ class _System(C.Structure):
         ("tk_col", C.POINTER(C.c_int)),
         ("tk_val", C.POINTER(C.c_double)),
         ("tk_diag", C.POINTER(C.c_double)),
+        ("corr_bra", C.POINTER(C.c_double)),
     ]
 
 
@@ -166,7 +167,7 @@ class System:
     def __init__(self, rowptr, col, val, h0diag, m, dt, hbar=None, dot_mode=DOT_BILINEAR,
                  norm_mode=NORM_COMPLEX, noise=NOISE_NONE, ka_substeps=1, sigma=None, tau=None,
                  sigma_static=0.0, static_eps=None, seed=0, reorth=0, m_min=0, m_tol=1e-7, zz_omega=None,
-                 zz_coeff=None, tk=None):
+                 zz_coeff=None, tk=None, corr_bra=None):
         """tk: optional Taylor-Krylov mode (p, m_B, rowptr_B, col_B, val_B, diag_B), B's off-diagonal CSR
         and diagonal."""
         self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
@@ -190,6 +191,7 @@ class System:
                        np.ascontiguousarray(tdiag, dtype=np.float64))
         else:
             self.tk = (0, 0, None, None, None, None)
+        self.corr_bra = None if corr_bra is None else np.ascontiguousarray(corr_bra, dtype=np.complex128)
         _ip = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_int))
         self.s = _System(
             self.n,
@@ -201,6 +203,7 @@ class System:
             _dp(self.sigma), _dp(self.tau), float(sigma_static), _dp(self.static_eps), seed, int(reorth),
             int(m_min), float(m_tol), self.n_osc, _dp(self.zz_omega), _dp(self.zz_coeff),
             self.tk[0], self.tk[1], _ip(self.tk[2]), _ip(self.tk[3]), _dp(self.tk[4]), _dp(self.tk[5]),
+            None if self.corr_bra is None else _dp(self.corr_bra.view(np.float64)),
         )
 
     def dense(self, diag=None):
