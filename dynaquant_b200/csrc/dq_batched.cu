@@ -575,29 +575,35 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_warp(int n, int B, int bpc, 
     }
 }
 
-// SpMM over a TMA-fed shared-memory ring (staged = 6; complex64, packed
-// records, R <= 3, TC = 32 trajectories, 2 per lane; one 512-thread CTA per
-// SM).  The CTA owns rows [r0, r1) of one chunk.  Ring block b holds rows
+// SpMM over a TMA-fed shared-memory ring (staged = 6, LT = 2; staged = 7,
+// LT = 4; complex64, packed records, R <= 3, TC = 32 trajectories, LT per
+// lane; one 512-thread CTA per SM).  The CTA owns rows [r0, r1) of one chunk.  Ring block b holds rows
 // y0 + b SR .. (y0 = r0 - halo, SR = 16 R rows: one block of R rows per
 // warp per step); the ring has NB = 2hb + D + 1 blocks, so while step s
 // gathers from blocks s .. s + 2hb the boxes of the next D blocks are in
 // flight, and block s + NB is issued into block s's place once step s is
 // done.  Warp w owns row block (r0 + s SR)/R + w: its records arrive 32 at a
 // time (one coalesced 16-byte load per lane, the next batch in flight) into
-// a per-warp buffer; lanes 0-15 take the even records and lanes 16-31 the
-// odd ones of every batch for the same 32 trajectories, and one shuffle
-// adds the halves.  Every gather is a 16-byte shared load; no global load
-// sits on the gathers' dependency chain.  Each mbarrier wait is bounded.
+// a per-warp buffer; the warp's lanes form 32 / (32 / LT) groups of 32 / LT
+// lanes, group g takes records g, g + groups, ... of every batch for the same
+// 32 trajectories, and shuffles add the groups.  With LT = 4 each record's
+// coefficients serve twice the FMAs of LT = 2 for the same record traffic and
+// slot arithmetic.  Every gather is a 16-byte shared load (two with LT = 4);
+// no global load sits on the gathers' dependency chain.  Each mbarrier wait
+// is bounded.
 constexpr int kRingThreads = 512;
 
-template <int R, bool kBilinear, bool kWrite>
+template <int R, bool kBilinear, bool kWrite, int LT = 2>
 __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int rows_per_cta, int hb, int D, int j,
                                                               const int* __restrict__ bptr,
                                                               const float4* __restrict__ rec,
                                                               const float* __restrict__ d, float* __restrict__ w,
                                                               BatchedScalars S, int nch,
                                                               const __grid_constant__ CUtensorMap tmap) {
-    constexpr int TPT = 2, TC = 32;
+    constexpr int TPT = LT, TC = 32;
+    constexpr int GL = TC / TPT;   // lanes per record group
+    constexpr int NG = 32 / GL;    // record groups per warp
+    constexpr int QN = 8 / NG;     // records per group per pass (8 records per warp pass)
     constexpr int kWarps = kRingThreads / 32;
     constexpr int SR = kWarps * R;
     constexpr size_t row_reals = TC * 2;
@@ -605,13 +611,28 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
     __shared__ __align__(8) uint64_t bars[32];
     __shared__ float4 rbuf[kWarps][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int half = lane >> 4, hl = lane & 15;
+    const int half = lane / GL, hl = lane % GL;   // record group, lane within it
     const int NB = 2 * hb + D + 1;
     const int W = NB * SR;
     const int halo = hb * SR;
     const int chunk = blockIdx.y;
     if (chunk_converged(S, chunk)) return;
-    const int b0 = chunk * TC + hl * TPT;
+    // trajectories of this lane within the chunk: 2 hl, 2 hl + 1 (and, with
+    // LT = 4, 16 + 2 hl, 17 + 2 hl), so each group's 16-byte shared loads
+    // cover 128 contiguous bytes of a ring row (no bank conflicts)
+    auto tj = [&](int t) { return (t < 2) ? 2 * hl + t : 16 + 2 * hl + (t - 2); };
+    const int cb = chunk * TC;
+    // one lane's values from a row of 32 interleaved complex64 (shared or global)
+    auto ld_lane = [&](const float* rowp) {
+        CV<float, TPT> v;
+        const float4 a4 = *reinterpret_cast<const float4*>(rowp + 4 * hl);
+        v.v[0] = a4.x; v.v[1] = a4.y; v.v[2] = a4.z; v.v[3] = a4.w;
+        if constexpr (TPT == 4) {
+            const float4 b4 = *reinterpret_cast<const float4*>(rowp + 32 + 4 * hl);
+            v.v[4] = b4.x; v.v[5] = b4.y; v.v[6] = b4.z; v.v[7] = b4.w;
+        }
+        return v;
+    };
     const int r0 = blockIdx.x * rows_per_cta;
     const int r1 = min(n, r0 + rows_per_cta);
     const int nsteps = r1 > r0 ? (r1 - r0 + SR - 1) / SR : 0;
@@ -636,7 +657,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
     double sc[TPT], ar[TPT], ai[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) {
-        sc[t] = S.sc[(size_t)j * B + b0 + t];
+        sc[t] = S.sc[(size_t)j * B + cb + tj(t)];
         ar[t] = 0.0;
         ai[t] = 0.0;
     }
@@ -666,10 +687,10 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
         float dd[R][TPT];
 #pragma unroll
         for (int i = 0; i < R; ++i) {
-            const size_t bse = (size_t)min(row0 + i, n - 1) * B + b0;
+            const size_t bse = (size_t)min(row0 + i, n - 1) * B + cb;
 #pragma unroll
             for (int t = 0; t < TPT; ++t) {
-                dd[i][t] = (has_blk && row0 + i < r1) ? __ldg(d + bse + t) : 0.f;
+                dd[i][t] = (has_blk && row0 + i < r1) ? __ldg(d + bse + tj(t)) : 0.f;
                 acc[i].v[2 * t] = 0.f;
                 acc[i].v[2 * t + 1] = 0.f;
             }
@@ -694,7 +715,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
         auto slot = [&](int c) {
             int t = c - base + q0;
             t -= (t >= W) ? W : 0;
-            return ring + (size_t)t * row_reals + hl * TPT * 2;
+            return ring + (size_t)t * row_reals;
         };
         if (has_blk) {
             for (int e0 = pb; e0 < pe; e0 += 32) {
@@ -704,16 +725,17 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
                 if (e0 + 32 < pe) nxt = (e0 + 32 + lane < pe) ? __ldg(rec + e0 + 32 + lane) : pad(k);
                 else nxt = (has_next && lane < pen - pbn) ? __ldg(rec + pbn + lane) : pad(kn);
                 const int cnt = min(32, pe - e0);   // a multiple of 4
-                // this half's records: e = 2q + half (slots past cnt are padding)
+                // this group's records: e + NG q (slots past cnt are padding;
+                // e + NG (QN - 1) <= 31 since e <= 24 + NG - 1)
                 for (int e = half; e < cnt; e += 8) {
-                    float4 r[4];
-                    CV<float, TPT> y[4];
+                    float4 r[QN];
+                    CV<float, TPT> y[QN];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) r[q] = rbuf[warp][e + 2 * q];
+                    for (int q = 0; q < QN; ++q) r[q] = rbuf[warp][e + NG * q];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) y[q] = ldv<float, TPT, false>(slot(__float_as_int(r[q].x)), 0);
+                    for (int q = 0; q < QN; ++q) y[q] = ld_lane(slot(__float_as_int(r[q].x)));
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
+                    for (int q = 0; q < QN; ++q) {
                         cfma<float, TPT>(acc[0], r[q].y, y[q]);
                         if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], r[q].z, y[q]);
                         if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], r[q].w, y[q]);
@@ -722,11 +744,13 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
             }
         }
         if (pe <= pb) nxt = (has_next && lane < pen - pbn) ? __ldg(rec + pbn + lane) : pad(kn);
-        // halves add up; lanes 0-15 finish the block
+        // the groups add up; group 0 finishes the block
 #pragma unroll
-        for (int i = 0; i < R; ++i)
+        for (int off = GL; off < 32; off <<= 1)
 #pragma unroll
-            for (int v = 0; v < 2 * TPT; ++v) acc[i].v[v] += __shfl_xor_sync(0xffffffffu, acc[i].v[v], 16);
+            for (int i = 0; i < R; ++i)
+#pragma unroll
+                for (int v = 0; v < 2 * TPT; ++v) acc[i].v[v] += __shfl_xor_sync(0xffffffffu, acc[i].v[v], off);
         if (has_blk && half == 0) {
             float far[TPT], fai[TPT];   // this block's alpha terms, one conversion per block
 #pragma unroll
@@ -735,7 +759,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
             for (int i = 0; i < R; ++i) {
                 const int row = row0 + i;
                 if (row >= r1) break;
-                xo[i] = ldv<float, TPT, false>(slot(row), 0);
+                xo[i] = ld_lane(slot(row));
 #pragma unroll
                 for (int t = 0; t < TPT; ++t) {
                     acc[i].v[2 * t] = fmaf(dd[i][t], xo[i].v[2 * t], acc[i].v[2 * t]);
@@ -752,7 +776,10 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
                         if (kBilinear) { far[t] += xr * ur - xi * ui; fai[t] += xr * ui + xi * ur; }
                         else { far[t] += xr * ur + xi * ui; fai[t] += xr * ui - xi * ur; }
                     }
-                    stv<float, TPT>(w, (size_t)row * B + b0, o);
+                    float* wr = w + 2 * ((size_t)row * B + cb);
+                    *reinterpret_cast<float4*>(wr + 4 * hl) = make_float4(o.v[0], o.v[1], o.v[2], o.v[3]);
+                    if constexpr (TPT == 4)
+                        *reinterpret_cast<float4*>(wr + 32 + 4 * hl) = make_float4(o.v[4], o.v[5], o.v[6], o.v[7]);
                 } else {
 #pragma unroll
                     for (int t = 0; t < TPT; ++t)
@@ -778,7 +805,9 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
     double2* scratch = reinterpret_cast<double2*>(smem_raw);   // the ring is free now
     if (chunk_reduce_s<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk, scratch)) {
         if (threadIdx.x < TC) {
-            const int b = chunk * TC + threadIdx.x;
+            // red[i] belongs to trajectory tj(i % TPT) of lane i / TPT
+            const int li = threadIdx.x / TPT, ti = threadIdx.x % TPT;
+            const int b = chunk * TC + ((ti < 2) ? 2 * li + ti : 16 + 2 * li + (ti - 2));
             const double s2 = S.sc[(size_t)j * B + b];
             const double2 v = red[threadIdx.x];
             if (kWrite) {
@@ -2154,6 +2183,24 @@ static cudaError_t win_attr_r(int R, int bytes) {
 
 constexpr size_t kWinSmemMax = 200 * 1024;
 
+// dynamic shared memory limit of every ring SpMM instance for R rows per block
+template <int LT, int R>
+static cudaError_t ring_attr_r(int bytes) {
+    cudaError_t e = cudaFuncSetAttribute(k_spmm_ring<R, true, true, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spmm_ring<R, true, false, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spmm_ring<R, false, true, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_spmm_ring<R, false, false, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
+
+template <int LT>
+static cudaError_t ring_attr(int R, int bytes) {
+    return R == 1 ? ring_attr_r<LT, 1>(bytes) : R == 2 ? ring_attr_r<LT, 2>(bytes) : ring_attr_r<LT, 3>(bytes);
+}
+
 template <typename Real, int TPT, int R>
 static cudaError_t fused_attr(int bytes) {
     cudaError_t e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, false, false>,
@@ -2221,11 +2268,13 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
-    if (staged < 0 || staged > 6) return DQ_ERR_ARG;
+    if (staged < 0 || staged > 7) return DQ_ERR_ARG;
     // reorthogonalisation runs between the axpy and the next SpMM: not in the fused forms
     if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4)) return DQ_ERR_ARG;
-    // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane, one CTA per SM
-    if (staged == 6 && (!bs->mixed || R > 3 || tc != 32 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
+    // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane in the other
+    // kernels (the ring itself takes 2 per lane with staged 6, 4 with staged 7), one CTA per SM
+    const bool ring = staged == 6 || staged == 7;
+    if (ring && (!bs->mixed || R > 3 || tc != 32 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
         return DQ_ERR_ARG;
     if (staged == 5 && tc / tpt > 512) return DQ_ERR_ARG;
     // warp-per-block forms: complex64 packed records, one warp spans the chunk
@@ -2290,15 +2339,17 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         dq_status st = build_fmaps(c, tc, f_sr);
         if (st) return st;
     }
-    if (staged == 6) {
+    if (ring) {
         // ring SpMM: SR = 16 R rows per step; the deepest prefetch (D boxes)
-        // whose ring fits one CTA per SM
+        // whose ring fits one CTA per SM; the ring doubles as the reduction
+        // scratch (512 / (32 / LT) x 32 double2)
         const int SR = (kRingThreads / 32) * R;
         const int hb = (bs->bw + SR - 1) / SR;
         constexpr size_t kStatic = 11 * 1024;   // record buffers, barriers, reduction slots, reserve
+        const size_t min_sm = staged == 7 ? 32768 : 16384;
         for (int D = 4; D >= 1; --D) {
             const int NB = 2 * hb + D + 1;
-            const size_t sm = std::max<size_t>((size_t)NB * SR * 32 * 2 * sizeof(float), 16384);
+            const size_t sm = std::max<size_t>((size_t)NB * SR * 32 * 2 * sizeof(float), min_sm);
             if (NB <= 32 && sm + kStatic <= 227 * 1024) {
                 f_D = D; f_smem = sm; f_sr = SR; f_hb = hb;
                 break;
@@ -2310,23 +2361,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         f_rpc = ((f_rpc + SR - 1) / SR) * SR;
         f_gx = (n + f_rpc - 1) / f_rpc;
         if (f_gx > kMaxCtasPerChunk || (size_t)f_gx * B * 2 > bs->partial_cap) return DQ_ERR_ARG;
-        cudaError_t e = cudaSuccess;
-        for (int v = 0; v < 4 && e == cudaSuccess; ++v) {
-            const bool bil = v & 1, wr = v & 2;
-            const void* fn = nullptr;
-            switch (R) {
-                case 1: fn = bil ? (wr ? (const void*)k_spmm_ring<1, true, true> : (const void*)k_spmm_ring<1, true, false>)
-                                 : (wr ? (const void*)k_spmm_ring<1, false, true> : (const void*)k_spmm_ring<1, false, false>);
-                        break;
-                case 2: fn = bil ? (wr ? (const void*)k_spmm_ring<2, true, true> : (const void*)k_spmm_ring<2, true, false>)
-                                 : (wr ? (const void*)k_spmm_ring<2, false, true> : (const void*)k_spmm_ring<2, false, false>);
-                        break;
-                default: fn = bil ? (wr ? (const void*)k_spmm_ring<3, true, true> : (const void*)k_spmm_ring<3, true, false>)
-                                  : (wr ? (const void*)k_spmm_ring<3, false, true> : (const void*)k_spmm_ring<3, false, false>);
-                        break;
-            }
-            e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f_smem);
-        }
+        cudaError_t e = staged == 7 ? ring_attr<4>(R, (int)f_smem) : ring_attr<2>(R, (int)f_smem);
         if (e != cudaSuccess) {
             cudaGetLastError();
             return DQ_ERR_ARG;
@@ -2459,8 +2494,8 @@ dq_status batched_mirror_tiling(dq_ctx* c, BatchedState* dst) {
         c->bat = src;
         if (st) return st;
     }
-    if (src->staged == 1 || src->staged == 6) {
-        const int SR = src->staged == 6 ? src->f_sr : (kBThreads / (src->TC / src->TPT)) * src->R;
+    if (src->staged == 1 || src->staged == 6 || src->staged == 7) {
+        const int SR = src->staged >= 6 ? src->f_sr : (kBThreads / (src->TC / src->TPT)) * src->R;
         c->bat = dst;
         dq_status st = build_tmaps(c, src->TC, SR);
         c->bat = src;
@@ -2645,18 +2680,26 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w, int cy0, int 
 #undef DQ_WIN_R
         return;
     }
-    if (bs->staged == 6) {
+    if (bs->staged == 6 || bs->staged == 7) {
         if constexpr (sizeof(Real) == 4 && TPT == 2) {
             const dim3 grid(bs->f_gx, ncy);
             const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
             const CUtensorMap& tm = bs->tmaps[j];
-#define DQ_RING_R(RR)                                                                                              \
-    k_spmm_ring<RR, kBil, kWrite><<<grid, kRingThreads, bs->f_smem, c->stream>>>(n, B, bs->f_rpc, bs->f_hb, bs->f_D, j, \
-                                                                               f.bptr, rec, d, w, bs->s, bs->chunks, tm)
-            switch (bs->R) {
-                case 1: DQ_RING_R(1); break;
-                case 2: DQ_RING_R(2); break;
-                default: DQ_RING_R(3); break;
+#define DQ_RING_R(RR, LT)                                                                                          \
+    k_spmm_ring<RR, kBil, kWrite, LT><<<grid, kRingThreads, bs->f_smem, c->stream>>>(                              \
+        n, B, bs->f_rpc, bs->f_hb, bs->f_D, j, f.bptr, rec, d, w, bs->s, bs->chunks, tm)
+            if (bs->staged == 7) {
+                switch (bs->R) {
+                    case 1: DQ_RING_R(1, 4); break;
+                    case 2: DQ_RING_R(2, 4); break;
+                    default: DQ_RING_R(3, 4); break;
+                }
+            } else {
+                switch (bs->R) {
+                    case 1: DQ_RING_R(1, 2); break;
+                    case 2: DQ_RING_R(2, 2); break;
+                    default: DQ_RING_R(3, 2); break;
+                }
             }
 #undef DQ_RING_R
         }

@@ -22,6 +22,7 @@ template <typename Real, int TPT> struct VL;
 template <> struct VL<float, 1> { using T = float2; };
 template <> struct VL<float, 2> { using T = float4; };
 template <> struct VL<double, 1> { using T = double2; };
+template <> struct VL<float, 4> { using T = float4; };   // two per value
 
 template <typename Real, int TPT>
 struct CV { Real v[2 * TPT]; };   // interleaved (re, im) per trajectory
@@ -30,8 +31,16 @@ template <typename Real, int TPT, bool kLdg>
 __device__ __forceinline__ CV<Real, TPT> ldv(const Real* base, size_t idx) {
     using T = typename VL<Real, TPT>::T;
     const T* p = reinterpret_cast<const T*>(base + 2 * idx);
-    T t = kLdg ? __ldg(p) : *p;
     CV<Real, TPT> v;
+    if constexpr (TPT == 4) {
+        static_assert(sizeof(Real) == 4, "4 trajectories per lane: complex64 only");
+        const T a = kLdg ? __ldg(p) : p[0];
+        const T b = kLdg ? __ldg(p + 1) : p[1];
+        v.v[0] = a.x; v.v[1] = a.y; v.v[2] = a.z; v.v[3] = a.w;
+        v.v[4] = b.x; v.v[5] = b.y; v.v[6] = b.z; v.v[7] = b.w;
+        return v;
+    }
+    T t = kLdg ? __ldg(p) : *p;
     if constexpr (TPT == 2) {
         v.v[0] = t.x; v.v[1] = t.y; v.v[2] = t.z; v.v[3] = t.w;
     } else {
@@ -44,7 +53,12 @@ template <typename Real, int TPT>
 __device__ __forceinline__ void stv(Real* base, size_t idx, const CV<Real, TPT>& v) {
     using T = typename VL<Real, TPT>::T;
     T t;
-    if constexpr (TPT == 2) {
+    if constexpr (TPT == 4) {
+        T* q = reinterpret_cast<T*>(base + 2 * idx);
+        q[0] = make_float4(v.v[0], v.v[1], v.v[2], v.v[3]);
+        q[1] = make_float4(v.v[4], v.v[5], v.v[6], v.v[7]);
+        return;
+    } else if constexpr (TPT == 2) {
         t.x = v.v[0]; t.y = v.v[1]; t.z = v.v[2]; t.w = v.v[3];
     } else {
         t.x = v.v[0]; t.y = v.v[1];

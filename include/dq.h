@@ -233,7 +233,10 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * through L1 with one warp per row block (records fetched 32 at a time;
  * complex64, traj_chunk = 32 vec), 4 is the fused form with warp-owned row
  * blocks (complex64, traj_chunk = 32 vec, ctas_per_sm 1), 5 is the L1 form
- * in 512-thread CTAs (one sliding gather window per CTA).  groups splits the
+ * in 512-thread CTAs (one sliding gather window per CTA), 6 gathers from a
+ * TMA-fed shared-memory ring with warp-owned row blocks and 2 trajectories
+ * per lane, 7 the same ring with 4 trajectories per lane (both complex64,
+ * traj_chunk 32, vec 2, ctas_per_sm 1, rows_per_block <= 3).  groups splits the
  * trajectory chunks into groups whose m Lanczos iterations run one group
  * after another, so a group's Krylov slabs stay resident in L2 (must divide
  * n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run

@@ -221,10 +221,12 @@ def test_tube_fused_iterations_match_oracle(oracle, tiling):
 @pytest.mark.parametrize("B,tiling", [(32, (32, 1, 4, 1, 3, 1)), (32, (32, 1, 4, 2, 3, 1)), (32, (32, 1, 3, 3, 3, 1)),
                                       (64, (64, 2, 3, 3, 3, 1)), (64, (32, 1, 2, 3, 3, 2)),
                                       (32, (32, 2, 1, 1, 6, 1)), (32, (32, 2, 1, 2, 6, 1)), (32, (32, 2, 1, 3, 6, 1)),
-                                      (64, (32, 2, 1, 3, 6, 1))])
+                                      (64, (32, 2, 1, 3, 6, 1)), (32, (32, 2, 1, 1, 7, 1)), (32, (32, 2, 1, 2, 7, 1)),
+                                      (32, (32, 2, 1, 3, 7, 1)), (64, (32, 2, 1, 3, 7, 1))])
 def test_tube_warp_spmm_matches_oracle(oracle, B, tiling):
-    """Warp-per-block SpMMs: staged = 3 gathers through L1, staged = 6 from a TMA-fed shared-memory
-    ring; both read each block's packed records 32 at a time into a per-warp buffer."""
+    """Warp-per-block SpMMs: staged = 3 gathers through L1, staged = 6 and 7 from a TMA-fed
+    shared-memory ring (2 and 4 trajectories per lane); all read each block's packed records 32 at a
+    time into a per-warp buffer."""
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
     s = systems.tube(20, 40)
