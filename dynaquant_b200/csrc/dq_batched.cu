@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int traj0, 
                                                       const double* __restrict__ coeff,
                                                       const double* __restrict__ eps, double* __restrict__ deps,
                                                       Real* __restrict__ d, BatchedScalars S, ZZParams zz) {
-    const Tile<TPT> T(TC, rpc, n);
+    const Tile<TPT> T(TC, rpc, n, 0, true);
     const int step = *S.step;
     if (noise == DQ_NOISE_ZZ) {
         // sum_osc c cos(omega t + phi) + eps (gpuSysHelper.cu:134-177), frac(omega t / 2 pi) shared
@@ -1547,7 +1547,7 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
         }
     }
     __shared__ double2 red[kMaxTC];
-    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 1 * nch, red, T.chunk)) {
+    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 1 * nch, red, T.chunk, T.bx)) {
         if (threadIdx.x < TC) {
             const int b = T.chunk * TC + threadIdx.x;
             double bt = sqrt(red[threadIdx.x].x);
@@ -1747,20 +1747,21 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
                                                         Real* __restrict__ slabs, size_t slab_stride,
                                                         const cd* __restrict__ psi0, BatchedScalars S) {
     const Tile<TPT> T(TC, rpc, n);
+    const int ch = T.chunk;
     const int step = *S.step;
     __shared__ double2 yts[kMaxM * kMaxTC];
     for (int e = threadIdx.x; e < m * TC; e += blockDim.x) {
-        const int j = 1 + e / TC, b = blockIdx.y * TC + e % TC;
+        const int j = 1 + e / TC, b = ch * TC + e % TC;
         const size_t k = (size_t)j * B + b;
         yts[e] = make_double2(S.yt[2 * k], S.yt[2 * k + 1]);
     }
     __syncthreads();
-    const int tl = T.b0 - blockIdx.y * TC;   // trajectory lane within the chunk
+    const int tl = T.b0 - ch * TC;   // trajectory lane within the chunk
     double nn[TPT], cr[TPT], ci[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) { nn[t] = 0.0; cr[t] = 0.0; ci[t] = 0.0; }
     Real* r1 = slabs + 2 * slab_stride;
-    if (S.mchunk) m = S.mchunk[blockIdx.y];   // adaptive: the chunk's largest Krylov dimension
+    if (S.mchunk) m = S.mchunk[ch];   // adaptive: the chunk's largest Krylov dimension
     for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
         const size_t base = (size_t)row * B + T.b0;
         double accr[TPT], acci[TPT];
@@ -1820,9 +1821,9 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
     double zero[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) zero[t] = 0.0;
-    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 3 * gridDim.y, red, T.chunk)) {
+    if (chunk_reduce<TPT>(nn, zero, TC, S.partial, S.tickets + 3 * gridDim.y, red, T.chunk, T.bx)) {
         if (threadIdx.x < TC) {
-            const int b = blockIdx.y * TC + threadIdx.x;
+            const int b = ch * TC + threadIdx.x;
             const double n2 = red[threadIdx.x].x;
             S.norm2[b] = n2;
             S.sc[B + b] = 1.0 / sqrt(n2);   // sc[1][b]: next step's q_1 = psi / ||psi||
@@ -1834,16 +1835,16 @@ __global__ void __launch_bounds__(kBThreads) k_combine_b(int n, int B, int TC, i
     // ticket runs after every block of the chunk passed the first one, so the
     // chunk's norms are published by then
     double* part2 = S.partial + (size_t)gridDim.y * gridDim.x * TC * 2;
-    if (chunk_reduce<TPT>(cr, ci, TC, part2, S.tickets + 4 * gridDim.y, red, T.chunk)) {
+    if (chunk_reduce<TPT>(cr, ci, TC, part2, S.tickets + 4 * gridDim.y, red, T.chunk, T.bx)) {
         if (threadIdx.x == 0) {
             double sr = 0.0, si = 0.0;
             for (int t = 0; t < TC; ++t) {
-                const int b = blockIdx.y * TC + t;
+                const int b = ch * TC + t;
                 const double s1 = 1.0 / sqrt(__ldcg(&S.norm2[b]));
                 sr += red[t].x * s1;
                 si += red[t].y * s1;
             }
-            double* cp = S.corr + ((size_t)(step + 1) * gridDim.y + blockIdx.y) * 2;
+            double* cp = S.corr + ((size_t)(step + 1) * gridDim.y + ch) * 2;
             cp[0] = sr;
             cp[1] = si;
         }

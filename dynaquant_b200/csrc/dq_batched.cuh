@@ -117,15 +117,26 @@ __device__ __forceinline__ bool chunk_converged(const BatchedScalars& S, int chu
 // Thread -> (row lane, trajectory lane) map and the CTA's row range.
 template <int TPT>
 struct Tile {
-    int tr, rl, RPC, b0, r0, r1, chunk;
-    __device__ __forceinline__ Tile(int TC, int rows_per_cta, int n, int cy0 = 0) {
+    int tr, rl, RPC, b0, r0, r1, chunk, bx;
+    // chunk_fast: consecutive blocks take the chunks of one row range (the
+    // linear block id runs over chunks first), so the pieces of every site's
+    // trajectory row are read at about the same time; bx is the row-range
+    // index either way (the reduction's partial slot).
+    __device__ __forceinline__ Tile(int TC, int rows_per_cta, int n, int cy0 = 0, bool chunk_fast = false) {
         const int TPR = TC / TPT;
         tr = threadIdx.x % TPR;
         rl = threadIdx.x / TPR;
         RPC = blockDim.x / TPR;
-        chunk = blockIdx.y + cy0;
+        if (chunk_fast) {
+            const int L = blockIdx.y * gridDim.x + blockIdx.x;
+            chunk = L % gridDim.y + cy0;
+            bx = L / gridDim.y;
+        } else {
+            chunk = blockIdx.y + cy0;
+            bx = blockIdx.x;
+        }
         b0 = chunk * TC + tr * TPT;
-        r0 = blockIdx.x * rows_per_cta;
+        r0 = bx * rows_per_cta;
         r1 = min(n, r0 + rows_per_cta);
     }
 };
@@ -189,14 +200,14 @@ namespace dq {
 template <int TPT>
 __device__ __forceinline__ bool chunk_reduce_s(const double (&ar)[TPT], const double (&ai)[TPT], int TC,
                                                double* partial, unsigned int* ticket, double2* red_out, int chunk,
-                                               double2* sm) {
+                                               double2* sm, int bx = -1) {
     const int TPR = TC / TPT;
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int RPC = blockDim.x / TPR;
 #pragma unroll
     for (int t = 0; t < TPT; ++t) sm[rl * TC + tr * TPT + t] = make_double2(ar[t], ai[t]);
     __syncthreads();
-    double* mypart = partial + ((size_t)chunk * gridDim.x + blockIdx.x) * TC * 2;
+    double* mypart = partial + ((size_t)chunk * gridDim.x + (bx < 0 ? (int)blockIdx.x : bx)) * TC * 2;
     if (threadIdx.x < TC) {
         double sr = 0.0, si = 0.0;
         for (int r = 0; r < RPC; ++r) {
@@ -241,9 +252,10 @@ __device__ __forceinline__ bool chunk_reduce_s(const double (&ar)[TPT], const do
 
 template <int TPT>
 __device__ __forceinline__ bool chunk_reduce(const double (&ar)[TPT], const double (&ai)[TPT], int TC,
-                                             double* partial, unsigned int* ticket, double2* red_out, int chunk) {
+                                             double* partial, unsigned int* ticket, double2* red_out, int chunk,
+                                             int bx = -1) {
     __shared__ double2 sm[kBThreads * 2];
-    return chunk_reduce_s<TPT>(ar, ai, TC, partial, ticket, red_out, chunk, sm);
+    return chunk_reduce_s<TPT>(ar, ai, TC, partial, ticket, red_out, chunk, sm, bx);
 }
 
 }  // namespace dq
