@@ -132,7 +132,7 @@ void dq_destroy(dq_ctx* c) {
     cudaFree(c->d_rowptr); cudaFree(c->d_col); cudaFree(c->d_val); cudaFree(c->d_valf); cudaFree(c->d_h0);
     cudaFree(c->d_static); cudaFree(c->d_sigma); cudaFree(c->d_invtau); cudaFree(c->d_coeff);
     cudaFree(c->d_psi0); cudaFree(c->d_bra); cudaFree(c->d_pops); cudaFree(c->d_corr); cudaFree(c->d_erracc);
-    cudaFree(c->d_zz_omega); cudaFree(c->d_zz_coeff); cudaFree(c->d_zz_u);
+    cudaFree(c->d_zz_omega); cudaFree(c->d_zz_coeff);
     tk_free(c);
     cudaFree(c->d_ipr); cudaFree(c->d_ipr_partial); cudaFree(c->d_ipr_ticket);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -245,10 +245,7 @@ dq_status dq_set_zz_spectral_density(dq_ctx* c, int n_osc, const double* omega, 
     dq_status st;
     if ((st = upload(c, &c->d_zz_omega, c->zz_omega.data(), (size_t)n_osc))) return st;
     if ((st = upload(c, &c->d_zz_coeff, c->zz_coeff.data(), (size_t)n_osc))) return st;
-    cudaFree(c->d_zz_u);
-    c->d_zz_u = nullptr;
-    DQ_CU(cudaMalloc(&c->d_zz_u, sizeof(float) * (size_t)c->cfg.n_traj * n_osc * c->n));
-    c->ready = false;   // the ensemble's phase buffer follows at the next reset
+    c->ready = false;
     return DQ_OK;
 }
 

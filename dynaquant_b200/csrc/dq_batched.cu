@@ -60,15 +60,72 @@ __global__ void k_traj_init_b(int n, int B, int traj0, uint64_t seed, const doub
     }
 }
 
-// ZZ phase fractions of every (oscillator, site, trajectory), [osc][site][traj]
-__global__ void k_zz_phases_b(int n, int B, int traj0, int n_osc, uint64_t seed, float* __restrict__ u) {
-    const size_t total = (size_t)n * B * n_osc;
-    for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < total; x += (size_t)gridDim.x * blockDim.x) {
-        const int b = (int)(x % B);
-        const size_t r = x / B;
-        const int i = (int)(r % n), o = (int)(r / n);
-        u[x] = zz_phase(seed, (uint32_t)(traj0 + b), (uint32_t)i, (uint32_t)o);
+// ZZ noise sums of kZZBlock consecutive steps [start, start + kZZBlock) for
+// every (site, trajectory): zzD[t][site][traj] = sum_osc c cos(omega (start +
+// t) dt + phi), in oscillator order as two fused multiply-adds per term
+// (gpuSysHelper.cu:134-177 sums c cos(omega t + phi) every step).  One
+// thread per trajectory pair of a site draws both phases of an oscillator from
+// one Philox block and reuses their sin/cos for all kZZBlock steps; the
+// steps' factors (c cos(omega t), c sin(omega t)) come from a shared table
+// filled 32 oscillators at a time.  The kernel leaves at once when the step
+// about to run already lies in the stored block (start is *zz_start).
+constexpr int kZZBlock = 16;
+constexpr int kZZTile = 32;
+constexpr int kZZThreads = 128;
+
+__global__ void __launch_bounds__(kZZThreads) k_zz_block_b(int n, int B, int traj0, uint64_t seed, ZZParams zz,
+                                                          BatchedScalars S, const int* __restrict__ zz_start,
+                                                          double* __restrict__ zzD) {
+    const int step = *S.step, start = *zz_start;
+    if (step >= start && step - start < kZZBlock) return;   // uniform over the grid
+    __shared__ double fc[kZZTile][kZZBlock], fs[kZZTile][kZZBlock];
+    const int hp = (B + 1) / 2;   // trajectory pairs per site
+    const long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = x < (long long)n * hp;
+    const int site = active ? (int)(x / hp) : 0;
+    const int b = active ? 2 * (int)(x % hp) : 0;
+    const bool has1 = b + 1 < B;
+    double a0[kZZBlock], a1[kZZBlock];
+#pragma unroll
+    for (int t = 0; t < kZZBlock; ++t) { a0[t] = 0.0; a1[t] = 0.0; }
+    for (int o0 = 0; o0 < zz.n_osc; o0 += kZZTile) {
+        const int no = min(kZZTile, zz.n_osc - o0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < no * kZZBlock; e += blockDim.x) {
+            const int o = e / kZZBlock, t = e % kZZBlock;
+            zz_factors(zz.omega[o0 + o], zz.coeff[o0 + o], step + t, zz.dt, fc[o][t], fs[o][t]);
+        }
+        __syncthreads();
+        if (active) {
+            for (int o = 0; o < no; ++o) {
+                float u0, u1;
+                zz_phase_pair(seed, (uint32_t)((traj0 + b) >> 1), (uint32_t)site, (uint32_t)(o0 + o), u0, u1);
+                double s0, c0, s1, c1;
+                own_sincos_2pi((double)u0, s0, c0);
+                own_sincos_2pi((double)u1, s1, c1);
+#pragma unroll
+                for (int t = 0; t < kZZBlock; ++t) {
+                    const double cc = fc[o][t], cs = fs[o][t];
+                    a0[t] = __fma_rn(-cs, s0, __fma_rn(cc, c0, a0[t]));
+                    a1[t] = __fma_rn(-cs, s1, __fma_rn(cc, c1, a1[t]));
+                }
+            }
+        }
     }
+    if (!active) return;
+    const size_t se = (size_t)n * B, xi = (size_t)site * B + b;
+#pragma unroll
+    for (int t = 0; t < kZZBlock; ++t) {
+        zzD[t * se + xi] = a0[t];
+        if (has1) zzD[t * se + xi + 1] = a1[t];
+    }
+}
+
+// Records the block k_zz_block_b computed (run after it, so that no block of
+// that kernel reads the new start).
+__global__ void k_zz_mark(BatchedScalars S, int* zz_start) {
+    const int step = *S.step, start = *zz_start;
+    if (!(step >= start && step - start < kZZBlock)) *zz_start = step;
 }
 
 template <typename Real>
@@ -93,28 +150,17 @@ __global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int traj0, 
                                                       const double* __restrict__ invtau,
                                                       const double* __restrict__ coeff,
                                                       const double* __restrict__ eps, double* __restrict__ deps,
-                                                      Real* __restrict__ d, BatchedScalars S, ZZParams zz) {
+                                                      Real* __restrict__ d, BatchedScalars S,
+                                                      const double* __restrict__ zzD, const int* __restrict__ zz_start) {
     const Tile<TPT> T(TC, rpc, n, 0, true);
     const int step = *S.step;
     if (noise == DQ_NOISE_ZZ) {
-        // sum_osc c cos(omega t + phi) + eps (gpuSysHelper.cu:134-177), frac(omega t / 2 pi) shared
-        __shared__ double w[kMaxZZOsc];
-        for (int o = threadIdx.x; o < zz.n_osc; o += blockDim.x) w[o] = zz_wfrac(zz.omega[o], step, zz.dt);
-        __syncthreads();
-        const size_t stride = (size_t)n * B;
+        // eps + this step's row of the block of noise sums (k_zz_block_b)
+        const double* D = zzD + (size_t)(step - *zz_start) * n * B;
         for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
             const size_t x = (size_t)row * B + T.b0;
-            double acc[TPT];
 #pragma unroll
-            for (int t = 0; t < TPT; ++t) acc[t] = 0.0;
-            const float* u = zz.u + x;
-            for (int o = 0; o < zz.n_osc; ++o) {
-                const double wo = w[o], co = __ldg(zz.coeff + o);
-#pragma unroll
-                for (int t = 0; t < TPT; ++t) acc[t] = __dadd_rn(acc[t], zz_term(wo, co, __ldg(u + (size_t)o * stride + t)));
-            }
-#pragma unroll
-            for (int t = 0; t < TPT; ++t) d[x + t] = (Real)__dadd_rn(acc[t], eps[x + t]);
+            for (int t = 0; t < TPT; ++t) d[x + t] = (Real)__dadd_rn(D[x + t], eps[x + t]);
         }
         return;
     }
@@ -2524,6 +2570,11 @@ static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed) {
     DQ_CU(cudaMalloc(&bs->diag, (size_t)n * B * real_sz));
     DQ_CU(cudaMalloc(&bs->eps, sizeof(double) * (size_t)n * B));
     DQ_CU(cudaMalloc(&bs->deps, sizeof(double) * (size_t)n * B));
+    if (c->cfg.noise_model == DQ_NOISE_ZZ) {
+        DQ_CU(cudaMalloc(&bs->zzD, sizeof(double) * (size_t)kZZBlock * n * B));
+        DQ_CU(cudaMalloc(&bs->zz_start, sizeof(int)));
+        DQ_CU(cudaMemsetAsync(bs->zz_start, 0xC0, sizeof(int), c->stream));   // no block stored
+    }
     const size_t LB = (size_t)kMaxL * B;
     // partial capacity: up to 16 CTAs per SM over all chunks, 2 doubles per trajectory
     bs->partial_cap = (size_t)std::min(kMaxCtasPerChunk, bs->sms * 16) * B * 2;
@@ -2597,6 +2648,7 @@ void batched_free_ws(BatchedState* bs) {
         for (auto& f : bs->fmt) free_fmt(f);
     cudaFree(bs->wB);
     cudaFree(bs->slabs); cudaFree(bs->diag); cudaFree(bs->eps); cudaFree(bs->deps);
+    cudaFree(bs->zzD); cudaFree(bs->zz_start);
     cudaFree(bs->scal_mem); cudaFree(bs->s.tickets); cudaFree(bs->s.status); cudaFree(bs->s.mtraj);
     delete bs;
 }
@@ -2611,11 +2663,12 @@ dq_status batched_reset(dq_ctx* c) {
     k_traj_init_b<<<blocks, thr, 0, c->stream>>>(n, B, c->traj0, c->cfg.seed, c->d_h0, c->d_static, c->cfg.sigma_static,
                                                  c->d_sigma, c->cfg.noise_model, bs->eps, bs->deps);
     if (c->cfg.noise_model == DQ_NOISE_ZZ) {
-        if (B != c->cfg.n_traj) {
-            c->err = "batched: ZZ phases are laid out for n_traj trajectories";
-            return DQ_ERR_STATE;
+        if (!bs->zzD) {
+            // the density was set after this workspace was made
+            DQ_CU(cudaMalloc(&bs->zzD, sizeof(double) * (size_t)kZZBlock * n * B));
+            DQ_CU(cudaMalloc(&bs->zz_start, sizeof(int)));
         }
-        k_zz_phases_b<<<bs->sms * 16, 256, 0, c->stream>>>(n, B, c->traj0, c->zz_n_osc, c->cfg.seed, c->d_zz_u);
+        DQ_CU(cudaMemsetAsync(bs->zz_start, 0xC0, sizeof(int), c->stream));   // no block stored
     }
     const size_t real_sz = bs->mixed ? sizeof(float) : sizeof(double);
     const size_t slab = (size_t)n * B * 2 * real_sz;
@@ -2865,7 +2918,6 @@ static ZZParams zz_params(const dq_ctx* c) {
         zz.n_osc = c->zz_n_osc;
         zz.omega = c->d_zz_omega;
         zz.coeff = c->d_zz_coeff;
-        zz.u = c->d_zz_u;
         zz.dt = c->cfg.dt;
     }
     return zz;
@@ -2891,9 +2943,15 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
     const double sqrt_subdt = sqrt(subdt);
     const dim3 grid(bs->gx, bs->chunks);
     mark(DQ_KIND_NOISE);
+    if (c->cfg.noise_model == DQ_NOISE_ZZ) {
+        const long long pairs = (long long)n * ((B + 1) / 2);
+        k_zz_block_b<<<(unsigned)((pairs + kZZThreads - 1) / kZZThreads), kZZThreads, 0, st>>>(
+            n, B, c->traj0, c->cfg.seed, zz_params(c), bs->s, bs->zz_start, bs->zzD);
+        k_zz_mark<<<1, 1, 0, st>>>(bs->s, bs->zz_start);
+    }
     k_noise_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, c->traj0, TC, rpc, c->cfg.noise_model, ns, subdt, sqrt_subdt,
                                                      c->cfg.seed, c->d_sigma, c->d_invtau, c->d_coeff, bs->eps,
-                                                     bs->deps, (Real*)bs->diag, bs->s, zz_params(c));
+                                                     bs->deps, (Real*)bs->diag, bs->s, bs->zzD, bs->zz_start);
     if (after_noise) (*after_noise)();
     const bool adaptive = bs->s.mtraj != nullptr;
     if (adaptive) {

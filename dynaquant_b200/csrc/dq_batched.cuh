@@ -178,6 +178,8 @@ struct dq::BatchedState {
     void* diag = nullptr;       // Real [n][B]
     double* eps = nullptr;      // [n][B]
     double* deps = nullptr;     // [n][B]
+    double* zzD = nullptr;      // ZZ noise sums of a block of steps [kZZBlock][n][B]
+    int* zz_start = nullptr;    // first step of that block
     dq::BatchedScalars s{};
     double* scal_mem = nullptr;
     size_t partial_cap = 0;     // doubles per partial region

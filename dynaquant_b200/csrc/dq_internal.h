@@ -73,13 +73,12 @@ struct dq_ctx {
     dq::cd* d_psi0 = nullptr;
     dq::cd* d_bra = nullptr;               // correlation bra (null: psi0)
     int nnz_off = 0;
-    // ZZ real noise: oscillators (angular frequency rad/fs, amplitude) and
-    // the ensemble's phase fractions (the plain path draws them per step)
+    // ZZ real noise: oscillators (angular frequency rad/fs, amplitude); the
+    // phases are Philox draws made where they are used
     int zz_n_osc = 0;
     std::vector<double> zz_omega, zz_coeff;
     double* d_zz_omega = nullptr;
     double* d_zz_coeff = nullptr;
-    float* d_zz_u = nullptr;   // ensemble phase fractions [osc][site][traj]
 
     // plain path: per trajectory state [traj][site], work buffers
     double* d_eps_p = nullptr;
@@ -163,7 +162,6 @@ void batched_noise_arrays(dq_ctx* c, const double** eps, const double** deps);
 // kernels of dq_batched.cu also launched by the Taylor-Krylov ensemble
 __global__ void k_traj_init_b(int n, int B, int traj0, uint64_t seed, const double* h0, const double* static_eps,
                               double sigma_static, const double* sigma, int noise, double* eps, double* deps);
-__global__ void k_zz_phases_b(int n, int B, int traj0, int n_osc, uint64_t seed, float* u);
 // implemented in dq_tk_ensemble.cu
 dq_status tk_ensemble_reset(dq_ctx* c);
 dq_status tk_ensemble_run(dq_ctx* c, int n_steps);

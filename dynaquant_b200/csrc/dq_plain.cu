@@ -40,19 +40,22 @@ __global__ void k_traj_init_plain(int n, int n_traj, int traj0, uint64_t seed, c
     }
 }
 
-// ZZ diagonal of one trajectory at step: sum_osc c cos(omega t + phi) + eps
-// (gpuSysHelper.cu:134-177); the phases are drawn from Philox here, one per (site, osc)
+// ZZ diagonal of one trajectory at step: eps + sum_osc c cos(omega t + phi)
+// (gpuSysHelper.cu:134-177), summed as two fused multiply-adds per oscillator
+// with the step's factors (c cos(omega t), c sin(omega t)) shared in shared
+// memory; the phases are drawn from Philox here, one per (site, osc)
 __global__ void k_noise_zz(int n, int traj, int step, uint64_t seed, ZZParams zz, const double* __restrict__ eps,
                            double* __restrict__ diag, PlainScalars* ps) {
-    __shared__ double w[kMaxZZOsc];
+    __shared__ double ccw[kMaxZZOsc], csw[kMaxZZOsc];
     if (blockIdx.x == 0 && threadIdx.x == 0) ps->sc[1] = 1.0;   // q_1 = psi_in
-    for (int o = threadIdx.x; o < zz.n_osc; o += blockDim.x) w[o] = zz_wfrac(zz.omega[o], step, zz.dt);
+    for (int o = threadIdx.x; o < zz.n_osc; o += blockDim.x)
+        zz_factors(zz.omega[o], zz.coeff[o], step, zz.dt, ccw[o], csw[o]);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double acc = 0.0;
     for (int o = 0; o < zz.n_osc; ++o)
-        acc = __dadd_rn(acc, zz_term(w[o], zz.coeff[o], zz_phase(seed, (uint32_t)traj, (uint32_t)i, (uint32_t)o)));
+        acc = zz_acc(acc, ccw[o], csw[o], zz_phase(seed, (uint32_t)traj, (uint32_t)i, (uint32_t)o));
     diag[i] = __dadd_rn(acc, eps[i]);
 }
 

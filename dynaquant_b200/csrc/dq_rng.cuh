@@ -179,20 +179,40 @@ __device__ __forceinline__ double zz_wfrac(double omega, int step, double dt) {
     return __dsub_rn(w, floor(w));
 }
 
-// coeff cos(2 pi frac(w + u)) of one oscillator
-__device__ __forceinline__ double zz_term(double w, double coeff, float u) {
-    double x = __dadd_rn(w, (double)u);
-    if (x >= 1.0) x = __dsub_rn(x, 1.0);
-    double sn, cs;
-    own_sincos_2pi(x, sn, cs);
-    return __dmul_rn(coeff, cs);
+// (c cos(omega t), c sin(omega t)) of one oscillator at t = step dt
+__device__ __forceinline__ void zz_factors(double omega, double coeff, int step, double dt, double& ccw,
+                                           double& csw) {
+    double sw, cw;
+    own_sincos_2pi(zz_wfrac(omega, step, dt), sw, cw);
+    ccw = __dmul_rn(coeff, cw);
+    csw = __dmul_rn(coeff, sw);
+}
+
+// acc + c cos(omega t + 2 pi u) as two fused multiply-adds
+__device__ __forceinline__ double zz_acc(double acc, double ccw, double csw, float u) {
+    double su, cu;
+    own_sincos_2pi((double)u, su, cu);
+    acc = __fma_rn(ccw, cu, acc);
+    return __fma_rn(-csw, su, acc);
+}
+
+// the phases of trajectories 2 tpair and 2 tpair + 1 from one Philox block
+__device__ __forceinline__ void zz_phase_pair(uint64_t seed, uint32_t tpair, uint32_t site, uint32_t osc, float& u0,
+                                              float& u1) {
+    uint32_t c[4] = {site, osc, tpair, P_ZZPHASE << 24};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const uint64_t a = ((uint64_t)c[1] << 32) | c[0];
+    const uint64_t b = ((uint64_t)c[3] << 32) | c[2];
+    u0 = __double2float_rn(__dmul_rn((double)(a >> 11), 0x1.0p-53));
+    u1 = __double2float_rn(__dmul_rn((double)(b >> 11), 0x1.0p-53));
+    if (u0 >= 1.0f) u0 = 0.0f;
+    if (u1 >= 1.0f) u1 = 0.0f;
 }
 
 struct ZZParams {
     int n_osc = 0;
     const double* omega = nullptr;   // rad/fs
     const double* coeff = nullptr;   // cm^-1
-    const float* u = nullptr;        // phase fractions
     double dt = 0.0;
 };
 

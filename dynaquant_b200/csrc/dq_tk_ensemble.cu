@@ -72,9 +72,10 @@ __global__ void k_tke_noise(int n, int B, int traj0, int step, int noise, int ns
                             uint64_t seed, const double* __restrict__ sigma, const double* __restrict__ invtau,
                             const double* __restrict__ coeff, ZZParams zz, const double* __restrict__ eps,
                             double* __restrict__ deps, double* __restrict__ diag) {
-    __shared__ double w[kMaxZZOsc];
+    __shared__ double ccw[kMaxZZOsc], csw[kMaxZZOsc];
     if (noise == DQ_NOISE_ZZ) {
-        for (int o = threadIdx.x; o < zz.n_osc; o += blockDim.x) w[o] = zz_wfrac(zz.omega[o], step, zz.dt);
+        for (int o = threadIdx.x; o < zz.n_osc; o += blockDim.x)
+            zz_factors(zz.omega[o], zz.coeff[o], step, zz.dt, ccw[o], csw[o]);
         __syncthreads();
     }
     const int b = blockIdx.y * blockDim.x + threadIdx.x;
@@ -91,9 +92,8 @@ __global__ void k_tke_noise(int n, int B, int traj0, int step, int noise, int ns
             v = __dadd_rn(__dmul_rn(normal(seed, P_GAUSS, traj0 + b, step, row, 0), sigma[row]), eps[x]);
         } else if (noise == DQ_NOISE_ZZ) {
             double a = 0.0;
-            const float* u = zz.u + x;
-            const size_t stride = (size_t)n * B;
-            for (int o = 0; o < zz.n_osc; ++o) a = __dadd_rn(a, zz_term(w[o], zz.coeff[o], u[(size_t)o * stride]));
+            for (int o = 0; o < zz.n_osc; ++o)
+                a = zz_acc(a, ccw[o], csw[o], zz_phase(seed, (uint32_t)(traj0 + b), (uint32_t)row, (uint32_t)o));
             v = __dadd_rn(a, eps[x]);
         } else {
             v = eps[x];
@@ -429,8 +429,6 @@ dq_status tk_ensemble_reset(dq_ctx* c) {
     const int thr = std::min(256, ((B + 31) / 32) * 32);
     k_traj_init_b<<<blocks, thr, 0, c->stream>>>(n, B, c->traj0, c->cfg.seed, c->d_h0, c->d_static,
                                                  c->cfg.sigma_static, c->d_sigma, c->cfg.noise_model, t->eps, t->deps);
-    if (c->cfg.noise_model == DQ_NOISE_ZZ)
-        k_zz_phases_b<<<148 * 16, 256, 0, c->stream>>>(n, B, c->traj0, c->zz_n_osc, c->cfg.seed, c->d_zz_u);
     k_tke_set_psi0<<<148 * 8, 256, 0, c->stream>>>(n, B, c->d_psi0, t->psi);
     k_tke_init_obs<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops, c->d_corr, c->ipr_on ? c->d_ipr : nullptr,
                                              c->d_bra != nullptr);
@@ -453,7 +451,6 @@ dq_status tk_ensemble_run(dq_ctx* c, int n_steps) {
         zz.n_osc = c->zz_n_osc;
         zz.omega = c->d_zz_omega;
         zz.coeff = c->d_zz_coeff;
-        zz.u = c->d_zz_u;
         zz.dt = c->cfg.dt;
     }
     const bool bil = c->cfg.dot_mode == DQ_DOT_BILINEAR;

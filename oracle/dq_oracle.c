@@ -380,22 +380,39 @@ float dqo_zz_phase(uint64_t seed, uint32_t traj, uint32_t site, uint32_t osc) {
     return u;
 }
 
-void dqo_noise_update_zz(const dqo_system *sys, int step, const double *eps, const float *u, double *diag) {
-    const int n = sys->n;
+/* The step's oscillator factors (c cos(omega t), c sin(omega t)), t = step dt,
+ * with the angle reduced as frac(omega t / 2 pi). */
+void dqo_zz_factors(const dqo_system *sys, int step, double *ccw, double *csw) {
     const double t = (double)step * sys->dt;
+    for (int o = 0; o < sys->n_osc; ++o) {
+        double w = (sys->zz_omega[o] * t) * ZZ_INV_2PI;
+        w = w - floor(w);
+        double sw, cw;
+        dqo_sincos_2pi(w, &sw, &cw);
+        ccw[o] = sys->zz_coeff[o] * cw;
+        csw[o] = sys->zz_coeff[o] * sw;
+    }
+}
+
+/* diag_i = eps_i + sum_o c_o cos(omega_o t + 2 pi u_oi), summed as
+ * acc <- fma(c cos(omega t), cos(2 pi u), acc); acc <- fma(-c sin(omega t), sin(2 pi u), acc)
+ * in oscillator order (gpuSysHelper.cu:134-177 sums c cos(omega t + phi)). */
+void dqo_noise_update_zz(const dqo_system *sys, int step, const double *eps, const float *u, double *diag) {
+    const int n = sys->n, no = sys->n_osc;
+    double *ccw = (double *)malloc(sizeof(double) * 2 * (size_t)no);
+    double *csw = ccw + no;
+    dqo_zz_factors(sys, step, ccw, csw);
     for (int i = 0; i < n; ++i) {
         double acc = 0.0;
-        for (int o = 0; o < sys->n_osc; ++o) {
-            double w = (sys->zz_omega[o] * t) * ZZ_INV_2PI;
-            w = w - floor(w);
-            double x = w + (double)u[(size_t)o * n + i];
-            if (x >= 1.0) x = x - 1.0;
-            double sn, cs;
-            dqo_sincos_2pi(x, &sn, &cs);
-            acc = acc + sys->zz_coeff[o] * cs;
+        for (int o = 0; o < no; ++o) {
+            double su, cu;
+            dqo_sincos_2pi((double)u[(size_t)o * n + i], &su, &cu);
+            acc = fma(ccw[o], cu, acc);
+            acc = fma(-csw[o], su, acc);
         }
         diag[i] = acc + eps[i];
     }
+    free(ccw);
 }
 
 /* ------------------------------------------------------------------ */

@@ -120,9 +120,12 @@ void dqo_zz_coefficients(int n_osc, const double *omega_invcm, const double *J, 
 /* Phase fraction (phi / 2 pi, float) of oscillator osc at site for a
  * trajectory: Philox keyed (seed, ZZPHASE, trajectory pair, osc, site). */
 float dqo_zz_phase(uint64_t seed, uint32_t traj, uint32_t site, uint32_t osc);
-/* diag_i = sum_osc coeff cos(2 pi frac(omega t / 2 pi + u_osc,i)) + eps_i at
- * t = step dt; u is [osc][site]. */
+/* diag_i = eps_i + sum_osc coeff cos(omega t + 2 pi u_osc,i) at t = step dt,
+ * summed in oscillator order as two fused multiply-adds per oscillator with
+ * the factors of dqo_zz_factors and sin/cos(2 pi u); u is [osc][site]. */
 void dqo_noise_update_zz(const dqo_system *sys, int step, const double *eps, const float *u, double *diag);
+/* (coeff cos(omega t), coeff sin(omega t)) per oscillator, angle frac(omega t / 2 pi) */
+void dqo_zz_factors(const dqo_system *sys, int step, double *ccw, double *csw);
 
 /* ---- ensemble run ---- */
 /* Runs trajectories traj0..traj0+n_traj-1 for n_steps from psi0 (n complex).
