@@ -211,6 +211,39 @@ AGG = dict(name="tubes60xL_8aggregates_B512_adaptive_m8-32", around=60, Ls=(34, 
            B=(240, 120, 64, 32, 24, 16, 8, 8), m=32, m_min=8, m_tol=1e-7, dt=0.5, steps=2000)
 
 
+def zz_leg(s, tiling):
+    """The ZZ real-noise model (the reference's own example uses it) on the bench tube: 253 oscillators
+    of a synthetic Ohmic spectral density on the reference's frequency grid (dOmega = 8.1357 cm^-1,
+    T = 77 K) standing in for its spectral-density file; 256 trajectories, mixed precision, the bench's
+    tiling; device time of 48 graph-captured steps (three 16-step noise blocks)."""
+    import torch
+    import dynaquant_b200 as dq
+    w = WORKLOAD
+    B, K = 256, 48
+    p = dq.Propagator(s.n, m=w["m"], n_traj=B, dt=w["dt"], noise=dq.NOISE_ZZ, sigma_static=w["sigma_static"],
+                      seed=w["seed"], dot=dq.DOT_HERMITIAN, precision=dq.PREC_MIXED, pop_every=16,
+                      max_steps=K + 32)
+    p.set_system(s)
+    om = 8.1357 * np.arange(1, 254)
+    p.set_zz_spectral_density(om, 60.0 * (om / 120.0) * np.exp(-om / 120.0), 8.1357, 77.0)
+    p.set_initial_state(s.bright_state())
+    p.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
+                 tiling["staged"], tiling["groups"])
+    p.reset()
+    p.run(16)
+    st = torch.cuda.ExternalStream(p.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    p.run(K)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    p.close()
+    return {"workload": "tube60x500_B256_m20_ZZ253", "value": B / (ms / 1e3), "unit": "traj-steps/s",
+            "ms_per_step": ms, "note": "noise sums computed 16 steps at a time; synthetic Ohmic density"}
+
+
 def aggregates_leg():
     """Eight tubes 60 x L with 512 trajectories split about as 1/L (multiples of 8), adaptive Krylov
     dimension 8..32 at tolerance 1e-7, dt 0.5 fs, 2000 steps: all aggregates in one graph per step
@@ -476,6 +509,7 @@ def run_ours(args, rank, world, local_rank):
                    "note": "classical Gram-Schmidt against q_1..q_j after every iteration, FP64 sums; 8 steps"}
     adjoint = adjoint_leg()
     aggregates = aggregates_leg()
+    zz = zz_leg(s, tiling)
     traffic, traffic_src = measured_traffic(tiling["staged"])
     cpu_v, cpu_sample = cpu_baseline_sample(s, os.cpu_count() or 1)
     clocks = clk.summary()
@@ -506,6 +540,7 @@ def run_ours(args, rank, world, local_rank):
         "with_reorth": with_reorth,
         "adjoint": adjoint,
         "aggregates": aggregates,
+        "zz_noise": zz,
         "cpu_baseline": {"value": cpu_v, "unit": "traj-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
                          "sample": cpu_sample},
         "clocks": clocks,
