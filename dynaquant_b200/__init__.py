@@ -284,10 +284,25 @@ class Propagator:
             raise ValueError("target must hold fft_len values")
         self._check(self.L.dq_adjoint_setup(self.h, n_steps, fft_len, float(scale), _lib.dptr(self._target),
                                             checkpoint_every))
+        self._adj_T = int(n_steps)
 
     def forward(self) -> float:
         loss = C.c_double()
         self._check(self.L.dq_forward(self.h, C.byref(loss)))
+        return loss.value
+
+    def forward_shard(self):
+        """Forward run of this shard; returns its raw correlation sums (steps + 1) for the all-reduce."""
+        corr = np.zeros(self._adj_T + 1, dtype=np.complex128)
+        self._check(self.L.dq_forward_shard(self.h, _lib.dptr(corr.view(np.float64))))
+        return corr
+
+    def forward_reduced(self, corr_sums, n_traj_total) -> float:
+        """Loss of the whole ensemble from the correlation sums of all shards; prepares backward()."""
+        corr = np.ascontiguousarray(corr_sums, dtype=np.complex128)
+        loss = C.c_double()
+        self._check(self.L.dq_forward_reduced(self.h, _lib.dptr(corr.view(np.float64)), int(n_traj_total),
+                                              C.byref(loss)))
         return loss.value
 
     def backward(self):

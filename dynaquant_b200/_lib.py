@@ -30,7 +30,7 @@ EXPORTS = [
     "dq_set_initial_state", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
-    "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward",
+    "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward", "dq_forward_shard", "dq_forward_reduced",
     "dq_group_create", "dq_group_destroy", "dq_group_last_error", "dq_group_run",
     "dq_write_populations", "dq_write_states", "dq_write_spectrum", "dq_write_spectrum_mean",
 ]
@@ -122,6 +122,8 @@ def load(path: str = LIB_PATH):
     L.dq_adjoint_setup.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp, C.c_int]
     L.dq_forward.argtypes = [vp, dp]
     L.dq_backward.argtypes = [vp, dp, dp]
+    L.dq_forward_shard.argtypes = [vp, dp]
+    L.dq_forward_reduced.argtypes = [vp, dp, C.c_int, C.POINTER(C.c_double)]
     L.dq_group_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
     L.dq_group_destroy.argtypes = [vp]
     L.dq_group_destroy.restype = None

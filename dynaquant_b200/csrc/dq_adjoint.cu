@@ -50,6 +50,7 @@ template <> struct R2<double> { using T = double2; };
 struct AdjointState {
     int T = 0, len = 0, K = 0, n_seg = 0;
     double scale = 0.0;
+    double inv_norm = 0.0;   // 1 / trajectories of the ensemble mean (all shards)
     bool forward_done = false;
     size_t slab_bytes = 0, diag_bytes = 0;
     double* d_target = nullptr;
@@ -513,7 +514,7 @@ static void launch_grad(dq_ctx* c, AdjointState* a, int t, int slot, int write_l
     k_adj_grad<Real, MMV><<<grid, kAdjThreads, smem, c->stream>>>(                                                  \
         n, B, m, a->rows_per_cta, G, (const Real*)slot_V(a, m, slot), (Real*)a->ws2->slabs, slab_reals,          \
         (const Real*)(a->seg_diag + (size_t)slot * a->diag_bytes),                                                 \
-        c->d_psi0, a->d_G + t, 1.0 / B, write_lam, (const T2*)a->d_coef, a->d_lpart, a->d_gsite, a->d_gcpl)
+        c->d_psi0, a->d_G + t, a->inv_norm, write_lam, (const T2*)a->d_coef, a->d_lpart, a->d_gsite, a->d_gcpl)
     switch (mm_bucket(m)) {
         case 8: DQ_GRAD(8); break;
         case 16: DQ_GRAD(16); break;
@@ -720,8 +721,13 @@ dq_status dq_adjoint_setup(dq_ctx* c, int n_steps, int fft_len, double scale, co
     return DQ_OK;
 }
 
-dq_status dq_forward(dq_ctx* c, double* loss) {
-    if (!c) return DQ_ERR_ARG;
+}  // extern "C"
+
+namespace dq {
+// The forward run of the adjoint: every step of this context's trajectories
+// with checkpoints and the stored last segment; the correlation sums end in
+// c->d_corr.
+static dq_status forward_run(dq_ctx* c) {
     AdjointState* a = c->adj;
     if (!a) return fail(c, DQ_ERR_STATE, "forward: call dq_adjoint_setup first");
     if (c->scales.size() > (size_t)kAdjMaxClasses) return fail(c, DQ_ERR_ARG, "adjoint: at most 8 coupling classes");
@@ -759,13 +765,50 @@ dq_status dq_forward(dq_ctx* c, double* loss) {
     c->steps_done = a->T;
     c->last_path = 1;
     if ((st = batched_collect_corr(c))) return st;
-    if ((st = fft_inverse(c, a->len, c->d_corr, a->T + 1, 1.0 / B, a->d_spec))) return st;
+    return read_device_status(c, "forward");
+}
+
+// Loss of the ensemble-mean correlation (c->d_corr holds the sums over
+// n_total trajectories) and the adjoint source of the backward pass.
+static dq_status forward_loss(dq_ctx* c, int n_total, double* loss) {
+    AdjointState* a = c->adj;
+    dq_status st;
+    a->inv_norm = 1.0 / n_total;
+    if ((st = fft_inverse(c, a->len, c->d_corr, a->T + 1, a->inv_norm, a->d_spec))) return st;
     k_adj_loss<<<1, 1024, 0, c->stream>>>(a->len, a->scale, a->d_target, a->d_spec, a->d_g, a->d_loss);
     if ((st = fft_inverse(c, a->len, a->d_g, a->len, 1.0, a->d_G))) return st;
     if ((st = read_device_status(c, "forward"))) return st;
     if (loss) DQ_CU(cudaMemcpy(loss, a->d_loss, sizeof(double), cudaMemcpyDeviceToHost));
     a->forward_done = true;
     return DQ_OK;
+}
+}  // namespace dq
+
+extern "C" {
+
+dq_status dq_forward(dq_ctx* c, double* loss) {
+    if (!c) return DQ_ERR_ARG;
+    dq_status st;
+    if ((st = forward_run(c))) return st;
+    return forward_loss(c, c->bat->B, loss);
+}
+
+dq_status dq_forward_shard(dq_ctx* c, dq_cdouble* corr_sums) {
+    if (!c || !corr_sums) return DQ_ERR_ARG;
+    dq_status st;
+    if ((st = forward_run(c))) return st;
+    DQ_CU(cudaMemcpy(corr_sums, c->d_corr, sizeof(cd) * (size_t)(c->adj->T + 1), cudaMemcpyDeviceToHost));
+    return DQ_OK;
+}
+
+dq_status dq_forward_reduced(dq_ctx* c, const dq_cdouble* corr_sums, int n_traj_total, double* loss) {
+    if (!c || !corr_sums) return DQ_ERR_ARG;
+    AdjointState* a = c->adj;
+    if (!a || !c->bat || c->steps_done != a->T || c->last_path != 1)
+        return fail(c, DQ_ERR_STATE, "forward_reduced: run dq_forward_shard first");
+    if (n_traj_total < c->bat->B) return fail(c, DQ_ERR_ARG, "forward_reduced: fewer trajectories than this shard");
+    DQ_CU(cudaMemcpy(c->d_corr, corr_sums, sizeof(cd) * (size_t)(a->T + 1), cudaMemcpyHostToDevice));
+    return forward_loss(c, n_traj_total, loss);
 }
 
 dq_status dq_backward(dq_ctx* c, double* grad_sites, double* grad_classes) {
@@ -786,12 +829,12 @@ dq_status dq_backward(dq_ctx* c, double* grad_sites, double* grad_classes) {
     const int init_blocks = std::min(n, bs->sms * 8);
     const int thr = std::min(256, ((B + 31) / 32) * 32);
     unsigned char* w_slab1 = (unsigned char*)w2->slabs + a->slab_bytes;
-    if (bs->mixed) k_lambda_init<float><<<init_blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, a->d_G + a->T, 1.0 / B,
+    if (bs->mixed) k_lambda_init<float><<<init_blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, a->d_G + a->T, a->inv_norm,
                                                                             (float*)w_slab1);
-    else k_lambda_init<double><<<init_blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, a->d_G + a->T, 1.0 / B,
+    else k_lambda_init<double><<<init_blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, a->d_G + a->T, a->inv_norm,
                                                                    (double*)w_slab1);
-    if (bs->mixed) k_lambda_init_norm<float><<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, a->d_G + a->T, 1.0 / B, w2->s);
-    else k_lambda_init_norm<double><<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, a->d_G + a->T, 1.0 / B, w2->s);
+    if (bs->mixed) k_lambda_init_norm<float><<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, a->d_G + a->T, a->inv_norm, w2->s);
+    else k_lambda_init_norm<double><<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, a->d_G + a->T, a->inv_norm, w2->s);
     DQ_CU(cudaGetLastError());
     const size_t small_smem = pade_smem_bytes(2 * m);
     const int sc_blocks = (B + 255) / 256;

@@ -11,8 +11,14 @@ gloo on CPU) sums the observable records (populations, correlation, IPR) and
 installs them in every rank's context, whose getters and file writers then
 report the whole ensemble.
 
+The spectrum-loss gradient shards the same way (sharded_gradient): every rank
+runs its trajectories forward, one all-reduce sums the correlation, each rank
+computes the loss of the whole ensemble's mean and back-propagates through
+its own trajectories, and a second all-reduce sums the gradients.
+
 An engine is any object with set_trajectory_offset, run, observable_sums,
-set_observable_sums and ipr_enabled (Propagator has them).
+set_observable_sums and ipr_enabled (Propagator has them); sharded_gradient
+also needs forward_shard, forward_reduced and backward.
 """
 from __future__ import annotations
 
@@ -27,6 +33,28 @@ def _dist():
 def shard_range(rank: int, n_traj_per_rank: int) -> tuple[int, int]:
     """Global trajectory indices [first, last) of a rank's shard."""
     return rank * n_traj_per_rank, (rank + 1) * n_traj_per_rank
+
+
+def _allreduce(arr, group=None):
+    """Sum of a float64 numpy array over the group's ranks (NCCL on the rank's GPU, or gloo)."""
+    import torch
+    dist = _dist()
+    backend = dist.get_backend(group)
+    device = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    t = torch.from_numpy(np.ascontiguousarray(arr, dtype=np.float64)).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return t.cpu().numpy()
+
+
+def sharded_gradient(engine, n_traj_total: int, group=None):
+    """Loss of the whole ensemble and this rank's share summed into the full gradient:
+    (loss, grad_sites, grad_classes), identical on every rank."""
+    corr = engine.forward_shard()
+    corr_all = _allreduce(corr.view(np.float64), group).view(np.complex128)
+    loss = engine.forward_reduced(corr_all, n_traj_total)
+    gs, gc = engine.backward()
+    flat = _allreduce(np.concatenate([gs, gc]), group)
+    return loss, flat[:len(gs)], flat[len(gs):]
 
 
 def allreduce_observables(engine, n_traj_total: int, group=None) -> None:

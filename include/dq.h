@@ -370,6 +370,16 @@ DQ_API dq_status dq_forward(dq_ctx *ctx, double *loss);
  * be NULL).  Overwrites the
  * ensemble's current states (the next dq_run starts from dq_reset). */
 DQ_API dq_status dq_backward(dq_ctx *ctx, double *grad_sites, double *grad_classes);
+/* The same gradient for an ensemble sharded over contexts (one per rank,
+ * dq_set_trajectory_offset; no reference counterpart).  dq_forward_shard runs
+ * this context's trajectories and returns its raw correlation sums (steps + 1
+ * complex, host); after the caller sums them over all shards,
+ * dq_forward_reduced installs the sums of the whole ensemble of n_traj_total
+ * trajectories, computes the loss of its mean (*loss, may be NULL) and
+ * prepares dq_backward, whose gradients are then this shard's part: their
+ * sum over the shards is the gradient of the whole ensemble's loss. */
+DQ_API dq_status dq_forward_shard(dq_ctx *ctx, dq_cdouble *corr_sums);
+DQ_API dq_status dq_forward_reduced(dq_ctx *ctx, const dq_cdouble *corr_sums, int n_traj_total, double *loss);
 
 #ifdef __cplusplus
 }

@@ -78,3 +78,47 @@ def test_sharded_ensemble_nccl_single_rank():
         ens.engine.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-9), (1, 1e-5)])
+def test_sharded_adjoint_equals_whole_ensemble(precision, tol):
+    """Two shards of 8 trajectories (forward_shard, summed correlation, forward_reduced, summed
+    gradients) give the loss and gradient of one context of 16 trajectories."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    N, T, LEN = 48, 10, 16
+    s = systems.chain(N, -300.0)
+    rng = np.random.default_rng(2)
+    eps0 = rng.normal(0.0, 80.0, N)
+    x = np.arange(N)
+    psi0 = np.exp(-((x - N / 2) ** 2) / 30.0 + 0.4j * x)
+    psi0 /= np.linalg.norm(psi0)
+    target = rng.normal(0.0, 0.05, LEN)
+
+    def make(B, offset=None):
+        p = dq.Propagator(N, m=12, n_traj=B, dt=2.0, noise=dq.NOISE_OU, seed=23, dot=dq.DOT_HERMITIAN,
+                          precision=precision, max_steps=T)
+        p.set_system(s)
+        p.set_noise_params(np.full(N, 60.0), np.full(N, 80.0))
+        p.set_static_energies(eps0)
+        p.set_initial_state(psi0)
+        if offset is not None:
+            p.set_trajectory_offset(offset)
+        p.adjoint_setup(T, LEN, 1.0 / LEN, target, checkpoint_every=4)
+        return p
+
+    whole = make(16)
+    loss_w = whole.forward()
+    gs_w, gc_w = whole.backward()
+    shards = [make(8, 0), make(8, 8)]
+    corr = sum(p.forward_shard() for p in shards)
+    losses = [p.forward_reduced(corr, 16) for p in shards]
+    grads = [p.backward() for p in shards]
+    gs = grads[0][0] + grads[1][0]
+    gc = grads[0][1] + grads[1][1]
+    assert losses[0] == losses[1]
+    assert losses[0] == pytest.approx(loss_w, rel=tol)
+    assert np.abs(gs - gs_w).max() <= tol * np.abs(gs_w).max()
+    assert gc[0] == pytest.approx(gc_w[0], rel=tol)
+    for p in [whole] + shards:
+        p.close()

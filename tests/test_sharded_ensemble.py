@@ -97,3 +97,58 @@ def test_shard_ranges_cover_the_ensemble():
     ranges = [shard_range(r, 6) for r in range(4)]
     assert ranges[0] == (0, 6) and ranges[-1] == (18, 24)
     assert all(a[1] == b[0] for a, b in zip(ranges, ranges[1:]))
+
+
+class FakeGradEngine:
+    """forward_shard / forward_reduced / backward of a made-up loss, to check the collective steps."""
+    ipr_enabled = False
+
+    def __init__(self, rank):
+        self.rank = rank
+        self.seen = None
+
+    def set_trajectory_offset(self, t0):
+        self.t0 = t0
+
+    def forward_shard(self):
+        return np.array([1.0 + self.rank, 2.0j * (self.rank + 1)])
+
+    def forward_reduced(self, corr, n_total):
+        self.seen = (corr.copy(), n_total)
+        return float(abs(corr[0]) / n_total)
+
+    def backward(self):
+        return np.full(3, 10.0 ** self.rank), np.array([self.rank + 0.5])
+
+
+def _grad_worker(rank, world, port, out_dir):
+    import torch.distributed as dist
+
+    from dynaquant_b200.ensemble import sharded_gradient
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        e = FakeGradEngine(rank)
+        loss, gs, gc = sharded_gradient(e, 2 * world)
+        np.savez(os.path.join(out_dir, f"g{rank}.npz"), loss=loss, gs=gs, gc=gc, corr=e.seen[0], n=e.seen[1])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_gradient_collectives(tmp_path):
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_grad_worker, args=(r, world, port, str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+        if p.is_alive():
+            p.kill()
+    assert all(p.exitcode == 0 for p in procs)
+    for r in range(world):
+        g = np.load(tmp_path / f"g{r}.npz")
+        assert np.allclose(g["corr"], [3.0, 6.0j])        # summed over both ranks
+        assert int(g["n"]) == 4
+        assert float(g["loss"]) == pytest.approx(0.75)
+        assert np.allclose(g["gs"], 11.0) and np.allclose(g["gc"], [2.0])
