@@ -244,6 +244,39 @@ def zz_leg(s, tiling):
             "ms_per_step": ms, "note": "noise sums computed 16 steps at a time; synthetic Ohmic density"}
 
 
+def large_leg():
+    """The largest workload: tube 120 x 1000 = 120,000 sites, 40 A cutoff, 1024 trajectories, m = 24,
+    dt 0.5 fs, mixed precision, autotuned tiling; device time of 8 graph-captured steps after 2 warm-up
+    steps (parity with the FP64 path at this size is a GPU test)."""
+    import torch
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    w = WORKLOAD
+    s = systems.tube(120, 1000, cutoff=40.0)
+    B, K, W = 1024, 8, 2
+    p = dq.Propagator(s.n, m=24, n_traj=B, dt=w["dt"], noise=dq.NOISE_OU, sigma_static=w["sigma_static"],
+                      seed=w["seed"], dot=dq.DOT_HERMITIAN, precision=dq.PREC_MIXED, pop_every=16,
+                      max_steps=W + K + 4)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, w["sigma"]), np.full(s.n, w["tau"]))
+    p.set_initial_state(s.bright_state())
+    tiling = p.autotune()
+    p.reset()
+    p.run(W)
+    st = torch.cuda.ExternalStream(p.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    p.run(K)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    p.close()
+    return {"workload": "tube120x1000_B1024_m24", "n_sites": s.n, "nnz_per_row": (s.nnz - s.n) / s.n,
+            "value": B / (ms / 1e3), "unit": "traj-steps/s", "ms_per_step": ms,
+            "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged")}}
+
+
 def aggregates_leg():
     """Eight tubes 60 x L with 512 trajectories split about as 1/L (multiples of 8), adaptive Krylov
     dimension 8..32 at tolerance 1e-7, dt 0.5 fs, 2000 steps: all aggregates in one graph per step
@@ -510,6 +543,7 @@ def run_ours(args, rank, world, local_rank):
     adjoint = adjoint_leg()
     aggregates = aggregates_leg()
     zz = zz_leg(s, tiling)
+    large = large_leg()
     traffic, traffic_src = measured_traffic(tiling["staged"])
     cpu_v, cpu_sample = cpu_baseline_sample(s, os.cpu_count() or 1)
     clocks = clk.summary()
@@ -541,6 +575,7 @@ def run_ours(args, rank, world, local_rank):
         "adjoint": adjoint,
         "aggregates": aggregates,
         "zz_noise": zz,
+        "large_tube": large,
         "cpu_baseline": {"value": cpu_v, "unit": "traj-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
                          "sample": cpu_sample},
         "clocks": clocks,
