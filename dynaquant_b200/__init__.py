@@ -115,6 +115,11 @@ class Propagator:
         psi0 = np.ascontiguousarray(psi0, dtype=np.complex128)
         self._check(self.L.dq_set_initial_state(self.h, _lib.dptr(psi0.view(np.float64))))
 
+    def set_initial_dipole(self, mu):
+        """psi0 = mu / |mu| from one direction's transition dipoles (absorption)."""
+        mu = np.ascontiguousarray(mu, dtype=np.float64)
+        self._check(self.L.dq_set_initial_dipole(self.h, _lib.dptr(mu)))
+
     def reset(self):
         self._check(self.L.dq_reset(self.h))
 

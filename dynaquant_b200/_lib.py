@@ -27,7 +27,7 @@ EXPORTS = [
     "dq_set_hamiltonian_csr", "dq_set_coupling_classes", "dq_set_noise_params", "dq_set_static_energies",
     "dq_set_zz_spectral_density", "dq_set_taylor_krylov", "dq_set_ipr", "dq_get_ipr", "dq_write_ipr",
     "dq_set_correlation_bra", "dq_set_trajectory_offset", "dq_get_observable_sums", "dq_set_observable_sums",
-    "dq_set_initial_state", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
+    "dq_set_initial_state", "dq_set_initial_dipole", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
     "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward", "dq_forward_shard", "dq_forward_reduced",
@@ -100,6 +100,7 @@ def load(path: str = LIB_PATH):
     L.dq_write_ipr.argtypes = [vp, C.c_char_p]
     L.dq_set_static_energies.argtypes = [vp, dp]
     L.dq_set_initial_state.argtypes = [vp, dp]
+    L.dq_set_initial_dipole.argtypes = [vp, dp]
     L.dq_reset.argtypes = [vp]
     L.dq_prop_step.argtypes = [vp, C.c_int, C.c_int, vp, vp, dp]
     L.dq_run_plain.argtypes = [vp, C.c_int]

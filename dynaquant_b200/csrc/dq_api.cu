@@ -406,7 +406,24 @@ dq_status dq_set_initial_state(dq_ctx* c, const dq_cdouble* psi0) {
     DQ_CU(cudaMemcpyAsync(c->d_psi0, psi0, sizeof(cd) * c->n, cudaMemcpyHostToDevice, c->stream));
     DQ_CU(cudaStreamSynchronize(c->stream));
     c->have_psi0 = true;
+    c->ready = false;   // the next run starts every trajectory from it
     return DQ_OK;
+}
+
+// spectraClass.cu:440-458: psi0 = mu / |mu| for one polarisation direction
+dq_status dq_set_initial_dipole(dq_ctx* c, const double* mu) {
+    if (!c) return DQ_ERR_ARG;
+    if (!mu) return fail(c, DQ_ERR_ARG, "initial dipole is null");
+    double s = 0.0;
+    for (int i = 0; i < c->n; ++i) s += mu[i] * mu[i];
+    const double nrm = sqrt(s);
+    if (!(nrm > 0.0) || !std::isfinite(nrm)) return fail(c, DQ_ERR_ARG, "initial dipole: zero or non-finite norm");
+    std::vector<dq_cdouble> psi0(c->n);
+    for (int i = 0; i < c->n; ++i) {
+        psi0[i].re = mu[i] / nrm;
+        psi0[i].im = 0.0;
+    }
+    return dq_set_initial_state(c, psi0.data());
 }
 
 static dq_status check_ready(dq_ctx* c) {

@@ -173,6 +173,10 @@ DQ_API dq_status dq_set_static_energies(dq_ctx *ctx, const double *eps);
 /* Initial state (host, N complex); replaces setInitState /
  * initStateAsBasisVector / spectraClass::prepInitState. */
 DQ_API dq_status dq_set_initial_state(dq_ctx *ctx, const dq_cdouble *psi0);
+/* Initial state from one polarisation direction's transition dipoles (host,
+ * N real): psi0 = mu / |mu| (spectraClass.cu:440-458, the absorption run's
+ * state; its correlation is then <mu/|mu| | psi(t)>). */
+DQ_API dq_status dq_set_initial_dipole(dq_ctx *ctx, const double *mu);
 /* Redraws static disorder and OU offsets for every trajectory, sets every
  * trajectory to psi0 and clears the observable records (prepAnalysesForNextRun,
  * systemClass.cu:1554-1608). */

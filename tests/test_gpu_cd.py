@@ -77,3 +77,25 @@ def test_cd_spectrum_mean_file(tmp_path):
         assert float(parts[3]) == pytest.approx(spec[fid].real, rel=1e-5, abs=1e-12)
     for p in props:
         p.close()
+
+
+def test_absorption_state_from_dipoles():
+    """dq_set_initial_dipole gives psi0 = mu/|mu|: the same run as the helper's state."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(12, 8)
+    mu, _ = _geometry(s.n)
+    psi0, sc = spectra.absorption_directions(mu)[0]
+    a = _prop(s, psi0, psi0, dq.PREC_FP64)
+    a.set_correlation_bra(None)
+    a.run(T)
+    b = _prop(s, psi0, psi0, dq.PREC_FP64)
+    b.set_correlation_bra(None)
+    b.set_initial_dipole(mu[:, 0])
+    b.run(T)
+    assert np.abs(a.populations() - b.populations()).max() <= 1e-15
+    assert np.abs(a.correlation() - b.correlation()).max() <= 1e-15
+    with pytest.raises(dq.DQError):
+        b.set_initial_dipole(np.zeros(s.n))
+    a.close()
+    b.close()
