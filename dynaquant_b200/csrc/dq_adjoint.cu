@@ -400,21 +400,51 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_cls(int n, int B, int m, in
 #pragma unroll
         for (int q = 0; q < kAdjMaxClasses; ++q) acc[q] = 0.0;
         if (valid) {
-            for (int p = rowptr[row]; p < rowptr[row + 1]; ++p) {
-                if (skip0 && cls[p] == 0) continue;
-                const size_t xk = (size_t)col[p] * B + b;
-                Real rr = 0;
+            // the row's couplings (of the gathered classes) in batches of KP:
+            // for each Krylov index the batch's gathers are independent loads,
+            // so a batch keeps up to KP x m loads in flight instead of a chain
+            // per entry (KP = 8 against 4 and 2: 179 vs 203 and 204 us per
+            // launch on the 64 x 64 lattice, 232 us one entry at a time)
+            constexpr int KP = 8;
+            const int pe = rowptr[row + 1];
+            int p = rowptr[row];
+            while (p < pe) {
+                size_t xk[KP];
+                int qk[KP];
+                double vk[KP];
+#pragma unroll
+                for (int k = 0; k < KP; ++k) { xk[k] = x; qk[k] = 0; vk[k] = 0.0; }
+                int nk = 0;
+                for (; p < pe && nk < KP; ++p) {
+                    const int q = cls[p];
+                    if (skip0 && q == 0) continue;
+                    const size_t xv = (size_t)col[p] * B + b;
+                    const double vv = vbase[p];
+#pragma unroll
+                    for (int k = 0; k < KP; ++k)   // register slots, no indexed local array
+                        if (k == nk) { xk[k] = xv; qk[k] = q; vk[k] = vv; }
+                    ++nk;
+                }
+                if (nk == 0) break;   // the rest of the row is class 0
+                Real rr[KP];
+#pragma unroll
+                for (int k = 0; k < KP; ++k) rr[k] = 0;
 #pragma unroll
                 for (int c = 0; c < MM; ++c) {
                     if (c < m) {
-                        const T2 v = *reinterpret_cast<const T2*>(sV + (size_t)c * slab_reals + 2 * xk);
-                        rr = fma(tr[c], v.x, fma(-ti[c], v.y, rr));   // Re(t v)
+#pragma unroll
+                        for (int k = 0; k < KP; ++k) {   // unused slots read the own row, weight 0
+                            const T2 v = *reinterpret_cast<const T2*>(sV + (size_t)c * slab_reals + 2 * xk[k]);
+                            rr[k] = fma(tr[c], v.x, fma(-ti[c], v.y, rr[k]));   // Re(t v)
+                        }
                     }
                 }
-                const double contrib = vbase[p] * (double)rr;
-                const int q = cls[p];
 #pragma unroll
-                for (int k = 0; k < kAdjMaxClasses; ++k) acc[k] += (k == q) ? contrib : 0.0;
+                for (int k = 0; k < KP; ++k) {
+                    const double contrib = vk[k] * (double)rr[k];
+#pragma unroll
+                    for (int q = 0; q < kAdjMaxClasses; ++q) acc[q] += (q == qk[k]) ? contrib : 0.0;
+                }
             }
         }
 #pragma unroll
