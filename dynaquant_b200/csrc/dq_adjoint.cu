@@ -63,6 +63,15 @@ struct AdjointState {
     unsigned char* seg_V = nullptr;
     double* seg_sc = nullptr;            // K x kScalBlock(B)
     unsigned char* seg_diag = nullptr;   // K diagonals
+    // a second set of segment slots: while the backward sweep reads one set,
+    // the next segment is recomputed into the other on a second stream
+    // (absent when the memory is short; the sweep then waits for each recompute)
+    unsigned char* seg_V2 = nullptr;
+    double* seg_sc2 = nullptr;
+    unsigned char* seg_diag2 = nullptr;
+    cudaStream_t rstream = nullptr;
+    cudaEvent_t ev_go = nullptr, ev_rec[2] = {nullptr, nullptr}, ev_sweep[2] = {nullptr, nullptr};
+    int cur_set = 0;
     unsigned char* ck_psi = nullptr;     // states at the starts of segments 0..n_seg-2
     double* ck_n2 = nullptr;
     double* ck_deps = nullptr;           // OU offsets at those starts
@@ -503,7 +512,15 @@ __global__ void k_grad_final(int n, int G, const double* __restrict__ gsite, con
 
 static void free_adj_buffers(AdjointState* a) {
     cudaFree(a->d_target); cudaFree(a->d_spec); cudaFree(a->d_g); cudaFree(a->d_G); cudaFree(a->d_loss);
+    // the two sets swap places (use_set); both fields always hold one each
     cudaFree(a->seg_V); cudaFree(a->seg_sc); cudaFree(a->seg_diag);
+    cudaFree(a->seg_V2); cudaFree(a->seg_sc2); cudaFree(a->seg_diag2);
+    if (a->rstream) cudaStreamDestroy(a->rstream);
+    if (a->ev_go) cudaEventDestroy(a->ev_go);
+    for (int k = 0; k < 2; ++k) {
+        if (a->ev_rec[k]) cudaEventDestroy(a->ev_rec[k]);
+        if (a->ev_sweep[k]) cudaEventDestroy(a->ev_sweep[k]);
+    }
     cudaFree(a->ck_psi); cudaFree(a->ck_n2); cudaFree(a->ck_deps);
     cudaFree(a->d_coef); cudaFree(a->d_lpart); cudaFree(a->d_gsite); cudaFree(a->d_gcpl); cudaFree(a->d_gout);
     cudaFree(a->d_erracc_save);
@@ -525,6 +542,16 @@ static cudaError_t grad_attr(int bytes) {
     cudaError_t e = cudaFuncSetAttribute(k_adj_grad<Real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_adj_cls<Real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+// Makes set k (segment s uses set s % 2) the one seg_V / seg_sc / seg_diag
+// name; with a single set every segment uses it.
+static void use_set(AdjointState* a, int k) {
+    if (!a->seg_V2 || a->cur_set == k) return;
+    std::swap(a->seg_V, a->seg_V2);
+    std::swap(a->seg_sc, a->seg_sc2);
+    std::swap(a->seg_diag, a->seg_diag2);
+    a->cur_set = k;
 }
 
 static unsigned char* slot_V(AdjointState* a, int m, int slot) {
@@ -720,6 +747,23 @@ dq_status dq_adjoint_setup(dq_ctx* c, int n_steps, int fft_len, double scale, co
         if ((st = check_cuda(c, cudaMalloc(&a->seg_V, a->slab_bytes * (m + 1) * K), "adjoint Krylov bases"))) break;
         if ((st = check_cuda(c, cudaMalloc(&a->seg_sc, sizeof(double) * scal_block(B) * K), "adjoint alloc"))) break;
         if ((st = check_cuda(c, cudaMalloc(&a->seg_diag, a->diag_bytes * K), "adjoint diagonals"))) break;
+        if (n_seg > 1 && (size_t)2 * K * per_step + (size_t)(n_seg - 1) * per_ck <= avail) {
+            // second set of segment slots for the overlapped backward; without it the
+            // backward runs its recomputes and sweeps one after another
+            if (cudaMalloc(&a->seg_V2, a->slab_bytes * (m + 1) * K) != cudaSuccess ||
+                cudaMalloc(&a->seg_sc2, sizeof(double) * scal_block(B) * K) != cudaSuccess ||
+                cudaMalloc(&a->seg_diag2, a->diag_bytes * K) != cudaSuccess ||
+                cudaStreamCreateWithFlags(&a->rstream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&a->ev_go, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&a->ev_rec[0], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&a->ev_rec[1], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&a->ev_sweep[0], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&a->ev_sweep[1], cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                cudaFree(a->seg_V2); cudaFree(a->seg_sc2); cudaFree(a->seg_diag2);
+                a->seg_V2 = nullptr; a->seg_sc2 = nullptr; a->seg_diag2 = nullptr;
+            }
+        }
         if (n_seg > 1) {
             if ((st = check_cuda(c, cudaMalloc(&a->ck_psi, a->slab_bytes * (n_seg - 1)), "adjoint checkpoints"))) break;
             if ((st = check_cuda(c, cudaMalloc(&a->ck_n2, sizeof(double) * B * (n_seg - 1)), "adjoint alloc"))) break;
@@ -791,6 +835,7 @@ static dq_status forward_run(dq_ctx* c) {
         for (int k = s * a->K; k < (s + 1) * a->K; ++k)
             if ((st = batched_step_eager(c, nullptr, false))) return st;
     }
+    use_set(a, (a->n_seg - 1) % 2);
     if ((st = run_segment(c, a, last_s0, a->T, true))) return st;
     c->steps_done = a->T;
     c->last_path = 1;
@@ -868,19 +913,47 @@ dq_status dq_backward(dq_ctx* c, double* grad_sites, double* grad_classes) {
     DQ_CU(cudaGetLastError());
     const size_t small_smem = pade_smem_bytes(2 * m);
     const int sc_blocks = (B + 255) / 256;
+    // restore segment s's start and recompute its steps into set s % 2, on
+    // the stream c->stream names
+    auto recompute = [&](int s) -> dq_status {
+        const int s0 = s * a->K, s1 = std::min(a->T, s0 + a->K);
+        use_set(a, s % 2);
+        DQ_CU(cudaMemcpyAsync((unsigned char*)bs->slabs + a->slab_bytes, a->ck_psi + (size_t)s * a->slab_bytes,
+                              a->slab_bytes, cudaMemcpyDeviceToDevice, c->stream));
+        DQ_CU(cudaMemcpyAsync(bs->s.norm2, a->ck_n2 + (size_t)s * B, sizeof(double) * B, cudaMemcpyDeviceToDevice,
+                              c->stream));
+        DQ_CU(cudaMemcpyAsync(bs->deps, a->ck_deps + (size_t)s * n * B, sizeof(double) * (size_t)n * B,
+                              cudaMemcpyDeviceToDevice, c->stream));
+        k_set_sc1<<<sc_blocks, 256, 0, c->stream>>>(B, bs->s);
+        k_set_step<<<1, 32, 0, c->stream>>>(bs->s, s0);
+        return run_segment(c, a, s0, s1, false);
+    };
+    // With two slot sets the recompute of segment s - 1 runs on a second
+    // stream while the sweep of segment s runs here: the recompute touches the
+    // main workspace and set (s - 1) % 2 only, the sweep the second workspace
+    // and set s % 2; events order a set's recompute before its sweep and its
+    // previous sweep before its next recompute.
+    const bool overlap = a->seg_V2 != nullptr && a->n_seg > 1;
+    cudaStream_t main_stream = c->stream;
+    if (overlap) {
+        DQ_CU(cudaEventRecord(a->ev_go, main_stream));
+        DQ_CU(cudaStreamWaitEvent(a->rstream, a->ev_go, 0));
+    }
     for (int s = a->n_seg - 1; s >= 0; --s) {
         const int s0 = s * a->K, s1 = std::min(a->T, s0 + a->K);
-        if (s + 1 < a->n_seg) {
-            // restore the segment start and recompute its steps
-            DQ_CU(cudaMemcpyAsync((unsigned char*)bs->slabs + a->slab_bytes, a->ck_psi + (size_t)s * a->slab_bytes,
-                                  a->slab_bytes, cudaMemcpyDeviceToDevice, c->stream));
-            DQ_CU(cudaMemcpyAsync(bs->s.norm2, a->ck_n2 + (size_t)s * B, sizeof(double) * B, cudaMemcpyDeviceToDevice,
-                                  c->stream));
-            DQ_CU(cudaMemcpyAsync(bs->deps, a->ck_deps + (size_t)s * n * B, sizeof(double) * (size_t)n * B,
-                                  cudaMemcpyDeviceToDevice, c->stream));
-            k_set_sc1<<<sc_blocks, 256, 0, c->stream>>>(B, bs->s);
-            k_set_step<<<1, 32, 0, c->stream>>>(bs->s, s0);
-            if ((st = run_segment(c, a, s0, s1, false))) return st;
+        if (overlap) {
+            if (s >= 1) {
+                if (s + 1 < a->n_seg) DQ_CU(cudaStreamWaitEvent(a->rstream, a->ev_sweep[(s + 1) % 2], 0));
+                c->stream = a->rstream;
+                st = recompute(s - 1);
+                c->stream = main_stream;
+                if (st) return st;
+                DQ_CU(cudaEventRecord(a->ev_rec[(s - 1) % 2], a->rstream));
+            }
+            if (s + 1 < a->n_seg) DQ_CU(cudaStreamWaitEvent(main_stream, a->ev_rec[s % 2], 0));
+            use_set(a, s % 2);
+        } else if (s + 1 < a->n_seg) {
+            if ((st = recompute(s))) return st;
         }
         for (int t = s1 - 1; t >= s0; --t) {
             const int slot = t - s0;
@@ -906,6 +979,12 @@ dq_status dq_backward(dq_ctx* c, double* grad_sites, double* grad_classes) {
             if (t > 0) k_lam_norm<<<sc_blocks, 256, 0, c->stream>>>(B, a->row_ctas, a->d_lpart, w2->s);
             DQ_CU(cudaGetLastError());
         }
+        if (overlap) DQ_CU(cudaEventRecord(a->ev_sweep[s % 2], main_stream));
+    }
+    if (overlap) {
+        // every recompute (and its error-estimate sums) done before the restore below
+        DQ_CU(cudaEventRecord(a->ev_go, a->rstream));
+        DQ_CU(cudaStreamWaitEvent(main_stream, a->ev_go, 0));
     }
     k_grad_final<<<a->fin_blocks, 256, 0, c->stream>>>(n, G, a->d_gsite, a->d_gcpl, a->d_gout);
     if (a->n_cls) k_cls_final<<<a->fin_blocks, 256, 0, c->stream>>>(n, G, a->n_cls, a->d_gcls, a->d_gcls_out);
