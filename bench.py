@@ -130,7 +130,7 @@ SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha)", "k_spmm_blk_tube60x500.md")
               2: ("k_lanczos_fused (r_{j+1} + SpMM + alpha, beta)", None),
               3: ("k_spmm_warp (L1 gathers, warp per block + alpha)", None),
               4: ("k_lanczos_fw (fused, warp-owned blocks)", None),
-              5: ("k_spmm_blk, 512-thread CTAs (L1 gathers + alpha)", None),
+              5: ("k_spmm_blk, 512-thread CTAs (L1 gathers + alpha)", "k_spmm_blk512_tube60x500.md"),
               6: ("k_spmm_ring (TMA ring gathers + alpha)", "k_spmm_ring_tube60x500.md"),
               7: ("k_spmm_ring, 4 trajectories per lane (TMA ring gathers + alpha)", None)}
 
