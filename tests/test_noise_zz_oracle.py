@@ -76,3 +76,15 @@ def test_zz_run_conserves_norm(oracle):
     r0 = S0.run(2, 20, psi0, pop_every=5)
     assert np.abs(r["pops"] - r0["pops"]).max() > 1e-3
 
+
+
+def test_zz_coefficients_pinned_to_reference_log(oracle):
+    """The reference's example run prints oscillator 0 of its spectral density (out:63-65): J = 2.08274,
+    T = 77 K, omega = 0.00153248 rad/fs, G = 14.7683, coeff = 8.74586 (6 significant digits), with the
+    file's spacing dOmega = 8.1357 cm^-1 also its first frequency."""
+    d_omega = 8.1357
+    w, c = oracle.zz_coefficients(np.array([d_omega]), np.array([2.08274]), d_omega, 77.0)
+    assert float(f"{w[0]:.6g}") == 0.00153248
+    assert float(f"{c[0]:.6g}") == 8.74586
+    G = 2.08274 / (1.0 - np.exp(-d_omega / (KB * 77.0)))
+    assert float(f"{G:.6g}") == 14.7683
