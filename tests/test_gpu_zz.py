@@ -38,11 +38,13 @@ def _oracle_run(oracle, s, B, steps, seed=21, dt=2.0, m=12):
     return S.run(B, steps, s.bright_state(), pop_every=4, threads=8)
 
 
-def test_zz_plain_and_ensemble_fp64(oracle):
+@pytest.mark.parametrize("B", [6, 5])
+def test_zz_plain_and_ensemble_fp64(oracle, B):
+    """24 steps cross the ensemble's 16-step noise blocks; B = 5 leaves one trajectory without a pair."""
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
     s = systems.tube(12, 10)
-    B, T = 6, 24
+    T = 24
     ref = _oracle_run(oracle, s, B, T)
     p = _prop(s, B, T, dq.PREC_FP64)
     p.run_plain(T)
@@ -92,7 +94,7 @@ def test_zz_noise_changes_with_density(oracle):
 def test_zz_adjoint_matches_oracle(oracle):
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
-    N, B, T, LEN = 48, 8, 10, 16
+    N, B, T, LEN = 48, 8, 20, 32   # 20 steps, checkpoints every 8: recomputed segments start mid-block
     s = systems.chain(N, -300.0)
     rng = np.random.default_rng(3)
     eps0 = rng.normal(0.0, 80.0, N)
@@ -107,7 +109,7 @@ def test_zz_adjoint_matches_oracle(oracle):
     p.set_zz_spectral_density(omega, J, dw, TEMP)
     p.set_static_energies(eps0)
     p.set_initial_state(psi0)
-    p.adjoint_setup(T, LEN, 1.0 / LEN, target)
+    p.adjoint_setup(T, LEN, 1.0 / LEN, target, checkpoint_every=8)
     loss = p.forward()
     gs, gc = p.backward()
     rp, col, val, _ = s.off_diagonal()
