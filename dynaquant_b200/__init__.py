@@ -220,6 +220,10 @@ class Propagator:
         self._check(self.L.dq_write_spectrum(self.h, str(corr_path).encode(), str(spec_path).encode(),
                                              float(scaling)))
 
+    def set_line_dressing(self, sigma_fs):
+        """Gaussian line-shape dressing of the correlation before transforms (0 turns it off)."""
+        self._check(self.L.dq_set_line_dressing(self.h, float(sigma_fs)))
+
     def write_ipr(self, path):
         """invParticRat.dat: the ensemble-mean inverse participation ratio of steps 0..steps-1."""
         self._check(self.L.dq_write_ipr(self.h, str(path).encode()))

@@ -7,6 +7,9 @@
 // the host, spectraClass.cu:641-690).  The correlation is zero-padded to the
 // requested power-of-two length first.  Spectra are computed once per run,
 // so log2(n) small launches are ample.
+#include <algorithm>
+#include <cmath>
+
 #include "dq_internal.h"
 
 namespace dq {
@@ -41,8 +44,31 @@ dq_status fft_inverse(dq_ctx* c, int len, const cd* in, int n_in, double scale, 
     return check_cuda(c, cudaGetLastError(), "inverse DFT");
 }
 
-dq_status spectrum(dq_ctx* c, int len, cd* d_out) {
-    return fft_inverse(c, len, c->d_corr, c->steps_done + 1, 1.0 / c->cfg.n_traj, d_out);
+// gpuSpectraHelper.cu:16-42: the correlation point k is dressed with a
+// Gaussian of time dt (k + 1) (the reference's offset by one) for k < n_dress
+__global__ void k_dress(int n_dress, double sigma, double dt, cd* __restrict__ x) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_dress; k += gridDim.x * blockDim.x) {
+        const double t = dt * (k + 1);
+        const double g = exp(-0.5 * (t / sigma) * (t / sigma));
+        x[k] = cscale(x[k], g);
+    }
+}
+
+dq_status dress_correlation(dq_ctx* c, int n_dress, cd* x) {
+    if (!(c->dress_sigma > 0.0) || n_dress <= 0) return DQ_OK;
+    k_dress<<<std::max(1, std::min(148 * 4, (n_dress + 255) / 256)), 256, 0, c->stream>>>(n_dress, c->dress_sigma,
+                                                                                       c->cfg.dt, x);
+    return check_cuda(c, cudaGetLastError(), "line-shape dressing");
+}
+
+// the ensemble-mean correlation (dressed when set), zero-padded to len, inverse DFT
+dq_status spectrum(dq_ctx* c, int len, cd* d_out, cd* d_tmp) {
+    const int np = c->steps_done + 1;
+    dq_status st = check_cuda(c, cudaMemcpyAsync(d_tmp, c->d_corr, sizeof(cd) * np, cudaMemcpyDeviceToDevice,
+                                                 c->stream), "spectrum copy");
+    if (!st) st = dress_correlation(c, c->steps_done, d_tmp);
+    if (!st) st = fft_inverse(c, len, d_tmp, np, 1.0 / observed_trajectories(c), d_out);
+    return st;
 }
 
 }  // namespace dq
@@ -59,12 +85,22 @@ extern "C" dq_status dq_get_spectrum(dq_ctx* c, int len, dq_cdouble* out) {
         if (st) return st;
     }
     cd* d = nullptr;
-    dq_status st = check_cuda(c, cudaMalloc(&d, sizeof(cd) * (size_t)len), "spectrum alloc");
+    dq_status st = check_cuda(c, cudaMalloc(&d, sizeof(cd) * ((size_t)len + c->steps_done + 1)), "spectrum alloc");
     if (st) return st;
-    st = spectrum(c, len, d);
+    st = spectrum(c, len, d, d + len);
     if (!st) st = check_cuda(c, cudaMemcpyAsync(out, d, sizeof(cd) * (size_t)len, cudaMemcpyDeviceToHost, c->stream),
                              "spectrum copy");
     if (!st) st = check_cuda(c, cudaStreamSynchronize(c->stream), "spectrum sync");
     cudaFree(d);
     return st;
+}
+
+extern "C" dq_status dq_set_line_dressing(dq_ctx* c, double sigma_fs) {
+    if (!c) return DQ_ERR_ARG;
+    if (!(sigma_fs >= 0.0) || !std::isfinite(sigma_fs)) {
+        c->err = "line_dressing: sigma must be >= 0 (0 turns the dressing off)";
+        return DQ_ERR_ARG;
+    }
+    c->dress_sigma = sigma_fs;
+    return DQ_OK;
 }

@@ -101,6 +101,7 @@ struct dq_ctx {
     int last_path = 0;            // 0: dq_run_plain, 1: dq_run, 2: reduced sums set, 3: Taylor-Krylov dq_run
     int traj0 = 0;                // index of trajectory 0 in the whole (sharded) ensemble: the Philox key
     int obs_traj = 0;             // trajectories behind the observable sums when set from a reduction
+    double dress_sigma = 0.0;     // Gaussian line-shape dressing of M(t) before transforms (fs; 0 = off)
 
     // Taylor-Krylov mode (tk_p > 0): the auxiliary matrix B (off-diagonal
     // CSR + diagonal), its Krylov basis and the Taylor work vectors
@@ -168,6 +169,8 @@ dq_status tk_ensemble_run(dq_ctx* c, int n_steps);
 dq_status tk_ensemble_states(dq_ctx* c, dq_cdouble* out);
 void tk_ensemble_free(dq_ctx* c);
 // implemented in dq_fft.cu
+// M(k) *= exp(-(dt (k + 1) / sigma)^2 / 2) for k < n_dress (spectraClass.cu:583-600)
+dq_status dress_correlation(dq_ctx* c, int n_dress, cd* x);
 dq_status fft_inverse(dq_ctx* c, int len, const cd* in, int n_in, double scale, cd* out);
 // implemented in dq_adjoint.cu
 void adjoint_free(dq_ctx* c);

@@ -205,6 +205,8 @@ static dq_status scaled_spectrum(dq_ctx* c, double scaling, std::vector<cd>& cor
     corr.assign(len, cd{0.0, 0.0});
     spec.assign(len, cd{0.0, 0.0});
     st = check_cuda(c, cudaMemcpyAsync(d, c->d_corr, sizeof(cd) * len, cudaMemcpyDeviceToDevice, c->stream), "copy");
+    // optional Gaussian dressing of M(t) before the transform; the file shows the dressed M(t)
+    if (!st) st = dress_correlation(c, T, d);
     if (!st) {
         const int blocks = std::max(1, std::min(148 * 4, (len + 127) / 128));
         k_idft_direct<<<blocks, 128, 0, c->stream>>>(len, d, 1.0 / observed_trajectories(c), d + len);

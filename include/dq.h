@@ -297,6 +297,14 @@ DQ_API dq_status dq_get_noise_state(dq_ctx *ctx, int traj, double *eps, double *
  * n_in correlation points zero-padded to len (a power of two), on the GPU.
  * Replaces spectraClass::singleSpectraCalc's cufftExecZ2Z (spectraClass.cu:621). */
 DQ_API dq_status dq_get_spectrum(dq_ctx *ctx, int len, dq_cdouble *out);
+/* Optional Gaussian line-shape dressing (lineShapeDressing /
+ * gaussLineshapeWidth; spectraClass.cu:583-600, gpuSpectraHelper.cu:16-42):
+ * before every transform (dq_get_spectrum, dq_write_spectrum[_mean]) the
+ * ensemble-mean correlation point k < steps is multiplied by
+ * exp(-(dt (k + 1) / sigma)^2 / 2), the time offset by one step as in the
+ * reference; the correlation file shows the dressed values.  sigma in fs;
+ * 0 turns it off. */
+DQ_API dq_status dq_set_line_dressing(dq_ctx *ctx, double sigma_fs);
 
 /* ---- the reference's output files ---- */
 /* pops.dat of popPrintClass (popPrintClass.cu:160-522): header numsims / dt /

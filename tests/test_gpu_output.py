@@ -116,3 +116,29 @@ def test_spectrum_files(tmp_path):
         assert float(parts[3]) == pytest.approx(spec[fid].real * float(f), rel=1e-5, abs=1e-9)
         assert float(parts[4]) == pytest.approx(spec[fid].imag * float(f), rel=1e-5, abs=1e-9)
     p.close()
+
+
+def test_line_dressing(tmp_path):
+    """Gaussian line-shape dressing: M(k) exp(-(dt (k+1) / sigma)^2 / 2) for k < steps before the
+    transforms (the reference's offset by one), in the files and in dq_get_spectrum."""
+    p, s = _prop(steps=20)
+    corr = p.correlation()
+    plain = p.spectrum(32)
+    sigma = 7.0
+    p.set_line_dressing(sigma)
+    k = np.arange(21)
+    g = np.where(k < 20, np.exp(-0.5 * ((k + 1) * 1.0 / sigma) ** 2), 1.0)
+    dressed = corr * g
+    spec = p.spectrum(32)
+    ref = np.fft.ifft(np.concatenate([dressed, np.zeros(11)])) * 32
+    assert np.abs(spec - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.abs(spec - plain).max() > 1e-6
+    p.write_spectrum(tmp_path / "c.dat", tmp_path / "s.dat", 1.0)
+    row = open(tmp_path / "c.dat").read().splitlines()[1 + 5].split()
+    assert float(row[2]) == pytest.approx(dressed[5].real, rel=1e-5, abs=1e-12)
+    p.set_line_dressing(0.0)
+    assert np.abs(p.spectrum(32) - plain).max() == 0.0
+    import dynaquant_b200 as dq
+    with pytest.raises(dq.DQError):
+        p.set_line_dressing(-1.0)
+    p.close()
