@@ -1539,6 +1539,20 @@ __global__ void __launch_bounds__(kFwThreads, 1) k_lanczos_fw(int n, int B, int 
     }
 }
 
+// last read of a value before it is overwritten: evict-first (ld.global.cs)
+template <typename Real, int TPT>
+__device__ __forceinline__ CV<Real, TPT> ldv_cs(const Real* base, size_t idx) {
+    using T = typename VL<Real, TPT>::T;
+    const T t = __ldcs(reinterpret_cast<const T*>(base + 2 * idx));
+    CV<Real, TPT> v;
+    if constexpr (TPT == 2) {
+        v.v[0] = t.x; v.v[1] = t.y; v.v[2] = t.z; v.v[3] = t.w;
+    } else {
+        v.v[0] = t.x; v.v[1] = t.y;
+    }
+    return v;
+}
+
 // r_{j+1} = w - alpha_j q_j - beta_{j-1} q_{j-1};  beta_j = ||r_{j+1}||
 template <typename Real, int TPT>
 __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, int rpc, int j,
@@ -1564,13 +1578,13 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
         const size_t base = (size_t)row * B + T.b0;
         const size_t base2 = (size_t)(has2 ? row2 : row) * B + T.b0;
         CV<Real, TPT> u[2], x[2], xm[2];
-        u[0] = ldv<Real, TPT, false>(w, base);
+        u[0] = ldv_cs<Real, TPT>(w, base);
         x[0] = ldv<Real, TPT, false>(rj, base);
-        u[1] = ldv<Real, TPT, false>(w, base2);
+        u[1] = ldv_cs<Real, TPT>(w, base2);
         x[1] = ldv<Real, TPT, false>(rj, base2);
         if (j > 1) {
-            xm[0] = ldv<Real, TPT, false>(rjm, base);
-            xm[1] = ldv<Real, TPT, false>(rjm, base2);
+            xm[0] = ldv_cs<Real, TPT>(rjm, base);
+            xm[1] = ldv_cs<Real, TPT>(rjm, base2);
         }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
