@@ -138,3 +138,31 @@ def test_ipr_ensemble_matches_oracle(oracle, precision, tol, tmp_path):
     for k in (0, 3, T - 1):
         assert lines[2 + k] == "%d  %g" % (k, got[k])
     p.close()
+
+
+def test_taylor_krylov_with_zz_noise(oracle):
+    """Both Taylor-Krylov paths under the ZZ noise model against the oracle."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    from tests.test_noise_zz_oracle import ohmic_density
+    s = systems.tube(10, 6)
+    rng = np.random.default_rng(8)
+    (brp, bcol, bval, bdiag), full = _aux_matrix(s, rng)
+    omega, J, dw = ohmic_density()
+    w, c = oracle.zz_coefficients(omega, J, dw, 300.0)
+    B, T = 3, 12
+    prop = dq.Propagator(s.n, m=12, n_traj=B, dt=2.0, noise=dq.NOISE_ZZ, seed=13, dot=dq.DOT_HERMITIAN, pop_every=3,
+                         max_steps=T, precision=dq.PREC_FP64)
+    prop.set_system(s)
+    prop.set_zz_spectral_density(omega, J, dw, 300.0)
+    prop.set_initial_state(s.bright_state())
+    prop.set_taylor_krylov(4, 10, *full)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=12, dt=2.0, dot_mode=1, seed=13, noise=oracle.NOISE_ZZ, zz_omega=w,
+                      zz_coeff=c, tk=(4, 10, brp, bcol, bval, bdiag))
+    ref = S.run(B, T, s.bright_state(), pop_every=3, threads=4)
+    prop.run(T)
+    assert np.abs(prop.populations() - ref["pops"]).max() <= TOL_FP64
+    prop.run_plain(T)
+    assert np.abs(prop.populations() - ref["pops"]).max() <= TOL_FP64
+    prop.close()
