@@ -99,3 +99,24 @@ def test_absorption_state_from_dipoles():
         b.set_initial_dipole(np.zeros(s.n))
     a.close()
     b.close()
+
+
+def test_cd_bra_on_taylor_krylov_paths(oracle):
+    """The correlation bra on both Taylor-Krylov paths (B = the static Hamiltonian) against the oracle."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(10, 6)
+    mu, R = _geometry(s.n)
+    ket, bra, _ = spectra.cd_directions(mu, R)[0]
+    rp, col, val, d = s.off_diagonal()
+    frp, fcol, fval = s.rowptr, s.col, s.val      # B: the static Hamiltonian, diagonal included
+    p = _prop(s, ket, bra, dq.PREC_FP64, B=4)
+    p.set_taylor_krylov(3, 12, frp, fcol, fval)
+    S = oracle.System(rp, col, val, d, m=12, dt=2.0, dot_mode=1, noise=oracle.NOISE_OU, sigma=100.0, tau=50.0,
+                      seed=6, corr_bra=bra, tk=(3, 12, rp, col, val, d))
+    ref = S.run(4, T, ket, pop_every=4, threads=4)
+    p.run(T)
+    assert np.abs(p.correlation() - ref["corr"]).max() <= 1e-10
+    p.run_plain(T)
+    assert np.abs(p.correlation() - ref["corr"]).max() <= 1e-10
+    p.close()
