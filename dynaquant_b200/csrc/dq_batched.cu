@@ -2347,8 +2347,16 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
     const int RPC_spmm = (staged == 5 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
-    // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide
-    int gx = std::max(1, (bs->sms * kStreamCtasPerSm) / cpg);
+    // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide:
+    // one wave of kStreamCtasPerSm CTAs per SM while every thread still walks
+    // several rows, twice as many CTAs when that wave would leave each thread
+    // fewer than 4 rows (small systems are latency-bound, not bandwidth-bound)
+    int stream_per_sm = kStreamCtasPerSm;
+    {
+        const int g4 = std::max(1, (bs->sms * kStreamCtasPerSm) / cpg);
+        if ((n + g4 - 1) / g4 < 4 * RPC) stream_per_sm = 2 * kStreamCtasPerSm;
+    }
+    int gx = std::max(1, (bs->sms * stream_per_sm) / cpg);
     int rpc = (n + gx - 1) / gx;
     rpc = ((rpc + RPC - 1) / RPC) * RPC;
     gx = (n + rpc - 1) / rpc;

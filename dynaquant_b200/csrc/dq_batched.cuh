@@ -16,7 +16,8 @@ constexpr int kMaxTC = 64;
 constexpr int kMaxCtasPerChunk = 4096;
 // CTAs per SM of the streaming per-row kernels (noise, axpy, combine): one
 // wave of 256-thread CTAs at their ~64 registers per thread (4 resident per
-// SM); measured on the tube, 2, 3, 8 and 16 were all slower
+// SM); measured on the tube, 2, 3, 8 and 16 were all slower (small systems
+// take twice as many, see batched_set_tiling)
 constexpr int kStreamCtasPerSm = 4;
 constexpr int kMCheckStride = 4;   // adaptive Krylov dimension: checks at m_min, m_min + 4, ... below m
 
