@@ -73,7 +73,7 @@ constexpr int kZZBlock = 16;
 constexpr int kZZTile = 32;
 constexpr int kZZThreads = 128;
 
-__global__ void __launch_bounds__(kZZThreads) k_zz_block_b(int n, int B, int traj0, uint64_t seed, ZZParams zz,
+__global__ void __launch_bounds__(kZZThreads, 4) k_zz_block_b(int n, int B, int traj0, uint64_t seed, ZZParams zz,
                                                           BatchedScalars S, const int* __restrict__ zz_start,
                                                           double* __restrict__ zzD) {
     const int step = *S.step, start = *zz_start;
