@@ -4,7 +4,10 @@ Runs the benchmark workload (30,000-site dipole tube, 256 trajectories,
 m = 20, complex64) for a few steps with a fixed tiling, no autotuning and no
 CPU oracle, so a capture sees only the propagator's own launches:
 
-    python -m dynaquant_b200.profile_run --steps 2 [--tiling 32,2,4] [--B 256]
+    python -m dynaquant_b200.profile_run --steps 2 [--tiling 32,2,4] [--B 256] [--zz 253]
+
+--zz N swaps the OU noise for the ZZ model with N oscillators of an Ohmic
+spectral density on a 8.1357 cm^-1 grid at 77 K.
 """
 from __future__ import annotations
 
@@ -27,15 +30,21 @@ def main():
     ap.add_argument("--m", type=int, default=20)
     ap.add_argument("--tiling", default="")
     ap.add_argument("--fp64", action="store_true")
+    ap.add_argument("--zz", type=int, default=0)
     args = ap.parse_args()
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
     s = systems.tube(60, args.along, cutoff=25.0)
-    p = dq.Propagator(s.n, m=args.m, n_traj=args.B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=2024,
-                      dot=dq.DOT_HERMITIAN, precision=dq.PREC_FP64 if args.fp64 else dq.PREC_MIXED,
-                      pop_every=16, max_steps=args.steps + 4)
+    p = dq.Propagator(s.n, m=args.m, n_traj=args.B, dt=0.5, noise=dq.NOISE_ZZ if args.zz else dq.NOISE_OU,
+                      sigma_static=150.0, seed=2024, dot=dq.DOT_HERMITIAN,
+                      precision=dq.PREC_FP64 if args.fp64 else dq.PREC_MIXED, pop_every=16,
+                      max_steps=args.steps + 4)
     p.set_system(s)
-    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    if args.zz:
+        om = 8.1357 * np.arange(1, args.zz + 1)
+        p.set_zz_spectral_density(om, 60.0 * (om / 120.0) * np.exp(-om / 120.0), 8.1357, 77.0)
+    else:
+        p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
     p.set_initial_state(s.bright_state())
     if args.tiling:
         p.set_tiling(*[int(x) for x in args.tiling.split(",")])
