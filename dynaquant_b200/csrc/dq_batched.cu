@@ -393,12 +393,18 @@ __device__ __forceinline__ void union_any(int pb, int pe, const int* __restrict_
 
 // Row-blocked SpMM: w = H q_j for all trajectories of the chunk, R rows per
 // block.  kWrite: also alpha_j[b] = <q_j, w>_b; !kWrite: ||H q_j||_b only.
+// With rjm (kWrite, j >= 2) the kernel writes w = H q_j - beta_{j-1} q_{j-1}
+// instead and alpha_j = <q_j, w> (the ordering of Paige's stable variant):
+// q_{j-1} is one streaming read per row next to the latency-bound gathers,
+// and the axpy that follows reads two slabs instead of three.  The term is
+// folded into the accumulator's start value, -(beta_{j-1} sc_{j-1} / sc_j)
+// r_{j-1}, so it holds no registers across the gather loop.
 template <typename Real, int TPT, int R, bool kBilinear, bool kWrite, int NT = kBThreads>
 __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, int nb, int j,
                                                        const int* __restrict__ bptr, const int* __restrict__ bcol,
                                                        const Real* __restrict__ bcoef, const Real* __restrict__ d,
-                                                       const Real* __restrict__ rj, Real* __restrict__ w,
-                                                       BatchedScalars S, int cy0, int nch) {
+                                                       const Real* __restrict__ rj, const Real* __restrict__ rjm,
+                                                       Real* __restrict__ w, BatchedScalars S, int cy0, int nch) {
     const int TPR = TC / TPT;
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int RPC = blockDim.x / TPR;
@@ -407,11 +413,18 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
     const int b0 = chunk * TC + tr * TPT;
     const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
     double sc[TPT], ar[TPT], ai[TPT];
+    Real fm[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) {
         sc[t] = S.sc[(size_t)j * B + b0 + t];
         ar[t] = 0.0;
         ai[t] = 0.0;
+        fm[t] = 0;
+        if (rjm) {
+            // sc_j = 0 only after a breakdown, where beta_{j-1} = 0 as well
+            const size_t km = (size_t)(j - 1) * B + b0 + t;
+            fm[t] = sc[t] != 0.0 ? (Real)(S.beta[km] * S.sc[km] / sc[t]) : Real(0);
+        }
     }
     constexpr bool kPk = sizeof(Real) == 4 && R <= 3;
     const float4* rec = reinterpret_cast<const float4*>(bcoef);
@@ -438,6 +451,14 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
                 dd[i][t] = row0 + i < n ? __ldg(d + base + t) : Real(0);
                 acc[i].v[2 * t] = 0;
                 acc[i].v[2 * t + 1] = 0;
+            }
+            if (rjm) {
+                const CV<Real, TPT> xm = ldv_cs<Real, TPT>(rjm, base);
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    acc[i].v[2 * t] = -fm[t] * xm.v[2 * t];
+                    acc[i].v[2 * t + 1] = -fm[t] * xm.v[2 * t + 1];
+                }
             }
         }
         auto gather = [&](int c) { return ldv<Real, TPT, true>(rj, (size_t)c * B + b0); };
@@ -1539,21 +1560,8 @@ __global__ void __launch_bounds__(kFwThreads, 1) k_lanczos_fw(int n, int B, int 
     }
 }
 
-// last read of a value before it is overwritten: evict-first (ld.global.cs)
-template <typename Real, int TPT>
-__device__ __forceinline__ CV<Real, TPT> ldv_cs(const Real* base, size_t idx) {
-    using T = typename VL<Real, TPT>::T;
-    const T t = __ldcs(reinterpret_cast<const T*>(base + 2 * idx));
-    CV<Real, TPT> v;
-    if constexpr (TPT == 2) {
-        v.v[0] = t.x; v.v[1] = t.y; v.v[2] = t.z; v.v[3] = t.w;
-    } else {
-        v.v[0] = t.x; v.v[1] = t.y;
-    }
-    return v;
-}
-
-// r_{j+1} = w - alpha_j q_j - beta_{j-1} q_{j-1};  beta_j = ||r_{j+1}||
+// r_{j+1} = w - alpha_j q_j - beta_{j-1} q_{j-1};  beta_j = ||r_{j+1}||.
+// rjm == nullptr: the SpMM already subtracted beta_{j-1} q_{j-1} from w.
 template <typename Real, int TPT>
 __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, int rpc, int j,
                                                         const Real* __restrict__ w, const Real* __restrict__ rj,
@@ -1561,13 +1569,14 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
                                                         BatchedScalars S, int cy0, int nch) {
     const Tile<TPT> T(TC, rpc, n, cy0);
     if (chunk_converged(S, T.chunk)) return;
+    const bool prev = j > 1 && rjm != nullptr;
     double ajr[TPT], aji[TPT], bm[TPT], nn[TPT], zero[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) {
         const size_t k = (size_t)j * B + T.b0 + t;
         ajr[t] = S.alpha[2 * k] * S.sc[k];
         aji[t] = S.alpha[2 * k + 1] * S.sc[k];
-        bm[t] = (j > 1) ? S.beta[(size_t)(j - 1) * B + T.b0 + t] * S.sc[(size_t)(j - 1) * B + T.b0 + t] : 0.0;
+        bm[t] = prev ? S.beta[(size_t)(j - 1) * B + T.b0 + t] * S.sc[(size_t)(j - 1) * B + T.b0 + t] : 0.0;
         nn[t] = 0.0;
         zero[t] = 0.0;
     }
@@ -1582,7 +1591,7 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
         x[0] = ldv<Real, TPT, false>(rj, base);
         u[1] = ldv_cs<Real, TPT>(w, base2);
         x[1] = ldv<Real, TPT, false>(rj, base2);
-        if (j > 1) {
+        if (prev) {
             xm[0] = ldv_cs<Real, TPT>(rjm, base);
             xm[1] = ldv_cs<Real, TPT>(rjm, base2);
         }
@@ -1595,7 +1604,7 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
                 const double xr = x[h].v[2 * t], xi = x[h].v[2 * t + 1];
                 double rr = (double)u[h].v[2 * t] - (ajr[t] * xr - aji[t] * xi);
                 double ri = (double)u[h].v[2 * t + 1] - (ajr[t] * xi + aji[t] * xr);
-                if (j > 1) {
+                if (prev) {
                     rr -= bm[t] * (double)xm[h].v[2 * t];
                     ri -= bm[t] * (double)xm[h].v[2 * t + 1];
                 }
@@ -2733,8 +2742,11 @@ struct StepTimer {
     }
 };
 
+// The forms that run k_spmm_blk (L1 gathers, 256- or 512-thread CTAs).
+static bool spmm_subtracts_prev(const BatchedState* bs) { return bs->staged == 0 || bs->staged == 5; }
+
 template <typename Real, int TPT, bool kBil, bool kWrite>
-static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w, int cy0, int ncy) {
+static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real* w, int cy0, int ncy) {
     BatchedState* bs = c->bat;
     const BlockFmt& f = bs->fmt[r_index(bs->R)];
     const int n = c->n, B = bs->B, TC = bs->TC;
@@ -2803,11 +2815,11 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, Real* w, int cy0, int 
 #define DQ_SPMM_R(RR)                                                                                             \
     if (bs->staged == 5)                                                                                         \
         k_spmm_blk<Real, TPT, RR, kBil, kWrite, 512><<<grid, 512, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j,     \
-                                                                                 f.bptr, f.bcol, cf, d, rj, w,   \
+                                                                                 f.bptr, f.bcol, cf, d, rj, rjm, w, \
                                                                                  bs->s, cy0, bs->chunks);        \
     else                                                                                                         \
         k_spmm_blk<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j,    \
-                                                                                   f.bptr, f.bcol, cf, d, rj, w, \
+                                                                                   f.bptr, f.bcol, cf, d, rj, rjm, w, \
                                                                                    bs->s, cy0, bs->chunks)
     switch (bs->R) {
         case 1: DQ_SPMM_R(1); break;
@@ -2911,8 +2923,10 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
         return DQ_OK;
     }
     if (tm) tm->mark(DQ_KIND_SPMM, st);
-    if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_spmm<Real, TPT, true, true>(c, j, slab(j), slab(0), cy0, ncy);
-    else launch_spmm<Real, TPT, false, true>(c, j, slab(j), slab(0), cy0, ncy);
+    // the row-blocked L1 forms subtract beta_{j-1} q_{j-1} themselves
+    const Real* rjm = (!fused && j > 1 && spmm_subtracts_prev(bs)) ? slab(j - 1) : nullptr;
+    if (c->cfg.dot_mode == DQ_DOT_BILINEAR) launch_spmm<Real, TPT, true, true>(c, j, slab(j), rjm, slab(0), cy0, ncy);
+    else launch_spmm<Real, TPT, false, true>(c, j, slab(j), rjm, slab(0), cy0, ncy);
     if (fused) {
         // fused form: the first SpMM only; r_2 comes from the next fused launch
         if (j == c->cfg.m) {
@@ -2922,8 +2936,9 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
         return DQ_OK;
     }
     if (tm) tm->mark(DQ_KIND_AXPY, st);
-    k_axpy_beta<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slab(0), slab(j), slab(j - 1),
-                                                       slab(j + 1), bs->s, cy0, bs->chunks);
+    k_axpy_beta<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slab(0), slab(j),
+                                                       rjm ? nullptr : slab(j - 1), slab(j + 1), bs->s, cy0,
+                                                       bs->chunks);
     if (c->cfg.reorth) {
         if (tm) tm->mark(DQ_KIND_AXPY, st);
         for (int k = 1; k <= j; ++k)
@@ -2999,7 +3014,7 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
             for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm, g * cpg, cpg);
             if (bs->staged != 2 && bs->staged != 4) {   // the fused form's last launch gave ||H q_{m+1}||
                 mark(DQ_KIND_SPMM_NORM);
-                launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, g * cpg, cpg);
+                launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, nullptr, g * cpg, cpg);
             }
         }
     }

@@ -53,6 +53,27 @@ __device__ __forceinline__ CV<Real, TPT> ldv(const Real* base, size_t idx) {
     return v;
 }
 
+// last read of a value before it is overwritten: evict-first (ld.global.cs)
+template <typename Real, int TPT>
+__device__ __forceinline__ CV<Real, TPT> ldv_cs(const Real* base, size_t idx) {
+    using T = typename VL<Real, TPT>::T;
+    const T* p = reinterpret_cast<const T*>(base + 2 * idx);
+    CV<Real, TPT> v;
+    if constexpr (TPT == 4) {
+        const T a = __ldcs(p), b = __ldcs(p + 1);
+        v.v[0] = a.x; v.v[1] = a.y; v.v[2] = a.z; v.v[3] = a.w;
+        v.v[4] = b.x; v.v[5] = b.y; v.v[6] = b.z; v.v[7] = b.w;
+        return v;
+    }
+    const T t = __ldcs(p);
+    if constexpr (TPT == 2) {
+        v.v[0] = t.x; v.v[1] = t.y; v.v[2] = t.z; v.v[3] = t.w;
+    } else {
+        v.v[0] = t.x; v.v[1] = t.y;
+    }
+    return v;
+}
+
 template <typename Real, int TPT>
 __device__ __forceinline__ void stv(Real* base, size_t idx, const CV<Real, TPT>& v) {
     using T = typename VL<Real, TPT>::T;
