@@ -126,11 +126,12 @@ def spmm_bytes(s, B):
 
 
 # SpMM form per tiling `staged` value: kernel name and the committed ncu summary of it
-SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha)", "k_spmm_blk_tube60x500.md"),
+SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", "k_spmm_blk_tube60x500.md"),
               2: ("k_lanczos_fused (r_{j+1} + SpMM + alpha, beta)", None),
               3: ("k_spmm_warp (L1 gathers, warp per block + alpha)", None),
               4: ("k_lanczos_fw (fused, warp-owned blocks)", None),
-              5: ("k_spmm_blk, 512-thread CTAs (L1 gathers + alpha)", "k_spmm_blk512_tube60x500.md"),
+              5: ("k_spmm_blk, 512-thread CTAs (L1 gathers + alpha, minus beta q_{j-1})",
+                  "k_spmm_blk512_tube60x500.md"),
               6: ("k_spmm_ring (TMA ring gathers + alpha)", "k_spmm_ring_tube60x500.md"),
               7: ("k_spmm_ring, 4 trajectories per lane (TMA ring gathers + alpha)", None)}
 
@@ -456,6 +457,9 @@ def run_ours(args, rank, world, local_rank):
         # CSR; writes r_{j+1} and w)
         spmm_ms = prof["fused_iter"][0]
     bytes_spmm = spmm_bytes(s, B)
+    if tiling["staged"] in (0, 5):
+        # the L1 forms also read q_{j-1} (8 B per site-trajectory) in m - 1 of the step's m launches
+        bytes_spmm += 8.0 * s.n * B * (w["m"] - 1) / w["m"]
     if tiling["staged"] in (2, 4):
         bytes_spmm += 24.0 * s.n * B   # + r_j, r_{j-1} reads and the r_{j+1} write
     achieved = bytes_spmm / (spmm_ms / 1e3) / 1e9
