@@ -33,6 +33,8 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(name="tube60x500_B256_m20", around=60, along=500, cutoff=25.0, m=20, B=256, dt=0.5,
                 sigma_static=150.0, sigma=250.0, tau=50.0, seed=2024)
 METRIC = "traj-steps/s (batched mixed vs plain FP64, pop err<=1e-6); backward/forward time"
+# CUDA device of this rank (LOCAL_RANK under torchrun); every context of the run is created on it
+DEVICE = 0
 
 
 def _peaks():
@@ -109,7 +111,7 @@ def make_prop(s, B, precision, seed, max_steps, pop_every=16, reorth=0):
     w = WORKLOAD
     p = dq.Propagator(s.n, m=w["m"], n_traj=B, dt=w["dt"], noise=dq.NOISE_OU, sigma_static=w["sigma_static"],
                       seed=seed, dot=dq.DOT_HERMITIAN, precision=precision, pop_every=pop_every,
-                      max_steps=max_steps, reorth=reorth)
+                      max_steps=max_steps, reorth=reorth, device=DEVICE)
     p.set_system(s)
     p.set_noise_params(np.full(s.n, w["sigma"]), np.full(s.n, w["tau"]))
     p.set_initial_state(s.bright_state())
@@ -223,7 +225,7 @@ def zz_leg(s, tiling):
     B, K = 256, 48
     p = dq.Propagator(s.n, m=w["m"], n_traj=B, dt=w["dt"], noise=dq.NOISE_ZZ, sigma_static=w["sigma_static"],
                       seed=w["seed"], dot=dq.DOT_HERMITIAN, precision=dq.PREC_MIXED, pop_every=16,
-                      max_steps=K + 32)
+                      max_steps=K + 32, device=DEVICE)
     p.set_system(s)
     om = 8.1357 * np.arange(1, 254)
     p.set_zz_spectral_density(om, 60.0 * (om / 120.0) * np.exp(-om / 120.0), 8.1357, 77.0)
@@ -257,7 +259,7 @@ def large_leg():
     B, K, W = 1024, 8, 2
     p = dq.Propagator(s.n, m=24, n_traj=B, dt=w["dt"], noise=dq.NOISE_OU, sigma_static=w["sigma_static"],
                       seed=w["seed"], dot=dq.DOT_HERMITIAN, precision=dq.PREC_MIXED, pop_every=16,
-                      max_steps=W + K + 4)
+                      max_steps=W + K + 4, device=DEVICE)
     p.set_system(s)
     p.set_noise_params(np.full(s.n, w["sigma"]), np.full(s.n, w["tau"]))
     p.set_initial_state(s.bright_state())
@@ -294,7 +296,8 @@ def aggregates_leg():
             s = systems.tube(a["around"], L, cutoff=w["cutoff"])
             p = dq.Propagator(s.n, m=a["m"], n_traj=B, dt=a["dt"], noise=dq.NOISE_OU, sigma_static=w["sigma_static"],
                               seed=seed0 + i, dot=dq.DOT_HERMITIAN, precision=dq.PREC_MIXED, pop_every=50,
-                              max_steps=a["steps"] + 8, m_min=a["m_min"], m_tol=a["m_tol"])
+                              max_steps=a["steps"] + 8, m_min=a["m_min"], m_tol=a["m_tol"],
+                              device=DEVICE)
             p.set_system(s)
             p.set_noise_params(np.full(s.n, w["sigma"]), np.full(s.n, w["tau"]))
             p.set_initial_state(s.bright_state())
@@ -350,7 +353,7 @@ def adjoint_leg():
 
     def make(prec, e, scales=(1.0, 1.0)):
         p = dq.Propagator(n, m=a["m"], n_traj=a["B"], dt=a["dt"], noise=dq.NOISE_OU, seed=a["seed"],
-                          dot=dq.DOT_HERMITIAN, precision=prec, max_steps=T)
+                          dot=dq.DOT_HERMITIAN, precision=prec, max_steps=T, device=DEVICE)
         p.set_system(lat)
         p.set_coupling_classes(lat.cls_off, list(scales))
         p.set_noise_params(np.full(n, a["sigma"]), np.full(n, a["tau"]))
@@ -417,8 +420,9 @@ def adjoint_leg():
 def run_ours(args, rank, world, local_rank):
     import torch
     import dynaquant_b200 as dq
+    global DEVICE
     torch.cuda.set_device(local_rank)
-    dev = local_rank
+    dev = DEVICE = local_rank
     w = WORKLOAD
     B = w["B"]
     s = build_system()

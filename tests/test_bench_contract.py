@@ -63,3 +63,23 @@ def test_reference_arm_prints_one_contract_line():
     assert d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "traj-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
+
+
+def test_contexts_are_made_on_the_ranks_device(monkeypatch):
+    # under torchrun every rank's contexts must land on its LOCAL_RANK device, not on device 0
+    import dynaquant_b200 as dq
+
+    made = []
+
+    class FakePropagator:
+        def __init__(self, *a, **kw):
+            made.append(kw)
+
+        def __getattr__(self, name):
+            return lambda *a, **kw: None
+
+    monkeypatch.setattr(dq, "Propagator", FakePropagator)
+    monkeypatch.setattr(bench, "DEVICE", 3)
+    s = systems.tube(6, 10, cutoff=25.0)
+    bench.make_prop(s, 2, dq.PREC_MIXED, 1, max_steps=8)
+    assert made and made[-1]["device"] == 3
