@@ -54,7 +54,7 @@ def store(k: str, entry: dict) -> None:
     d[k] = entry
     try:
         os.makedirs(os.path.dirname(p), exist_ok=True)
-        tmp = p + ".tmp"
+        tmp = f"{p}.{os.getpid()}.tmp"   # one per process: ranks of one node may store at once
         with open(tmp, "w") as f:
             json.dump(d, f, indent=1, sort_keys=True)
         os.replace(tmp, p)
