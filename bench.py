@@ -417,6 +417,78 @@ def adjoint_leg():
     return out
 
 
+def secondary_legs(s, B, seed, tiling, value):
+    """The N = 1 extras of the JSON line: the plain FP64 path, the population error against the oracle,
+    full reorthogonalisation, the adjoint, the aggregates, ZZ noise, the large tube and the CPU baseline."""
+    import torch
+    import dynaquant_b200 as dq
+    w = WORKLOAD
+    # ---- plain FP64 per-trajectory GPU path on the same workload ---------------
+    pp = make_prop(s, 2, dq.PREC_FP64, seed, max_steps=64)
+    plain_steps = 20
+    pp.run_plain(2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pp.run_plain(plain_steps)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    pp.close()
+    plain = 2 * plain_steps / plain_s
+    # ---- population error of the mixed path vs the FP64 oracle -------------
+    pop_err = None
+    try:
+        from oracle import oracle as O
+        O.build()
+        rp, col, val, diag = s.off_diagonal()
+        S = O.System(rp, col, val, diag, m=w["m"], dt=w["dt"], dot_mode=O.DOT_HERMITIAN, noise=O.NOISE_OU,
+                     sigma=w["sigma"], tau=w["tau"], sigma_static=w["sigma_static"], seed=seed)
+        nT, nS = 4, 32
+        ref = S.run(nT, nS, s.bright_state(), pop_every=8, threads=os.cpu_count() or 1)
+        pm = make_prop(s, nT, dq.PREC_MIXED, seed, max_steps=nS, pop_every=8)
+        pm.run(nS)
+        pop_err = float(np.abs(pm.populations() - ref["pops"]).max())
+        pm.close()
+    except Exception as e:  # pragma: no cover - reported, not hidden
+        pop_err = f"unavailable: {e}"
+    # ---- the same step with full FP64 reorthogonalisation ------------------------
+    pr = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=16, reorth=1)
+    if tiling["staged"] in (2, 4):   # the fused forms cannot reorthogonalise between iterations
+        pr.set_tiling(32, 2, 2, 3, 0, 1)
+    else:
+        pr.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
+                      tiling["staged"], tiling["groups"])
+    pr.reset()
+    pr.run(2)
+    rs = torch.cuda.ExternalStream(pr.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(rs)
+    pr.run(8)
+    e1.record(rs)
+    torch.cuda.synchronize()
+    reorth_ms = e0.elapsed_time(e1) / 8
+    pr.close()
+    with_reorth = {"value": B / (reorth_ms / 1e3), "unit": "traj-steps/s", "ms_per_step": reorth_ms,
+                   "note": "classical Gram-Schmidt against q_1..q_j after every iteration, FP64 sums; 8 steps"}
+    adjoint = adjoint_leg()
+    aggregates = aggregates_leg()
+    zz = zz_leg(s, tiling)
+    large = large_leg()
+    cpu_v, cpu_sample = cpu_baseline_sample(s, os.cpu_count() or 1)
+    return {
+        "plain_fp64": {"value": plain, "unit": "traj-steps/s", "speedup_batched_mixed": value / plain,
+                       "sample": f"2 trajectories x {plain_steps} steps, dq_run_plain"},
+        "pop_err_vs_fp64_oracle": pop_err,
+        "with_reorth": with_reorth,
+        "adjoint": adjoint,
+        "aggregates": aggregates,
+        "zz_noise": zz,
+        "large_tube": large,
+        "cpu_baseline": {"value": cpu_v, "unit": "traj-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
+                         "sample": cpu_sample},
+    }
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import dynaquant_b200 as dq
@@ -501,57 +573,6 @@ def run_ours(args, rank, world, local_rank):
                    "(N > 1: all-reduce of the observable sums), populations + correlation download"}
     if rank != 0:
         return
-    # ---- plain FP64 per-trajectory GPU path on the same workload ---------------
-    pp = make_prop(s, 2, dq.PREC_FP64, seed, max_steps=64)
-    plain_steps = 20
-    pp.run_plain(2)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    pp.run_plain(plain_steps)
-    torch.cuda.synchronize()
-    plain_s = time.perf_counter() - t0
-    pp.close()
-    plain = 2 * plain_steps / plain_s
-    # ---- population error of the mixed path vs the FP64 oracle -------------
-    pop_err = None
-    try:
-        from oracle import oracle as O
-        O.build()
-        rp, col, val, diag = s.off_diagonal()
-        S = O.System(rp, col, val, diag, m=w["m"], dt=w["dt"], dot_mode=O.DOT_HERMITIAN, noise=O.NOISE_OU,
-                     sigma=w["sigma"], tau=w["tau"], sigma_static=w["sigma_static"], seed=seed)
-        nT, nS = 4, 32
-        ref = S.run(nT, nS, s.bright_state(), pop_every=8, threads=os.cpu_count() or 1)
-        pm = make_prop(s, nT, dq.PREC_MIXED, seed, max_steps=nS, pop_every=8)
-        pm.run(nS)
-        pop_err = float(np.abs(pm.populations() - ref["pops"]).max())
-        pm.close()
-    except Exception as e:  # pragma: no cover - reported, not hidden
-        pop_err = f"unavailable: {e}"
-    # ---- the same step with full FP64 reorthogonalisation ------------------------
-    pr = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=16, reorth=1)
-    if tiling["staged"] in (2, 4):   # the fused forms cannot reorthogonalise between iterations
-        pr.set_tiling(32, 2, 2, 3, 0, 1)
-    else:
-        pr.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
-                      tiling["staged"], tiling["groups"])
-    pr.reset()
-    pr.run(2)
-    rs = torch.cuda.ExternalStream(pr.stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(rs)
-    pr.run(8)
-    e1.record(rs)
-    torch.cuda.synchronize()
-    reorth_ms = e0.elapsed_time(e1) / 8
-    pr.close()
-    with_reorth = {"value": B / (reorth_ms / 1e3), "unit": "traj-steps/s", "ms_per_step": reorth_ms,
-                   "note": "classical Gram-Schmidt against q_1..q_j after every iteration, FP64 sums; 8 steps"}
-    adjoint = adjoint_leg()
-    aggregates = aggregates_leg()
-    zz = zz_leg(s, tiling)
-    large = large_leg()
     traffic, traffic_src = measured_traffic(tiling["staged"])
     cpu_v, cpu_sample = cpu_baseline_sample(s, os.cpu_count() or 1)
     clocks = clk.summary()
@@ -576,18 +597,13 @@ def run_ours(args, rank, world, local_rank):
                      "traffic_source": (traffic_src + " (ncu dram bytes, one launch)") if traffic_src else None},
         "kernels_ms_per_launch": {k: v[0] for k, v in prof.items()},
         "eager_step_ms": step_ms_eager,
-        "plain_fp64": {"value": plain, "unit": "traj-steps/s", "speedup_batched_mixed": value / world / plain,
-                       "sample": f"2 trajectories x {plain_steps} steps, dq_run_plain"},
-        "pop_err_vs_fp64_oracle": pop_err,
-        "with_reorth": with_reorth,
-        "adjoint": adjoint,
-        "aggregates": aggregates,
-        "zz_noise": zz,
-        "large_tube": large,
-        "cpu_baseline": {"value": cpu_v, "unit": "traj-steps/s", "cores": os.cpu_count() or 1, "kind": "port",
-                         "sample": cpu_sample},
         "clocks": clocks,
     }
+    if world == 1:
+        line.update(secondary_legs(s, B, seed, tiling, value))
+    else:
+        line["note"] = ("the secondary legs (plain FP64, oracle error, reorthogonalisation, adjoint, aggregates, "
+                        "ZZ, large tube) and the CPU baseline run at N = 1 only")
     print(json.dumps(line), flush=True)
 
 
