@@ -686,6 +686,7 @@ extern "C" {
 
 dq_status dq_adjoint_setup(dq_ctx* c, int n_steps, int fft_len, double scale, const double* target,
                            int checkpoint_every) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (c->cfg.dot_mode != DQ_DOT_HERMITIAN) return fail(c, DQ_ERR_ARG, "adjoint: needs the Hermitian Lanczos dot");
     if (c->cfg.reorth) return fail(c, DQ_ERR_ARG, "adjoint: not with reorthogonalisation (the recurrence is used)");
@@ -862,6 +863,7 @@ static dq_status forward_loss(dq_ctx* c, int n_total, double* loss) {
 extern "C" {
 
 dq_status dq_forward(dq_ctx* c, double* loss) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     dq_status st;
     if ((st = forward_run(c))) return st;
@@ -869,6 +871,7 @@ dq_status dq_forward(dq_ctx* c, double* loss) {
 }
 
 dq_status dq_forward_shard(dq_ctx* c, dq_cdouble* corr_sums) {
+    DeviceScope dev_scope(c);
     if (!c || !corr_sums) return DQ_ERR_ARG;
     dq_status st;
     if ((st = forward_run(c))) return st;
@@ -877,6 +880,7 @@ dq_status dq_forward_shard(dq_ctx* c, dq_cdouble* corr_sums) {
 }
 
 dq_status dq_forward_reduced(dq_ctx* c, const dq_cdouble* corr_sums, int n_traj_total, double* loss) {
+    DeviceScope dev_scope(c);
     if (!c || !corr_sums) return DQ_ERR_ARG;
     AdjointState* a = c->adj;
     if (!a || !c->bat || c->steps_done != a->T || c->last_path != 1)
@@ -887,6 +891,7 @@ dq_status dq_forward_reduced(dq_ctx* c, const dq_cdouble* corr_sums, int n_traj_
 }
 
 dq_status dq_backward(dq_ctx* c, double* grad_sites, double* grad_classes) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     AdjointState* a = c->adj;
     if (!a || !a->forward_done || !c->bat || c->steps_done != a->T)

@@ -92,6 +92,11 @@ dq_status dq_create(const dq_config* cfg, dq_ctx** out) {
     c->hbar = cfg->hbar > 0 ? cfg->hbar : reference_hbar();
     c->tau_im = -cfg->dt / c->hbar;   // propagate.cu:90-93: expCoeff = (0, -dt/hbar)
     dq_status st = DQ_OK;
+    int prev_device = -1;
+    if (cudaGetDevice(&prev_device) != cudaSuccess) {
+        cudaGetLastError();
+        prev_device = -1;
+    }
     do {
         if ((st = check_cuda(c, cudaSetDevice(cfg->device), "cudaSetDevice"))) break;
         if ((st = check_cuda(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "stream"))) break;
@@ -105,10 +110,12 @@ dq_status dq_create(const dq_config* cfg, dq_ctx** out) {
     } while (0);
     if (st != DQ_OK) {
         dq_destroy(c);
-        return st;
+    } else {
+        *out = c;
     }
-    *out = c;
-    return DQ_OK;
+    // the caller's current device is left as it was
+    if (prev_device >= 0 && prev_device != cfg->device) cudaSetDevice(prev_device);
+    return st;
 }
 
 static void tk_free(dq_ctx* c) {
@@ -124,7 +131,7 @@ static void tk_free(dq_ctx* c) {
 
 void dq_destroy(dq_ctx* c) {
     if (!c) return;
-    cudaSetDevice(c->cfg.device);
+    DeviceScope dev_scope(c);
     if (c->stream) cudaStreamSynchronize(c->stream);
     adjoint_free(c);
     batched_free(c);
@@ -144,6 +151,7 @@ const char* dq_last_error(const dq_ctx* c) { return c ? c->err.c_str() : "null c
 void* dq_get_stream(dq_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 dq_status dq_set_hamiltonian_csr(dq_ctx* c, int n, const int* rowptr, const int* col, const double* val) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (n != c->n || !rowptr || !col || !val) return fail(c, DQ_ERR_ARG, "hamiltonian: size or null pointer");
     if (rowptr[0] != 0) return fail(c, DQ_ERR_ARG, "hamiltonian: rowptr[0] != 0");
@@ -191,6 +199,7 @@ dq_status dq_set_hamiltonian_csr(dq_ctx* c, int n, const int* rowptr, const int*
 }
 
 dq_status dq_set_coupling_classes(dq_ctx* c, const int* cls, int n_classes, const double* scales) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (!c->have_ham) return fail(c, DQ_ERR_STATE, "coupling classes: set the Hamiltonian first");
     if (!cls || !scales || n_classes < 1) return fail(c, DQ_ERR_ARG, "coupling classes: null or empty");
@@ -203,6 +212,7 @@ dq_status dq_set_coupling_classes(dq_ctx* c, const int* cls, int n_classes, cons
 }
 
 dq_status dq_set_noise_params(dq_ctx* c, const double* sigma, const double* tau) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (!sigma) return fail(c, DQ_ERR_ARG, "noise params: sigma is null");
     if (c->cfg.noise_model == DQ_NOISE_OU && !tau) return fail(c, DQ_ERR_ARG, "noise params: OU needs tau");
@@ -228,6 +238,7 @@ dq_status dq_set_noise_params(dq_ctx* c, const double* sigma, const double* tau)
 
 dq_status dq_set_zz_spectral_density(dq_ctx* c, int n_osc, const double* omega, const double* J, double d_omega,
                                      double temperature) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (n_osc < 1 || n_osc > kMaxZZOsc || !omega || !J || !(temperature > 0) || !(d_omega > 0))
         return fail(c, DQ_ERR_ARG, "zz: 1..1024 oscillators, positive spacing and temperature");
@@ -250,6 +261,7 @@ dq_status dq_set_zz_spectral_density(dq_ctx* c, int n_osc, const double* omega, 
 }
 
 dq_status dq_set_taylor_krylov(dq_ctx* c, int p, int m_b, const int* rowptr, const int* col, const double* val) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (p == 0) {
         tk_free(c);
@@ -305,6 +317,7 @@ dq_status dq_set_taylor_krylov(dq_ctx* c, int p, int m_b, const int* rowptr, con
 }
 
 dq_status dq_set_ipr(dq_ctx* c, int enable) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (enable && !c->d_ipr) {
         DQ_CU(cudaMalloc(&c->d_ipr, sizeof(double) * (size_t)(c->cfg.max_steps + 1)));
@@ -319,6 +332,7 @@ dq_status dq_set_ipr(dq_ctx* c, int enable) {
 }
 
 dq_status dq_get_ipr(dq_ctx* c, double* out, int* n_values) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (!c->ipr_on) return fail(c, DQ_ERR_STATE, "get_ipr: the inverse participation ratio is not enabled");
     const int nv = c->steps_done + 1;
@@ -332,6 +346,7 @@ dq_status dq_get_ipr(dq_ctx* c, double* out, int* n_values) {
 }
 
 dq_status dq_set_correlation_bra(dq_ctx* c, const dq_cdouble* bra) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (!bra) {
         cudaFree(c->d_bra);
@@ -349,6 +364,7 @@ dq_status dq_set_correlation_bra(dq_ctx* c, const dq_cdouble* bra) {
 }
 
 dq_status dq_set_trajectory_offset(dq_ctx* c, int traj0) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (traj0 < 0 || traj0 % 2) return fail(c, DQ_ERR_ARG, "trajectory_offset: must be even and >= 0");
     c->traj0 = traj0;
@@ -357,6 +373,7 @@ dq_status dq_set_trajectory_offset(dq_ctx* c, int traj0) {
 }
 
 dq_status dq_get_observable_sums(dq_ctx* c, double* pops, dq_cdouble* corr, double* ipr) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (c->last_path == 1 && c->bat) {
         dq_status st = batched_collect_corr(c);
@@ -375,6 +392,7 @@ dq_status dq_get_observable_sums(dq_ctx* c, double* pops, dq_cdouble* corr, doub
 
 dq_status dq_set_observable_sums(dq_ctx* c, const double* pops, const dq_cdouble* corr, const double* ipr,
                                  int n_traj_total) {
+    DeviceScope dev_scope(c);
     if (!c || !pops || !corr || n_traj_total < 1) return DQ_ERR_ARG;
     if (ipr && !c->ipr_on) return fail(c, DQ_ERR_STATE, "observable_sums: the inverse participation ratio is off");
     const int nrec = c->steps_done / c->cfg.pop_every + 1, np = c->steps_done + 1;
@@ -388,6 +406,7 @@ dq_status dq_set_observable_sums(dq_ctx* c, const double* pops, const dq_cdouble
 }
 
 dq_status dq_set_static_energies(dq_ctx* c, const double* eps) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (!eps) {
         c->static_eps.clear();
@@ -400,6 +419,7 @@ dq_status dq_set_static_energies(dq_ctx* c, const double* eps) {
 }
 
 dq_status dq_set_initial_state(dq_ctx* c, const dq_cdouble* psi0) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (!psi0) return fail(c, DQ_ERR_ARG, "initial state is null");
     c->psi0.assign(psi0, psi0 + c->n);
@@ -412,6 +432,7 @@ dq_status dq_set_initial_state(dq_ctx* c, const dq_cdouble* psi0) {
 
 // spectraClass.cu:440-458: psi0 = mu / |mu| for one polarisation direction
 dq_status dq_set_initial_dipole(dq_ctx* c, const double* mu) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (!mu) return fail(c, DQ_ERR_ARG, "initial dipole is null");
     double s = 0.0;
@@ -436,6 +457,7 @@ static dq_status check_ready(dq_ctx* c) {
 }
 
 dq_status dq_reset(dq_ctx* c) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     dq_status st;
     if ((st = check_ready(c))) return st;
@@ -455,6 +477,7 @@ dq_status dq_reset(dq_ctx* c) {
 }
 
 dq_status dq_prop_step(dq_ctx* c, int traj, int step, const dq_cdouble* psi_in, dq_cdouble* psi_out, double* err_est) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (traj < 0 || traj >= c->cfg.n_traj || step < 0 || !psi_in || !psi_out || psi_in == psi_out)
         return fail(c, DQ_ERR_ARG, "prop_step: bad trajectory, step or pointers");
@@ -479,6 +502,7 @@ dq_status dq_prop_step(dq_ctx* c, int traj, int step, const dq_cdouble* psi_in, 
 }
 
 dq_status dq_run_plain(dq_ctx* c, int n_steps) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (n_steps < 0 || n_steps > c->cfg.max_steps) return fail(c, DQ_ERR_ARG, "run_plain: n_steps out of range");
     dq_status st;
@@ -509,6 +533,7 @@ dq_status dq_run_plain(dq_ctx* c, int n_steps) {
 }
 
 dq_status dq_run(dq_ctx* c, int n_steps) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (n_steps < 0 || c->steps_done + n_steps > c->cfg.max_steps)
         return fail(c, DQ_ERR_ARG, "run: steps exceed max_steps");
@@ -541,6 +566,7 @@ dq_status dq_run(dq_ctx* c, int n_steps) {
 }
 
 dq_status dq_get_populations(dq_ctx* c, double* out, int* n_records) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     int nrec = c->steps_done / c->cfg.pop_every + 1;
     if (n_records) *n_records = nrec;
@@ -553,6 +579,7 @@ dq_status dq_get_populations(dq_ctx* c, double* out, int* n_records) {
 }
 
 dq_status dq_get_correlation(dq_ctx* c, dq_cdouble* out, int* n_points) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     int np = c->steps_done + 1;
     if (n_points) *n_points = np;
@@ -569,6 +596,7 @@ dq_status dq_get_correlation(dq_ctx* c, dq_cdouble* out, int* n_points) {
 }
 
 dq_status dq_get_states(dq_ctx* c, dq_cdouble* out) {
+    DeviceScope dev_scope(c);
     if (!c || !out) return DQ_ERR_ARG;
     if (c->last_path == 3 && c->tke) return tk_ensemble_states(c, out);
     if (!c->bat) return fail(c, DQ_ERR_STATE, "get_states: no ensemble state (run dq_run first)");
@@ -576,6 +604,7 @@ dq_status dq_get_states(dq_ctx* c, dq_cdouble* out) {
 }
 
 dq_status dq_get_error_accum(dq_ctx* c, double* out) {
+    DeviceScope dev_scope(c);
     if (!c || !out) return DQ_ERR_ARG;
     DQ_CU(cudaStreamSynchronize(c->stream));
     DQ_CU(cudaMemcpy(out, c->d_erracc, sizeof(double) * c->cfg.n_traj, cudaMemcpyDeviceToHost));
@@ -587,6 +616,7 @@ int dq_steps_done(const dq_ctx* c) { return c ? c->steps_done : -1; }
 }  // extern "C"
 
 extern "C" dq_status dq_get_noise_state(dq_ctx* c, int traj, double* eps, double* deps) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (traj < 0 || traj >= c->cfg.n_traj) return fail(c, DQ_ERR_ARG, "noise_state: bad trajectory");
     const int n = c->n;
@@ -606,6 +636,7 @@ extern "C" dq_status dq_get_noise_state(dq_ctx* c, int traj, double* eps, double
 }
 
 extern "C" dq_status dq_profile_step(dq_ctx* c, int n_steps, double* ms_per_launch, int* launches, int n_kinds) {
+    DeviceScope dev_scope(c);
     if (!c || !ms_per_launch || n_kinds < 1) return DQ_ERR_ARG;
     if (n_steps < 1 || c->steps_done + n_steps > c->cfg.max_steps)
         return fail(c, DQ_ERR_ARG, "profile_step: steps exceed max_steps");
@@ -641,6 +672,7 @@ static dq_status ensure_batched(dq_ctx* c) {
 
 extern "C" dq_status dq_set_tiling(dq_ctx* c, int traj_chunk, int vec, int ctas_per_sm, int rows_per_block,
                                    int staged, int groups) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     dq_status st;
     if ((st = ensure_batched(c))) return st;
@@ -652,6 +684,7 @@ extern "C" dq_status dq_set_tiling(dq_ctx* c, int traj_chunk, int vec, int ctas_
 
 extern "C" dq_status dq_get_tiling(dq_ctx* c, int* traj_chunk, int* vec, int* ctas_per_sm, int* rows_per_block,
                                    int* staged, int* groups) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     dq_status st;
     if ((st = ensure_batched(c))) return st;
@@ -660,6 +693,7 @@ extern "C" dq_status dq_get_tiling(dq_ctx* c, int* traj_chunk, int* vec, int* ct
 }
 
 extern "C" dq_status dq_autotune(dq_ctx* c, int reps, double* best_ms) {
+    DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (reps < 1) reps = 5;
     dq_status st;
@@ -690,6 +724,7 @@ extern "C" dq_status dq_autotune(dq_ctx* c, int reps, double* best_ms) {
 }
 
 extern "C" dq_status dq_time_iteration(dq_ctx* c, int reps, double* ms) {
+    DeviceScope dev_scope(c);
     if (!c || !ms) return DQ_ERR_ARG;
     if (reps < 1) reps = 5;
     dq_status st;

@@ -74,6 +74,7 @@ dq_status spectrum(dq_ctx* c, int len, cd* d_out, cd* d_tmp) {
 }  // namespace dq
 
 extern "C" dq_status dq_get_spectrum(dq_ctx* c, int len, dq_cdouble* out) {
+    dq::DeviceScope dev_scope(c);
     using namespace dq;
     if (!c || !out) return DQ_ERR_ARG;
     if (len < 2 || (len & (len - 1)) != 0) {
@@ -96,6 +97,7 @@ extern "C" dq_status dq_get_spectrum(dq_ctx* c, int len, dq_cdouble* out) {
 }
 
 extern "C" dq_status dq_set_line_dressing(dq_ctx* c, double sigma_fs) {
+    dq::DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     if (!(sigma_fs >= 0.0) || !std::isfinite(sigma_fs)) {
         c->err = "line_dressing: sigma must be >= 0 (0 turns the dressing off)";

@@ -49,8 +49,8 @@ dq_status dq_group_create(dq_ctx* const* members, int n_members, dq_group** out)
     dq_group* g = new dq_group();
     g->members.assign(members, members + n_members);
     g->device = members[0]->cfg.device;
-    cudaError_t e = cudaSetDevice(g->device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+    dq::DeviceScope dev_scope(g->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
     g->events.assign(n_members + 1, nullptr);
     for (int i = 0; e == cudaSuccess && i <= n_members; ++i)
         e = cudaEventCreateWithFlags(&g->events[i], cudaEventDisableTiming);
@@ -64,7 +64,7 @@ dq_status dq_group_create(dq_ctx* const* members, int n_members, dq_group** out)
 
 void dq_group_destroy(dq_group* g) {
     if (!g) return;
-    cudaSetDevice(g->device);
+    dq::DeviceScope dev_scope(g->device);
     if (g->stream) cudaStreamSynchronize(g->stream);
     for (auto ev : g->events)
         if (ev) cudaEventDestroy(ev);
@@ -78,7 +78,7 @@ dq_status dq_group_run(dq_group* g, int n_steps) {
     if (!g) return DQ_ERR_ARG;
     if (n_steps < 0) return gfail(g, DQ_ERR_ARG, "group run: negative step count");
     if (n_steps == 0) return DQ_OK;
-    DQ_GCU(cudaSetDevice(g->device));
+    dq::DeviceScope dev_scope(g->device);
     // every member's ensemble exists and is ready, as dq_run would make it
     for (dq_ctx* c : g->members) {
         if (c->steps_done + n_steps > c->cfg.max_steps)

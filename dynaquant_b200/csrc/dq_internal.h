@@ -130,6 +130,29 @@ namespace dq {
 // The bra of the correlation M(t) = <bra|psi(t)>: psi0 unless one was set.
 inline const cd* corr_bra(const dq_ctx* c) { return c->d_bra ? c->d_bra : c->d_psi0; }
 
+// Makes a context's device current for the length of one entry point and gives
+// the caller's current device back on return, so contexts on several GPUs can
+// be driven from one thread in any order (no synchronisation involved).
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int device) {
+        int cur = -1;
+        if (device < 0 || cudaGetDevice(&cur) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        if (cur == device) return;
+        if (cudaSetDevice(device) == cudaSuccess) prev = cur;
+        else cudaGetLastError();
+    }
+    explicit DeviceScope(const dq_ctx* c) : DeviceScope(c ? c->cfg.device : -1) {}
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 // Trajectories the observable sums stand for (their divisor for means).
 inline int observed_trajectories(const dq_ctx* c) {
     if (c->obs_traj > 0) return c->obs_traj;

@@ -76,6 +76,7 @@ bool read_text_header(FILE* f, int* numsims, double* dt, int* steps, int* sites)
 extern "C" {
 
 dq_status dq_write_populations(dq_ctx* c, const char* path, int binary, int continuation) {
+    DeviceScope dev_scope(c);
     if (!c || !path) return DQ_ERR_ARG;
     std::vector<double> sums;
     int nrec = 0;
@@ -151,6 +152,7 @@ dq_status dq_write_populations(dq_ctx* c, const char* path, int binary, int cont
 }
 
 dq_status dq_write_states(dq_ctx* c, const char* folder) {
+    DeviceScope dev_scope(c);
     if (!c || !folder) return DQ_ERR_ARG;
     if (!c->bat && !c->tke) return ofail(c, DQ_ERR_STATE, "write_states: no ensemble state (run dq_run first)");
     const int n = c->n, nr = c->cfg.n_traj;
@@ -175,6 +177,7 @@ dq_status dq_write_states(dq_ctx* c, const char* folder) {
 // line "k  IPR_k" per step k = 0..steps-1 with the ensemble mean of
 // 1 / sum_i |psi_i(k)|^4 printed like an ostream at its default precision.
 dq_status dq_write_ipr(dq_ctx* c, const char* path) {
+    DeviceScope dev_scope(c);
     if (!c || !path) return DQ_ERR_ARG;
     int nv = 0;
     dq_status st = dq_get_ipr(c, nullptr, &nv);
@@ -255,6 +258,7 @@ static dq_status write_spectrum_files(dq_ctx* c, int T, double dt, const std::ve
 }
 
 dq_status dq_write_spectrum(dq_ctx* c, const char* corr_path, const char* spec_path, double scaling) {
+    DeviceScope dev_scope(c);
     if (!c || !corr_path || !spec_path) return DQ_ERR_ARG;
     std::vector<cd> corr, spec;
     dq_status st = scaled_spectrum(c, scaling, corr, spec);
@@ -276,7 +280,11 @@ dq_status dq_write_spectrum_mean(dq_ctx* const* ctxs, int n_ctx, const double* s
         if (!c) return DQ_ERR_ARG;
         if (c->steps_done != T || c->cfg.dt != c0->cfg.dt)
             return ofail(c0, DQ_ERR_ARG, "write_spectrum_mean: the contexts differ in steps done or dt");
-        dq_status st = scaled_spectrum(c, scalings[k], ci, si);
+        dq_status st;
+        {
+            DeviceScope dev_scope(c);
+            st = scaled_spectrum(c, scalings[k], ci, si);
+        }
         if (st) {
             if (c != c0) c0->err = c->err;
             return st;
