@@ -84,7 +84,8 @@ typedef struct dq_config {
                                EXPOKIT term beta_j |E(j-1, j)| <= m_tol, or m (the plain path keeps m) */
     double m_tol;           /* adaptive Krylov dimension: tolerance (0 selects 1e-7) */
     int max_steps;          /* capacity of the correlation / population records */
-    int device;             /* CUDA device ordinal */
+    int device;             /* CUDA device ordinal; every call on the context makes it current for
+                               its duration and gives the caller's current device back */
 } dq_config;
 
 /* Fills defaults: m 16, dt 1, reference hbar, no noise, 1 substep,
