@@ -22,6 +22,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -55,7 +56,9 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        # raw samples: $DQ_CLOCKS_DIR if set, else the temporary directory (the JSON line carries the summary)
+        self.path = os.path.join(os.environ.get("DQ_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"clocks_bench_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
