@@ -22,8 +22,8 @@ import json
 import os
 import statistics
 import subprocess
-import tempfile
 import sys
+import tempfile
 import time
 
 import numpy as np
