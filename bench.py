@@ -131,7 +131,7 @@ def spmm_bytes(s, B):
 
 
 # SpMM form per tiling `staged` value: kernel name and the committed ncu summary of it
-SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", "k_spmm_blk_tube60x500.md"),
+SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", None),
               2: ("k_lanczos_fused (r_{j+1} + SpMM + alpha, beta)", None),
               3: ("k_spmm_warp (L1 gathers, warp per block + alpha)", None),
               4: ("k_lanczos_fw (fused, warp-owned blocks)", None),
