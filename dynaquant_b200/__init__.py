@@ -27,7 +27,10 @@ def reference_hbar() -> float:
 
 
 class Propagator:
-    """One context of the C ABI: a system, its trajectories and observables."""
+    """One context of the C ABI: a system, its trajectories and observables.
+
+    `device` is the CUDA ordinal the context lives on; every call runs there and
+    leaves the caller's current device as it was."""
 
     def __init__(self, n_sites, m=16, n_traj=1, dt=1.0, hbar=0.0, noise=NOISE_NONE, ka_substeps=1,
                  sigma_static=0.0, seed=0, dot=DOT_HERMITIAN, norm=NORM_COMPLEX, precision=PREC_MIXED,
