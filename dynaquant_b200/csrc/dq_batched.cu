@@ -188,24 +188,25 @@ __global__ void __launch_bounds__(kBThreads) k_noise_b(int n, int B, int traj0, 
             }
             d[x] = (Real)v0;
             d[x + 1] = (Real)v1;
-            continue;
-        }
+        } else {
 #pragma unroll
-        for (int t = 0; t < TPT; ++t) {
-            const int b = T.b0 + t;
-            const size_t x = (size_t)row * B + b;
-            double v;
-            if (noise == DQ_NOISE_OU) {
-                double cur = ou_update(deps[x], invtau[row], coeff[row], subdt, sqrt_subdt, ns, seed, traj0 + b, step, row);
-                deps[x] = cur;
-                v = __dadd_rn(cur, eps[x]);
-            } else if (noise == DQ_NOISE_GAUSS) {
-                double xi = normal(seed, P_GAUSS, traj0 + b, step, row, 0);
-                v = __dadd_rn(__dmul_rn(xi, sigma[row]), eps[x]);
-            } else {
-                v = eps[x];
+            for (int t = 0; t < TPT; ++t) {
+                const int b = T.b0 + t;
+                const size_t x = (size_t)row * B + b;
+                double v;
+                if (noise == DQ_NOISE_OU) {
+                    double cur =
+                        ou_update(deps[x], invtau[row], coeff[row], subdt, sqrt_subdt, ns, seed, traj0 + b, step, row);
+                    deps[x] = cur;
+                    v = __dadd_rn(cur, eps[x]);
+                } else if (noise == DQ_NOISE_GAUSS) {
+                    double xi = normal(seed, P_GAUSS, traj0 + b, step, row, 0);
+                    v = __dadd_rn(__dmul_rn(xi, sigma[row]), eps[x]);
+                } else {
+                    v = eps[x];
+                }
+                d[x] = (Real)v;
             }
-            d[x] = (Real)v;
         }
     }
 }
