@@ -72,3 +72,24 @@ def test_create_rejects_bad_config_without_gpu(lib):
     cfg.dot_mode = _lib.DOT_BILINEAR   # reorthogonalisation needs the Hermitian product
     assert lib.dq_create(C.byref(cfg), C.byref(h)) == _lib.DQ_ERR_ARG
     assert h.value is None
+
+
+def test_no_cpu_fallback_without_a_gpu(lib):
+    # a valid configuration on a machine without a GPU is refused with a CUDA error, never run on the host
+    import ctypes as C
+
+    import pytest
+    import torch
+
+    from dynaquant_b200 import _lib
+    import dynaquant_b200 as dq
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    cfg = _lib.Config()
+    lib.dq_config_default(C.byref(cfg))
+    cfg.n_sites = 100
+    h = C.c_void_p()
+    assert lib.dq_create(C.byref(cfg), C.byref(h)) == _lib.DQ_ERR_CUDA
+    assert h.value is None
+    with pytest.raises(dq.DQError):
+        dq.Propagator(100, m=8, n_traj=2)
