@@ -47,20 +47,61 @@ def _peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+    """SM clock and throttle reasons sampled DURING the timed region.
+
+    A thread reads NVML every 5 ms (read-only queries of the device this rank
+    runs on, found by its PCI bus id), so even a timed region of tens of
+    milliseconds gets samples; `nvidia-smi --query-gpu ... -lms 200` runs beside
+    it as a second record for longer regions.  Raw samples go to
+    $DQ_CLOCKS_DIR (else the temporary directory); the JSON line carries the
+    median, maximum and the reasons seen."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvmlClocksEventReason*)
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, device):
         self.device = device
         self.proc = None
-        # raw samples: $DQ_CLOCKS_DIR if set, else the temporary directory (the JSON line carries the summary)
-        self.path = os.path.join(os.environ.get("DQ_CLOCKS_DIR", tempfile.gettempdir()),
-                                 f"clocks_bench_{os.getpid()}.csv")
+        self.thread = None
+        self.samples = []
+        d = os.environ.get("DQ_CLOCKS_DIR", tempfile.gettempdir())
+        self.path = os.path.join(d, f"clocks_bench_{os.getpid()}.csv")
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        pr = torch.cuda.get_device_properties(self.device)
+        bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+        try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _poll(self):
+        nv, h = self.nv, self.h
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), sm, mx, rs))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
 
     def __enter__(self):
+        import threading
+        try:
+            self.nv, self.h = self._handle()
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.thread = None
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
@@ -72,6 +113,9 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -79,11 +123,15 @@ class Clocks:
             except Exception:
                 self.proc.kill()
             self.f.close()
+        if self.samples:
+            with open(self.path.replace(".csv", "_nvml.csv"), "w") as f:
+                for t, sm, mx, rs in self.samples:
+                    f.write(f"{t:.4f},{sm},{mx},{rs:#x}\n")
 
-    def summary(self):
-        if not self.proc or not os.path.exists(self.path):
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    def _smi(self):
         sm, mx, reasons = [], [], set()
+        if not self.proc or not os.path.exists(self.path):
+            return sm, mx, reasons
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
@@ -97,10 +145,19 @@ class Clocks:
             for nm, v in zip(names, f[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        return sm, mx, reasons
+
+    def summary(self):
+        if self.samples:
+            sm = [x[1] for x in self.samples]
+            reasons = sorted(nm for nm, b in self.BITS.items() if any(x[3] & b for x in self.samples))
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(x[2] for x in self.samples),
+                    "reasons": reasons, "samples": len(sm), "source": "nvml every 5 ms"}
+        sm, mx, reasons = self._smi()
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi every 200 ms"}
 
 
 def build_system():
@@ -119,6 +176,21 @@ def make_prop(s, B, precision, seed, max_steps, pop_every=16, reorth=0):
     p.set_noise_params(np.full(s.n, w["sigma"]), np.full(s.n, w["tau"]))
     p.set_initial_state(s.bright_state())
     return p
+
+
+def plain_roofline(s, value):
+    """HBM roofline of the plain FP64 per-trajectory path: algorithmic bytes per trajectory-step
+    48 m N + 16 (m+1) N + 16 N + m (20 (z+1) N + 4 (N+1)) (complex128 vectors, the reference's
+    complex128 CSR values re-read by every SpMV) at the measured rate."""
+    w = WORKLOAD
+    m, n = w["m"], s.n
+    z = (s.nnz - s.n) / s.n
+    per = 48.0 * m * n + 16.0 * (m + 1) * n + 16.0 * n + m * (20.0 * (z + 1) * n + 4.0 * (n + 1))
+    peak, kind = _peaks()
+    gbs = value * per / 1e9
+    return {"bytes_per_traj_step": per, "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+            "peak_kind": kind, "note": "about 45 launches per trajectory-step, one trajectory at a time: "
+                                       "launch-latency bound, not HBM bound"}
 
 
 def spmm_bytes(s, B):
@@ -437,22 +509,47 @@ def secondary_legs(s, B, seed, tiling, value):
     plain_s = time.perf_counter() - t0
     pp.close()
     plain = 2 * plain_steps / plain_s
-    # ---- population error of the mixed path vs the FP64 oracle -------------
-    pop_err = None
+    # ---- population error of the mixed path: vs the FP64 oracle (a short run of a few
+    # trajectories) and vs the oracle-pinned batched FP64 path over the configuration's own
+    # 4096 steps for all 256 trajectories -------------------------------------------------
+    pop_err = {}
     try:
         from oracle import oracle as O
         O.build()
         rp, col, val, diag = s.off_diagonal()
         S = O.System(rp, col, val, diag, m=w["m"], dt=w["dt"], dot_mode=O.DOT_HERMITIAN, noise=O.NOISE_OU,
                      sigma=w["sigma"], tau=w["tau"], sigma_static=w["sigma_static"], seed=seed)
-        nT, nS = 4, 32
-        ref = S.run(nT, nS, s.bright_state(), pop_every=8, threads=os.cpu_count() or 1)
-        pm = make_prop(s, nT, dq.PREC_MIXED, seed, max_steps=nS, pop_every=8)
+        nT, nS = 4, 64
+        ref = S.run(nT, nS, s.bright_state(), pop_every=16, threads=os.cpu_count() or 1)
+        pm = make_prop(s, nT, dq.PREC_MIXED, seed, max_steps=nS, pop_every=16)
         pm.run(nS)
-        pop_err = float(np.abs(pm.populations() - ref["pops"]).max())
+        d = np.abs(pm.populations() - ref["pops"]).max()
+        pop_err["vs_oracle"] = {"abs": float(d), "rel": float(d / ref["pops"].max()), "trajectories": nT,
+                                "steps": nS}
         pm.close()
     except Exception as e:  # pragma: no cover - reported, not hidden
-        pop_err = f"unavailable: {e}"
+        pop_err["vs_oracle"] = f"unavailable: {e}"
+    T_long = 4096
+    res = {}
+    for prec in (dq.PREC_FP64, dq.PREC_MIXED):
+        pl = make_prop(s, B, prec, seed, max_steps=T_long, pop_every=16)
+        if prec == dq.PREC_MIXED:
+            pl.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
+                          tiling["staged"], tiling["groups"])
+        else:
+            pl.autotune()
+        pl.reset()
+        pl.run(T_long)
+        res[prec] = pl.populations()
+        pl.close()
+    d_abs = np.abs(res[dq.PREC_MIXED] - res[dq.PREC_FP64]).max(axis=1)
+    d_rel = d_abs / res[dq.PREC_FP64].max(axis=1)
+    recs = [k for k in (1, 4, 16, 64, 128, 256) if k < len(d_abs)]
+    pop_err["vs_fp64_ensemble"] = {
+        "abs": float(d_abs.max()), "rel": float(d_rel.max()), "trajectories": B, "steps": T_long,
+        "by_step": {str(16 * k): [float(d_abs[k]), float(d_rel[k])] for k in recs},
+        "note": "max over sites and records of |p_mixed - p_fp64| (rel: / max p of the record); the batched FP64 "
+                "path matches the oracle to 1e-10 (tests)"}
     # ---- the same step with full FP64 reorthogonalisation ------------------------
     pr = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=16, reorth=1)
     if tiling["staged"] in (2, 4):   # the fused forms cannot reorthogonalise between iterations
@@ -480,7 +577,8 @@ def secondary_legs(s, B, seed, tiling, value):
     cpu_v, cpu_sample = cpu_baseline_sample(s, os.cpu_count() or 1)
     return {
         "plain_fp64": {"value": plain, "unit": "traj-steps/s", "speedup_batched_mixed": value / plain,
-                       "sample": f"2 trajectories x {plain_steps} steps, dq_run_plain"},
+                       "sample": f"2 trajectories x {plain_steps} steps, dq_run_plain",
+                       "roofline": plain_roofline(s, plain)},
         "pop_err_vs_fp64_oracle": pop_err,
         "with_reorth": with_reorth,
         "adjoint": adjoint,
@@ -545,24 +643,46 @@ def run_ours(args, rank, world, local_rank):
     step_ms_eager = sum(v[0] * v[1] for v in prof.values()) / 2
     kernels_per_step = sum(v[1] for v in prof.values()) // 2
     # ---- end to end through the C ABI with host buffers --------------------
+    # each phase ends in a device synchronisation so the host clock attributes its work
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    p2 = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=K + 8)
+    marks = []
+
+    def mark(name):
+        torch.cuda.synchronize()
+        marks.append((name, time.perf_counter()))
+
+    mark("start")
+    p2 = dq.Propagator(s.n, m=w["m"], n_traj=B, dt=w["dt"], noise=dq.NOISE_OU, sigma_static=w["sigma_static"],
+                       seed=seed, dot=dq.DOT_HERMITIAN, precision=dq.PREC_MIXED, pop_every=16, max_steps=K + 8,
+                       device=DEVICE)
+    mark("create")
+    p2.set_system(s)
+    mark("csr_upload")
+    p2.set_noise_params(np.full(s.n, w["sigma"]), np.full(s.n, w["tau"]))
+    p2.set_initial_state(s.bright_state())
     p2.set_trajectory_offset(rank * B)
+    mark("noise_params_and_psi0")
     p2.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
                   tiling["staged"], tiling["groups"])
+    mark("workspace_and_block_format")
     p2.reset()
-    p2.run(K)
+    mark("reset")
+    p2.run(1)
+    mark("capture_and_first_step")
+    p2.run(K - 1)
+    mark("steps")
     if world > 1:
         # the ensemble's one exchange: observable sums all-reduced over the ranks (NCCL)
         from dynaquant_b200.ensemble import allreduce_observables
         allreduce_observables(p2, B * world)
+        mark("allreduce")
     pops = p2.populations()
     corr = p2.correlation()
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
+    mark("download")
+    e2e_s = marks[-1][1] - marks[0][1]
+    breakdown = {marks[i][0]: 1e3 * (marks[i][1] - marks[i - 1][1]) for i in range(1, len(marks))}
     p2.close()
     if world > 1:
         t = torch.tensor([e2e_s], device="cuda")
@@ -571,9 +691,11 @@ def run_ours(args, rank, world, local_rank):
     h2d = s.nnz * 12 + (s.n + 1) * 4 + s.n * 16 * 2 + s.n * 16
     d2h = pops.nbytes + corr.nbytes
     e2e = {"value": B * K * world / e2e_s, "unit": "traj-steps/s", "h2d_bytes_per_step": h2d / K,
-           "d2h_bytes_per_step": d2h / K,
-           "note": "whole job through the C ABI from host arrays: CSR/noise/psi0 upload, reset, K steps, "
-                   "(N > 1: all-reduce of the observable sums), populations + correlation download"}
+           "d2h_bytes_per_step": d2h / K, "breakdown_ms": breakdown,
+           "note": "whole job through the C ABI from host arrays: context, CSR/noise/psi0 upload, ensemble "
+                   "workspace, reset, K steps (the first one captures the step graph), (N > 1: all-reduce of the "
+                   "observable sums), populations + correlation download; host clock, a device sync after each "
+                   "phase"}
     if rank != 0:
         return
     traffic, traffic_src = measured_traffic(tiling["staged"])

@@ -154,6 +154,10 @@ class Propagator:
         self._check(self.L.dq_time_iteration(self.h, reps, C.byref(ms)))
         return ms.value
 
+    def debug_set_wait_cycles(self, cycles):
+        """Test hook: budget of the TMA-fed SpMM forms' barrier waits on this device (<= 0: default)."""
+        self._check(self.L.dq_debug_set_wait_cycles(self.h, int(cycles)))
+
     def autotune_raw(self, reps=5):
         ms = C.c_double()
         self._check(self.L.dq_autotune(self.h, reps, C.byref(ms)))

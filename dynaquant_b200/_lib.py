@@ -30,10 +30,36 @@ EXPORTS = [
     "dq_set_initial_state", "dq_set_initial_dipole", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_set_line_dressing", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
-    "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward", "dq_forward_shard", "dq_forward_reduced",
+    "dq_debug_set_wait_cycles", "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward", "dq_forward_shard", "dq_forward_reduced",
     "dq_group_create", "dq_group_destroy", "dq_group_last_error", "dq_group_run",
     "dq_write_populations", "dq_write_states", "dq_write_spectrum", "dq_write_spectrum_mean",
+    # include/dq_host.h
+    "dq_infile_defaults", "dq_infile_parse", "dq_infile_split_line", "dq_infile_run",
 ]
+
+HOST_PATH_MAX = 1024
+ENS_AVG_NONE, ENS_AVG_FIRST, ENS_AVG_CONTINUATION = 0, 1, 2
+SIM_CONST_HAM, SIM_HSR, SIM_KUBO_ANDERSON, SIM_ZZ_REAL_NOISE, SIM_ZZ_COMPLEX_NOISE = range(5)
+PROP_LANCZOS, PROP_TAYLOR_LANCZOS = 0, 1
+
+
+class InFile(C.Structure):
+    """struct dq_infile (include/dq_host.h)."""
+    _fields_ = [
+        ("dt", C.c_double), ("totalsteps", C.c_int), ("ensembleavgmode", C.c_int), ("ensembleruns", C.c_int),
+        ("m", C.c_int), ("ka_substeps", C.c_int), ("absorbspec", C.c_int), ("cdspec", C.c_int),
+        ("lineshapedress", C.c_int), ("gausswidth", C.c_double), ("dostatelooping", C.c_int),
+        ("stepsperloop", C.c_int), ("writeoutpops", C.c_int), ("printallpops", C.c_int),
+        ("writebinarypops", C.c_int), ("printpop", C.c_int * 10), ("print_partic", C.c_int),
+        ("writeoutstates", C.c_int), ("initstate", C.c_int), ("initfromfile", C.c_int), ("propmode", C.c_int),
+        ("simtype", C.c_int), ("staticdis", C.c_int), ("sigmastatdis", C.c_double), ("temperature", C.c_double),
+        ("debug_diags", C.c_int), ("tk_p", C.c_int), ("tk_m_aux", C.c_int),
+    ] + [(nm, C.c_char * HOST_PATH_MAX) for nm in (
+        "hamfile", "statefile", "outfile", "tkmatfile", "outfolder", "hsr_stddevfile", "ka_paramsfile",
+        "zz_specd_file", "dipolefile", "posfile", "initstatefile")] + [
+        ("precision", C.c_int), ("seed", C.c_uint64), ("pop_every", C.c_int),
+        ("n_assignments", C.c_int), ("n_unknown", C.c_int),
+    ]
 
 
 class Config(C.Structure):
@@ -119,6 +145,7 @@ def load(path: str = LIB_PATH):
     L.dq_get_tiling.argtypes = [vp, ip, ip, ip, ip, ip, ip]
     L.dq_autotune.argtypes = [vp, C.c_int, dp]
     L.dq_time_iteration.argtypes = [vp, C.c_int, dp]
+    L.dq_debug_set_wait_cycles.argtypes = [vp, C.c_int]
     L.dq_krylov_step_static.argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, C.c_int, C.c_double, C.c_double, C.c_int,
                                         C.c_int, vp, dp, C.c_char_p, C.c_int]
     L.dq_adjoint_setup.argtypes = [vp, C.c_int, C.c_int, C.c_double, dp, C.c_int]
@@ -136,9 +163,15 @@ def load(path: str = LIB_PATH):
     L.dq_write_states.argtypes = [vp, C.c_char_p]
     L.dq_write_spectrum.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_double]
     L.dq_write_spectrum_mean.argtypes = [C.POINTER(vp), C.c_int, dp, C.c_char_p, C.c_char_p]
+    inp = C.POINTER(InFile)
+    L.dq_infile_defaults.argtypes = [inp]
+    L.dq_infile_defaults.restype = None
+    L.dq_infile_parse.argtypes = [C.c_char_p, inp, C.c_char_p, C.c_int]
+    L.dq_infile_run.argtypes = [inp, C.c_char_p, C.c_int, C.c_char_p, C.c_int]
+    L.dq_infile_split_line.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_char_p, C.c_int]
     for name in EXPORTS:
         if name not in ("dq_config_default", "dq_destroy", "dq_last_error", "dq_get_stream", "dq_steps_done",
-                        "dq_group_destroy", "dq_group_last_error"):
+                        "dq_group_destroy", "dq_group_last_error", "dq_infile_defaults"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -539,9 +539,9 @@ static int mm_bucket(int m) { return m <= 8 ? 8 : m <= 16 ? 16 : 24; }
 
 template <typename Real, int MM>
 static cudaError_t grad_attr(int bytes) {
-    cudaError_t e = cudaFuncSetAttribute(k_adj_grad<Real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = raise_smem_limit(k_adj_grad<Real, MM>, bytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_adj_cls<Real, MM>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return raise_smem_limit(k_adj_cls<Real, MM>, bytes);
 }
 
 // Makes set k (segment s uses set s % 2) the one seg_V / seg_sc / seg_diag
@@ -607,8 +607,7 @@ template <typename Real>
 static cudaError_t set_attrs(int m) {
     const int CS = m * (2 * m + 2);
     const int smem = CS * kAdjTraj * (int)sizeof(typename R2<Real>::T);
-    cudaError_t e = cudaFuncSetAttribute(k_adj_small<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)pade_smem_bytes(2 * m));
+    cudaError_t e = raise_smem_limit(k_adj_small<Real>, (int)pade_smem_bytes(2 * m));
     if (e != cudaSuccess) return e;
     switch (mm_bucket(m)) {
         case 8: return grad_attr<Real, 8>(smem);

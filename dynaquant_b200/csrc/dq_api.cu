@@ -734,3 +734,9 @@ extern "C" dq_status dq_time_iteration(dq_ctx* c, int reps, double* ms) {
     c->ready = false;
     return DQ_OK;
 }
+
+extern "C" dq_status dq_debug_set_wait_cycles(dq_ctx* c, int cycles) {
+    DeviceScope dev_scope(c);
+    if (!c) return DQ_ERR_ARG;
+    return batched_set_wait_cycles(c, cycles);
+}

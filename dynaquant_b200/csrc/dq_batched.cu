@@ -42,6 +42,11 @@
 
 namespace dq {
 
+// Budget of the bounded mbarrier waits in SM cycles: kWaitCycles (about 2 s)
+// unless a test lowers it through dq_debug_set_wait_cycles to make the waits
+// run out on purpose.  The drains after a timeout always use kWaitCycles.
+__device__ long long g_dq_wait_cycles = kWaitCycles;
+
 // ---------------------------------------------------------------------------
 __global__ void k_traj_init_b(int n, int B, int traj0, uint64_t seed, const double* __restrict__ h0,
                               const double* __restrict__ static_eps, double sigma_static,
@@ -767,13 +772,15 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
         // them, later steps for the one block that is new)
         const int bl = s + 2 * hb;
         int failed = -1;
+        const long long budget = g_dq_wait_cycles;
         for (int q = (s == 0 ? 0 : bl); q <= bl; ++q)
-            if (failed < 0 && !mbar_wait_bounded(&bars[q % NB], (uint32_t)((q / NB) & 1))) failed = q;
+            if (failed < 0 && !mbar_wait_bounded(&bars[q % NB], (uint32_t)((q / NB) & 1), budget)) failed = q;
         if (__syncthreads_or(failed >= 0)) {
             if (threadIdx.x == 0) {
                 atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
-                // let every copy still in flight land (bounded) before leaving
-                for (int q = (failed >= 0 ? failed : bl) + 1; q <= issued; ++q)
+                // let every copy still in flight land (bounded) before leaving:
+                // from the box this thread gave up on, or past the ones it saw land
+                for (int q = (failed >= 0 ? failed : bl + 1); q <= issued; ++q)
                     mbar_wait_bounded(&bars[q % NB], (uint32_t)((q / NB) & 1));
             }
             return;
@@ -960,12 +967,16 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
             tma_load_2d(slot(y), &tmap, &bars[(s + 1) & 1], xc, y);
         }
         if (s + 1 < nsteps) issued = s + 1;
-        const bool ok = mbar_wait_bounded(&bars[s & 1], (uint32_t)((s >> 1) & 1));
+        const bool ok = mbar_wait_bounded(&bars[s & 1], (uint32_t)((s >> 1) & 1), g_dq_wait_cycles);
         if (__syncthreads_or(!ok)) {
-            // a copy never completed: flag it, give the copy in flight a
-            // bounded chance to land, and leave without reducing
-            if (threadIdx.x == 0) atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
-            if (issued > s) mbar_wait_bounded(&bars[issued & 1], (uint32_t)((issued >> 1) & 1));
+            // a copy never completed: flag it, give the copies in flight (this
+            // step's and the next one's) a bounded chance to land, and leave
+            // without reducing
+            if (threadIdx.x == 0) {
+                atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
+                mbar_wait_bounded(&bars[s & 1], (uint32_t)((s >> 1) & 1));
+                if (issued > s) mbar_wait_bounded(&bars[issued & 1], (uint32_t)((issued >> 1) & 1));
+            }
             return;
         }
         const int k = a / R + rl;
@@ -1157,11 +1168,12 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
 #pragma unroll
             for (int t = 0; t < TPT; ++t) dd[i][t] = (has_blk && row < r1) ? __ldg(d + base + t) : Real(0);
         }
-        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1));
+        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1), g_dq_wait_cycles);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
-                for (int q = p + 1; q <= issued; ++q) mbar_wait_bounded(&bars[q % D], (uint32_t)((q / D) & 1));
+                // box p itself may still be in flight: drain p .. issued
+                for (int q = p; q <= issued; ++q) mbar_wait_bounded(&bars[q % D], (uint32_t)((q / D) & 1));
             }
             return;
         }
@@ -1395,11 +1407,12 @@ __global__ void __launch_bounds__(kFwThreads, 1) k_lanczos_fw(int n, int B, int 
             pe = __ldg(bptr + k + 1);
             nxt = lane < pe - pb ? __ldg(rec + pb + lane) : zero4;
         }
-        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1));
+        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1), g_dq_wait_cycles);
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
-                for (int q = p + 1; q <= issued; ++q) mbar_wait_bounded(&bars[q % D], (uint32_t)((q / D) & 1));
+                // box p itself may still be in flight: drain p .. issued
+                for (int q = p; q <= issued; ++q) mbar_wait_bounded(&bars[q % D], (uint32_t)((q / D) & 1));
             }
             return;
         }
@@ -2232,12 +2245,11 @@ static dq_status build_fmaps(dq_ctx* c, int tc, int sr) {
 template <typename Real, int TPT, int R>
 static cudaError_t win_attr(int bytes) {
     cudaError_t e = cudaSuccess;
-    e = cudaFuncSetAttribute(k_spmm_win<Real, TPT, R, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    e = raise_smem_limit(k_spmm_win<Real, TPT, R, false, true>, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_spmm_win<Real, TPT, R, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = raise_smem_limit(k_spmm_win<Real, TPT, R, true, true>, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_spmm_win<Real, TPT, R, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 bytes);
+        e = raise_smem_limit(k_spmm_win<Real, TPT, R, false, false>, bytes);
     return e;
 }
 
@@ -2257,13 +2269,13 @@ constexpr size_t kWinSmemMax = 200 * 1024;
 // dynamic shared memory limit of every ring SpMM instance for R rows per block
 template <int LT, int R>
 static cudaError_t ring_attr_r(int bytes) {
-    cudaError_t e = cudaFuncSetAttribute(k_spmm_ring<R, true, true, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = raise_smem_limit(k_spmm_ring<R, true, true, LT>, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_spmm_ring<R, true, false, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = raise_smem_limit(k_spmm_ring<R, true, false, LT>, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_spmm_ring<R, false, true, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = raise_smem_limit(k_spmm_ring<R, false, true, LT>, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_spmm_ring<R, false, false, LT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = raise_smem_limit(k_spmm_ring<R, false, false, LT>, bytes);
     return e;
 }
 
@@ -2274,17 +2286,13 @@ static cudaError_t ring_attr(int R, int bytes) {
 
 template <typename Real, int TPT, int R>
 static cudaError_t fused_attr(int bytes) {
-    cudaError_t e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, false, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = raise_smem_limit(k_lanczos_fused<Real, TPT, R, false, false>, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, true, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = raise_smem_limit(k_lanczos_fused<Real, TPT, R, true, false>, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, false, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = raise_smem_limit(k_lanczos_fused<Real, TPT, R, false, true>, bytes);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_lanczos_fused<Real, TPT, R, true, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = raise_smem_limit(k_lanczos_fused<Real, TPT, R, true, true>, bytes);
     return e;
 }
 
@@ -2307,7 +2315,7 @@ static cudaError_t fw_attr(int bytes) {
                       : v == 1 ? (const void*)k_lanczos_fw<TPT, R, true, false>
                       : v == 2 ? (const void*)k_lanczos_fw<TPT, R, false, true>
                                : (const void*)k_lanczos_fw<TPT, R, true, true>;
-        e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        e = raise_smem_limit(f, bytes);
     }
     return e;
 }
@@ -2636,8 +2644,8 @@ static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed) {
         bs->s.cdone = bs->s.mtraj + B;
         bs->s.mchunk = bs->s.cdone + B;
     }
-    DQ_CU(cudaFuncSetAttribute(k_pade_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pade_smem_bytes(m + 2)));
-    DQ_CU(cudaFuncSetAttribute(k_mcheck_b, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pade_smem_bytes(m + 2)));
+    DQ_CU(raise_smem_limit(k_pade_b, (int)pade_smem_bytes(m + 2)));
+    DQ_CU(raise_smem_limit(k_mcheck_b, (int)pade_smem_bytes(m + 2)));
     // default tiling (dq_autotune refines it)
     int tpt = bs->mixed ? 2 : 1;
     int tc = 16;
@@ -3194,6 +3202,12 @@ dq_status batched_collect_corr(dq_ctx* c) {
     k_corr_collect<<<std::max(1, std::min(bs->sms, (np + 255) / 256)), 256, 0, c->stream>>>(np, bs->chunks, bs->s.corr,
                                                                                               c->d_corr);
     return check_cuda(c, cudaGetLastError(), "corr collect");
+}
+
+// dq_debug_set_wait_cycles: the budget every bounded wait of this device reads
+dq_status batched_set_wait_cycles(dq_ctx* c, int cycles) {
+    const long long v = cycles > 0 ? (long long)cycles : kWaitCycles;
+    return check_cuda(c, cudaMemcpyToSymbol(g_dq_wait_cycles, &v, sizeof(v)), "wait budget");
 }
 
 }  // namespace dq

@@ -61,4 +61,17 @@ __device__ __forceinline__ bool last_block_ticket(unsigned int* counter, unsigne
     return is_last;
 }
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` and never
+// lowers it.  The limit is one attribute of the function for the whole device,
+// shared by every context and call there, so a context with a smaller Krylov
+// dimension or window must not shrink what another one launches with.
+template <typename F>
+inline cudaError_t raise_smem_limit(F* f, int bytes) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return e;
+    if (a.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 }  // namespace dq

@@ -182,6 +182,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
 void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged, int* groups);
 dq_status batched_invalidate_blocks(dq_ctx* c);
 dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms);
+dq_status batched_set_wait_cycles(dq_ctx* c, int cycles);
 void batched_noise_arrays(dq_ctx* c, const double** eps, const double** deps);
 // kernels of dq_batched.cu also launched by the Taylor-Krylov ensemble
 __global__ void k_traj_init_b(int n, int B, int traj0, uint64_t seed, const double* h0, const double* static_eps,

@@ -22,6 +22,7 @@
 
 #include "dq_internal.h"
 #include "dq_rng.cuh"
+#include <cuda.h>
 
 namespace dq {
 
@@ -447,10 +448,13 @@ dq_status plain_alloc(dq_ctx* c) {
     DQ_CU(cudaMalloc(&c->d_ps, sizeof(PlainScalars)));
     DQ_CU(cudaMemsetAsync(c->d_ps, 0, sizeof(PlainScalars), c->stream));
     DQ_CU(cudaMemsetAsync(c->d_Q, 0, sizeof(cd) * (size_t)n * (m + 2), c->stream));
-    size_t smem = pade_smem_bytes(m + 2);
-    DQ_CU(cudaFuncSetAttribute(k_pade_plain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    DQ_CU(cudaFuncSetAttribute(k_pade_tk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)pade_smem_bytes(kMaxL)));
+    // the limit is a per-function attribute shared by every context (and by
+    // dq_krylov_step_static) on the device, so it is always set to the largest
+    // Krylov dimension: a later context or call with a larger m never meets a
+    // limit lowered by one with a smaller m
+    (void)m;
+    DQ_CU(raise_smem_limit(k_pade_plain, (int)pade_smem_bytes(kMaxL)));
+    DQ_CU(raise_smem_limit(k_pade_tk, (int)pade_smem_bytes(kMaxL)));
     return DQ_OK;
 }
 
@@ -598,7 +602,9 @@ dq_status plain_observe_initial(dq_ctx* c) {
 // first call on a device the entry point, with that device current, asks the
 // runtime for the array's device address (cudaGetSymbolAddress) and raises
 // the Padé kernel's shared-memory limit; that first call should come before
-// any stream capture.  Every call on a device shares the one array and leaves
+// any stream capture.  The address is kept per device together with the
+// driver context it belongs to and looked up again when that context changed
+// (after a cudaDeviceReset).  Every call on a device shares the one array and leaves
 // the last call's contents in it (each call clears what must start at zero),
 // so calls that overlap on the GPU (different streams, or host threads
 // without ordering) race and must be serialised by the caller.
@@ -614,10 +620,32 @@ namespace {
 struct StaticScratch {
     bool init = false;
     unsigned char* ptr = nullptr;
+    CUcontext ctx = nullptr;   // the context the address belongs to
 };
 constexpr int kMaxDevices = 64;
 StaticScratch g_static_scratch[kMaxDevices];
 std::mutex g_static_mu;
+
+// The current driver context (the device's primary context after the
+// runtime's set-up): a cudaDeviceReset replaces it, and with it the module
+// and the array's device address, so a cached address is only valid for the
+// context it was taken in.
+CUcontext current_context() {
+    using Fn = CUresult (*)(CUcontext*);
+    static Fn fn = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<Fn>(p);
+        looked = true;
+    }
+    CUcontext c = nullptr;
+    if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return c;
+}
 
 void write_err(char* buf, int len, const char* msg) {
     if (buf && len > 0) snprintf(buf, (size_t)len, "%s", msg);
@@ -629,14 +657,20 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 namespace dq {
 
-// clears what a step expects at zero and starts the recurrence at q_1 = psi_in
+// clears what a step expects at zero and starts the recurrence at q_1 =
+// psi_in.  The status word is left as it is: a device error of a call that
+// did not read it back stays recorded until a call with err_est reports it.
 __global__ void k_static_begin(PlainScalars* ps) {
     if (threadIdx.x == 0) {
         ps->sc[1] = 1.0;
         ps->beta[0] = cmk(0.0, 0.0);
-        ps->status = 0;
         for (int k = 0; k < 4; ++k) ps->ticket[k] = 0;
     }
+}
+
+// zeroes the status word once a call has read it back
+__global__ void k_static_clear_status(PlainScalars* ps) {
+    if (threadIdx.x == 0) ps->status = 0;
 }
 
 }  // namespace dq
@@ -676,17 +710,20 @@ extern "C" dq_status dq_krylov_step_static(int n, const int* rowptr, const int* 
     {
         std::lock_guard<std::mutex> lock(g_static_mu);
         StaticScratch& sc = g_static_scratch[dev];
-        if (!sc.init) {
+        // NULL on a thread the runtime has not yet bound to the device's context:
+        // then the address is simply looked up again below
+        CUcontext ctx = current_context();
+        if (!sc.init || ctx != sc.ctx) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_dq_static_scratch);
             if (e == cudaSuccess)
-                e = cudaFuncSetAttribute(k_pade_plain, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)pade_smem_bytes(kMaxL));
+                e = raise_smem_limit(k_pade_plain, (int)pade_smem_bytes(kMaxL));
             if (e != cudaSuccess) {
                 write_err(errbuf, errbuf_len, cudaGetErrorString(e));
                 return DQ_ERR_CUDA;
             }
             sc.ptr = static_cast<unsigned char*>(p);
+            sc.ctx = current_context();   // bound by the runtime call above
             sc.init = true;
         }
         base = sc.ptr;
@@ -735,7 +772,10 @@ extern "C" dq_status dq_krylov_step_static(int n, const int* rowptr, const int* 
         }
         *err_est = hv[0];
         if (status) {
-            write_err(errbuf, errbuf_len, "krylov_step_static: device reported an error (breakdown/NaN/Padé)");
+            k_static_clear_status<<<1, 32, 0, st>>>(ps);
+            write_err(errbuf, errbuf_len,
+                      "krylov_step_static: device reported an error (breakdown/NaN/Padé) in this call or in an "
+                      "earlier one that passed err_est = NULL");
             return status;
         }
     }

@@ -412,7 +412,7 @@ static dq_status tk_ensemble_alloc(dq_ctx* c) {
     DQ_CU(cudaMemsetAsync(t->s.ticket, 0, sizeof(unsigned int) * 8, c->stream));
     DQ_CU(cudaMalloc(&t->s.status, sizeof(int)));
     DQ_CU(cudaMemsetAsync(t->s.status, 0, sizeof(int), c->stream));
-    DQ_CU(cudaFuncSetAttribute(k_tke_pade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pade_smem_bytes(kMaxL)));
+    DQ_CU(raise_smem_limit(k_tke_pade, (int)pade_smem_bytes(kMaxL)));
     return DQ_OK;
 }
 

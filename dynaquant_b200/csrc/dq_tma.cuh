@@ -1,7 +1,9 @@
 // dq_tma.cuh — TMA tensor loads and mbarrier waits (inline PTX, sm_100a).
 //
-// Every wait is bounded: after kWaitCycles SM cycles the caller gets false
-// and must record DQ_ERR_TIMEOUT and leave; nothing here spins forever.
+// Every wait is bounded: after its budget (kWaitCycles SM cycles unless a
+// test lowered it) the caller gets false and must record DQ_ERR_TIMEOUT, let
+// its own copies in flight land (waits with the full kWaitCycles budget) and
+// leave; nothing here spins forever.
 // No multicast form is used: every load reads this GPU's own memory into
 // the issuing CTA's shared memory.
 #pragma once
@@ -42,11 +44,35 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Non-blocking test of the phase with the given parity.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Budgets below this many cycles are shorter than one suspended try_wait may
+// take, so they poll with test_wait instead and end on the cycle count.
+constexpr long long kPollBudget = 1LL << 20;
+
+// Bounded wait for the phase with the given parity; false once `budget` SM
+// cycles have passed without it.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long budget = kWaitCycles) {
     const long long t0 = clock64();
+    if (budget < kPollBudget) {
+        while (!mbar_test_wait(bar, parity)) {
+            if (clock64() - t0 > budget) return false;
+        }
+        return true;
+    }
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > budget) return false;
     }
     return true;
 }

@@ -12,8 +12,8 @@ its parsing is in systemClass.cu and sparseMatrixClasses.cu):
   returns (sigma, tau) for set_noise_params.
 * read_hsr_stddev -- ``hsr_stddevfile``: one standard deviation per line (systemClass.cu:912-975).
 * read_initial_state -- ``initstatefile``: ``BASE_ZERO``/``BASE_ONE``, a comment line, then
-  ``site amplitude`` lines up to an optional ``END``; normalised as the reference does
-  (systemClass.cu:1385-1481).
+  ``site amplitude`` lines up to an optional ``END``; amplitudes rounded to float as the
+  reference reads them, then normalised as the reference does (systemClass.cu:1385-1481).
 * read_vectors3 -- ``dipolefile`` / ``posfile``: three columns per site (spectraClass.cu:300-430).
 * read_spectral_density -- ``zz_specd_file``: ``dOmega nOsc`` then ``omega J`` lines
   (systemClass.cu:1077-1207); returns (d_omega, omega, J) for set_zz_spectral_density.
@@ -99,7 +99,8 @@ def read_initial_state(path, n):
             i = int(p[0]) - off
             if not 0 <= i < n:
                 raise ValueError(f"{path}: site {i} outside 0..{n - 1}")
-            psi[i] = float(p[1])   # a later line for the same site replaces it, as in the reference
+            # the reference reads the amplitude into a float; a later line for the same site replaces it
+            psi[i] = float(np.float32(p[1]))
     nrm = np.linalg.norm(psi)
     if nrm == 0.0:
         raise ValueError(f"{path}: the state is zero")

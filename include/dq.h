@@ -204,7 +204,9 @@ DQ_API dq_status dq_run_plain(dq_ctx *ctx, int n_steps);
  * step psi_out = exp(-i H dt/hbar) psi_in by m-step Lanczos + Padé + renorm
  * for H = diag + offdiag, where rowptr/col/val is the OFF-DIAGONAL CSR and
  * diag this step's diagonal; every pointer is DEVICE memory owned by the
- * caller (psi_in and psi_out may not alias).  Work is ordered on `stream`
+ * caller (psi_in and psi_out may not alias).  psi_in must have unit norm: it
+ * is the first Krylov vector as given, as dq_prop_step and the reference's
+ * step take it (psi_out is renormalised to unit norm).  Work is ordered on `stream`
  * (a cudaStream_t, NULL = legacy default stream).  Scratch is one static
  * 16 MiB device array per GPU (held until process exit), so it accepts
  * (m+3)*n*16 bytes + ~70 KB <= 16 MiB (about 55,000 sites at m = 16) and
@@ -212,8 +214,12 @@ DQ_API dq_status dq_run_plain(dq_ctx *ctx, int n_steps);
  * on a device looks up the array's device address and should come before
  * any stream capture.  All calls on a device share the array (each clears
  * what must start at zero): calls that overlap on the GPU race.  If err_est
- * is non-NULL the call synchronises `stream` and writes the EXPOKIT error
- * estimate.  errbuf (may be NULL) receives a message on failure. */
+ * is non-NULL the call synchronises `stream`, writes the EXPOKIT error
+ * estimate and returns the device status (breakdown, non-finite value, Padé
+ * scaling).  With err_est == NULL the call does not synchronise and cannot
+ * report a device error itself: the error stays recorded in the array and the
+ * next call on the device that passes err_est returns it (and clears it).
+ * errbuf (may be NULL) receives a message on failure. */
 DQ_API dq_status dq_krylov_step_static(int n, const int *rowptr, const int *col, const double *val,
                                        const double *diag, const dq_cdouble *psi_in, dq_cdouble *psi_out, int m,
                                        double dt, double hbar, int dot_mode, int norm_mode, void *stream,
@@ -257,6 +263,14 @@ DQ_API dq_status dq_autotune(dq_ctx *ctx, int reps, double *best_ms);
 /* Mean device time of one Lanczos iteration (SpMM + axpy) under the current
  * tiling, over reps launches; the ensemble restarts at the next dq_run. */
 DQ_API dq_status dq_time_iteration(dq_ctx *ctx, int reps, double *ms);
+/* Test hook, no reference counterpart: sets the budget (SM cycles) of the
+ * bounded shared-memory barrier waits of the TMA-fed SpMM forms on the
+ * context's device; cycles <= 0 restores the default (about 2 s).  A tiny
+ * budget makes those waits give up on purpose: the kernels then record
+ * DQ_ERR_TIMEOUT, let their own copies in flight land (with the default
+ * budget) and return, and dq_run reports the status.  It applies to every
+ * context on the device until changed again. */
+DQ_API dq_status dq_debug_set_wait_cycles(dq_ctx *ctx, int cycles);
 
 /* Kernel kinds of one ensemble step, for dq_profile_step. */
 enum {

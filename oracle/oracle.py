@@ -22,9 +22,29 @@ P_OU, P_GAUSS, P_OU_INIT, P_STATIC, P_ZZPHASE = 1, 2, 3, 4, 5
 
 
 def build() -> str:
-    """Compile liboracle.so with its Makefile (no-op when up to date)."""
+    """Compile liboracle.so with its Makefile (no-op when up to date), and, where the
+    reference's sources are present, its input-line functions into _ref/."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=False)
     return _LIB
+
+
+REF_INFILE = os.path.join(_HERE, "_ref", "libref_infile.so")
+
+
+def ref_parse_line(line: str):
+    """The reference's own stringSplit + stringTrim on one input line (cppUtility.cpp:82-106):
+    (key, value), None for a line without '=' or a key with '!', or "throws" where the
+    reference's substr would throw.  Needs _ref/libref_infile.so."""
+    L = C.CDLL(REF_INFILE)
+    k = C.create_string_buffer(4096)
+    v = C.create_string_buffer(4096)
+    rc = L.ref_parse_line(line.encode(), k, len(k), v, len(v))
+    if rc == -1:
+        return "throws"
+    if rc != 1:
+        return None
+    return k.value.decode(), v.value.decode()
 
 
 class _System(C.Structure):

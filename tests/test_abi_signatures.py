@@ -13,7 +13,8 @@ from dynaquant_b200 import _lib  # noqa: E402
 
 
 def _declarations():
-    text = open(os.path.join(ROOT, "include", "dq.h")).read()
+    inc = os.path.join(ROOT, "include")
+    text = "".join(open(os.path.join(inc, h)).read() for h in sorted(os.listdir(inc)) if h.endswith(".h"))
     text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
     out = {}
     for m in re.finditer(r"DQ_API\s+([\w\s\*]+?)\b(dq_\w+)\s*\(([^)]*)\)\s*;", text):
