@@ -210,7 +210,9 @@ SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", None),
               5: ("k_spmm_blk, 512-thread CTAs (L1 gathers + alpha, minus beta q_{j-1})",
                   "k_spmm_blk512_tube60x500.md"),
               6: ("k_spmm_ring (TMA ring gathers + alpha)", "k_spmm_ring_tube60x500.md"),
-              7: ("k_spmm_ring, 4 trajectories per lane (TMA ring gathers + alpha)", None)}
+              7: ("k_spmm_ring, 4 trajectories per lane (TMA ring gathers + alpha)", None),
+              8: ("k_lanczos_p (one launch per iteration: gathers p_j, writes q_j and p_{j+1}, alpha and beta)",
+                  None)}
 
 
 def measured_traffic(staged):
@@ -552,7 +554,7 @@ def secondary_legs(s, B, seed, tiling, value):
                 "path matches the oracle to 1e-10 (tests)"}
     # ---- the same step with full FP64 reorthogonalisation ------------------------
     pr = make_prop(s, B, dq.PREC_MIXED, seed, max_steps=16, reorth=1)
-    if tiling["staged"] in (2, 4):   # the fused forms cannot reorthogonalise between iterations
+    if tiling["staged"] in (2, 4, 8):   # the fused forms cannot reorthogonalise between iterations
         pr.set_tiling(32, 2, 2, 3, 0, 1)
     else:
         pr.set_tiling(tiling["traj_chunk"], tiling["vec"], tiling["ctas_per_sm"], tiling["rows_per_block"],
@@ -629,7 +631,7 @@ def run_ours(args, rank, world, local_rank):
     p.close()
     peak, peak_kind = _peaks()
     spmm_ms = prof["spmm_alpha"][0]
-    if tiling["staged"] in (2, 4):
+    if tiling["staged"] in (2, 4, 8):
         # fused forms: the dominant launch is the whole iteration (reads w, r_j, r_{j-1}, d and the
         # CSR; writes r_{j+1} and w)
         spmm_ms = prof["fused_iter"][0]
@@ -639,6 +641,9 @@ def run_ours(args, rank, world, local_rank):
         bytes_spmm += 8.0 * s.n * B * (w["m"] - 1) / w["m"]
     if tiling["staged"] in (2, 4):
         bytes_spmm += 24.0 * s.n * B   # + r_j, r_{j-1} reads and the r_{j+1} write
+    if tiling["staged"] == 8:
+        # p-form launch j (2 < j <= m): reads p_j, q_{j-1}, q_{j-2} and d, writes q_j and p_{j+1}
+        bytes_spmm = 44.0 * s.n * B + 8.0 * (s.nnz - s.n) + 4.0 * (s.n + 1)
     achieved = bytes_spmm / (spmm_ms / 1e3) / 1e9
     step_ms_eager = sum(v[0] * v[1] for v in prof.values()) / 2
     kernels_per_step = sum(v[1] for v in prof.values()) // 2

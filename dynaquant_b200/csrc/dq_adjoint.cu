@@ -161,8 +161,8 @@ __global__ void k_lambda_init_norm(int n, int B, const cd* __restrict__ psi0, co
 //   M[a][b]  = tau |lam| scW_a N_ab scV_b                  (a, b = 1..m)
 //   P[a][c]  = sum_b M'_ab K_bc, H q^V_b = sum_c K_bc r^V_c (c = 1..m+1)
 //   yw[a]    = |lam| conj(E_a0) scW_a
-// with M'_ab = tau |lam| scW_a N_ab and K from r_{b+1} = H q_b - alpha_b q_b
-// - beta_{b-1} q_{b-1} (the axpy's own relation, complex alpha).
+// with M'_ab = tau |lam| scW_a N_ab and K from beta_b q_{b+1} = H q_b -
+// alpha_b q_b - beta_{b-1} q_{b-1} (complex alpha), q_c = sc_c r_c.
 template <typename Real>
 __global__ void k_adj_small(int m, int B, double tau_im, BatchedScalars SV, BatchedScalars SW,
                             typename R2<Real>::T* __restrict__ coef) {
@@ -213,7 +213,9 @@ __global__ void k_adj_small(int m, int B, double tau_im, BatchedScalars SV, Batc
     for (int e = threadIdx.x; e < m * (m + 1); e += blockDim.x) {
         const int a = e / (m + 1) + 1, cc = e % (m + 1) + 1;
         cd p = cmk(0.0, 0.0);
-        if (cc - 1 >= 1) p = cadd(p, mp(a, cc - 1));
+        // H q_{c-1} holds r_c with weight beta_{c-1} sc_c (1 when the slab keeps
+        // the unnormalised residual, beta_{c-1} when it keeps q_c itself)
+        if (cc - 1 >= 1) p = cadd(p, cscale(mp(a, cc - 1), SV.beta[(size_t)(cc - 1) * B + b] * scv(cc)));
         if (cc <= m) {
             const size_t k = (size_t)cc * B + b;
             p = cadd(p, cmul(mp(a, cc), cmk(SV.alpha[2 * k] * scv(cc), SV.alpha[2 * k + 1] * scv(cc))));

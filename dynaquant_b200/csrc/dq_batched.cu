@@ -518,6 +518,260 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
     }
 }
 
+// K per-trajectory real sums of one block: summed over the block's row lanes
+// in shared memory (one quantity at a time through `sm`, blockDim.x * TPT
+// doubles), stored as partial[chunk][block][K][TC]; one ticket per chunk, and
+// the last block adds the blocks' partials in a fixed order (deterministic).
+// Returns true in that block, with the totals in red_out[q * TC + t].
+template <int K, int TPT>
+__device__ __forceinline__ bool chunk_reduce_multi(const double (&v)[K][TPT], int TC, double* partial,
+                                                   unsigned int* ticket, double* red_out, int chunk, double* sm) {
+    const int TPR = TC / TPT;
+    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int RPC = blockDim.x / TPR;
+    double* mypart = partial + ((size_t)chunk * gridDim.x + blockIdx.x) * K * TC;
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) sm[rl * TC + tr * TPT + t] = v[q][t];
+        __syncthreads();
+        if (threadIdx.x < TC) {
+            double s = 0.0;
+            for (int r = 0; r < RPC; ++r) s += sm[r * TC + threadIdx.x];
+            mypart[q * TC + threadIdx.x] = s;
+        }
+        __syncthreads();
+    }
+    const bool last = last_block_ticket(ticket + chunk, gridDim.x);
+    if (last) {
+        const int per = blockDim.x / TC;
+        const int tl = threadIdx.x % TC, part = threadIdx.x / TC;
+        const double* base = partial + (size_t)chunk * gridDim.x * K * TC;
+#pragma unroll
+        for (int q = 0; q < K; ++q) {
+            double s = 0.0;
+            for (unsigned int g = part; g < gridDim.x; g += per) s += __ldcg(base + ((size_t)g * K + q) * TC + tl);
+            sm[part * TC + tl] = s;
+            __syncthreads();
+            if (threadIdx.x < TC) {
+                double a = 0.0;
+                for (int p = 0; p < per; ++p) a += sm[p * TC + threadIdx.x];
+                red_out[q * TC + threadIdx.x] = a;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) ticket[chunk] = 0;
+        __syncthreads();
+    }
+    return last;
+}
+
+// One Lanczos iteration in one launch without the axpy pass (staged = 8).
+// Instead of the residual, iteration j - 1 leaves p_j = H q_{j-1} -
+// beta_{j-2} q_{j-2} in HBM together with alpha_{j-1} = <q_{j-1}, p_j> and
+// beta_{j-1} = ||p_j - alpha_{j-1} q_{j-1}||, the latter from three sums of
+// the same pass (||p_j||^2 - 2 Re(conj(alpha) <q, p_j>) + |alpha|^2 ||q||^2,
+// all FP64 over the stored values).  Iteration j gathers only p_j:
+//   q_j     = (p_j - alpha_{j-1} q_{j-1}) / beta_{j-1}                 (stored, unit norm)
+//   H q_j   = (H p_j - alpha_{j-1} (p_j + beta_{j-2} q_{j-2})) / beta_{j-1}
+//             (H q_{j-1} = p_j + beta_{j-2} q_{j-2} by the recurrence)
+//   p_{j+1} = H q_j - beta_{j-1} q_{j-1}                                 (stored)
+// and sums <q_j, p_{j+1}> (the alpha form), the Hermitian <q_j, p_{j+1}>,
+// ||p_{j+1}||^2 and ||q_j||^2 for alpha_j and beta_j: the ordering of
+// Paige's variant (lanczosClass.cu:405-526 in exact arithmetic).  Per
+// site-trajectory it moves p_j, q_{j-1}, q_{j-2}, the diagonal, q_j and
+// p_{j+1} (44 B in complex64) where the SpMM + axpy pair moves 52 B, in one
+// launch instead of two.  kMode 0 (j = 1): gathers psi = r_1 (q_1 = sc_1 r_1)
+// and writes p_2 only; kMode 2 (j = m + 1): writes q_{m+1} and gives
+// ||H q_{m+1}|| (nav) instead of p_{m+2}.  The slabs q_j, j >= 2, are stored
+// normalised (sc_j = 1).  Gathers go through L1 over row blocks of R rows as
+// in k_spmm_blk; the per-row arithmetic after the gather runs in FP64.
+template <typename Real, int TPT, int R, bool kBilinear, int kMode, int NT>
+__global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc, int nb, int j,
+                                                  const int* __restrict__ bptr, const int* __restrict__ bcol,
+                                                  const Real* __restrict__ bcoef, const Real* __restrict__ d,
+                                                  const Real* __restrict__ pin, const Real* __restrict__ qm1,
+                                                  const Real* __restrict__ qm2, Real* __restrict__ qout,
+                                                  Real* __restrict__ pout, BatchedScalars S, int nch) {
+    constexpr bool kFirst = kMode == 0, kLast = kMode == 2;
+    constexpr int K = kLast ? 1 : (kBilinear ? 6 : 4);
+    const int TPR = TC / TPT;
+    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int RPC = blockDim.x / TPR;
+    const int chunk = blockIdx.y;
+    const int b0 = chunk * TC + tr * TPT;
+    const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
+    // per-trajectory coefficients of this iteration, in shared memory (read
+    // once per row after the gathers, so they hold no registers across them):
+    // [0] alpha_r, [1] alpha_i, [2] 1/beta_{j-1}, [3] beta_{j-1}, [4] sc_{j-1}
+    // (sc_1 for j = 1), [5], [6] alpha_{j-1} beta_{j-2} sc_{j-2} (the q_{j-2}
+    // term of H q_j)
+    __shared__ double cf[7][kMaxTC];
+    for (int t = threadIdx.x; t < TC; t += blockDim.x) {
+        const int b = chunk * TC + t;
+        double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if constexpr (kFirst) {
+            v[4] = S.sc[(size_t)B + b];
+        } else {
+            const size_t km = (size_t)(j - 1) * B + b;
+            v[0] = S.alpha[2 * km];
+            v[1] = S.alpha[2 * km + 1];
+            v[3] = S.beta[km];
+            v[2] = v[3] > 0.0 ? 1.0 / v[3] : 0.0;
+            v[4] = S.sc[km];
+            if (j >= 3) {
+                const size_t k2 = (size_t)(j - 2) * B + b;
+                v[5] = v[0] * S.beta[k2] * S.sc[k2];
+                v[6] = v[1] * S.beta[k2] * S.sc[k2];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 7; ++q) cf[q][t] = v[q];
+    }
+    __syncthreads();
+    double sum[K][TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t)
+#pragma unroll
+        for (int q = 0; q < K; ++q) sum[q][t] = 0.0;
+    constexpr bool kPk = sizeof(Real) == 4 && R <= 3;
+    const float4* rec = reinterpret_cast<const float4*>(bcoef);
+    BlkPre P;
+    if constexpr (kPk) blk_prefetch(P, k0 + rl < k1, k0 + rl, bptr, rec);
+    for (int k = k0 + rl; k < k1; k += RPC) {
+        const int row0 = k * R;
+        BlkPre cur;
+        if constexpr (kPk) {
+            cur = P;
+            blk_prefetch(P, k + RPC < k1, k + RPC, bptr, rec);
+        }
+        // the diagonal is loaded before the gathers; the rows of q_{j-1} and
+        // q_{j-2} are only prefetched into L2 then (no registers held across
+        // the gather loop) and read after it together with the block's own
+        // rows of the gathered vector, which its neighbours' gathers have
+        // just brought into L1
+        CV<Real, TPT> acc[R];
+        Real dd[R][TPT];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int row = min(row0 + i, n - 1);
+            const size_t base = (size_t)row * B + b0;
+            if constexpr (!kFirst) {
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(qm1 + 2 * base));
+                if (qm2) asm volatile("prefetch.global.L2 [%0];" ::"l"(qm2 + 2 * base));
+            }
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                dd[i][t] = row0 + i < n ? __ldg(d + base + t) : Real(0);
+                acc[i].v[2 * t] = 0;
+                acc[i].v[2 * t + 1] = 0;
+            }
+        }
+        auto gather = [&](int c) { return ldv<Real, TPT, true>(pin, (size_t)c * B + b0); };
+        if constexpr (kPk) union_loop_pre<TPT, R>(cur, rec, acc, gather);
+        else union_any<Real, TPT, R>(__ldg(bptr + k), __ldg(bptr + k + 1), bcol, bcoef, acc, gather);
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int row = row0 + i;
+            if (row >= n) break;
+            const size_t base = (size_t)row * B + b0;
+            const CV<Real, TPT> po = ldv<Real, TPT, true>(pin, base);
+            CV<Real, TPT> x1, x2;
+#pragma unroll
+            for (int v = 0; v < 2 * TPT; ++v) x1.v[v] = x2.v[v] = 0;
+            if constexpr (!kFirst) {
+                x1 = ldv<Real, TPT, true>(qm1, base);
+                if (qm2) x2 = ldv_cs<Real, TPT>(qm2, base);
+            }
+            CV<Real, TPT> oq, op;
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                const int tt = tr * TPT + t;
+                const double a_r = cf[0][tt], a_i = cf[1][tt], ib = cf[2][tt], b1 = cf[3][tt], s1 = cf[4][tt];
+                const double c2r = cf[5][tt], c2i = cf[6][tt];
+                const double pr = po.v[2 * t], pi = po.v[2 * t + 1];
+                // H p at this row: gathered off-diagonal part plus the diagonal
+                const double hr = (double)fma(dd[i][t], po.v[2 * t], acc[i].v[2 * t]);
+                const double hi = (double)fma(dd[i][t], po.v[2 * t + 1], acc[i].v[2 * t + 1]);
+                double qr, qi, ur, ui;   // q_j and the vector whose products are summed
+                if constexpr (kFirst) {
+                    qr = s1 * pr;
+                    qi = s1 * pi;
+                    ur = s1 * hr;     // p_2 = H q_1
+                    ui = s1 * hi;
+                } else {
+                    const double y1r = s1 * x1.v[2 * t], y1i = s1 * x1.v[2 * t + 1];
+                    const double y2r = x2.v[2 * t], y2i = x2.v[2 * t + 1];
+                    qr = (pr - (a_r * y1r - a_i * y1i)) * ib;
+                    qi = (pi - (a_r * y1i + a_i * y1r)) * ib;
+                    // H q_j = (H p - alpha p - alpha beta_{j-2} sc_{j-2} r_{j-2}) / beta_{j-1}
+                    const double gr = (hr - (a_r * pr - a_i * pi) - (c2r * y2r - c2i * y2i)) * ib;
+                    const double gi = (hi - (a_r * pi + a_i * pr) - (c2r * y2i + c2i * y2r)) * ib;
+                    if constexpr (kLast) {
+                        ur = gr;
+                        ui = gi;
+                    } else {
+                        ur = gr - b1 * y1r;   // p_{j+1} = H q_j - beta_{j-1} q_{j-1}
+                        ui = gi - b1 * y1i;
+                    }
+                }
+                oq.v[2 * t] = (Real)qr;
+                oq.v[2 * t + 1] = (Real)qi;
+                op.v[2 * t] = (Real)ur;
+                op.v[2 * t + 1] = (Real)ui;
+                // the sums use the stored (rounded) values that the next iteration reads
+                const double sqr = kFirst ? qr : (double)oq.v[2 * t], sqi = kFirst ? qi : (double)oq.v[2 * t + 1];
+                const double spr = kLast ? ur : (double)op.v[2 * t], spi = kLast ? ui : (double)op.v[2 * t + 1];
+                if constexpr (kLast) {
+                    sum[0][t] += spr * spr + spi * spi;
+                } else {
+                    if (kBilinear) {
+                        sum[0][t] += sqr * spr - sqi * spi;
+                        sum[1][t] += sqr * spi + sqi * spr;
+                    } else {
+                        sum[0][t] += sqr * spr + sqi * spi;
+                        sum[1][t] += sqr * spi - sqi * spr;
+                    }
+                    if constexpr (kBilinear) {
+                        sum[K - 2][t] += sqr * spr + sqi * spi;
+                        sum[K - 1][t] += sqr * spi - sqi * spr;
+                    }
+                    sum[2][t] += spr * spr + spi * spi;
+                    sum[3][t] += sqr * sqr + sqi * sqi;
+                }
+            }
+            if constexpr (!kFirst) stv<Real, TPT>(qout, base, oq);
+            if constexpr (!kLast) stv<Real, TPT>(pout, base, op);
+        }
+    }
+    __shared__ double red[K * kMaxTC];
+    __shared__ double rsm[NT * TPT > kMaxTC * 8 ? NT * TPT : kMaxTC * 8];
+    if (chunk_reduce_multi<K, TPT>(sum, TC, S.partial, S.tickets + (kLast ? 2 : 0) * nch, red, chunk, rsm)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            if constexpr (kLast) {
+                S.nav[b] = sqrt(red[threadIdx.x]);
+            } else {
+                const double ar = red[threadIdx.x], ai = red[TC + threadIdx.x];
+                const double hr = kBilinear ? red[(K - 2) * TC + threadIdx.x] : ar;
+                const double hi = kBilinear ? red[(K - 1) * TC + threadIdx.x] : ai;
+                const double np = red[2 * TC + threadIdx.x], nq = red[3 * TC + threadIdx.x];
+                const double b2 = np - 2.0 * (ar * hr + ai * hi) + (ar * ar + ai * ai) * nq;
+                double bt = sqrt(fmax(b2, 0.0));
+                if (!isfinite(b2)) atomicCAS(S.status, 0, DQ_ERR_NAN);
+                // lucky breakdown: invariant Krylov space, continue with q_{j+1} = 0
+                const size_t kj = (size_t)j * B + b;
+                const double scale = sqrt(ar * ar + ai * ai) + (j > 1 ? S.beta[(size_t)(j - 1) * B + b] : 0.0);
+                if (bt <= kBreakdownRel * scale) bt = 0.0;
+                S.alpha[2 * kj] = ar;
+                S.alpha[2 * kj + 1] = ai;
+                S.beta[kj] = bt;
+                S.sc[(size_t)(j + 1) * B + b] = bt > 0.0 ? 1.0 : 0.0;
+            }
+        }
+    }
+}
+
 // Warp-per-block SpMM (staged = 3; complex64, packed records, R <= 3).  All
 // 32 lanes of a warp work on one block of R rows for TC = 32 TPT
 // trajectories, so the block's column-union records are one warp-uniform
@@ -2347,15 +2601,17 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
-    if (staged < 0 || staged > 7) return DQ_ERR_ARG;
+    if (staged < 0 || staged > 8) return DQ_ERR_ARG;
     // reorthogonalisation runs between the axpy and the next SpMM: not in the fused forms
-    if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4)) return DQ_ERR_ARG;
+    if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4 || staged == 8)) return DQ_ERR_ARG;
+    // p-form iteration: one launch per iteration over all chunks
+    if (staged == 8 && (groups != 1 || c->cfg.m < 2)) return DQ_ERR_ARG;
     // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane in the other
     // kernels (the ring itself takes 2 per lane with staged 6, 4 with staged 7), one CTA per SM
     const bool ring = staged == 6 || staged == 7;
     if (ring && (!bs->mixed || R > 3 || tc != 32 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
         return DQ_ERR_ARG;
-    if (staged == 5 && tc / tpt > 512) return DQ_ERR_ARG;
+    if ((staged == 5 || staged == 8) && tc / tpt > 512) return DQ_ERR_ARG;
     // warp-per-block forms: complex64 packed records, one warp spans the chunk
     if ((staged == 3 || staged == 4) && (!bs->mixed || R > 3 || tc != 32 * tpt)) return DQ_ERR_ARG;
     const int ri = r_index(R);
@@ -2364,7 +2620,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (groups < 1 || chunks % groups) return DQ_ERR_ARG;
     const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
-    const int RPC_spmm = (staged == 5 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
+    const int RPC_spmm = (staged == 5 || staged == 8 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
     // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide:
     // one wave of kStreamCtasPerSm CTAs per SM while every thread still walks
     // several rows, twice as many CTAs when that wave would leave each thread
@@ -2388,6 +2644,14 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->fmt[ri].bptr) {
         dq_status st = build_fmt(c, R, bs->fmt[ri]);
         if (st) return st;
+    }
+    if (staged == 8) {
+        // six sums per trajectory per CTA in the partials; p_j ping-pongs between slab 0 and wB
+        if ((size_t)gxs * B * 6 > bs->partial_cap) return DQ_ERR_ARG;
+        if (!bs->wB) {
+            const size_t real_sz = bs->mixed ? sizeof(float) : sizeof(double);
+            DQ_CU(cudaMalloc(&bs->wB, (size_t)n * B * 2 * real_sz));
+        }
     }
     int halo = 0, wmask = 0, rpc_win = 0, gxw = 0;
     size_t smem = 0;
@@ -2580,6 +2844,10 @@ dq_status batched_mirror_tiling(dq_ctx* c, BatchedState* dst) {
         dq_status st = build_fmaps(c, src->TC, src->f_sr);
         c->bat = src;
         if (st) return st;
+    }
+    if (src->staged == 8 && !dst->wB) {
+        const size_t real_sz = dst->mixed ? sizeof(float) : sizeof(double);
+        DQ_CU(cudaMalloc(&dst->wB, (size_t)c->n * dst->B * 2 * real_sz));
     }
     if (src->staged == 1 || src->staged == 6 || src->staged == 7) {
         const int SR = src->staged >= 6 ? src->f_sr : (kBThreads / (src->TC / src->TPT)) * src->R;
@@ -2898,6 +3166,56 @@ static void launch_fw(dq_ctx* c, int j) {
 #undef DQ_FW_R
 }
 
+// One launch of the p-form iteration (staged = 8) for iteration j of m:
+// j = 1 gathers psi (slab 1) and writes p_2; 2 <= j <= m gathers p_j, writes
+// q_j and p_{j+1}; j = m + 1 writes q_{m+1} and ||H q_{m+1}||.  p_j lives in
+// slab 0 for even j and in wB for odd j, so no launch reads the buffer it
+// writes.
+template <typename Real, int TPT, bool kBil, int kMode>
+static void launch_pform_m(dq_ctx* c, int j) {
+    BatchedState* bs = c->bat;
+    const BlockFmt& f = bs->fmt[r_index(bs->R)];
+    const int n = c->n, B = bs->B;
+    const size_t se = (size_t)n * B;
+    Real* slabs = (Real*)bs->slabs;
+    auto slab = [&](int k) { return slabs + 2 * se * k; };
+    auto pbuf = [&](int k) { return (k % 2 == 0) ? slabs : (Real*)bs->wB; };
+    const Real* pin = kMode == 0 ? slab(1) : pbuf(j);
+    const Real* qm1 = kMode == 0 ? nullptr : slab(j - 1);
+    const Real* qm2 = (kMode != 0 && j >= 3) ? slab(j - 2) : nullptr;
+    Real* qout = kMode == 0 ? nullptr : slab(j);
+    Real* pout = kMode == 2 ? nullptr : pbuf(j + 1);
+    const dim3 grid(bs->gxs, bs->chunks);
+#define DQ_PF_R(RR)                                                                                               \
+    k_lanczos_p<Real, TPT, RR, kBil, kMode, 512><<<grid, 512, 0, c->stream>>>(                                     \
+        n, B, bs->TC, bs->bpc, f.nb, j, f.bptr, f.bcol, (const Real*)f.bcoef, (const Real*)bs->diag, pin, qm1, qm2, \
+        qout, pout, bs->s, bs->chunks)
+    switch (bs->R) {
+        case 1: DQ_PF_R(1); break;
+        case 2: DQ_PF_R(2); break;
+        case 3: if constexpr (sizeof(Real) == 4) DQ_PF_R(3); break;
+        case 4: DQ_PF_R(4); break;
+        default: DQ_PF_R(8); break;
+    }
+#undef DQ_PF_R
+}
+
+template <typename Real, int TPT>
+static void launch_pform(dq_ctx* c, int j) {
+    const int m = c->cfg.m;
+    const bool bil = c->cfg.dot_mode == DQ_DOT_BILINEAR;
+    if (j == 1) {
+        if (bil) launch_pform_m<Real, TPT, true, 0>(c, j);
+        else launch_pform_m<Real, TPT, false, 0>(c, j);
+    } else if (j <= m) {
+        if (bil) launch_pform_m<Real, TPT, true, 1>(c, j);
+        else launch_pform_m<Real, TPT, false, 1>(c, j);
+    } else {
+        if (bil) launch_pform_m<Real, TPT, true, 2>(c, j);
+        else launch_pform_m<Real, TPT, false, 2>(c, j);
+    }
+}
+
 template <typename Real, int TPT, bool kLast>
 static void launch_fused_any(dq_ctx* c, int j) {
     if constexpr (sizeof(Real) == 4) {
@@ -2921,6 +3239,16 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
     auto slab = [&](int k) { return slabs + 2 * se * k; };
     const dim3 grid(bs->gx, ncy);
     const bool fused = bs->staged == 2 || bs->staged == 4;
+    if (bs->staged == 8) {
+        // p-form: one launch per iteration, and the last one gives ||H q_{m+1}||
+        if (tm) tm->mark(j == 1 ? DQ_KIND_SPMM : DQ_KIND_FUSED, st);
+        launch_pform<Real, TPT>(c, j);
+        if (j == c->cfg.m) {
+            if (tm) tm->mark(DQ_KIND_SPMM_NORM, st);
+            launch_pform<Real, TPT>(c, j + 1);
+        }
+        return DQ_OK;
+    }
     if (fused && j >= 2) {
         // iteration j of the fused form produces r_j; the last one also r_{m+1}
         if (tm) tm->mark(DQ_KIND_FUSED, st);
@@ -3021,7 +3349,7 @@ static dq_status enqueue_step(dq_ctx* c, StepTimer* tm, const std::function<void
         const int cpg = bs->chunks / bs->groups;
         for (int g = 0; g < bs->groups; ++g) {
             for (int j = 1; j <= m; ++j) enqueue_iteration<Real, TPT>(c, j, tm, g * cpg, cpg);
-            if (bs->staged != 2 && bs->staged != 4) {   // the fused form's last launch gave ||H q_{m+1}||
+            if (bs->staged != 2 && bs->staged != 4 && bs->staged != 8) {   // the fused forms' last launch gave ||H q_{m+1}||
                 mark(DQ_KIND_SPMM_NORM);
                 launch_spmm<Real, TPT, false, false>(c, m + 1, slab(m + 1), nullptr, nullptr, g * cpg, cpg);
             }
@@ -3141,14 +3469,26 @@ dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
     DQ_CU(cudaEventCreate(&e0));
     DQ_CU(cudaEventCreate(&e1));
     const bool fused = c->bat->staged == 2 || c->bat->staged == 4;
+    const bool pform = c->bat->staged == 8;
     const int jt = std::min(3, c->cfg.m);
+    auto pf = [&](int j) {
+        BatchedState* bs = c->bat;
+        if (!bs->mixed) launch_pform<double, 1>(c, j);
+        else if (bs->TPT == 2) launch_pform<float, 2>(c, j);
+        else launch_pform<float, 1>(c, j);
+    };
     auto one = [&]() {
         if (fused) fused_iteration_any(c, jt);
+        else if (pform) pf(jt);
         else enqueue_iteration_any(c, 1);
     };
     if (fused) {
         enqueue_iteration_any(c, 1);
         if (jt == 3) fused_iteration_any(c, 2);
+    }
+    if (pform) {
+        pf(1);
+        if (jt == 3) pf(2);
     }
     one();   // warm-up
     DQ_CU(cudaEventRecord(e0, c->stream));

@@ -247,7 +247,10 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * in 512-thread CTAs (one sliding gather window per CTA), 6 gathers from a
  * TMA-fed shared-memory ring with warp-owned row blocks and 2 trajectories
  * per lane, 7 the same ring with 4 trajectories per lane (both complex64,
- * traj_chunk 32, vec 2, ctas_per_sm 1, rows_per_block <= 3).  groups splits the
+ * traj_chunk 32, vec 2, ctas_per_sm 1, rows_per_block <= 3), 8 runs each
+ * Lanczos iteration as one L1-gather launch without the axpy pass (it keeps
+ * p_j = H q_{j-1} - beta_{j-2} q_{j-2} instead of the residual and gathers
+ * that; 512-thread CTAs; groups 1, no reorthogonalisation or adaptive m).  groups splits the
  * trajectory chunks into groups whose m Lanczos iterations run one group
  * after another, so a group's Krylov slabs stay resident in L2 (must divide
  * n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run

@@ -49,7 +49,8 @@ def _oracle(oracle, s, eps0, psi0, target, scale_c=1.0, noise=True):
                                 target, seed=SEED, **kw)
 
 
-@pytest.mark.parametrize("noise,tiling", [(True, None), (False, None), (True, (8, 1, 2, 2, 2, 1))])
+@pytest.mark.parametrize("noise,tiling", [(True, None), (False, None), (True, (8, 1, 2, 2, 2, 1)),
+                                          (True, (8, 1, 1, 2, 8, 1))])
 def test_adjoint_fp64_matches_oracle(oracle, noise, tiling):
     import dynaquant_b200 as dq
     s, eps0, psi0, target = _problem()

@@ -278,3 +278,64 @@ def test_tube_fused_warp_blocks_match_oracle(oracle, B, tiling):
         else:   # the bilinear dot: populations stay normalised and finite
             assert np.isfinite(p.populations()).all()
         p.close()
+
+
+@pytest.mark.parametrize("tag,dot", [("herm", 1), ("bil", 0)])
+@pytest.mark.parametrize("R", [1, 2, 4])
+def test_pform_iteration_fp64_matches_golden(tag, dot, R):
+    """One launch per Lanczos iteration without the axpy pass (staged = 8, p_j = H q_{j-1} - beta q_{j-2}
+    kept instead of the residual) in complex128 reproduces the golden run."""
+    import dynaquant_b200 as dq
+    g = _golden()
+    p = _chain_prop(dq.PREC_FP64, dot)
+    p.set_tiling(4, 1, 1, R, 8, 1)
+    assert p.get_tiling() == (4, 1, 1, R, 8, 1)
+    p.run(G.CHAIN["n_steps"])
+    assert np.abs(p.populations() - g[f"{tag}_pops"]).max() < POP_TOL_FP64
+    assert np.abs(p.correlation() - g[f"{tag}_corr"]).max() < POP_TOL_FP64
+    assert np.allclose(p.error_accum(), g[f"{tag}_err"], rtol=1e-3, atol=1e-14)
+    if tag == "herm":
+        assert np.abs(p.states() - g["herm_psi_final"]).max() < 1e-10
+    p.close()
+
+
+@pytest.mark.parametrize("dot", [1, 0])
+@pytest.mark.parametrize("tc,vec,R", [(32, 2, 3), (64, 2, 3), (32, 1, 3), (32, 2, 1), (16, 1, 2), (64, 2, 4)])
+def test_pform_iteration_mixed_tube_matches_oracle(oracle, dot, tc, vec, R):
+    """The same form in complex64 on the dipole-coupled tube against the FP64 oracle."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 24)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=20, dt=0.5, dot_mode=dot, noise=2, sigma=250.0, tau=50.0,
+                      sigma_static=150.0, seed=9)
+    B, T = 64, 40
+    psi0 = s.bright_state()
+    ref = S.run(B, T, psi0, pop_every=8, threads=4)
+    p = dq.Propagator(s.n, m=20, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=9, dot=dot,
+                      pop_every=8, max_steps=T, precision=dq.PREC_MIXED)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    p.set_initial_state(psi0)
+    p.set_tiling(tc, vec, 1, R, 8, 1)
+    p.run(T)
+    err = np.abs(p.populations() - ref["pops"]).max()
+    assert err < POP_TOL_MIXED, err
+    assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
+    assert np.allclose(np.linalg.norm(p.states(), axis=1), 1.0, atol=1e-12)
+    p.close()
+
+
+def test_pform_refuses_what_it_cannot_do():
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    p = _chain_prop(dq.PREC_MIXED, 1, n_traj=8)
+    with pytest.raises(dq.DQError):
+        p.set_tiling(4, 2, 1, 3, 8, 2)    # trajectory groups
+    p.close()
+    q = dq.Propagator(G.CHAIN["n"], m=16, n_traj=8, reorth=1, precision=dq.PREC_MIXED)
+    q.set_system(systems.chain(G.CHAIN["n"], -300.0))
+    q.set_initial_state(G.chain_psi0())
+    with pytest.raises(dq.DQError):
+        q.set_tiling(8, 2, 1, 3, 8, 1)   # full reorthogonalisation
+    q.close()
