@@ -1901,40 +1901,79 @@ __global__ void __launch_bounds__(kBThreads) k_axpy_beta(int n, int B, int TC, i
 }
 
 // Full reorthogonalisation (Hermitian dot, cfg.reorth; classical
-// Gram-Schmidt once, FP64 sums): h_k = <q_k, r_{j+1}> per trajectory, one k
-// per launch, into h[k][b] (the combine-weight array, unused until the Padé
-// step); then r_{j+1} -= sum_k h_k q_k and beta_j, sc_{j+1} from its norm.
+// Gram-Schmidt once, FP64 sums): after the axpy of iteration j, h_k =
+// <q_k, r_{j+1}> for k = 1..j (k_reorth_dots_b), then r_{j+1} -= sum_k h_k q_k
+// and beta_j, sc_{j+1} from its norm (k_reorth_apply_b).
+// All h_k = <q_k, r_{j+1}>, k = 1..j, of full reorthogonalisation in one
+// launch (classical Gram-Schmidt in blocks of kReorthKB): blockIdx.z picks
+// the block of k, blockIdx.y the trajectory chunk, and each CTA reads r_{j+1}
+// and that block's q_k over its row range once, so an iteration reads
+// j + ceil(j / kReorthKB) slabs instead of the 2 j of one launch per k.
+// FP64 sums, one ticket per (k block, chunk); the last CTA of each writes
+// h_k into the combine-weight array (unused until the Padé step).
+constexpr int kReorthKB = 8;
+// ticket words per trajectory: regions 0..7 of the iteration kernels (one
+// ticket per chunk each), the population ticket at 8 B, and from 9 B one
+// region per block of k of the reorthogonalisation dots
+constexpr int kReorthTicket = 9;
+constexpr size_t kTicketWords = kReorthTicket + (kMaxL + kReorthKB - 1) / kReorthKB;
+
 template <typename Real, int TPT>
-__global__ void __launch_bounds__(kBThreads) k_reorth_dot_b(int n, int B, int TC, int rpc, int k,
-                                                           const Real* __restrict__ xk, const Real* __restrict__ r,
-                                                           BatchedScalars S, int cy0, int nch) {
-    const Tile<TPT> T(TC, rpc, n, cy0);
-    if (chunk_converged(S, T.chunk)) return;
-    double ar[TPT], ai[TPT], sck[TPT];
+__global__ void __launch_bounds__(kBThreads) k_reorth_dots_b(int n, int B, int TC, int rpc, int j,
+                                                            const Real* __restrict__ slabs, size_t slab_stride,
+                                                            BatchedScalars S, unsigned int* tickets, int cy0,
+                                                            int nch) {
+    constexpr int KQ = 2 * kReorthKB;   // complex h_k as two real sums each
+    const int chunk = blockIdx.y + cy0, kb = blockIdx.z;
+    const int k_first = 1 + kb * kReorthKB;
+    const int TPR = TC / TPT;
+    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int RPC = blockDim.x / TPR;
+    const int b0 = chunk * TC + tr * TPT;
+    const int r0 = blockIdx.x * rpc, r1 = min(n, r0 + rpc);
+    if (chunk_converged(S, chunk)) return;
+    const Real* r = slabs + 2 * slab_stride * (j + 1);
+    double h[KQ][TPT];
+    double sck[kReorthKB][TPT];
 #pragma unroll
-    for (int t = 0; t < TPT; ++t) {
-        ar[t] = 0.0;
-        ai[t] = 0.0;
-        sck[t] = S.sc[(size_t)k * B + T.b0 + t];
-    }
-    for (int row = T.r0 + T.rl; row < T.r1; row += T.RPC) {
-        const size_t base = (size_t)row * B + T.b0;
-        const CV<Real, TPT> x = ldv<Real, TPT, false>(xk, base);
-        const CV<Real, TPT> v = ldv<Real, TPT, false>(r, base);
+    for (int q = 0; q < kReorthKB; ++q)
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
-            const double qr = sck[t] * x.v[2 * t], qi = sck[t] * x.v[2 * t + 1];
-            const double vr = v.v[2 * t], vi = v.v[2 * t + 1];
-            ar[t] += qr * vr + qi * vi;   // conj(q) v
-            ai[t] += qr * vi - qi * vr;
+            const int k = k_first + q;
+            sck[q][t] = k <= j ? S.sc[(size_t)k * B + b0 + t] : 0.0;
+            h[2 * q][t] = h[2 * q + 1][t] = 0.0;
+        }
+    for (int row = r0 + rl; row < r1; row += RPC) {
+        const size_t base = (size_t)row * B + b0;
+        const CV<Real, TPT> v = ldv<Real, TPT, false>(r, base);
+#pragma unroll
+        for (int q = 0; q < kReorthKB; ++q) {
+            const int k = k_first + q;
+            if (k > j) break;
+            const CV<Real, TPT> x = ldv<Real, TPT, false>(slabs + 2 * slab_stride * k, base);
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                const double qr = sck[q][t] * x.v[2 * t], qi = sck[q][t] * x.v[2 * t + 1];
+                const double vr = v.v[2 * t], vi = v.v[2 * t + 1];
+                h[2 * q][t] += qr * vr + qi * vi;   // conj(q) v
+                h[2 * q + 1][t] += qr * vi - qi * vr;
+            }
         }
     }
-    __shared__ double2 red[kMaxTC];
-    if (chunk_reduce<TPT>(ar, ai, TC, S.partial, S.tickets + 7 * nch, red, T.chunk)) {
+    __shared__ double red[KQ * kMaxTC];
+    __shared__ double rsm[kBThreads * 2];
+    // each k block has its own tickets (one per chunk) and partial region
+    double* part = S.partial + (size_t)kb * nch * gridDim.x * KQ * TC;
+    if (chunk_reduce_multi<KQ, TPT>(h, TC, part, tickets + (size_t)kb * nch, red, chunk, rsm)) {
         if (threadIdx.x < TC) {
-            const size_t kb = (size_t)k * B + T.chunk * TC + threadIdx.x;
-            S.yt[2 * kb] = red[threadIdx.x].x;
-            S.yt[2 * kb + 1] = red[threadIdx.x].y;
+            const int b = chunk * TC + threadIdx.x;
+            for (int q = 0; q < kReorthKB; ++q) {
+                const int k = k_first + q;
+                if (k > j) break;
+                const size_t kbb = (size_t)k * B + b;
+                S.yt[2 * kbb] = red[(2 * q) * TC + threadIdx.x];
+                S.yt[2 * kbb + 1] = red[(2 * q + 1) * TC + threadIdx.x];
+            }
         }
     }
 }
@@ -2899,7 +2938,7 @@ static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed) {
     bs->s.norm2 = p; p += B;
     bs->s.partial = p; p += 2 * bs->partial_cap;
     bs->s.corr = p; p += corr_n;
-    const size_t nt = (size_t)8 * B + 8;
+    const size_t nt = kTicketWords * (size_t)B + 8;
     DQ_CU(cudaMalloc(&bs->s.tickets, sizeof(unsigned int) * nt));
     DQ_CU(cudaMemsetAsync(bs->s.tickets, 0, sizeof(unsigned int) * nt, c->stream));
     DQ_CU(cudaMalloc(&bs->s.status, sizeof(int) * 2));
@@ -2984,7 +3023,7 @@ dq_status batched_reset(dq_ctx* c) {
         k_set_psi0_b<float><<<blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, (float*)((char*)bs->slabs + slab));
     else
         k_set_psi0_b<double><<<blocks, thr, 0, c->stream>>>(n, B, c->d_psi0, (double*)((char*)bs->slabs + slab));
-    DQ_CU(cudaMemsetAsync(bs->s.tickets, 0, sizeof(unsigned int) * ((size_t)8 * B + 8), c->stream));
+    DQ_CU(cudaMemsetAsync(bs->s.tickets, 0, sizeof(unsigned int) * (kTicketWords * (size_t)B + 8), c->stream));
     k_set_norms_b<<<1, 256, 0, c->stream>>>(n, B, c->d_psi0, bs->s);
     k_init_obs_b<<<std::max(1, std::min(bs->sms, (n + 255) / 256)), 256, 0, c->stream>>>(n, B, c->d_psi0, c->d_pops,
                                                                                         bs->s, bs->chunks,
@@ -3278,9 +3317,15 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
                                                        bs->chunks);
     if (c->cfg.reorth) {
         if (tm) tm->mark(DQ_KIND_AXPY, st);
-        for (int k = 1; k <= j; ++k)
-            k_reorth_dot_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, k, slab(k), slab(j + 1), bs->s,
-                                                                  cy0, bs->chunks);
+        // every h_k in one launch: about two CTAs per SM over (rows, chunks, blocks of k)
+        const int nkb = (j + kReorthKB - 1) / kReorthKB;
+        const int TPR = TC / TPT, RPCr = kBThreads / TPR;
+        int gxr = std::max(1, (2 * bs->sms) / (ncy * nkb));
+        int rpcr = (n + gxr - 1) / gxr;
+        rpcr = ((rpcr + RPCr - 1) / RPCr) * RPCr;
+        gxr = (n + rpcr - 1) / rpcr;
+        k_reorth_dots_b<Real, TPT><<<dim3(gxr, ncy, nkb), kBThreads, 0, st>>>(
+            n, B, TC, rpcr, j, slabs, se, bs->s, bs->s.tickets + kReorthTicket * (size_t)B, cy0, bs->chunks);
         k_reorth_apply_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slabs, se, bs->s, cy0, bs->chunks);
     }
     return DQ_OK;

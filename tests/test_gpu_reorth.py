@@ -57,3 +57,19 @@ def test_reorth_rejects_fused_forms_and_adjoint():
     with pytest.raises(dq.DQError, match="reorth"):
         p.adjoint_setup(T, 32, 1.0, np.zeros(32))
     p.close()
+
+
+@pytest.mark.parametrize("tiling", [(4, 1, 2, 2, 0, 2), (8, 1, 1, 1, 5, 1), (4, 1, 2, 4, 0, 1)])
+def test_reorth_blocked_dots_under_other_tilings(oracle, tiling):
+    """The one-launch dots of every h_k (blocks of 8 k, tickets per block and chunk) with trajectory
+    groups, 512-thread SpMM CTAs and other row blocks, FP64, against the oracle."""
+    import dynaquant_b200 as dq
+    s = _system()
+    psi0 = s.bright_state((1.0, 0.0, 0.0))
+    ref = _oracle_run(oracle, s, psi0, 1)
+    q = _prop(s, psi0, dq.PREC_FP64)
+    q.set_tiling(*tiling)
+    q.run(T)
+    assert np.abs(q.populations() - ref["pops"]).max() < 1e-10
+    assert np.abs(q.correlation() - ref["corr"]).max() < 1e-9
+    q.close()
