@@ -193,6 +193,25 @@ def plain_roofline(s, value):
                                        "launch-latency bound, not HBM bound"}
 
 
+def dominant_kernel(s, B, m, staged, prof):
+    """(algorithmic bytes per launch, mean ms per launch, achieved GB/s) of the step's dominant
+    kernel under tiling form `staged`, from profile_step's per-kind launch times."""
+    ms = prof["spmm_alpha"][0]
+    if staged in (2, 4, 8):
+        # fused forms: the dominant launch is the whole iteration
+        ms = prof["fused_iter"][0]
+    b = spmm_bytes(s, B)
+    if staged in (0, 5):
+        # the L1 forms also read q_{j-1} (8 B per site-trajectory) in m - 1 of the step's m launches
+        b += 8.0 * s.n * B * (m - 1) / m
+    if staged in (2, 4):
+        b += 24.0 * s.n * B   # + r_j, r_{j-1} reads and the r_{j+1} write
+    if staged == 8:
+        # p-form launch j (2 < j <= m): reads p_j, q_{j-1}, q_{j-2} and d, writes q_j and p_{j+1}
+        b = 44.0 * s.n * B + 8.0 * (s.nnz - s.n) + 4.0 * (s.n + 1)
+    return b, ms, b / (ms / 1e3) / 1e9
+
+
 def spmm_bytes(s, B):
     """Algorithmic HBM bytes of one SpMM+alpha launch (complex64 path):
     read q_j (8 B) and the diagonal (4 B), write w (8 B) per site-trajectory,
@@ -351,16 +370,25 @@ def large_leg():
     e1.record(st)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / K
+    prof = p.profile_step(1)
     p.close()
+    b, kms, achieved = dominant_kernel(s, B, 24, tiling["staged"], prof)
+    peak, peak_kind = _peaks()
     return {"workload": "tube120x1000_B1024_m24", "n_sites": s.n, "nnz_per_row": (s.nnz - s.n) / s.n,
             "value": B / (ms / 1e3), "unit": "traj-steps/s", "ms_per_step": ms,
-            "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged")}}
+            "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged")},
+            "roofline": {"bound": "hbm", "kernel": SPMM_FORMS.get(tiling["staged"], ("SpMM + alpha",))[0],
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b, "ms_per_launch": kms},
+            "kernels_ms_per_launch": {k: v[0] for k, v in prof.items()}}
 
 
 def aggregates_leg():
     """Eight tubes 60 x L with 512 trajectories split about as 1/L (multiples of 8), adaptive Krylov
-    dimension 8..32 at tolerance 1e-7, dt 0.5 fs, 2000 steps: all aggregates in one graph per step
-    (dq_group_run) against the same aggregates run one after another (dq_run each)."""
+    dimension 8..32 at tolerance 1e-7, dt 0.5 fs, 2000 steps: every member's tiling from the project's
+    autotuner (cached per GPU model and size class), then all aggregates in one graph per step
+    (dq_group_run_timed: device time of the step launches, capture excluded) against the same aggregates
+    run one after another (dq_run each, device time on each member's stream)."""
     import torch
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
@@ -382,33 +410,38 @@ def aggregates_leg():
         return out
 
     ms = members(500)
+    tilings = []
+    for p in ms:
+        t = p.autotune()
+        tilings.append({k: t[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged", "groups")})
     g = dq.Group(ms)
     g.run(4)                       # warm-up (allocation, first capture)
     for p in ms:
         p.reset()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    g.run(a["steps"])
-    torch.cuda.synchronize()
-    t_group = time.perf_counter() - t0
+    t_group = g.run_timed(a["steps"]) / 1e3
     g.close()
     for p in ms:
         p.reset()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    t_seq = 0.0
     for p in ms:
+        st = torch.cuda.ExternalStream(p.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
         p.run(a["steps"])
-    torch.cuda.synchronize()
-    t_seq = time.perf_counter() - t0
+        e1.record(st)
+        torch.cuda.synchronize()
+        t_seq += e0.elapsed_time(e1) / 1e3
     n_sites = [p.n for p in ms]
     for p in ms:
         p.close()
     total = sum(a["B"]) * a["steps"]
     return {"workload": a["name"], "sites": n_sites, "trajectories": list(a["B"]), "steps": a["steps"],
             "value": total / t_group, "unit": "traj-steps/s", "sequential_value": total / t_seq,
-            "group_over_sequential": t_seq / t_group,
-            "note": "host wall clock around dq_group_run (one graph per step, a branch per aggregate) and around "
-                    "the eight dq_run calls; default tilings"}
+            "group_over_sequential": t_seq / t_group, "tilings": tilings,
+            "note": "device time (CUDA events) of the group's step launches, graph capture excluded, against the "
+                    "sum of the eight dq_run device times; tilings from the autotuner per member"}
 
 
 ADJ = dict(name="lattice64x64_B128_T2000_m16", L=64, J_nn=-250.0, J_nnn=40.0, B=128, dt=1.0, steps=2000, m=16,
@@ -630,21 +663,7 @@ def run_ours(args, rank, world, local_rank):
     prof = p.profile_step(2)
     p.close()
     peak, peak_kind = _peaks()
-    spmm_ms = prof["spmm_alpha"][0]
-    if tiling["staged"] in (2, 4, 8):
-        # fused forms: the dominant launch is the whole iteration (reads w, r_j, r_{j-1}, d and the
-        # CSR; writes r_{j+1} and w)
-        spmm_ms = prof["fused_iter"][0]
-    bytes_spmm = spmm_bytes(s, B)
-    if tiling["staged"] in (0, 5):
-        # the L1 forms also read q_{j-1} (8 B per site-trajectory) in m - 1 of the step's m launches
-        bytes_spmm += 8.0 * s.n * B * (w["m"] - 1) / w["m"]
-    if tiling["staged"] in (2, 4):
-        bytes_spmm += 24.0 * s.n * B   # + r_j, r_{j-1} reads and the r_{j+1} write
-    if tiling["staged"] == 8:
-        # p-form launch j (2 < j <= m): reads p_j, q_{j-1}, q_{j-2} and d, writes q_j and p_{j+1}
-        bytes_spmm = 44.0 * s.n * B + 8.0 * (s.nnz - s.n) + 4.0 * (s.n + 1)
-    achieved = bytes_spmm / (spmm_ms / 1e3) / 1e9
+    bytes_spmm, spmm_ms, achieved = dominant_kernel(s, B, w["m"], tiling["staged"], prof)
     step_ms_eager = sum(v[0] * v[1] for v in prof.values()) / 2
     kernels_per_step = sum(v[1] for v in prof.values()) // 2
     # ---- end to end through the C ABI with host buffers --------------------

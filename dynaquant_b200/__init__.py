@@ -353,6 +353,14 @@ class Group:
         if rc != 0:
             raise DQError(rc, self.L.dq_group_last_error(self.h).decode(errors="replace"))
 
+    def run_timed(self, n_steps) -> float:
+        """run() returning the device milliseconds of the step launches (graph capture excluded)."""
+        ms = C.c_double()
+        rc = self.L.dq_group_run_timed(self.h, n_steps, C.byref(ms))
+        if rc != 0:
+            raise DQError(rc, self.L.dq_group_last_error(self.h).decode(errors="replace"))
+        return ms.value
+
     def close(self):
         if getattr(self, "h", None):
             self.L.dq_group_destroy(self.h)

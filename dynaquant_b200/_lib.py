@@ -31,7 +31,7 @@ EXPORTS = [
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
     "dq_get_noise_state", "dq_set_line_dressing", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
     "dq_debug_set_wait_cycles", "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward", "dq_forward_shard", "dq_forward_reduced",
-    "dq_group_create", "dq_group_destroy", "dq_group_last_error", "dq_group_run",
+    "dq_group_create", "dq_group_destroy", "dq_group_last_error", "dq_group_run", "dq_group_run_timed",
     "dq_write_populations", "dq_write_states", "dq_write_spectrum", "dq_write_spectrum_mean",
     # include/dq_host.h
     "dq_infile_defaults", "dq_infile_parse", "dq_infile_split_line", "dq_infile_run",
@@ -159,6 +159,7 @@ def load(path: str = LIB_PATH):
     L.dq_group_last_error.argtypes = [vp]
     L.dq_group_last_error.restype = C.c_char_p
     L.dq_group_run.argtypes = [vp, C.c_int]
+    L.dq_group_run_timed.argtypes = [vp, C.c_int, dp]
     L.dq_write_populations.argtypes = [vp, C.c_char_p, C.c_int, C.c_int]
     L.dq_write_states.argtypes = [vp, C.c_char_p]
     L.dq_write_spectrum.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_double]

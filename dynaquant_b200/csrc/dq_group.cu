@@ -74,8 +74,11 @@ void dq_group_destroy(dq_group* g) {
 
 const char* dq_group_last_error(const dq_group* g) { return g ? g->err.c_str() : "null group"; }
 
-dq_status dq_group_run(dq_group* g, int n_steps) {
+dq_status dq_group_run(dq_group* g, int n_steps) { return dq_group_run_timed(g, n_steps, nullptr); }
+
+dq_status dq_group_run_timed(dq_group* g, int n_steps, double* device_ms) {
     if (!g) return DQ_ERR_ARG;
+    if (device_ms) *device_ms = 0.0;
     if (n_steps < 0) return gfail(g, DQ_ERR_ARG, "group run: negative step count");
     if (n_steps == 0) return DQ_OK;
     dq::DeviceScope dev_scope(g->device);
@@ -114,8 +117,23 @@ dq_status dq_group_run(dq_group* g, int n_steps) {
         return gcuda(g, e != cudaSuccess ? e : e2, "group graph capture");
     }
     e = cudaGraphInstantiate(&exec, graph, 0);
+    // device time of the launches alone (capture and instantiation excluded)
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    if (e == cudaSuccess && device_ms) {
+        e = cudaEventCreate(&t0);
+        if (e == cudaSuccess) e = cudaEventCreate(&t1);
+        if (e == cudaSuccess) e = cudaEventRecord(t0, g->stream);
+    }
     for (int k = 0; e == cudaSuccess && k < n_steps; ++k) e = cudaGraphLaunch(exec, g->stream);
+    if (e == cudaSuccess && device_ms) e = cudaEventRecord(t1, g->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+    if (e == cudaSuccess && device_ms) {
+        float ms = 0.f;
+        e = cudaEventElapsedTime(&ms, t0, t1);
+        *device_ms = ms;
+    }
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
     if (exec) cudaGraphExecDestroy(exec);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return gcuda(g, e, "group graph launch");

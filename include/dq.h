@@ -368,6 +368,10 @@ DQ_API void dq_group_destroy(dq_group *group);
 DQ_API const char *dq_group_last_error(const dq_group *group);
 /* Advances every member by n_steps (as dq_run does for one context). */
 DQ_API dq_status dq_group_run(dq_group *group, int n_steps);
+/* dq_group_run that also gives the device time of the n_steps graph
+ * launches in *device_ms (events on the group's stream; the capture of the
+ * step graph is excluded). */
+DQ_API dq_status dq_group_run_timed(dq_group *group, int n_steps, double *device_ms);
 
 /* ---- adjoint: gradient of a spectrum-fitting loss ----
  * No counterpart in the reference (it has no gradients).  The loss is
