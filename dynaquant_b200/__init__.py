@@ -155,7 +155,8 @@ class Propagator:
         return ms.value
 
     def debug_set_wait_cycles(self, cycles):
-        """Test hook: budget of the TMA-fed SpMM forms' barrier waits on this device (<= 0: default)."""
+        """Test hook: budget of the TMA-fed SpMM forms' barrier waits on this device (0: default; negative:
+        the ring form's CTAs first wait that many cycles on a barrier nothing completes, so they time out)."""
         self._check(self.L.dq_debug_set_wait_cycles(self.h, int(cycles)))
 
     def autotune_raw(self, reps=5):

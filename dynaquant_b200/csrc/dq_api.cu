@@ -675,7 +675,18 @@ extern "C" dq_status dq_set_tiling(dq_ctx* c, int traj_chunk, int vec, int ctas_
     DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;
     dq_status st;
-    if ((st = ensure_batched(c))) return st;
+    if (!c->bat) {
+        // a new workspace gets the requested tiling directly (no default blocks built first)
+        if ((st = check_ready(c))) return st;
+        if ((st = batched_alloc(c, false))) return st;
+        c->ready = false;
+        if ((st = batched_set_tiling(c, traj_chunk, vec, ctas_per_sm, rows_per_block, staged, groups))) {
+            dq_status st2 = batched_default_tiling(c);
+            if (st2) return st2;
+            return fail(c, st, "set_tiling: invalid tiling for this system");
+        }
+        return DQ_OK;
+    }
     if ((st = batched_set_tiling(c, traj_chunk, vec, ctas_per_sm, rows_per_block, staged, groups)))
         return fail(c, st, "set_tiling: invalid tiling for this system");
     c->ready = false;

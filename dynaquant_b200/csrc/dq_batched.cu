@@ -43,9 +43,17 @@
 namespace dq {
 
 // Budget of the bounded mbarrier waits in SM cycles: kWaitCycles (about 2 s)
-// unless a test lowers it through dq_debug_set_wait_cycles to make the waits
-// run out on purpose.  The drains after a timeout always use kWaitCycles.
+// unless a test lowers it through dq_debug_set_wait_cycles.  A negative value
+// is a test mode: each ring-SpMM CTA first waits |value| cycles on a barrier
+// that no copy completes, so its wait runs out for certain.  The drains after
+// a timeout always use kWaitCycles.
 __device__ long long g_dq_wait_cycles = kWaitCycles;
+
+// the budget of the forms without the forced-timeout mode
+__device__ __forceinline__ long long wait_budget() {
+    const long long b = g_dq_wait_cycles;
+    return b > 0 ? b : kWaitCycles;
+}
 
 // ---------------------------------------------------------------------------
 __global__ void k_traj_init_b(int n, int B, int traj0, uint64_t seed, const double* __restrict__ h0,
@@ -936,6 +944,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
     constexpr size_t row_reals = TC * 2;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bars[32];
+    __shared__ __align__(8) uint64_t never_bar;   // a barrier no copy completes (the timeout test hook)
     __shared__ float4 rbuf[kWarps][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int half = lane / GL, hl = lane % GL;   // record group, lane within it
@@ -975,6 +984,7 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
     };
     if (threadIdx.x == 0) {
         for (int q = 0; q < NB; ++q) mbar_init(&bars[q], 1);
+        mbar_init(&never_bar, 1);
         fence_barrier_init();
     }
     __syncthreads();
@@ -1027,8 +1037,14 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
         const int bl = s + 2 * hb;
         int failed = -1;
         const long long budget = g_dq_wait_cycles;
+        if (budget < 0 && s == 0) {
+            // test hook: wait (|budget| cycles) for a barrier that nothing
+            // completes, so the wait runs out and the timeout path below runs
+            if (!mbar_wait_bounded(&never_bar, 0u, -budget)) failed = 0;
+        }
         for (int q = (s == 0 ? 0 : bl); q <= bl; ++q)
-            if (failed < 0 && !mbar_wait_bounded(&bars[q % NB], (uint32_t)((q / NB) & 1), budget)) failed = q;
+            if (failed < 0 && !mbar_wait_bounded(&bars[q % NB], (uint32_t)((q / NB) & 1), budget < 0 ? kWaitCycles : budget))
+                failed = q;
         if (__syncthreads_or(failed >= 0)) {
             if (threadIdx.x == 0) {
                 atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
@@ -1221,7 +1237,7 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
             tma_load_2d(slot(y), &tmap, &bars[(s + 1) & 1], xc, y);
         }
         if (s + 1 < nsteps) issued = s + 1;
-        const bool ok = mbar_wait_bounded(&bars[s & 1], (uint32_t)((s >> 1) & 1), g_dq_wait_cycles);
+        const bool ok = mbar_wait_bounded(&bars[s & 1], (uint32_t)((s >> 1) & 1), wait_budget());
         if (__syncthreads_or(!ok)) {
             // a copy never completed: flag it, give the copies in flight (this
             // step's and the next one's) a bounded chance to land, and leave
@@ -1422,7 +1438,7 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
 #pragma unroll
             for (int t = 0; t < TPT; ++t) dd[i][t] = (has_blk && row < r1) ? __ldg(d + base + t) : Real(0);
         }
-        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1), g_dq_wait_cycles);
+        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1), wait_budget());
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
@@ -1661,7 +1677,7 @@ __global__ void __launch_bounds__(kFwThreads, 1) k_lanczos_fw(int n, int B, int 
             pe = __ldg(bptr + k + 1);
             nxt = lane < pe - pb ? __ldg(rec + pb + lane) : zero4;
         }
-        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1), g_dq_wait_cycles);
+        const bool ok = mbar_wait_bounded(&bars[st], (uint32_t)((p / D) & 1), wait_budget());
         if (__syncthreads_or(!ok)) {
             if (threadIdx.x == 0) {
                 atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
@@ -2900,7 +2916,7 @@ dq_status batched_mirror_tiling(dq_ctx* c, BatchedState* dst) {
 
 // Allocates and initialises one workspace of B trajectories and attaches it
 // to c->bat (the caller restores c->bat when the workspace is a second one).
-static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed) {
+static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed, bool default_tiling = true) {
     const int n = c->n, m = c->cfg.m;
     c->bat = bs;
     bs->B = B;
@@ -2953,7 +2969,15 @@ static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed) {
     }
     DQ_CU(raise_smem_limit(k_pade_b, (int)pade_smem_bytes(m + 2)));
     DQ_CU(raise_smem_limit(k_mcheck_b, (int)pade_smem_bytes(m + 2)));
-    // default tiling (dq_autotune refines it)
+    // default tiling (dq_autotune refines it); left out when the caller sets
+    // one right away, so only that tiling's coupling blocks are built
+    if (!default_tiling) return DQ_OK;
+    return batched_default_tiling(c);
+}
+
+dq_status batched_default_tiling(dq_ctx* c) {
+    BatchedState* bs = c->bat;
+    const int B = bs->B;
     int tpt = bs->mixed ? 2 : 1;
     int tc = 16;
     while (tc > tpt && B % tc) tc >>= 1;
@@ -2966,9 +2990,9 @@ static dq_status alloc_ws_into(dq_ctx* c, BatchedState* bs, int B, bool mixed) {
     return DQ_OK;
 }
 
-dq_status batched_alloc(dq_ctx* c) {
+dq_status batched_alloc(dq_ctx* c, bool default_tiling) {
     BatchedState* bs = new BatchedState();
-    return alloc_ws_into(c, bs, c->cfg.n_traj, c->cfg.precision == DQ_PREC_MIXED);
+    return alloc_ws_into(c, bs, c->cfg.n_traj, c->cfg.precision == DQ_PREC_MIXED, default_tiling);
 }
 
 BatchedState* batched_alloc_ws(dq_ctx* c, int B, bool mixed, dq_status* st) {
@@ -3590,8 +3614,9 @@ dq_status batched_collect_corr(dq_ctx* c) {
 }
 
 // dq_debug_set_wait_cycles: the budget every bounded wait of this device reads
+// (negative: the forced-timeout test mode of the ring SpMM)
 dq_status batched_set_wait_cycles(dq_ctx* c, int cycles) {
-    const long long v = cycles > 0 ? (long long)cycles : kWaitCycles;
+    const long long v = cycles != 0 ? (long long)cycles : kWaitCycles;
     return check_cuda(c, cudaMemcpyToSymbol(g_dq_wait_cycles, &v, sizeof(v)), "wait budget");
 }
 

@@ -169,7 +169,10 @@ dq_status plain_observe_initial(dq_ctx* c);
 dq_status check_cuda(dq_ctx* c, cudaError_t e, const char* what);
 dq_status read_status(dq_ctx* c, int code, const char* what);
 // implemented in dq_batched.cu
-dq_status batched_alloc(dq_ctx* c);
+// default_tiling = false leaves the tiling unset (TC = 0) for a caller that
+// sets one at once (batched_set_tiling, or batched_default_tiling)
+dq_status batched_alloc(dq_ctx* c, bool default_tiling = true);
+dq_status batched_default_tiling(dq_ctx* c);
 void batched_free(dq_ctx* c);
 dq_status batched_reset(dq_ctx* c);
 dq_status batched_run(dq_ctx* c, int n_steps);

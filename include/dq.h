@@ -268,11 +268,12 @@ DQ_API dq_status dq_autotune(dq_ctx *ctx, int reps, double *best_ms);
 DQ_API dq_status dq_time_iteration(dq_ctx *ctx, int reps, double *ms);
 /* Test hook, no reference counterpart: sets the budget (SM cycles) of the
  * bounded shared-memory barrier waits of the TMA-fed SpMM forms on the
- * context's device; cycles <= 0 restores the default (about 2 s).  A tiny
- * budget makes those waits give up on purpose: the kernels then record
- * DQ_ERR_TIMEOUT, let their own copies in flight land (with the default
- * budget) and return, and dq_run reports the status.  It applies to every
- * context on the device until changed again. */
+ * context's device; 0 restores the default (about 2 s).  A negative value
+ * makes every CTA of the ring form (staged 6/7) first wait -cycles cycles on
+ * a barrier that no copy ever completes: the wait runs out, the kernel
+ * records DQ_ERR_TIMEOUT, lets its own copies in flight land (with the
+ * default budget) and returns, and dq_run reports the status.  It applies
+ * to every context on the device until changed again. */
 DQ_API dq_status dq_debug_set_wait_cycles(dq_ctx *ctx, int cycles);
 
 /* Kernel kinds of one ensemble step, for dq_profile_step. */

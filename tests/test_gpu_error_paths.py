@@ -187,10 +187,10 @@ def test_huge_time_step_reports_pade_scaling_limit():
 
 
 def test_ring_spmm_wait_timeout_is_reported_and_context_recovers():
-    """The TMA-fed ring SpMM (staged 6) with its barrier-wait budget lowered to a
-    few cycles: its waits give up, each CTA lets its own copies land and leaves,
-    dq_run returns DQ_ERR_TIMEOUT; with the budget restored the same context
-    reproduces the clean run bit for bit."""
+    """The TMA-fed ring SpMM (staged 6) made to wait, with a budget of 20,000 cycles, on a barrier that
+    nothing completes: the wait gives up, each CTA lets its own copies land and leaves, dq_run returns
+    DQ_ERR_TIMEOUT; with the default budget restored the same context reproduces the clean run bit for
+    bit."""
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
     s = systems.tube(20, 24)
@@ -210,7 +210,7 @@ def test_ring_spmm_wait_timeout_is_reported_and_context_recovers():
         p.reset()
         p.run(T)
         clean = p.populations()
-        p.debug_set_wait_cycles(4)
+        p.debug_set_wait_cycles(-20000)   # a wait on a barrier that no copy completes, ~10 us
         p.reset()
         with pytest.raises(dq.DQError) as e:
             p.run(T)
