@@ -2649,6 +2649,37 @@ static size_t fused_smem(int tc, int sr, int hb, int D, size_t rsz) {
 
 // Tiling: TC trajectories per chunk, TPT per thread, ~ctas_per_sm CTAs per
 // SM, R rows per SpMM block, staged: TMA shared-memory window SpMM.
+// The L1-gather forms in 512-thread CTAs (k_spmm_blk of staged 5, k_lanczos_p
+// of staged 8) keep their gather window in L1: ask for the largest L1 share of
+// the SM's unified L1/shared memory (their own shared memory is a few KB).
+template <typename Real, int TPT, int R>
+static void prefer_l1_r() {
+    const int carve = cudaSharedmemCarveoutMaxL1;
+    auto set = [&](const void* f) { cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carve); };
+    set((const void*)k_spmm_blk<Real, TPT, R, false, true, 512>);
+    set((const void*)k_spmm_blk<Real, TPT, R, true, true, 512>);
+    set((const void*)k_spmm_blk<Real, TPT, R, false, false, 512>);
+    set((const void*)k_spmm_blk<Real, TPT, R, true, false, 512>);
+    set((const void*)k_lanczos_p<Real, TPT, R, false, 0, 512>);
+    set((const void*)k_lanczos_p<Real, TPT, R, false, 1, 512>);
+    set((const void*)k_lanczos_p<Real, TPT, R, false, 2, 512>);
+    set((const void*)k_lanczos_p<Real, TPT, R, true, 0, 512>);
+    set((const void*)k_lanczos_p<Real, TPT, R, true, 1, 512>);
+    set((const void*)k_lanczos_p<Real, TPT, R, true, 2, 512>);
+    cudaGetLastError();   // a hint: a refusal changes nothing
+}
+
+template <typename Real, int TPT>
+static void prefer_l1(int R) {
+    switch (R) {
+        case 1: prefer_l1_r<Real, TPT, 1>(); break;
+        case 2: prefer_l1_r<Real, TPT, 2>(); break;
+        case 3: if constexpr (sizeof(Real) == 4) prefer_l1_r<Real, TPT, 3>(); break;
+        case 4: prefer_l1_r<Real, TPT, 4>(); break;
+        default: prefer_l1_r<Real, TPT, 8>(); break;
+    }
+}
+
 dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R, int staged, int groups) {
     BatchedState* bs = c->bat;
     const int B = bs->B, n = c->n;
@@ -2832,6 +2863,11 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         if (e != cudaSuccess) return DQ_ERR_ARG;
         dq_status st = build_tmaps(c, tc, SR);
         if (st) return st;
+    }
+    if (staged == 5 || staged == 8) {
+        if (!bs->mixed) prefer_l1<double, 1>(R);
+        else if (tpt == 2) prefer_l1<float, 2>(R);
+        else prefer_l1<float, 1>(R);
     }
     bs->TC = tc;
     bs->TPT = tpt;
