@@ -654,7 +654,7 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
             blk_prefetch(P, k + RPC < k1, k + RPC, bptr, rec);
         }
         // the diagonal is loaded before the gathers; the rows of q_{j-1} and
-        // q_{j-2} are only prefetched into L2 then (no registers held across
+        // q_{j-2} are only prefetched into L1 then (no registers held across
         // the gather loop) and read after it together with the block's own
         // rows of the gathered vector, which its neighbours' gathers have
         // just brought into L1
@@ -665,8 +665,8 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
             const int row = min(row0 + i, n - 1);
             const size_t base = (size_t)row * B + b0;
             if constexpr (!kFirst) {
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(qm1 + 2 * base));
-                if (qm2) asm volatile("prefetch.global.L2 [%0];" ::"l"(qm2 + 2 * base));
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(qm1 + 2 * base));
+                if (qm2) asm volatile("prefetch.global.L1 [%0];" ::"l"(qm2 + 2 * base));
             }
 #pragma unroll
             for (int t = 0; t < TPT; ++t) {
@@ -1934,59 +1934,64 @@ constexpr int kReorthKB = 8;
 constexpr int kReorthTicket = 9;
 constexpr size_t kTicketWords = kReorthTicket + (kMaxL + kReorthKB - 1) / kReorthKB;
 
-template <typename Real, int TPT>
-__global__ void __launch_bounds__(kBThreads) k_reorth_dots_b(int n, int B, int TC, int rpc, int j,
-                                                            const Real* __restrict__ slabs, size_t slab_stride,
-                                                            BatchedScalars S, unsigned int* tickets, int cy0,
-                                                            int nch) {
+template <typename Real>
+__global__ void __launch_bounds__(kBThreads, 2) k_reorth_dots_b(int n, int B, int TC, int rpc, int j,
+                                                               const Real* __restrict__ slabs, size_t slab_stride,
+                                                               BatchedScalars S, unsigned int* tickets, int cy0,
+                                                               int nch) {
+    // one trajectory per lane whatever the tiling (fewer live sums per
+    // thread, so two CTAs fit per SM), two rows per trip so that 18
+    // independent loads are in flight per thread
     constexpr int KQ = 2 * kReorthKB;   // complex h_k as two real sums each
     const int chunk = blockIdx.y + cy0, kb = blockIdx.z;
     const int k_first = 1 + kb * kReorthKB;
-    const int TPR = TC / TPT;
-    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
-    const int RPC = blockDim.x / TPR;
-    const int b0 = chunk * TC + tr * TPT;
+    const int tr = threadIdx.x % TC, rl = threadIdx.x / TC;
+    const int RPC = blockDim.x / TC;
+    const int b = chunk * TC + tr;
     const int r0 = blockIdx.x * rpc, r1 = min(n, r0 + rpc);
     if (chunk_converged(S, chunk)) return;
     const Real* r = slabs + 2 * slab_stride * (j + 1);
-    double h[KQ][TPT];
-    double sck[kReorthKB][TPT];
+    double h[KQ][1];
+    double sck[kReorthKB];
 #pragma unroll
-    for (int q = 0; q < kReorthKB; ++q)
-#pragma unroll
-        for (int t = 0; t < TPT; ++t) {
-            const int k = k_first + q;
-            sck[q][t] = k <= j ? S.sc[(size_t)k * B + b0 + t] : 0.0;
-            h[2 * q][t] = h[2 * q + 1][t] = 0.0;
-        }
-    for (int row = r0 + rl; row < r1; row += RPC) {
-        const size_t base = (size_t)row * B + b0;
-        const CV<Real, TPT> v = ldv<Real, TPT, false>(r, base);
+    for (int q = 0; q < kReorthKB; ++q) {
+        const int k = k_first + q;
+        sck[q] = k <= j ? S.sc[(size_t)k * B + b] : 0.0;
+        h[2 * q][0] = h[2 * q + 1][0] = 0.0;
+    }
+    for (int row = r0 + rl; row < r1; row += 2 * RPC) {
+        const int row2 = row + RPC;
+        const bool two = row2 < r1;
+        const size_t base = (size_t)row * B + b, base2 = (size_t)(two ? row2 : row) * B + b;
+        const CV<Real, 1> v = ldv<Real, 1, false>(r, base);
+        const CV<Real, 1> v2 = ldv<Real, 1, false>(r, base2);
+        CV<Real, 1> x[kReorthKB], x2[kReorthKB];
 #pragma unroll
         for (int q = 0; q < kReorthKB; ++q) {
-            const int k = k_first + q;
-            if (k > j) break;
-            const CV<Real, TPT> x = ldv<Real, TPT, false>(slabs + 2 * slab_stride * k, base);
+            const int k = min(k_first + q, j);   // past j: a valid slab, weight 0
+            x[q] = ldv<Real, 1, false>(slabs + 2 * slab_stride * k, base);
+            x2[q] = ldv<Real, 1, false>(slabs + 2 * slab_stride * k, base2);
+        }
+        const double w2 = two ? 1.0 : 0.0;
 #pragma unroll
-            for (int t = 0; t < TPT; ++t) {
-                const double qr = sck[q][t] * x.v[2 * t], qi = sck[q][t] * x.v[2 * t + 1];
-                const double vr = v.v[2 * t], vi = v.v[2 * t + 1];
-                h[2 * q][t] += qr * vr + qi * vi;   // conj(q) v
-                h[2 * q + 1][t] += qr * vi - qi * vr;
-            }
+        for (int q = 0; q < kReorthKB; ++q) {
+            const double qr = sck[q] * x[q].v[0], qi = sck[q] * x[q].v[1];
+            const double pr = sck[q] * w2 * x2[q].v[0], pi = sck[q] * w2 * x2[q].v[1];
+            h[2 * q][0] += qr * v.v[0] + qi * v.v[1] + (pr * v2.v[0] + pi * v2.v[1]);   // conj(q) v
+            h[2 * q + 1][0] += qr * v.v[1] - qi * v.v[0] + (pr * v2.v[1] - pi * v2.v[0]);
         }
     }
     __shared__ double red[KQ * kMaxTC];
-    __shared__ double rsm[kBThreads * 2];
+    __shared__ double rsm[kBThreads];
     // each k block has its own tickets (one per chunk) and partial region
     double* part = S.partial + (size_t)kb * nch * gridDim.x * KQ * TC;
-    if (chunk_reduce_multi<KQ, TPT>(h, TC, part, tickets + (size_t)kb * nch, red, chunk, rsm)) {
+    if (chunk_reduce_multi<KQ, 1>(h, TC, part, tickets + (size_t)kb * nch, red, chunk, rsm)) {
         if (threadIdx.x < TC) {
-            const int b = chunk * TC + threadIdx.x;
+            const int bb = chunk * TC + threadIdx.x;
             for (int q = 0; q < kReorthKB; ++q) {
                 const int k = k_first + q;
                 if (k > j) break;
-                const size_t kbb = (size_t)k * B + b;
+                const size_t kbb = (size_t)k * B + bb;
                 S.yt[2 * kbb] = red[(2 * q) * TC + threadIdx.x];
                 S.yt[2 * kbb + 1] = red[(2 * q + 1) * TC + threadIdx.x];
             }
@@ -3377,14 +3382,16 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
                                                        bs->chunks);
     if (c->cfg.reorth) {
         if (tm) tm->mark(DQ_KIND_AXPY, st);
-        // every h_k in one launch: about two CTAs per SM over (rows, chunks, blocks of k)
+        // every h_k in one launch: about four CTAs per SM over (rows, chunks, blocks of k)
         const int nkb = (j + kReorthKB - 1) / kReorthKB;
-        const int TPR = TC / TPT, RPCr = kBThreads / TPR;
-        int gxr = std::max(1, (2 * bs->sms) / (ncy * nkb));
+        const int RPCr = kBThreads / TC;
+        int gxr = std::max(1, (4 * bs->sms) / (ncy * nkb));
+        // the partials of every (block of k, chunk, CTA) fit the two partial regions
+        while (gxr > 1 && (size_t)nkb * gxr * 2 * kReorthKB * B > 2 * bs->partial_cap) --gxr;
         int rpcr = (n + gxr - 1) / gxr;
-        rpcr = ((rpcr + RPCr - 1) / RPCr) * RPCr;
+        rpcr = ((rpcr + 2 * RPCr - 1) / (2 * RPCr)) * (2 * RPCr);
         gxr = (n + rpcr - 1) / rpcr;
-        k_reorth_dots_b<Real, TPT><<<dim3(gxr, ncy, nkb), kBThreads, 0, st>>>(
+        k_reorth_dots_b<Real><<<dim3(gxr, ncy, nkb), kBThreads, 0, st>>>(
             n, B, TC, rpcr, j, slabs, se, bs->s, bs->s.tickets + kReorthTicket * (size_t)B, cy0, bs->chunks);
         k_reorth_apply_b<Real, TPT><<<grid, kBThreads, 0, st>>>(n, B, TC, rpc, j, slabs, se, bs->s, cy0, bs->chunks);
     }

@@ -5,6 +5,9 @@ m = 20, complex64) for a few steps with a fixed tiling, no autotuning and no
 CPU oracle, so a capture sees only the propagator's own launches:
 
     python -m dynaquant_b200.profile_run --steps 2 [--tiling 32,2,4] [--B 256] [--zz 253]
+    python -m dynaquant_b200.profile_run --around 120 --along 1000 --cutoff 40 --m 24 --B 128
+
+(the second line: the 120,000-site tube of the large workload, with fewer trajectories).
 
 --zz N swaps the OU noise for the ZZ model with N oscillators of an Ohmic
 spectral density on a 8.1357 cm^-1 grid at 77 K.
@@ -26,7 +29,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--B", type=int, default=256)
+    ap.add_argument("--around", type=int, default=60)
     ap.add_argument("--along", type=int, default=500)
+    ap.add_argument("--cutoff", type=float, default=25.0)
     ap.add_argument("--m", type=int, default=20)
     ap.add_argument("--tiling", default="")
     ap.add_argument("--fp64", action="store_true")
@@ -34,7 +39,7 @@ def main():
     args = ap.parse_args()
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
-    s = systems.tube(60, args.along, cutoff=25.0)
+    s = systems.tube(args.around, args.along, cutoff=args.cutoff)
     p = dq.Propagator(s.n, m=args.m, n_traj=args.B, dt=0.5, noise=dq.NOISE_ZZ if args.zz else dq.NOISE_OU,
                       sigma_static=150.0, seed=2024, dot=dq.DOT_HERMITIAN,
                       precision=dq.PREC_FP64 if args.fp64 else dq.PREC_MIXED, pop_every=16,
