@@ -2005,6 +2005,14 @@ __global__ void __launch_bounds__(kBThreads) k_reorth_apply_b(int n, int B, int 
     const Tile<TPT> T(TC, rpc, n, cy0);
     if (chunk_converged(S, T.chunk)) return;
     Real* r = slabs + 2 * slab_stride * (j + 1);
+    // sc_k h_k of the CTA's trajectories, staged once instead of re-read per row
+    __shared__ double2 hs[kMaxL][kMaxTC];
+    for (int e = threadIdx.x; e < j * TC; e += blockDim.x) {
+        const int k = 1 + e / TC, t = e % TC;
+        const size_t kb = (size_t)k * B + T.chunk * TC + t;
+        hs[k][t] = make_double2(S.yt[2 * kb] * S.sc[kb], S.yt[2 * kb + 1] * S.sc[kb]);
+    }
+    __syncthreads();
     double nn[TPT], zero[TPT];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) { nn[t] = 0.0; zero[t] = 0.0; }
@@ -2014,14 +2022,23 @@ __global__ void __launch_bounds__(kBThreads) k_reorth_apply_b(int n, int B, int 
         double vr[TPT], vi[TPT];
 #pragma unroll
         for (int t = 0; t < TPT; ++t) { vr[t] = v0.v[2 * t]; vi[t] = v0.v[2 * t + 1]; }
-        for (int k = 1; k <= j; ++k) {
-            const CV<Real, TPT> x = ldv<Real, TPT, false>(slabs + 2 * slab_stride * k, base);
+        // eight q_k rows in flight at a time (the loads of a block are independent)
+        for (int k0 = 1; k0 <= j; k0 += kReorthKB) {
+            CV<Real, TPT> x[kReorthKB];
 #pragma unroll
-            for (int t = 0; t < TPT; ++t) {
-                const size_t kb = (size_t)k * B + T.b0 + t;
-                const double s = S.sc[kb], hr = S.yt[2 * kb] * s, hi = S.yt[2 * kb + 1] * s;
-                vr[t] -= hr * x.v[2 * t] - hi * x.v[2 * t + 1];
-                vi[t] -= hr * x.v[2 * t + 1] + hi * x.v[2 * t];
+            for (int q = 0; q < kReorthKB; ++q)
+                x[q] = ldv<Real, TPT, false>(slabs + 2 * slab_stride * min(k0 + q, j), base);
+#pragma unroll
+            for (int q = 0; q < kReorthKB; ++q) {
+                const int k = k0 + q;
+                if (k > j) break;
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    const double2 hk = hs[k][T.tr * TPT + t];
+                    const double hr = hk.x, hi = hk.y;
+                    vr[t] -= hr * x[q].v[2 * t] - hi * x[q].v[2 * t + 1];
+                    vi[t] -= hr * x[q].v[2 * t + 1] + hi * x[q].v[2 * t];
+                }
             }
         }
         CV<Real, TPT> o;
