@@ -201,7 +201,7 @@ def dominant_kernel(s, B, m, staged, prof):
         # fused forms: the dominant launch is the whole iteration
         ms = prof["fused_iter"][0]
     b = spmm_bytes(s, B)
-    if staged in (0, 5):
+    if staged in (0, 5, 9):
         # the L1 forms also read q_{j-1} (8 B per site-trajectory) in m - 1 of the step's m launches
         b += 8.0 * s.n * B * (m - 1) / m
     if staged in (2, 4):
@@ -231,6 +231,8 @@ SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", None),
               6: ("k_spmm_ring (TMA ring gathers + alpha)", "k_spmm_ring_tube60x500.md"),
               7: ("k_spmm_ring, 4 trajectories per lane (TMA ring gathers + alpha)", None),
               8: ("k_lanczos_p (one launch per iteration: gathers p_j, writes q_j and p_{j+1}, alpha and beta)",
+                  None),
+              9: ("k_spmm_cpa (gathers as asynchronous copies into shared memory + alpha, minus beta q_{j-1})",
                   None)}
 
 

@@ -405,6 +405,17 @@ __device__ __forceinline__ void union_any(int pb, int pe, const int* __restrict_
     }
 }
 
+// Rows of the gathered slab about to enter a CTA's gather window are
+// prefetched into L2, so that the gathers meet L2 hits instead of DRAM
+// latency: the whole first window at the start, then each block's rows
+// pf_lead rows ahead (the matrix bandwidth plus two CTA steps).
+__device__ __forceinline__ void prefetch_row_l2(const float* base, int row, int n, int B, int b0) {
+    if (row >= 0 && row < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 2 * ((size_t)row * B + b0)));
+}
+__device__ __forceinline__ void prefetch_row_l2(const double* base, int row, int n, int B, int b0) {
+    if (row >= 0 && row < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 2 * ((size_t)row * B + b0)));
+}
+
 // Row-blocked SpMM: w = H q_j for all trajectories of the chunk, R rows per
 // block.  kWrite: also alpha_j[b] = <q_j, w>_b; !kWrite: ||H q_j||_b only.
 // With rjm (kWrite, j >= 2) the kernel writes w = H q_j - beta_{j-1} q_{j-1}
@@ -418,7 +429,8 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
                                                        const int* __restrict__ bptr, const int* __restrict__ bcol,
                                                        const Real* __restrict__ bcoef, const Real* __restrict__ d,
                                                        const Real* __restrict__ rj, const Real* __restrict__ rjm,
-                                                       Real* __restrict__ w, BatchedScalars S, int cy0, int nch) {
+                                                       Real* __restrict__ w, BatchedScalars S, int cy0, int nch,
+                                                       int bw = -1, int pf_lead = 0) {
     const int TPR = TC / TPT;
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int RPC = blockDim.x / TPR;
@@ -426,6 +438,8 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
     if (chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + tr * TPT;
     const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
+    if (bw >= 0)
+        for (int r = k0 * R - bw + rl; r < k0 * R + pf_lead; r += RPC) prefetch_row_l2(rj, r, n, B, b0);
     double sc[TPT], ar[TPT], ai[TPT];
     Real fm[TPT];
 #pragma unroll
@@ -451,6 +465,9 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
             cur = P;
             blk_prefetch(P, k + RPC < k1, k + RPC, bptr, rec);
         }
+        if (bw >= 0)
+#pragma unroll
+            for (int i = 0; i < R; ++i) prefetch_row_l2(rj, row0 + pf_lead + i, n, B, b0);
         // the block's own rows and diagonal are loaded first and used only
         // after the union loop, so their latency hides under the gathers
         CV<Real, TPT> acc[R], xo[R];
@@ -600,7 +617,8 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
                                                   const Real* __restrict__ bcoef, const Real* __restrict__ d,
                                                   const Real* __restrict__ pin, const Real* __restrict__ qm1,
                                                   const Real* __restrict__ qm2, Real* __restrict__ qout,
-                                                  Real* __restrict__ pout, BatchedScalars S, int nch) {
+                                                  Real* __restrict__ pout, BatchedScalars S, int nch, int bw = -1,
+                                                  int pf_lead = 0) {
     constexpr bool kFirst = kMode == 0, kLast = kMode == 2;
     constexpr int K = kLast ? 1 : (kBilinear ? 6 : 4);
     const int TPR = TC / TPT;
@@ -644,6 +662,8 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
         for (int q = 0; q < K; ++q) sum[q][t] = 0.0;
     constexpr bool kPk = sizeof(Real) == 4 && R <= 3;
     const float4* rec = reinterpret_cast<const float4*>(bcoef);
+    if (bw >= 0)
+        for (int r = k0 * R - bw + rl; r < k0 * R + pf_lead; r += RPC) prefetch_row_l2(pin, r, n, B, b0);
     BlkPre P;
     if constexpr (kPk) blk_prefetch(P, k0 + rl < k1, k0 + rl, bptr, rec);
     for (int k = k0 + rl; k < k1; k += RPC) {
@@ -653,6 +673,9 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
             cur = P;
             blk_prefetch(P, k + RPC < k1, k + RPC, bptr, rec);
         }
+        if (bw >= 0)
+#pragma unroll
+            for (int i = 0; i < R; ++i) prefetch_row_l2(pin, row0 + pf_lead + i, n, B, b0);
         // the diagonal is loaded before the gathers; the rows of q_{j-1} and
         // q_{j-2} are only prefetched into L1 then (no registers held across
         // the gather loop) and read after it together with the block's own
@@ -775,6 +798,180 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
                 S.alpha[2 * kj + 1] = ai;
                 S.beta[kj] = bt;
                 S.sc[(size_t)(j + 1) * B + b] = bt > 0.0 ? 1.0 : 0.0;
+            }
+        }
+    }
+}
+
+// Row-blocked SpMM whose gathers are asynchronous copies into shared memory
+// (staged = 9; complex64, packed records, R <= 3, TC = 64, 2 trajectories per
+// lane, 512-thread CTAs).  In k_spmm_blk every gathered row waits in the
+// registers of the warp that asked for it, so the registers bound the gathers
+// in flight (four per warp).  Here lane l of the warp that owns a row block
+// issues cp.async.ca (16 bytes, through L1) of its two trajectories of each
+// gathered row into its own slot of a per-warp ring of kCpaStages groups of
+// four records, commits one group at a time and keeps kCpaStages - 1 groups in
+// flight (12 rows per warp); it reads each group back from its own slots
+// after cp.async.wait_group, so no lane waits for another and no barrier is
+// involved.  The block's records are staged once per block in a per-warp
+// shared buffer (at most kCpaMaxRec; dq_set_tiling refuses larger blocks) and
+// read by broadcast.  Everything after the gathers (the minus beta q_{j-1}
+// start value, the diagonal, alpha or the norm) is k_spmm_blk's.
+constexpr int kCpaStages = 4;
+constexpr int kCpaMaxRec = 128;
+constexpr int kCpaWarps = 16;
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+inline size_t cpa_smem_bytes() {
+    return (size_t)kCpaWarps * ((size_t)kCpaStages * 4 * 32 * sizeof(float4) + (size_t)kCpaMaxRec * sizeof(float4));
+}
+
+template <int R, bool kBilinear, bool kWrite>
+__global__ void __launch_bounds__(512, 1) k_spmm_cpa(int n, int B, int bpc, int nb, int j,
+                                                    const int* __restrict__ bptr, const float4* __restrict__ rec,
+                                                    const float* __restrict__ d, const float* __restrict__ rj,
+                                                    const float* __restrict__ rjm, float* __restrict__ w,
+                                                    BatchedScalars S, int nch, int bw = -1, int pf_lead = 0) {
+    constexpr int TPT = 2, TC = 64;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float4* ring = reinterpret_cast<float4*>(smem_raw) + (size_t)warp * kCpaStages * 4 * 32;
+    float4* recs = reinterpret_cast<float4*>(smem_raw) + (size_t)kCpaWarps * kCpaStages * 4 * 32 +
+                   (size_t)warp * kCpaMaxRec;
+    const int chunk = blockIdx.y;
+    if (chunk_converged(S, chunk)) return;
+    const int b0 = chunk * TC + lane * TPT;
+    const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
+    double sc[TPT], ar[TPT], ai[TPT];
+    float fm[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        sc[t] = S.sc[(size_t)j * B + b0 + t];
+        ar[t] = 0.0;
+        ai[t] = 0.0;
+        fm[t] = 0.f;
+        if (rjm) {
+            const size_t km = (size_t)(j - 1) * B + b0 + t;
+            fm[t] = sc[t] != 0.0 ? (float)(S.beta[km] * S.sc[km] / sc[t]) : 0.f;
+        }
+    }
+    const float* lane_src = rj + 2 * (size_t)b0;   // this lane's two trajectories of row 0
+    if (bw >= 0)
+        for (int r = k0 * R - bw + warp; r < k0 * R + pf_lead; r += kCpaWarps) prefetch_row_l2(rj, r, n, B, b0);
+    for (int k = k0 + warp; k < k1; k += kCpaWarps) {
+        const int row0 = k * R;
+        if (bw >= 0)
+#pragma unroll
+            for (int i = 0; i < R; ++i) prefetch_row_l2(rj, row0 + pf_lead + i, n, B, b0);
+        const int pb = __ldg(bptr + k), pe = __ldg(bptr + k + 1);
+        const int nrec = pe - pb;   // a multiple of 4, at most kCpaMaxRec
+        __syncwarp();   // every lane is done with the previous block's records
+        for (int e = lane; e < nrec; e += 32) recs[e] = __ldg(rec + pb + e);
+        // the block's own rows, diagonal and q_{j-1}, used after the gathers
+        CV<float, TPT> acc[R], xo[R];
+        float dd[R][TPT];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int row = min(row0 + i, n - 1);
+            const size_t base = (size_t)row * B + b0;
+            xo[i] = ldv<float, TPT, true>(rj, base);
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                dd[i][t] = row0 + i < n ? __ldg(d + base + t) : 0.f;
+                acc[i].v[2 * t] = 0.f;
+                acc[i].v[2 * t + 1] = 0.f;
+            }
+            if (rjm) {
+                const CV<float, TPT> xm = ldv_cs<float, TPT>(rjm, base);
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    acc[i].v[2 * t] = -fm[t] * xm.v[2 * t];
+                    acc[i].v[2 * t + 1] = -fm[t] * xm.v[2 * t + 1];
+                }
+            }
+        }
+        __syncwarp();   // the records are in the buffer
+        const int ng = nrec >> 2;
+        auto issue = [&](int g) {
+            float4* slot = ring + (size_t)(g % kCpaStages) * 4 * 32 + lane;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int c = __float_as_int(recs[4 * g + q].x);
+                cp_async16(slot + q * 32, lane_src + 2 * (size_t)c * B);
+            }
+        };
+#pragma unroll
+        for (int g = 0; g < kCpaStages - 1; ++g) {
+            if (g < ng) issue(g);
+            cp_async_commit();
+        }
+        for (int g = 0; g < ng; ++g) {
+            if (g + kCpaStages - 1 < ng) issue(g + kCpaStages - 1);
+            cp_async_commit();
+            cp_async_wait<kCpaStages - 1>();   // group g has landed in this lane's slots
+            const float4* slot = ring + (size_t)(g % kCpaStages) * 4 * 32 + lane;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float4 yv = slot[q * 32];
+                CV<float, TPT> y;
+                y.v[0] = yv.x; y.v[1] = yv.y; y.v[2] = yv.z; y.v[3] = yv.w;
+                const float4 r = recs[4 * g + q];
+                cfma<float, TPT>(acc[0], r.y, y);
+                if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], r.z, y);
+                if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], r.w, y);
+            }
+        }
+        cp_async_wait<0>();
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                acc[i].v[2 * t] = fmaf(dd[i][t], xo[i].v[2 * t], acc[i].v[2 * t]);
+                acc[i].v[2 * t + 1] = fmaf(dd[i][t], xo[i].v[2 * t + 1], acc[i].v[2 * t + 1]);
+            }
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int row = row0 + i;
+            if (row >= n) break;
+            const size_t base = (size_t)row * B + b0;
+            if (kWrite) {
+                const CV<float, TPT>& x = xo[i];
+                CV<float, TPT> o;
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    o.v[2 * t] = (float)(sc[t] * (double)acc[i].v[2 * t]);
+                    o.v[2 * t + 1] = (float)(sc[t] * (double)acc[i].v[2 * t + 1]);
+                    const double xr = x.v[2 * t], xi = x.v[2 * t + 1], ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
+                    if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
+                    else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+                }
+                stv<float, TPT>(w, base, o);
+            } else {
+#pragma unroll
+                for (int t = 0; t < TPT; ++t)
+                    ar[t] += (double)acc[i].v[2 * t] * acc[i].v[2 * t] + (double)acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
+            }
+        }
+    }
+    __syncthreads();   // the ring becomes the reduction scratch
+    __shared__ double2 red[kMaxTC];
+    double2* rscratch = reinterpret_cast<double2*>(smem_raw);
+    if (chunk_reduce_s<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk, rscratch)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            const double s = S.sc[(size_t)j * B + b];
+            const double2 v = red[threadIdx.x];
+            if (kWrite) {
+                S.alpha[2 * ((size_t)j * B + b)] = v.x * s * s;
+                S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s * s;
+            } else {
+                S.nav[b] = sqrt(v.x) * s;
             }
         }
     }
@@ -2484,6 +2681,7 @@ static dq_status build_fmt(dq_ctx* c, int R, BlockFmt& f) {
         }
         f.packed = true;
         f.nunion = rec.size();
+        for (int k = 0; k < nb; ++k) f.max_block = std::max(f.max_block, pptr[k + 1] - pptr[k]);
         DQ_CU(cudaMalloc(&f.bptr, sizeof(int) * (nb + 1)));
         DQ_CU(cudaMemcpy(f.bptr, pptr.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice));
         DQ_CU(cudaMalloc(&f.bcoef, sizeof(float4) * std::max<size_t>(rec.size(), 1)));
@@ -2671,6 +2869,15 @@ static size_t fused_smem(int tc, int sr, int hb, int D, size_t rsz) {
 
 // Tiling: TC trajectories per chunk, TPT per thread, ~ctas_per_sm CTAs per
 // SM, R rows per SpMM block, staged: TMA shared-memory window SpMM.
+template <int R>
+static cudaError_t cpa_attr(int bytes) {
+    cudaError_t e = raise_smem_limit(k_spmm_cpa<R, false, true>, bytes);
+    if (e == cudaSuccess) e = raise_smem_limit(k_spmm_cpa<R, true, true>, bytes);
+    if (e == cudaSuccess) e = raise_smem_limit(k_spmm_cpa<R, false, false>, bytes);
+    if (e == cudaSuccess) e = raise_smem_limit(k_spmm_cpa<R, true, false>, bytes);
+    return e;
+}
+
 // The L1-gather forms in 512-thread CTAs (k_spmm_blk of staged 5, k_lanczos_p
 // of staged 8) keep their gather window in L1: ask for the largest L1 share of
 // the SM's unified L1/shared memory (their own shared memory is a few KB).
@@ -2709,11 +2916,14 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
-    if (staged < 0 || staged > 8) return DQ_ERR_ARG;
+    if (staged < 0 || staged > 9) return DQ_ERR_ARG;
     // reorthogonalisation runs between the axpy and the next SpMM: not in the fused forms
     if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4 || staged == 8)) return DQ_ERR_ARG;
     // p-form iteration: one launch per iteration over all chunks
     if (staged == 8 && (groups != 1 || c->cfg.m < 2)) return DQ_ERR_ARG;
+    // asynchronous-copy gathers: complex64 packed records, one warp per 64-trajectory block, one CTA per SM
+    if (staged == 9 && (!bs->mixed || R > 3 || tc != 64 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
+        return DQ_ERR_ARG;
     // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane in the other
     // kernels (the ring itself takes 2 per lane with staged 6, 4 with staged 7), one CTA per SM
     const bool ring = staged == 6 || staged == 7;
@@ -2728,7 +2938,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (groups < 1 || chunks % groups) return DQ_ERR_ARG;
     const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
-    const int RPC_spmm = (staged == 5 || staged == 8 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
+    const int RPC_spmm = (staged == 5 || staged == 8 || staged == 9 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
     // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide:
     // one wave of kStreamCtasPerSm CTAs per SM while every thread still walks
     // several rows, twice as many CTAs when that wave would leave each thread
@@ -2752,6 +2962,20 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->fmt[ri].bptr) {
         dq_status st = build_fmt(c, R, bs->fmt[ri]);
         if (st) return st;
+    }
+    if (staged == 9) {
+        if (bs->fmt[ri].max_block > kCpaMaxRec) return DQ_ERR_ARG;
+        cudaError_t e = cudaSuccess;
+        const int bytes = (int)cpa_smem_bytes();
+        switch (R) {
+            case 1: e = cpa_attr<1>(bytes); break;
+            case 2: e = cpa_attr<2>(bytes); break;
+            default: e = cpa_attr<3>(bytes); break;
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return DQ_ERR_ARG;
+        }
     }
     if (staged == 8) {
         // six sums per trajectory per CTA in the partials; p_j ping-pongs between slab 0 and wB
@@ -3140,8 +3364,19 @@ struct StepTimer {
     }
 };
 
+// L2 prefetch of the gathered slab ahead of the L1-gather forms: the matrix
+// bandwidth (how far the window reaches back and ahead) and the lead of the
+// per-block prefetch, the bandwidth plus two CTA steps of row blocks.
+static int pf_bw(const BatchedState* bs) { return bs->bw; }
+static int pf_lead(const BatchedState* bs, int threads) {
+    const int TPR = bs->TC / bs->TPT;
+    return bs->bw + 2 * (threads / TPR) * bs->R;
+}
+
 // The forms that run k_spmm_blk (L1 gathers, 256- or 512-thread CTAs).
-static bool spmm_subtracts_prev(const BatchedState* bs) { return bs->staged == 0 || bs->staged == 5; }
+static bool spmm_subtracts_prev(const BatchedState* bs) {
+    return bs->staged == 0 || bs->staged == 5 || bs->staged == 9;
+}
 
 template <typename Real, int TPT, bool kBil, bool kWrite>
 static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real* w, int cy0, int ncy) {
@@ -3191,6 +3426,23 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real*
         }
         return;
     }
+    if (bs->staged == 9) {
+        if constexpr (sizeof(Real) == 4 && TPT == 2) {
+            const dim3 grid(bs->gxs, ncy);
+            const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
+            const size_t sm = cpa_smem_bytes();
+#define DQ_CPA_R(RR)                                                                                          \
+    k_spmm_cpa<RR, kBil, kWrite><<<grid, 512, sm, c->stream>>>(n, B, bs->bpc, f.nb, j, f.bptr, rec, d, rj, rjm, w, \
+                                                               bs->s, bs->chunks, pf_bw(bs), pf_lead(bs, 512))
+            switch (bs->R) {
+                case 1: DQ_CPA_R(1); break;
+                case 2: DQ_CPA_R(2); break;
+                default: DQ_CPA_R(3); break;
+            }
+#undef DQ_CPA_R
+        }
+        return;
+    }
     if (bs->staged == 3) {
         if constexpr (sizeof(Real) == 4) {
             const dim3 grid(bs->gxs, ncy);
@@ -3214,11 +3466,13 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real*
     if (bs->staged == 5)                                                                                         \
         k_spmm_blk<Real, TPT, RR, kBil, kWrite, 512><<<grid, 512, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j,     \
                                                                                  f.bptr, f.bcol, cf, d, rj, rjm, w, \
-                                                                                 bs->s, cy0, bs->chunks);        \
+                                                                                 bs->s, cy0, bs->chunks, pf_bw(bs),  \
+                                                                                 pf_lead(bs, 512));              \
     else                                                                                                         \
         k_spmm_blk<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j,    \
                                                                                    f.bptr, f.bcol, cf, d, rj, rjm, w, \
-                                                                                   bs->s, cy0, bs->chunks)
+                                                                                   bs->s, cy0, bs->chunks, pf_bw(bs), \
+                                                                                   pf_lead(bs, kBThreads))
     switch (bs->R) {
         case 1: DQ_SPMM_R(1); break;
         case 2: DQ_SPMM_R(2); break;
@@ -3310,7 +3564,7 @@ static void launch_pform_m(dq_ctx* c, int j) {
 #define DQ_PF_R(RR)                                                                                               \
     k_lanczos_p<Real, TPT, RR, kBil, kMode, 512><<<grid, 512, 0, c->stream>>>(                                     \
         n, B, bs->TC, bs->bpc, f.nb, j, f.bptr, f.bcol, (const Real*)f.bcoef, (const Real*)bs->diag, pin, qm1, qm2, \
-        qout, pout, bs->s, bs->chunks)
+        qout, pout, bs->s, bs->chunks, pf_bw(bs), pf_lead(bs, 512))
     switch (bs->R) {
         case 1: DQ_PF_R(1); break;
         case 2: DQ_PF_R(2); break;

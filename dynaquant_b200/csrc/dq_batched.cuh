@@ -174,6 +174,7 @@ struct Tile {
 // one gathered trajectory row serves R output rows.
 struct BlockFmt {
     int R = 0, nb = 0;
+    int max_block = 0;       // most union entries (records) of one block
     size_t nunion = 0;
     bool packed = false;     // 16-byte records {col, c0, c1, c2}, blocks padded to 4 entries
     int* bptr = nullptr;     // nb + 1

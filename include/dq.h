@@ -250,7 +250,10 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * traj_chunk 32, vec 2, ctas_per_sm 1, rows_per_block <= 3), 8 runs each
  * Lanczos iteration as one L1-gather launch without the axpy pass (it keeps
  * p_j = H q_{j-1} - beta_{j-2} q_{j-2} instead of the residual and gathers
- * that; 512-thread CTAs; groups 1, no reorthogonalisation or adaptive m).  groups splits the
+ * that; 512-thread CTAs; groups 1, no reorthogonalisation or adaptive m), 9
+ * is form 5 with its gathers issued as asynchronous copies into per-warp
+ * shared-memory rings (complex64, traj_chunk 64, vec 2, ctas_per_sm 1,
+ * rows_per_block <= 3, at most 128 union entries per block).  groups splits the
  * trajectory chunks into groups whose m Lanczos iterations run one group
  * after another, so a group's Krylov slabs stay resident in L2 (must divide
  * n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run

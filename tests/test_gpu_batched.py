@@ -339,3 +339,32 @@ def test_pform_refuses_what_it_cannot_do():
     with pytest.raises(dq.DQError):
         q.set_tiling(8, 2, 1, 3, 8, 1)   # full reorthogonalisation
     q.close()
+
+
+@pytest.mark.parametrize("dot", [1, 0])
+@pytest.mark.parametrize("R", [1, 2, 3])
+def test_async_copy_gather_spmm_mixed_tube_matches_oracle(oracle, dot, R):
+    """The SpMM whose gathers are asynchronous copies into shared memory (staged = 9) against the FP64
+    oracle on the dipole-coupled tube."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 24)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=20, dt=0.5, dot_mode=dot, noise=2, sigma=250.0, tau=50.0,
+                      sigma_static=150.0, seed=9)
+    B, T = 128, 40
+    psi0 = s.bright_state()
+    ref = S.run(B, T, psi0, pop_every=8, threads=4)
+    p = dq.Propagator(s.n, m=20, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=9, dot=dot,
+                      pop_every=8, max_steps=T, precision=dq.PREC_MIXED)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    p.set_initial_state(psi0)
+    p.set_tiling(64, 2, 1, R, 9, 1)
+    assert p.get_tiling() == (64, 2, 1, R, 9, 1)
+    p.run(T)
+    err = np.abs(p.populations() - ref["pops"]).max()
+    assert err < POP_TOL_MIXED, err
+    assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
+    assert np.allclose(p.error_accum(), ref["err"], rtol=1e-2, atol=1e-12)
+    p.close()
