@@ -408,13 +408,12 @@ __device__ __forceinline__ void union_any(int pb, int pe, const int* __restrict_
 // Rows of the gathered slab about to enter a CTA's gather window are
 // prefetched into L2, so that the gathers meet L2 hits instead of DRAM
 // latency: the whole first window at the start, then each block's rows
-// pf_lead rows ahead (the matrix bandwidth plus two CTA steps).
+// pf_lead rows ahead (the matrix bandwidth plus two CTA steps).  Complex64
+// slabs only; the FP64 overload does nothing.
 __device__ __forceinline__ void prefetch_row_l2(const float* base, int row, int n, int B, int b0) {
     if (row >= 0 && row < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 2 * ((size_t)row * B + b0)));
 }
-__device__ __forceinline__ void prefetch_row_l2(const double* base, int row, int n, int B, int b0) {
-    if (row >= 0 && row < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 2 * ((size_t)row * B + b0)));
-}
+__device__ __forceinline__ void prefetch_row_l2(const double*, int, int, int, int) {}
 
 // Row-blocked SpMM: w = H q_j for all trajectories of the chunk, R rows per
 // block.  kWrite: also alpha_j[b] = <q_j, w>_b; !kWrite: ||H q_j||_b only.
@@ -3367,7 +3366,8 @@ struct StepTimer {
 // L2 prefetch of the gathered slab ahead of the L1-gather forms: the matrix
 // bandwidth (how far the window reaches back and ahead) and the lead of the
 // per-block prefetch, the bandwidth plus two CTA steps of row blocks.
-static int pf_bw(const BatchedState* bs) { return bs->bw; }
+// (complex64 only: the FP64 path keeps no prefetch)
+static int pf_bw(const BatchedState* bs) { return bs->mixed ? bs->bw : -1; }
 static int pf_lead(const BatchedState* bs, int threads) {
     const int TPR = bs->TC / bs->TPT;
     return bs->bw + 2 * (threads / TPR) * bs->R;
