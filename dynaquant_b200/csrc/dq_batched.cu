@@ -42,6 +42,17 @@
 
 namespace dq {
 
+// The dynamic shared memory of a kernel begins right after its static shared
+// memory, and only 16-byte alignment of that start is guaranteed, whatever the
+// declaration says; TMA destinations need 128 bytes.  The TMA-fed kernels
+// therefore round the start up themselves, from 128 bytes of padding that
+// their launches add to the dynamic size (kSmemAlignPad).
+constexpr size_t kSmemAlignPad = 128;
+__device__ __forceinline__ unsigned char* align_smem128(unsigned char* p) {
+    const uint32_t a = smem_u32(p);
+    return p + ((128u - (a & 127u)) & 127u);
+}
+
 // Budget of the bounded mbarrier waits in SM cycles: kWaitCycles (about 2 s)
 // unless a test lowers it through dq_debug_set_wait_cycles.  A negative value
 // is a test mode: each ring-SpMM CTA first waits |value| cycles on a barrier
@@ -1138,7 +1149,8 @@ __global__ void __launch_bounds__(kRingThreads, 1) k_spmm_ring(int n, int B, int
     constexpr int kWarps = kRingThreads / 32;
     constexpr int SR = kWarps * R;
     constexpr size_t row_reals = TC * 2;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char* const smem_raw = align_smem128(smem_dyn);
     __shared__ __align__(8) uint64_t bars[32];
     __shared__ __align__(8) uint64_t never_bar;   // a barrier no copy completes (the timeout test hook)
     __shared__ float4 rbuf[kWarps][32];
@@ -1375,7 +1387,8 @@ __global__ void __launch_bounds__(kBThreads) k_spmm_win(int n, int B, int TC, in
                                                        const Real* __restrict__ d, Real* __restrict__ w,
                                                        BatchedScalars S, int cy0, int nch,
                                                        const __grid_constant__ CUtensorMap tmap) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char* const smem_raw = align_smem128(smem_dyn);
     Real* win = reinterpret_cast<Real*>(smem_raw);   // [W][TC] complex
     __shared__ __align__(8) uint64_t bars[2];
     const int TPR = TC / TPT;
@@ -1545,7 +1558,8 @@ __global__ void __launch_bounds__(kBThreads) k_lanczos_fused(int n, int B, int T
                                                             const Real* __restrict__ d, Real* __restrict__ r_out,
                                                             Real* __restrict__ w_out, BatchedScalars S, int nch,
                                                             const __grid_constant__ FusedMaps maps) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char* const smem_raw = align_smem128(smem_dyn);
     __shared__ __align__(8) uint64_t bars[4];
     __shared__ double cf[kMaxTC][5];   // cw, Re/Im(alpha sc), beta sc, per trajectory of the chunk
     const int TPR = TC / TPT;
@@ -1793,7 +1807,8 @@ __global__ void __launch_bounds__(kFwThreads, 1) k_lanczos_fw(int n, int B, int 
                                                          const __grid_constant__ FusedMaps maps) {
     constexpr int TC = 32 * TPT;
     constexpr int kWarps = kFwThreads / 32;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    unsigned char* const smem_raw = align_smem128(smem_dyn);
     __shared__ __align__(8) uint64_t bars[4];
     __shared__ float4 rbuf[kWarps][32];
     __shared__ double cf[TC][4];
@@ -3000,7 +3015,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
             if (SR > 256) continue;
             const int hb = (bs->bw + SR - 1) / SR;
             for (int D = 4; D >= 2; --D) {
-                const size_t sm = std::max<size_t>(fused_smem(tc, SR, hb, D, sizeof(float)), 16384);
+                const size_t sm = std::max<size_t>(fused_smem(tc, SR, hb, D, sizeof(float)), 16384) + kSmemAlignPad;
                 if (sm + kStatic <= 227 * 1024) {
                     f_D = D; f_smem = sm; f_sr = SR; f_hb = hb; f_rb = rb;
                     break;
@@ -3031,7 +3046,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         const size_t min_sm = staged == 7 ? 32768 : 16384;
         for (int D = 4; D >= 1; --D) {
             const int NB = 2 * hb + D + 1;
-            const size_t sm = std::max<size_t>((size_t)NB * SR * 32 * 2 * sizeof(float), min_sm);
+            const size_t sm = std::max<size_t>((size_t)NB * SR * 32 * 2 * sizeof(float), min_sm) + kSmemAlignPad;
             if (NB <= 32 && sm + kStatic <= 227 * 1024) {
                 f_D = D; f_smem = sm; f_sr = SR; f_hb = hb;
                 break;
@@ -3063,7 +3078,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         constexpr size_t kStatic = 6 * 1024;
         f_D = 0;
         for (int D = 4; D >= 2; --D) {
-            const size_t sm = fused_smem(tc, SR, f_hb, D, rsz);
+            const size_t sm = fused_smem(tc, SR, f_hb, D, rsz) + kSmemAlignPad;
             if (sm <= kWinSmemMax && (size_t)ctas_per_sm * (sm + kStatic) <= 228 * 1024) {
                 f_D = D;
                 f_smem = sm;
@@ -3094,7 +3109,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         halo = ((bs->bw + SR - 1) / SR) * SR;
         int W = 1;
         while (W < 2 * halo + 2 * SR) W <<= 1;
-        smem = (size_t)W * tc * 2 * rsz;
+        smem = (size_t)W * tc * 2 * rsz + kSmemAlignPad;
         if (smem > kWinSmemMax) return DQ_ERR_ARG;
         wmask = W - 1;
         const int fit = std::max(1, (int)((228 * 1024) / (smem + 12 * 1024)));
