@@ -416,16 +416,6 @@ __device__ __forceinline__ void union_any(int pb, int pe, const int* __restrict_
     }
 }
 
-// Rows of the gathered slab about to enter a CTA's gather window are
-// prefetched into L2, so that the gathers meet L2 hits instead of DRAM
-// latency: the whole first window at the start, then each block's rows
-// pf_lead rows ahead (the matrix bandwidth plus two CTA steps).  Complex64
-// slabs only; the FP64 overload does nothing.
-__device__ __forceinline__ void prefetch_row_l2(const float* base, int row, int n, int B, int b0) {
-    if (row >= 0 && row < n) asm volatile("prefetch.global.L2 [%0];" ::"l"(base + 2 * ((size_t)row * B + b0)));
-}
-__device__ __forceinline__ void prefetch_row_l2(const double*, int, int, int, int) {}
-
 // Row-blocked SpMM: w = H q_j for all trajectories of the chunk, R rows per
 // block.  kWrite: also alpha_j[b] = <q_j, w>_b; !kWrite: ||H q_j||_b only.
 // With rjm (kWrite, j >= 2) the kernel writes w = H q_j - beta_{j-1} q_{j-1}
@@ -439,8 +429,7 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
                                                        const int* __restrict__ bptr, const int* __restrict__ bcol,
                                                        const Real* __restrict__ bcoef, const Real* __restrict__ d,
                                                        const Real* __restrict__ rj, const Real* __restrict__ rjm,
-                                                       Real* __restrict__ w, BatchedScalars S, int cy0, int nch,
-                                                       int bw = -1, int pf_lead = 0) {
+                                                       Real* __restrict__ w, BatchedScalars S, int cy0, int nch) {
     const int TPR = TC / TPT;
     const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
     const int RPC = blockDim.x / TPR;
@@ -448,8 +437,6 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
     if (chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + tr * TPT;
     const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
-    if (bw >= 0)
-        for (int r = k0 * R - bw + rl; r < k0 * R + pf_lead; r += RPC) prefetch_row_l2(rj, r, n, B, b0);
     double sc[TPT], ar[TPT], ai[TPT];
     Real fm[TPT];
 #pragma unroll
@@ -475,9 +462,6 @@ __global__ void __launch_bounds__(NT) k_spmm_blk(int n, int B, int TC, int bpc, 
             cur = P;
             blk_prefetch(P, k + RPC < k1, k + RPC, bptr, rec);
         }
-        if (bw >= 0)
-#pragma unroll
-            for (int i = 0; i < R; ++i) prefetch_row_l2(rj, row0 + pf_lead + i, n, B, b0);
         // the block's own rows and diagonal are loaded first and used only
         // after the union loop, so their latency hides under the gathers
         CV<Real, TPT> acc[R], xo[R];
@@ -627,8 +611,7 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
                                                   const Real* __restrict__ bcoef, const Real* __restrict__ d,
                                                   const Real* __restrict__ pin, const Real* __restrict__ qm1,
                                                   const Real* __restrict__ qm2, Real* __restrict__ qout,
-                                                  Real* __restrict__ pout, BatchedScalars S, int nch, int bw = -1,
-                                                  int pf_lead = 0) {
+                                                  Real* __restrict__ pout, BatchedScalars S, int nch) {
     constexpr bool kFirst = kMode == 0, kLast = kMode == 2;
     constexpr int K = kLast ? 1 : (kBilinear ? 6 : 4);
     const int TPR = TC / TPT;
@@ -672,8 +655,6 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
         for (int q = 0; q < K; ++q) sum[q][t] = 0.0;
     constexpr bool kPk = sizeof(Real) == 4 && R <= 3;
     const float4* rec = reinterpret_cast<const float4*>(bcoef);
-    if (bw >= 0)
-        for (int r = k0 * R - bw + rl; r < k0 * R + pf_lead; r += RPC) prefetch_row_l2(pin, r, n, B, b0);
     BlkPre P;
     if constexpr (kPk) blk_prefetch(P, k0 + rl < k1, k0 + rl, bptr, rec);
     for (int k = k0 + rl; k < k1; k += RPC) {
@@ -683,9 +664,6 @@ __global__ void __launch_bounds__(NT) k_lanczos_p(int n, int B, int TC, int bpc,
             cur = P;
             blk_prefetch(P, k + RPC < k1, k + RPC, bptr, rec);
         }
-        if (bw >= 0)
-#pragma unroll
-            for (int i = 0; i < R; ++i) prefetch_row_l2(pin, row0 + pf_lead + i, n, B, b0);
         // the diagonal is loaded before the gathers; the rows of q_{j-1} and
         // q_{j-2} are only prefetched into L1 then (no registers held across
         // the gather loop) and read after it together with the block's own
@@ -847,7 +825,7 @@ __global__ void __launch_bounds__(512, 1) k_spmm_cpa(int n, int B, int bpc, int 
                                                     const int* __restrict__ bptr, const float4* __restrict__ rec,
                                                     const float* __restrict__ d, const float* __restrict__ rj,
                                                     const float* __restrict__ rjm, float* __restrict__ w,
-                                                    BatchedScalars S, int nch, int bw = -1, int pf_lead = 0) {
+                                                    BatchedScalars S, int nch) {
     constexpr int TPT = 2, TC = 64;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -872,13 +850,8 @@ __global__ void __launch_bounds__(512, 1) k_spmm_cpa(int n, int B, int bpc, int 
         }
     }
     const float* lane_src = rj + 2 * (size_t)b0;   // this lane's two trajectories of row 0
-    if (bw >= 0)
-        for (int r = k0 * R - bw + warp; r < k0 * R + pf_lead; r += kCpaWarps) prefetch_row_l2(rj, r, n, B, b0);
     for (int k = k0 + warp; k < k1; k += kCpaWarps) {
         const int row0 = k * R;
-        if (bw >= 0)
-#pragma unroll
-            for (int i = 0; i < R; ++i) prefetch_row_l2(rj, row0 + pf_lead + i, n, B, b0);
         const int pb = __ldg(bptr + k), pe = __ldg(bptr + k + 1);
         const int nrec = pe - pb;   // a multiple of 4, at most kCpaMaxRec
         __syncwarp();   // every lane is done with the previous block's records
@@ -3378,16 +3351,6 @@ struct StepTimer {
     }
 };
 
-// L2 prefetch of the gathered slab ahead of the L1-gather forms: the matrix
-// bandwidth (how far the window reaches back and ahead) and the lead of the
-// per-block prefetch, the bandwidth plus two CTA steps of row blocks.
-// (complex64 only: the FP64 path keeps no prefetch)
-static int pf_bw(const BatchedState* bs) { return bs->mixed ? bs->bw : -1; }
-static int pf_lead(const BatchedState* bs, int threads) {
-    const int TPR = bs->TC / bs->TPT;
-    return bs->bw + 2 * (threads / TPR) * bs->R;
-}
-
 // The forms that run k_spmm_blk (L1 gathers, 256- or 512-thread CTAs).
 static bool spmm_subtracts_prev(const BatchedState* bs) {
     return bs->staged == 0 || bs->staged == 5 || bs->staged == 9;
@@ -3448,7 +3411,7 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real*
             const size_t sm = cpa_smem_bytes();
 #define DQ_CPA_R(RR)                                                                                          \
     k_spmm_cpa<RR, kBil, kWrite><<<grid, 512, sm, c->stream>>>(n, B, bs->bpc, f.nb, j, f.bptr, rec, d, rj, rjm, w, \
-                                                               bs->s, bs->chunks, pf_bw(bs), pf_lead(bs, 512))
+                                                               bs->s, bs->chunks)
             switch (bs->R) {
                 case 1: DQ_CPA_R(1); break;
                 case 2: DQ_CPA_R(2); break;
@@ -3481,13 +3444,11 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real*
     if (bs->staged == 5)                                                                                         \
         k_spmm_blk<Real, TPT, RR, kBil, kWrite, 512><<<grid, 512, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j,     \
                                                                                  f.bptr, f.bcol, cf, d, rj, rjm, w, \
-                                                                                 bs->s, cy0, bs->chunks, pf_bw(bs),  \
-                                                                                 pf_lead(bs, 512));              \
+                                                                                 bs->s, cy0, bs->chunks);        \
     else                                                                                                         \
         k_spmm_blk<Real, TPT, RR, kBil, kWrite><<<grid, kBThreads, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j,    \
                                                                                    f.bptr, f.bcol, cf, d, rj, rjm, w, \
-                                                                                   bs->s, cy0, bs->chunks, pf_bw(bs), \
-                                                                                   pf_lead(bs, kBThreads))
+                                                                                   bs->s, cy0, bs->chunks)
     switch (bs->R) {
         case 1: DQ_SPMM_R(1); break;
         case 2: DQ_SPMM_R(2); break;
@@ -3579,7 +3540,7 @@ static void launch_pform_m(dq_ctx* c, int j) {
 #define DQ_PF_R(RR)                                                                                               \
     k_lanczos_p<Real, TPT, RR, kBil, kMode, 512><<<grid, 512, 0, c->stream>>>(                                     \
         n, B, bs->TC, bs->bpc, f.nb, j, f.bptr, f.bcol, (const Real*)f.bcoef, (const Real*)bs->diag, pin, qm1, qm2, \
-        qout, pout, bs->s, bs->chunks, pf_bw(bs), pf_lead(bs, 512))
+        qout, pout, bs->s, bs->chunks)
     switch (bs->R) {
         case 1: DQ_PF_R(1); break;
         case 2: DQ_PF_R(2); break;
