@@ -201,7 +201,7 @@ def dominant_kernel(s, B, m, staged, prof):
         # fused forms: the dominant launch is the whole iteration
         ms = prof["fused_iter"][0]
     b = spmm_bytes(s, B)
-    if staged in (0, 5, 9):
+    if staged in (0, 5, 9, 10):
         # the L1 forms also read q_{j-1} (8 B per site-trajectory) in m - 1 of the step's m launches
         b += 8.0 * s.n * B * (m - 1) / m
     if staged in (2, 4):
@@ -233,7 +233,8 @@ SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", None),
               8: ("k_lanczos_p (one launch per iteration: gathers p_j, writes q_j and p_{j+1}, alpha and beta)",
                   None),
               9: ("k_spmm_cpa (gathers as asynchronous copies into shared memory + alpha, minus beta q_{j-1})",
-                  None)}
+                  None),
+              10: ("k_spmm_wg (warp per row block, eight gathers in flight + alpha, minus beta q_{j-1})", None)}
 
 
 def measured_traffic(staged):

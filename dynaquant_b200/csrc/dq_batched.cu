@@ -960,6 +960,170 @@ __global__ void __launch_bounds__(512, 1) k_spmm_cpa(int n, int B, int bpc, int 
     }
 }
 
+// Row-blocked SpMM with eight gathers in flight per warp (staged = 10;
+// complex64, packed records, R <= 3, TC = 64, 2 trajectories per lane, one
+// 512-thread CTA per SM).  Each warp owns whole row blocks (k0 + warp,
+// k0 + warp + 16, ...), so the 16 warps of a CTA walk one sliding window of
+// rows together and every record of a block is warp-uniform.  The records
+// arrive 32 at a time (one coalesced 16-byte load per lane, the next batch or
+// the next block's first one in flight while the current one is used) into a
+// per-warp shared buffer; a group of eight gathers is issued from the eight
+// columns read there by broadcast, and the coefficients are read again only
+// after the gathers, so the registers a warp holds across its gather wait are
+// the eight gathered values and its accumulators.  That doubles the gathers
+// in flight per warp of k_spmm_blk (four) at the same occupancy.  Everything
+// after the gathers (the minus beta q_{j-1} start value, the diagonal, alpha
+// or the norm) is k_spmm_blk's.
+constexpr int kWgWarps = 16;
+
+template <int R, bool kBilinear, bool kWrite>
+__global__ void __launch_bounds__(512, 1) k_spmm_wg(int n, int B, int bpc, int nb, int j,
+                                                   const int* __restrict__ bptr, const float4* __restrict__ rec,
+                                                   const float* __restrict__ d, const float* __restrict__ rj,
+                                                   const float* __restrict__ rjm, float* __restrict__ w,
+                                                   BatchedScalars S, int cy0, int nch) {
+    constexpr int TPT = 2, TC = 64, G = 8;
+    __shared__ float4 rbuf[kWgWarps][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int chunk = blockIdx.y + cy0;
+    if (chunk_converged(S, chunk)) return;
+    const int b0 = chunk * TC + lane * TPT;
+    const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
+    double sc[TPT], ar[TPT], ai[TPT];
+    float fm[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        sc[t] = S.sc[(size_t)j * B + b0 + t];
+        ar[t] = 0.0;
+        ai[t] = 0.0;
+        fm[t] = 0.f;
+        if (rjm) {
+            const size_t km = (size_t)(j - 1) * B + b0 + t;
+            fm[t] = sc[t] != 0.0 ? (float)(S.beta[km] * S.sc[km] / sc[t]) : 0.f;
+        }
+    }
+    const float* lane_src = rj + 2 * (size_t)b0;   // this lane's two trajectories of row 0
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4* const buf = rbuf[warp];
+    int k = k0 + warp;
+    int pb = 0, pe = 0;
+    if (k < k1) {
+        pb = __ldg(bptr + k);
+        pe = __ldg(bptr + k + 1);
+    }
+    float4 nxt = (k < k1 && lane < pe - pb) ? __ldg(rec + pb + lane) : zero4;
+    while (k < k1) {
+        const int kn = k + kWgWarps;
+        int pbn = 0, pen = 0;
+        if (kn < k1) {
+            pbn = __ldg(bptr + kn);
+            pen = __ldg(bptr + kn + 1);
+        }
+        const int row0 = k * R;
+        // the block's own rows and diagonal are loaded first and used only
+        // after the gathers, so their latency hides under them
+        CV<float, TPT> acc[R], xo[R];
+        float dd[R][TPT];
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const size_t base = (size_t)min(row0 + i, n - 1) * B + b0;
+            xo[i] = ldv<float, TPT, true>(rj, base);
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                dd[i][t] = row0 + i < n ? __ldg(d + base + t) : 0.f;
+                acc[i].v[2 * t] = 0.f;
+                acc[i].v[2 * t + 1] = 0.f;
+            }
+            if (rjm) {
+                const CV<float, TPT> xm = ldv_cs<float, TPT>(rjm, base);
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    acc[i].v[2 * t] = -fm[t] * xm.v[2 * t];
+                    acc[i].v[2 * t + 1] = -fm[t] * xm.v[2 * t + 1];
+                }
+            }
+        }
+        for (int e0 = pb; e0 < pe; e0 += 32) {
+            __syncwarp();   // every lane is done with the previous batch
+            buf[lane] = nxt;
+            __syncwarp();
+            if (e0 + 32 < pe) nxt = (e0 + 32 + lane < pe) ? __ldg(rec + e0 + 32 + lane) : zero4;
+            else nxt = (kn < k1 && lane < pen - pbn) ? __ldg(rec + pbn + lane) : zero4;
+            const int cnt = min(32, pe - e0);   // a multiple of 4
+            for (int e = 0; e < cnt; e += G) {
+                const bool two = e + 4 < cnt;   // warp-uniform: the group's second half exists
+                CV<float, TPT> y[G];
+#pragma unroll
+                for (int q = 0; q < G; ++q) {
+                    if (q < 4 || two) {
+                        const int c = __float_as_int(buf[e + q].x);
+                        const float4 v = __ldg(reinterpret_cast<const float4*>(lane_src + 2 * (size_t)c * B));
+                        y[q].v[0] = v.x; y[q].v[1] = v.y; y[q].v[2] = v.z; y[q].v[3] = v.w;
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < G; ++q) {
+                    if (q < 4 || two) {
+                        const float4 r = buf[e + q];
+                        cfma<float, TPT>(acc[0], r.y, y[q]);
+                        if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], r.z, y[q]);
+                        if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], r.w, y[q]);
+                    }
+                }
+            }
+        }
+        if (pe <= pb) nxt = (kn < k1 && lane < pen - pbn) ? __ldg(rec + pbn + lane) : zero4;
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                acc[i].v[2 * t] = fmaf(dd[i][t], xo[i].v[2 * t], acc[i].v[2 * t]);
+                acc[i].v[2 * t + 1] = fmaf(dd[i][t], xo[i].v[2 * t + 1], acc[i].v[2 * t + 1]);
+            }
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int row = row0 + i;
+            if (row >= n) break;
+            const size_t base = (size_t)row * B + b0;
+            if (kWrite) {
+                const CV<float, TPT>& x = xo[i];
+                CV<float, TPT> o;
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    o.v[2 * t] = (float)(sc[t] * (double)acc[i].v[2 * t]);
+                    o.v[2 * t + 1] = (float)(sc[t] * (double)acc[i].v[2 * t + 1]);
+                    const double xr = x.v[2 * t], xi = x.v[2 * t + 1], ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
+                    if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
+                    else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+                }
+                stv<float, TPT>(w, base, o);
+            } else {
+#pragma unroll
+                for (int t = 0; t < TPT; ++t)
+                    ar[t] += (double)acc[i].v[2 * t] * acc[i].v[2 * t] + (double)acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
+            }
+        }
+        k = kn;
+        pb = pbn;
+        pe = pen;
+    }
+    __shared__ double2 red[kMaxTC];
+    __shared__ double2 rscratch[512 * 2];
+    if (chunk_reduce_s<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk, rscratch)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            const double s = S.sc[(size_t)j * B + b];
+            const double2 v = red[threadIdx.x];
+            if (kWrite) {
+                S.alpha[2 * ((size_t)j * B + b)] = v.x * s * s;
+                S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s * s;
+            } else {
+                S.nav[b] = sqrt(v.x) * s;
+            }
+        }
+    }
+}
+
 // Warp-per-block SpMM (staged = 3; complex64, packed records, R <= 3).  All
 // 32 lanes of a warp work on one block of R rows for TC = 32 TPT
 // trajectories, so the block's column-union records are one warp-uniform
@@ -2885,6 +3049,17 @@ static void prefer_l1_r() {
     cudaGetLastError();   // a hint: a refusal changes nothing
 }
 
+template <int R>
+static void prefer_l1_wg() {
+    const int carve = cudaSharedmemCarveoutMaxL1;
+    auto set = [&](const void* f) { cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carve); };
+    set((const void*)k_spmm_wg<R, false, true>);
+    set((const void*)k_spmm_wg<R, true, true>);
+    set((const void*)k_spmm_wg<R, false, false>);
+    set((const void*)k_spmm_wg<R, true, false>);
+    cudaGetLastError();   // a hint: a refusal changes nothing
+}
+
 template <typename Real, int TPT>
 static void prefer_l1(int R) {
     switch (R) {
@@ -2903,7 +3078,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
-    if (staged < 0 || staged > 9) return DQ_ERR_ARG;
+    if (staged < 0 || staged > 10) return DQ_ERR_ARG;
     // reorthogonalisation runs between the axpy and the next SpMM: not in the fused forms
     if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4 || staged == 8)) return DQ_ERR_ARG;
     // p-form iteration: one launch per iteration over all chunks
@@ -2911,6 +3086,8 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     // asynchronous-copy gathers: complex64 packed records, one warp per 64-trajectory block, one CTA per SM
     if (staged == 9 && (!bs->mixed || R > 3 || tc != 64 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
         return DQ_ERR_ARG;
+    // eight gathers in flight per warp: the same restrictions, chunk groups allowed
+    if (staged == 10 && (!bs->mixed || R > 3 || tc != 64 || tpt != 2 || ctas_per_sm != 1)) return DQ_ERR_ARG;
     // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane in the other
     // kernels (the ring itself takes 2 per lane with staged 6, 4 with staged 7), one CTA per SM
     const bool ring = staged == 6 || staged == 7;
@@ -2925,7 +3102,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (groups < 1 || chunks % groups) return DQ_ERR_ARG;
     const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
-    const int RPC_spmm = (staged == 5 || staged == 8 || staged == 9 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
+    const int RPC_spmm = (staged == 5 || staged == 8 || staged == 9 || staged == 10 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
     // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide:
     // one wave of kStreamCtasPerSm CTAs per SM while every thread still walks
     // several rows, twice as many CTAs when that wave would leave each thread
@@ -3101,6 +3278,13 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         if (!bs->mixed) prefer_l1<double, 1>(R);
         else if (tpt == 2) prefer_l1<float, 2>(R);
         else prefer_l1<float, 1>(R);
+    }
+    if (staged == 10) {
+        switch (R) {
+            case 1: prefer_l1_wg<1>(); break;
+            case 2: prefer_l1_wg<2>(); break;
+            default: prefer_l1_wg<3>(); break;
+        }
     }
     bs->TC = tc;
     bs->TPT = tpt;
@@ -3353,7 +3537,7 @@ struct StepTimer {
 
 // The forms that run k_spmm_blk (L1 gathers, 256- or 512-thread CTAs).
 static bool spmm_subtracts_prev(const BatchedState* bs) {
-    return bs->staged == 0 || bs->staged == 5 || bs->staged == 9;
+    return bs->staged == 0 || bs->staged == 5 || bs->staged == 9 || bs->staged == 10;
 }
 
 template <typename Real, int TPT, bool kBil, bool kWrite>
@@ -3418,6 +3602,22 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real*
                 default: DQ_CPA_R(3); break;
             }
 #undef DQ_CPA_R
+        }
+        return;
+    }
+    if (bs->staged == 10) {
+        if constexpr (sizeof(Real) == 4 && TPT == 2) {
+            const dim3 grid(bs->gxs, ncy);
+            const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
+#define DQ_WG_R(RR)                                                                                          \
+    k_spmm_wg<RR, kBil, kWrite><<<grid, 512, 0, c->stream>>>(n, B, bs->bpc, f.nb, j, f.bptr, rec, d, rj, rjm, w, \
+                                                             bs->s, cy0, bs->chunks)
+            switch (bs->R) {
+                case 1: DQ_WG_R(1); break;
+                case 2: DQ_WG_R(2); break;
+                default: DQ_WG_R(3); break;
+            }
+#undef DQ_WG_R
         }
         return;
     }

@@ -253,10 +253,12 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * that; 512-thread CTAs; groups 1, no reorthogonalisation or adaptive m), 9
  * is form 5 with its gathers issued as asynchronous copies into per-warp
  * shared-memory rings (complex64, traj_chunk 64, vec 2, ctas_per_sm 1,
- * rows_per_block <= 3, at most 128 union entries per block).  groups splits the
- * trajectory chunks into groups whose m Lanczos iterations run one group
- * after another, so a group's Krylov slabs stay resident in L2 (must divide
- * n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run
+ * rows_per_block <= 3, at most 128 union entries per block), 10 is form 5
+ * with one warp per row block, its records in a per-warp shared buffer and
+ * eight gathers in flight per warp (complex64, traj_chunk 64, vec 2,
+ * ctas_per_sm 1, rows_per_block <= 3).  groups splits the trajectory chunks
+ * into groups whose m Lanczos iterations run one group after another, so a
+ * group's Krylov slabs stay resident in L2 (must divide n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run
  * (as dq_reset does). */
 DQ_API dq_status dq_set_tiling(dq_ctx *ctx, int traj_chunk, int vec, int ctas_per_sm, int rows_per_block,
                                int staged, int groups);

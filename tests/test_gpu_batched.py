@@ -341,11 +341,13 @@ def test_pform_refuses_what_it_cannot_do():
     q.close()
 
 
+@pytest.mark.parametrize("staged", [9, 10])
 @pytest.mark.parametrize("dot", [1, 0])
 @pytest.mark.parametrize("R", [1, 2, 3])
-def test_async_copy_gather_spmm_mixed_tube_matches_oracle(oracle, dot, R):
-    """The SpMM whose gathers are asynchronous copies into shared memory (staged = 9) against the FP64
-    oracle on the dipole-coupled tube."""
+def test_async_copy_gather_spmm_mixed_tube_matches_oracle(oracle, dot, R, staged):
+    """The SpMM whose gathers are asynchronous copies into shared memory (staged = 9), and the one with
+    eight register gathers in flight per warp (staged = 10), against the FP64 oracle on the
+    dipole-coupled tube."""
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
     s = systems.tube(20, 24)
@@ -360,8 +362,8 @@ def test_async_copy_gather_spmm_mixed_tube_matches_oracle(oracle, dot, R):
     p.set_system(s)
     p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
     p.set_initial_state(psi0)
-    p.set_tiling(64, 2, 1, R, 9, 1)
-    assert p.get_tiling() == (64, 2, 1, R, 9, 1)
+    p.set_tiling(64, 2, 1, R, staged, 1)
+    assert p.get_tiling() == (64, 2, 1, R, staged, 1)
     p.run(T)
     err = np.abs(p.populations() - ref["pops"]).max()
     assert err < POP_TOL_MIXED, err
