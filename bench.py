@@ -197,15 +197,18 @@ def dominant_kernel(s, B, m, staged, prof):
     """(algorithmic bytes per launch, mean ms per launch, achieved GB/s) of the step's dominant
     kernel under tiling form `staged`, from profile_step's per-kind launch times."""
     ms = prof["spmm_alpha"][0]
-    if staged in (2, 4, 8):
+    if staged in (2, 4, 8, 11):
         # fused forms: the dominant launch is the whole iteration
         ms = prof["fused_iter"][0]
     b = spmm_bytes(s, B)
-    if staged in (0, 5, 9, 10):
+    if staged in (0, 5, 9, 10, 11):
         # the L1 forms also read q_{j-1} (8 B per site-trajectory) in m - 1 of the step's m launches
         b += 8.0 * s.n * B * (m - 1) / m
     if staged in (2, 4):
         b += 24.0 * s.n * B   # + r_j, r_{j-1} reads and the r_{j+1} write
+    if staged == 11:
+        # SpMM launch bytes plus the axpy's (w and q_j read, r_{j+1} written) in the same launch
+        b += 24.0 * s.n * B
     if staged == 8:
         # p-form launch j (2 < j <= m): reads p_j, q_{j-1}, q_{j-2} and d, writes q_j and p_{j+1}
         b = 44.0 * s.n * B + 8.0 * (s.nnz - s.n) + 4.0 * (s.n + 1)
@@ -234,7 +237,9 @@ SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", None),
                   None),
               9: ("k_spmm_cpa (gathers as asynchronous copies into shared memory + alpha, minus beta q_{j-1})",
                   None),
-              10: ("k_spmm_wg (warp per row block, eight gathers in flight + alpha, minus beta q_{j-1})", None)}
+              10: ("k_spmm_wg (warp per row block, eight gathers in flight + alpha, minus beta q_{j-1})", None),
+              11: ("k_spmm_wg with the axpy (one cooperative launch per iteration: SpMM + alpha, wait, r_{j+1}, beta)",
+                   None)}
 
 
 def measured_traffic(staged):

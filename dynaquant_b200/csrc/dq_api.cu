@@ -172,6 +172,17 @@ dq_status dq_set_hamiltonian_csr(dq_ctx* c, int n, const int* rowptr, const int*
         }
         rp[i + 1] = (int)cl.size();
     }
+    // the device builder of the packed coupling blocks merges sorted rows;
+    // the bandwidth sizes the shared-memory windows
+    bool sorted = true;
+    int bw = 0;
+    for (int i = 0; i < n; ++i)
+        for (int p = rp[i]; p < rp[i + 1]; ++p) {
+            if (p > rp[i] && cl[p] < cl[p - 1]) sorted = false;
+            bw = std::max(bw, std::abs(cl[p] - i));
+        }
+    c->rows_sorted = sorted;
+    c->bw = bw;
     c->rowptr = rp;
     c->col = cl;
     c->val_base = vb;
@@ -714,7 +725,7 @@ extern "C" dq_status dq_autotune(dq_ctx* c, int reps, double* best_ms) {
     double best = 1e30;
     const int vecs[2] = {2, 1};
     for (int groups = 1; groups <= 8; groups <<= 1)
-        for (int staged = 0; staged <= 10; ++staged)
+        for (int staged = 0; staged <= 11; ++staged)
             for (int vi = 0; vi < 2; ++vi)
                 for (int tc = 4; tc <= 64; tc <<= 1)
                     for (int cps = 1; cps <= 8; cps <<= 1)

@@ -28,6 +28,7 @@
 //   k_combine_b, k_pop_b
 // captured once into a CUDA graph and replayed per step; the step index lives
 // in device memory.
+#include <climits>
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -976,17 +977,22 @@ __global__ void __launch_bounds__(512, 1) k_spmm_cpa(int n, int B, int bpc, int 
 // or the norm) is k_spmm_blk's.
 constexpr int kWgWarps = 16;
 
-template <int R, bool kBilinear, bool kWrite>
+template <int R, bool kBilinear, bool kWrite, bool kAxpy = false>
 __global__ void __launch_bounds__(512, 1) k_spmm_wg(int n, int B, int bpc, int nb, int j,
                                                    const int* __restrict__ bptr, const float4* __restrict__ rec,
                                                    const float* __restrict__ d, const float* __restrict__ rj,
                                                    const float* __restrict__ rjm, float* __restrict__ w,
-                                                   BatchedScalars S, int cy0, int nch) {
+                                                   BatchedScalars S, int cy0, int nch, float* __restrict__ rjp = nullptr) {
     constexpr int TPT = 2, TC = 64, G = 8;
     __shared__ float4 rbuf[kWgWarps][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int chunk = blockIdx.y + cy0;
-    if (chunk_converged(S, chunk)) return;
+    // kAxpy: the chunk's alpha generation before this block can arrive at the
+    // alpha ticket, so the increment by the ticket's last block is always seen
+    unsigned int* const gen = S.tickets + 7 * (size_t)nch + chunk;
+    unsigned int gen0 = 0;
+    if (kAxpy && threadIdx.x == 0) gen0 = ld_acquire_u32(gen);
+    if (!kAxpy && chunk_converged(S, chunk)) return;
     const int b0 = chunk * TC + lane * TPT;
     const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
     double sc[TPT], ar[TPT], ai[TPT];
@@ -1109,7 +1115,9 @@ __global__ void __launch_bounds__(512, 1) k_spmm_wg(int n, int B, int bpc, int n
     }
     __shared__ double2 red[kMaxTC];
     __shared__ double2 rscratch[512 * 2];
-    if (chunk_reduce_s<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk, rscratch)) {
+    const bool last = chunk_reduce_s<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk,
+                                          rscratch);
+    if (last) {
         if (threadIdx.x < TC) {
             const int b = chunk * TC + threadIdx.x;
             const double s = S.sc[(size_t)j * B + b];
@@ -1119,6 +1127,93 @@ __global__ void __launch_bounds__(512, 1) k_spmm_wg(int n, int B, int bpc, int n
                 S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s * s;
             } else {
                 S.nav[b] = sqrt(v.x) * s;
+            }
+        }
+    }
+    if constexpr (kAxpy) {
+        // The residual r_{j+1} = w - alpha_j q_j of this block's rows, in the
+        // same launch: every block of the chunk waits (bounded) for the alpha
+        // ticket's last block to publish alpha_j, then reads w, which it has
+        // just written, and q_j while both are still in L2.  The launch is
+        // cooperative, so all blocks are resident and the wait ends.
+        __shared__ int s_ok;
+        __syncthreads();   // the last block's alpha stores are done
+        if (threadIdx.x == 0) {
+            int ok = 1;
+            if (last) {
+                __threadfence();
+                atomicAdd(gen, 1u);
+            } else {
+                // a negative budget is the forced-timeout test mode: wait
+                // |budget| cycles for a generation that never comes
+                const long long budget = g_dq_wait_cycles;
+                const long long lim = budget < 0 ? -budget : budget;
+                const long long t0 = clock64();
+                ok = 0;
+                while (clock64() - t0 < lim) {
+                    if (budget > 0 && ld_acquire_u32(gen) != gen0) {
+                        ok = 1;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                if (!ok) atomicCAS(S.status, 0, DQ_ERR_TIMEOUT);
+            }
+            s_ok = ok;
+        }
+        __syncthreads();
+        const bool ok = s_ok != 0;
+        double ajr[TPT], aji[TPT], nn[TPT], zero[TPT];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+            const size_t kk = (size_t)j * B + b0 + t;
+            ajr[t] = __ldcg(&S.alpha[2 * kk]) * S.sc[kk];
+            aji[t] = __ldcg(&S.alpha[2 * kk + 1]) * S.sc[kk];
+            nn[t] = 0.0;
+            zero[t] = 0.0;
+        }
+        // after a timeout the block adds nothing but still takes its ticket,
+        // so the reduction stays consistent (the status reports the failure)
+        // four rows per warp per trip: eight independent loads in flight per lane
+        constexpr int kAx = 4;
+        const int rend = ok ? min(n, k1 * R) : 0;
+        for (int row = k0 * R + warp; row < rend; row += kAx * kWgWarps) {
+            float4 u[kAx], x[kAx];
+#pragma unroll
+            for (int h = 0; h < kAx; ++h) {
+                const int rr = row + h * kWgWarps;
+                const size_t base = (size_t)(rr < rend ? rr : row) * B + b0;
+                u[h] = __ldcg(reinterpret_cast<const float4*>(w + 2 * base));
+                x[h] = __ldg(reinterpret_cast<const float4*>(rj + 2 * base));
+            }
+#pragma unroll
+            for (int h = 0; h < kAx; ++h) {
+                const int rr = row + h * kWgWarps;
+                if (rr >= rend) break;
+                const float uv[4] = {u[h].x, u[h].y, u[h].z, u[h].w}, xv[4] = {x[h].x, x[h].y, x[h].z, x[h].w};
+                float ov[4];
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    const double xr = xv[2 * t], xi = xv[2 * t + 1];
+                    ov[2 * t] = (float)((double)uv[2 * t] - (ajr[t] * xr - aji[t] * xi));
+                    ov[2 * t + 1] = (float)((double)uv[2 * t + 1] - (ajr[t] * xi + aji[t] * xr));
+                    nn[t] += (double)ov[2 * t] * ov[2 * t] + (double)ov[2 * t + 1] * ov[2 * t + 1];
+                }
+                *reinterpret_cast<float4*>(rjp + 2 * ((size_t)rr * B + b0)) = make_float4(ov[0], ov[1], ov[2], ov[3]);
+            }
+        }
+        if (chunk_reduce_s<TPT>(nn, zero, TC, S.partial, S.tickets + 1 * nch, red, chunk, rscratch)) {
+            if (threadIdx.x < TC) {
+                const int b = chunk * TC + threadIdx.x;
+                double bt = sqrt(red[threadIdx.x].x);
+                if (!isfinite(bt)) atomicCAS(S.status, 0, DQ_ERR_NAN);
+                // lucky breakdown as in k_axpy_beta
+                const size_t kj = (size_t)j * B + b;
+                const double a0 = __ldcg(&S.alpha[2 * kj]), a1 = __ldcg(&S.alpha[2 * kj + 1]);
+                const double scale = sqrt(a0 * a0 + a1 * a1) + (j > 1 ? S.beta[(size_t)(j - 1) * B + b] : 0.0);
+                if (bt <= kBreakdownRel * scale) bt = 0.0;
+                S.beta[kj] = bt;
+                S.sc[(size_t)(j + 1) * B + b] = bt > 0.0 ? 1.0 / bt : 0.0;
             }
         }
     }
@@ -2774,10 +2869,93 @@ static inline float __int_as_float_host(int v) {
     return f;
 }
 
+// Packed column-union records on the device (complex64, R <= 3, rows with
+// non-decreasing columns): thread k merges the sorted column lists of block
+// k's rows, summing each row's duplicate columns in CSR order in FP64 before
+// the conversion, exactly as the host builder does, and pads the block to a
+// multiple of 4 records with zero coefficients on its first row.  With
+// pptr == nullptr it only counts (counts[k]); otherwise it writes the block's
+// records from rec[pptr[k]].
+template <int R>
+__global__ void k_fmt_packed(int n, int nb, const int* __restrict__ rowptr, const int* __restrict__ col,
+                             const double* __restrict__ val, const int* __restrict__ pptr, int* __restrict__ counts,
+                             float4* __restrict__ rec) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nb) return;
+    const int r0 = k * R;
+    int p[R], e[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const bool has = r0 + i < n;
+        p[i] = has ? rowptr[r0 + i] : 0;
+        e[i] = has ? rowptr[r0 + i + 1] : 0;
+    }
+    float4* out = pptr ? rec + pptr[k] : nullptr;
+    int cnt = 0;
+    for (;;) {
+        int cmin = INT_MAX;
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            if (p[i] < e[i]) cmin = min(cmin, col[p[i]]);
+        if (cmin == INT_MAX) break;
+        double cf[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+            while (p[i] < e[i] && col[p[i]] == cmin) cf[i] += val[p[i]++];
+        if (out) out[cnt] = make_float4(__int_as_float(cmin), (float)cf[0], (float)cf[1], (float)cf[2]);
+        ++cnt;
+    }
+    while (cnt % 4) {
+        if (out) out[cnt] = make_float4(__int_as_float(r0), 0.f, 0.f, 0.f);
+        ++cnt;
+    }
+    if (!out) counts[k] = cnt;
+}
+
+static dq_status build_fmt_packed_device(dq_ctx* c, int R, BlockFmt& f) {
+    const int n = c->n, nb = (n + R - 1) / R;
+    int* counts = nullptr;
+    DQ_CU(cudaMalloc(&counts, sizeof(int) * (size_t)nb));
+    const int thr = 256, grid = (nb + thr - 1) / thr;
+    auto launch = [&](const int* pptr, float4* rec) {
+        switch (R) {
+            case 1: k_fmt_packed<1><<<grid, thr, 0, c->stream>>>(n, nb, c->d_rowptr, c->d_col, c->d_val, pptr, counts, rec); break;
+            case 2: k_fmt_packed<2><<<grid, thr, 0, c->stream>>>(n, nb, c->d_rowptr, c->d_col, c->d_val, pptr, counts, rec); break;
+            default: k_fmt_packed<3><<<grid, thr, 0, c->stream>>>(n, nb, c->d_rowptr, c->d_col, c->d_val, pptr, counts, rec); break;
+        }
+    };
+    launch(nullptr, nullptr);
+    std::vector<int> pptr(nb + 1, 0);
+    cudaError_t e = cudaMemcpyAsync(pptr.data() + 1, counts, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(counts);
+    DQ_CU(e);
+    for (int k = 0; k < nb; ++k) {
+        f.max_block = std::max(f.max_block, pptr[k + 1]);
+        pptr[k + 1] += pptr[k];
+    }
+    f.packed = true;
+    f.nunion = (size_t)pptr[nb];
+    DQ_CU(cudaMalloc(&f.bptr, sizeof(int) * (nb + 1)));
+    DQ_CU(cudaMemcpyAsync(f.bptr, pptr.data(), sizeof(int) * (nb + 1), cudaMemcpyHostToDevice, c->stream));
+    DQ_CU(cudaMalloc(&f.bcoef, sizeof(float4) * std::max<size_t>(f.nunion, 1)));
+    if (f.nunion) launch(f.bptr, reinterpret_cast<float4*>(f.bcoef));
+    DQ_CU(cudaMalloc(&f.bcol, sizeof(int)));
+    // pptr (host) must outlive the upload that reads it
+    DQ_CU(cudaStreamSynchronize(c->stream));
+    return DQ_OK;
+}
+
 // Builds the row-blocked column-union form of the (scaled) off-diagonal CSR.
 static dq_status build_fmt(dq_ctx* c, int R, BlockFmt& f) {
     BatchedState* bs = c->bat;
     const int n = c->n, nb = (n + R - 1) / R;
+    if (bs->mixed && R <= 3 && c->rows_sorted && c->nnz_off > 0) {
+        bs->bw = c->bw;
+        f.R = R;
+        f.nb = nb;
+        return build_fmt_packed_device(c, R, f);
+    }
     std::vector<int> bptr(nb + 1, 0), bcol;
     std::vector<double> coef;
     std::vector<int> cols;
@@ -3057,6 +3235,8 @@ static void prefer_l1_wg() {
     set((const void*)k_spmm_wg<R, true, true>);
     set((const void*)k_spmm_wg<R, false, false>);
     set((const void*)k_spmm_wg<R, true, false>);
+    set((const void*)k_spmm_wg<R, false, true, true>);
+    set((const void*)k_spmm_wg<R, true, true, true>);
     cudaGetLastError();   // a hint: a refusal changes nothing
 }
 
@@ -3078,16 +3258,19 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
-    if (staged < 0 || staged > 10) return DQ_ERR_ARG;
+    if (staged < 0 || staged > 11) return DQ_ERR_ARG;
     // reorthogonalisation runs between the axpy and the next SpMM: not in the fused forms
-    if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4 || staged == 8)) return DQ_ERR_ARG;
+    if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4 || staged == 8 || staged == 11))
+        return DQ_ERR_ARG;
     // p-form iteration: one launch per iteration over all chunks
     if (staged == 8 && (groups != 1 || c->cfg.m < 2)) return DQ_ERR_ARG;
     // asynchronous-copy gathers: complex64 packed records, one warp per 64-trajectory block, one CTA per SM
     if (staged == 9 && (!bs->mixed || R > 3 || tc != 64 || tpt != 2 || ctas_per_sm != 1 || groups != 1))
         return DQ_ERR_ARG;
-    // eight gathers in flight per warp: the same restrictions, chunk groups allowed
-    if (staged == 10 && (!bs->mixed || R > 3 || tc != 64 || tpt != 2 || ctas_per_sm != 1)) return DQ_ERR_ARG;
+    // eight gathers in flight per warp (11: and the axpy in the same cooperative launch):
+    // the same restrictions, chunk groups allowed
+    if ((staged == 10 || staged == 11) && (!bs->mixed || R > 3 || tc != 64 || tpt != 2 || ctas_per_sm != 1))
+        return DQ_ERR_ARG;
     // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane in the other
     // kernels (the ring itself takes 2 per lane with staged 6, 4 with staged 7), one CTA per SM
     const bool ring = staged == 6 || staged == 7;
@@ -3102,7 +3285,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (groups < 1 || chunks % groups) return DQ_ERR_ARG;
     const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
-    const int RPC_spmm = (staged == 5 || staged == 8 || staged == 9 || staged == 10 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
+    const int RPC_spmm = (staged == 5 || staged >= 8 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
     // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide:
     // one wave of kStreamCtasPerSm CTAs per SM while every thread still walks
     // several rows, twice as many CTAs when that wave would leave each thread
@@ -3279,11 +3462,21 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
         else if (tpt == 2) prefer_l1<float, 2>(R);
         else prefer_l1<float, 1>(R);
     }
-    if (staged == 10) {
+    if (staged == 10 || staged == 11) {
         switch (R) {
             case 1: prefer_l1_wg<1>(); break;
             case 2: prefer_l1_wg<2>(); break;
             default: prefer_l1_wg<3>(); break;
+        }
+    }
+    if (staged == 11) {
+        // the cooperative launch needs every block of a chunk group resident at once
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmm_wg<3, false, true, true>, 512, 0) !=
+                cudaSuccess ||
+            occ < 1 || (size_t)gxs * cpg > (size_t)occ * bs->sms) {
+            cudaGetLastError();
+            return DQ_ERR_ARG;
         }
     }
     bs->TC = tc;
@@ -3537,7 +3730,7 @@ struct StepTimer {
 
 // The forms that run k_spmm_blk (L1 gathers, 256- or 512-thread CTAs).
 static bool spmm_subtracts_prev(const BatchedState* bs) {
-    return bs->staged == 0 || bs->staged == 5 || bs->staged == 9 || bs->staged == 10;
+    return bs->staged == 0 || bs->staged == 5 || bs->staged >= 9;
 }
 
 template <typename Real, int TPT, bool kBil, bool kWrite>
@@ -3605,7 +3798,7 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real*
         }
         return;
     }
-    if (bs->staged == 10) {
+    if (bs->staged == 10 || bs->staged == 11) {
         if constexpr (sizeof(Real) == 4 && TPT == 2) {
             const dim3 grid(bs->gxs, ncy);
             const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
@@ -3780,6 +3973,37 @@ static void launch_fused_any(dq_ctx* c, int j) {
     else launch_fused<Real, TPT, false, kLast>(c, j);
 }
 
+// Iteration j of staged 11: the SpMM of k_spmm_wg and the axpy in one
+// cooperative launch (every block resident, so the chunk barrier ends).
+template <bool kBil>
+static cudaError_t launch_iter_wg(dq_ctx* c, int j, const float* rj, const float* rjm, float* w, float* rjp, int cy0,
+                                  int ncy) {
+    BatchedState* bs = c->bat;
+    const BlockFmt& f = bs->fmt[r_index(bs->R)];
+    const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
+    const float* d = (const float*)bs->diag;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(bs->gxs, ncy);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    const int n = c->n, B = bs->B, bpc = bs->bpc, nb = f.nb, nch = bs->chunks;
+    const int* bptr = f.bptr;
+    switch (bs->R) {
+        case 1: return cudaLaunchKernelEx(&cfg, k_spmm_wg<1, kBil, true, true>, n, B, bpc, nb, j, bptr, rec, d, rj, rjm,
+                                          w, bs->s, cy0, nch, rjp);
+        case 2: return cudaLaunchKernelEx(&cfg, k_spmm_wg<2, kBil, true, true>, n, B, bpc, nb, j, bptr, rec, d, rj, rjm,
+                                          w, bs->s, cy0, nch, rjp);
+        default: return cudaLaunchKernelEx(&cfg, k_spmm_wg<3, kBil, true, true>, n, B, bpc, nb, j, bptr, rec, d, rj,
+                                           rjm, w, bs->s, cy0, nch, rjp);
+    }
+}
+
 template <typename Real, int TPT>
 static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int ncy) {
     BatchedState* bs = c->bat;
@@ -3790,6 +4014,18 @@ static dq_status enqueue_iteration(dq_ctx* c, int j, StepTimer* tm, int cy0, int
     auto slab = [&](int k) { return slabs + 2 * se * k; };
     const dim3 grid(bs->gx, ncy);
     const bool fused = bs->staged == 2 || bs->staged == 4;
+    if (bs->staged == 11) {
+        if constexpr (sizeof(Real) == 4 && TPT == 2) {
+            // SpMM (minus beta_{j-1} q_{j-1}) and axpy in one launch: r_{j+1} into slab j + 1
+            if (tm) tm->mark(DQ_KIND_FUSED, st);
+            const float* rjm = j > 1 ? slab(j - 1) : nullptr;
+            const cudaError_t e = c->cfg.dot_mode == DQ_DOT_BILINEAR
+                                      ? launch_iter_wg<true>(c, j, slab(j), rjm, slab(0), slab(j + 1), cy0, ncy)
+                                      : launch_iter_wg<false>(c, j, slab(j), rjm, slab(0), slab(j + 1), cy0, ncy);
+            if (e != cudaSuccess) return check_cuda(c, e, "cooperative iteration launch");
+        }
+        return DQ_OK;
+    }
     if (bs->staged == 8) {
         // p-form: one launch per iteration, and the last one gives ||H q_{m+1}||
         if (tm) tm->mark(j == 1 ? DQ_KIND_SPMM : DQ_KIND_FUSED, st);

@@ -48,6 +48,13 @@ __device__ __forceinline__ double block_sum(double v, double* scratch) {
 // publishes its partial, fences, and takes a ticket; the block that draws
 // the last ticket sums all partials in block order (deterministic) and resets
 // the counter for the next launch.  No block ever waits on another.
+// a GPU-scope acquire load (the partner of a fence + atomic by another block)
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ bool last_block_ticket(unsigned int* counter, unsigned int nblocks) {
     __shared__ bool is_last;
     __threadfence();

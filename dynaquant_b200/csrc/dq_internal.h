@@ -73,6 +73,8 @@ struct dq_ctx {
     dq::cd* d_psi0 = nullptr;
     dq::cd* d_bra = nullptr;               // correlation bra (null: psi0)
     int nnz_off = 0;
+    bool rows_sorted = false;              // every off-diagonal row's columns non-decreasing
+    int bw = 0;                            // bandwidth max |col - row| of the off-diagonal CSR
     // ZZ real noise: oscillators (angular frequency rad/fs, amplitude); the
     // phases are Philox draws made where they are used
     int zz_n_osc = 0;

@@ -256,7 +256,10 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * rows_per_block <= 3, at most 128 union entries per block), 10 is form 5
  * with one warp per row block, its records in a per-warp shared buffer and
  * eight gathers in flight per warp (complex64, traj_chunk 64, vec 2,
- * ctas_per_sm 1, rows_per_block <= 3).  groups splits the trajectory chunks
+ * ctas_per_sm 1, rows_per_block <= 3), 11 is form 10 with the axpy in the
+ * same launch: a cooperative launch in which each CTA waits (bounded) for its
+ * chunk's alpha_j and then forms r_{j+1} for its own rows while w and q_j are
+ * still in L2 (no reorthogonalisation or adaptive m).  groups splits the trajectory chunks
  * into groups whose m Lanczos iterations run one group after another, so a
  * group's Krylov slabs stay resident in L2 (must divide n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run
  * (as dq_reset does). */
@@ -277,8 +280,11 @@ DQ_API dq_status dq_time_iteration(dq_ctx *ctx, int reps, double *ms);
  * makes every CTA of the ring form (staged 6/7) first wait -cycles cycles on
  * a barrier that no copy ever completes: the wait runs out, the kernel
  * records DQ_ERR_TIMEOUT, lets its own copies in flight land (with the
- * default budget) and returns, and dq_run reports the status.  It applies
- * to every context on the device until changed again. */
+ * default budget) and returns, and dq_run reports the status.  The same
+ * budget bounds the per-chunk wait for alpha of the cooperative iteration
+ * form (staged 11); a negative value makes that wait look -cycles cycles for
+ * a generation that never comes, with the same outcome.  It applies to every
+ * context on the device until changed again. */
 DQ_API dq_status dq_debug_set_wait_cycles(dq_ctx *ctx, int cycles);
 
 /* Kernel kinds of one ensemble step, for dq_profile_step. */

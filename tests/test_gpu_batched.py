@@ -341,13 +341,13 @@ def test_pform_refuses_what_it_cannot_do():
     q.close()
 
 
-@pytest.mark.parametrize("staged", [9, 10])
+@pytest.mark.parametrize("staged", [9, 10, 11])
 @pytest.mark.parametrize("dot", [1, 0])
 @pytest.mark.parametrize("R", [1, 2, 3])
 def test_async_copy_gather_spmm_mixed_tube_matches_oracle(oracle, dot, R, staged):
-    """The SpMM whose gathers are asynchronous copies into shared memory (staged = 9), and the one with
-    eight register gathers in flight per warp (staged = 10), against the FP64 oracle on the
-    dipole-coupled tube."""
+    """The SpMM whose gathers are asynchronous copies into shared memory (staged = 9), the one with
+    eight register gathers in flight per warp (staged = 10) and that SpMM with the axpy in the same
+    cooperative launch (staged = 11), against the FP64 oracle on the dipole-coupled tube."""
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
     s = systems.tube(20, 24)
@@ -370,3 +370,62 @@ def test_async_copy_gather_spmm_mixed_tube_matches_oracle(oracle, dot, R, staged
     assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
     assert np.allclose(p.error_accum(), ref["err"], rtol=1e-2, atol=1e-12)
     p.close()
+
+
+@pytest.mark.parametrize("groups", [1, 2])
+def test_cooperative_iteration_chunk_groups_match_oracle(oracle, groups):
+    """Staged 11 (SpMM and axpy in one cooperative launch, a bounded wait per chunk for alpha) with
+    the chunks run as one launch or as two groups of one chunk each, against the FP64 oracle; the
+    group run also matches the one-launch run to FP32 rounding."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 24)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=16, dt=0.5, dot_mode=1, noise=2, sigma=250.0, tau=50.0,
+                      sigma_static=150.0, seed=21)
+    B, T = 128, 24
+    psi0 = s.bright_state()
+    ref = S.run(B, T, psi0, pop_every=4, threads=4)
+    p = dq.Propagator(s.n, m=16, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=21, dot=1,
+                      pop_every=4, max_steps=T, precision=dq.PREC_MIXED)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    p.set_initial_state(psi0)
+    p.set_tiling(64, 2, 1, 3, 11, groups)
+    assert p.get_tiling() == (64, 2, 1, 3, 11, groups)
+    p.run(T)
+    assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
+    assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
+    assert np.allclose(p.error_accum(), ref["err"], rtol=1e-2, atol=1e-12)
+    p.close()
+
+
+@pytest.mark.parametrize("R", [1, 2, 3])
+def test_device_block_format_matches_host_builder(R):
+    """The packed coupling blocks of the complex64 path are built on the device when every CSR row's
+    columns are sorted, and on the host otherwise.  The same tube with each row's entries reversed
+    (so the host builds the blocks) gives bit-identical populations and correlation: the two
+    builders produce the same records."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 24)
+    rp, col, val = np.asarray(s.rowptr), np.asarray(s.col), np.asarray(s.val)
+    col_r, val_r = col.copy(), val.copy()
+    for i in range(s.n):
+        a, b = rp[i], rp[i + 1]
+        col_r[a:b] = col[a:b][::-1]
+        val_r[a:b] = val[a:b][::-1]
+    B, T = 64, 12
+    out = []
+    for c, v in ((col, val), (col_r, val_r)):
+        p = dq.Propagator(s.n, m=16, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=3, dot=1,
+                          pop_every=4, max_steps=T, precision=dq.PREC_MIXED)
+        p.set_hamiltonian_csr(rp, c, v)
+        p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+        p.set_initial_state(s.bright_state())
+        p.set_tiling(64, 2, 1, R, 5, 1)
+        p.run(T)
+        out.append((p.populations(), p.correlation()))
+        p.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])

@@ -7,9 +7,9 @@ reach, and the error codes of the device status word.
   Padé is itself checked against scipy's expm at that norm.
 * Gaussian (HSR) noise on the ensemble path (gpuSysHelper.cu:32-66).
 * DQ_ERR_NAN from a non-finite initial state, DQ_ERR_SCALING from s >= 50
-  (padeClass.cu:618-623), and DQ_ERR_TIMEOUT from the TMA-fed SpMM when a
-  test hook lowers the budget of its bounded barrier waits so that they give
-  up on purpose.  Every failure is made on the host side: the inputs are
+  (padeClass.cu:618-623), and DQ_ERR_TIMEOUT from the TMA-fed SpMM and from
+  the cooperative iteration form's per-chunk wait when a test hook makes
+  their bounded waits give up on purpose.  Every failure is made on the host side: the inputs are
   ordinary numbers and every wait is bounded, so no GPU fault or hang can
   follow; after each failure the same context runs again and reproduces a
   clean run exactly.
@@ -211,6 +211,39 @@ def test_ring_spmm_wait_timeout_is_reported_and_context_recovers():
         p.run(T)
         clean = p.populations()
         p.debug_set_wait_cycles(-20000)   # a wait on a barrier that no copy completes, ~10 us
+        p.reset()
+        with pytest.raises(dq.DQError) as e:
+            p.run(T)
+        assert e.value.code == DQ_ERR_TIMEOUT
+    finally:
+        p.debug_set_wait_cycles(0)
+    p.reset()
+    p.run(T)
+    assert np.array_equal(p.populations(), clean)
+    p.close()
+
+
+def test_cooperative_iteration_wait_timeout_is_reported_and_context_recovers():
+    """Staged 11 runs the SpMM and the axpy in one cooperative launch, every block waiting (bounded)
+    for its chunk's alpha.  In the forced-timeout mode that wait looks for a generation that never
+    comes for 20,000 cycles: each block gives up, still takes its reduction ticket, dq_run returns
+    DQ_ERR_TIMEOUT, and with the default budget restored the same context reproduces the clean run
+    bit for bit."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 24)
+    B, T = 64, 6
+    p = dq.Propagator(s.n, m=12, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=5, dot=1,
+                      precision=dq.PREC_MIXED, pop_every=2, max_steps=T)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    p.set_initial_state(s.bright_state())
+    p.set_tiling(64, 2, 1, 3, 11, 1)
+    try:
+        p.reset()
+        p.run(T)
+        clean = p.populations()
+        p.debug_set_wait_cycles(-20000)
         p.reset()
         with pytest.raises(dq.DQError) as e:
             p.run(T)
