@@ -239,7 +239,7 @@ SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", None),
                   None),
               10: ("k_spmm_wg (warp per row block, eight gathers in flight + alpha, minus beta q_{j-1})", None),
               11: ("k_spmm_wg with the axpy (one cooperative launch per iteration: SpMM + alpha, wait, r_{j+1}, beta)",
-                   None)}
+                   "k_spmm_wg_tube60x500.md")}
 
 
 def measured_traffic(staged):

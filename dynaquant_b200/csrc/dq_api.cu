@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <utility>
 
 #include "dq_internal.h"
 
@@ -46,12 +47,9 @@ dq_status upload_couplings(dq_ctx* c) {
         if (!c->cls.empty()) s = c->scales[c->cls[k]];
         c->val[k] = s * c->val_base[k];
     }
-    std::vector<float> vf(c->val.begin(), c->val.end());
     dq_status st = batched_invalidate_blocks(c);
     if (st) return st;
-    st = upload(c, &c->d_val, c->val.data(), c->val.size());
-    if (st) return st;
-    return upload(c, &c->d_valf, vf.data(), vf.size());
+    return upload(c, &c->d_val, c->val.data(), c->val.size());
 }
 
 }  // namespace
@@ -136,7 +134,7 @@ void dq_destroy(dq_ctx* c) {
     adjoint_free(c);
     batched_free(c);
     plain_free(c);
-    cudaFree(c->d_rowptr); cudaFree(c->d_col); cudaFree(c->d_val); cudaFree(c->d_valf); cudaFree(c->d_h0);
+    cudaFree(c->d_rowptr); cudaFree(c->d_col); cudaFree(c->d_val); cudaFree(c->d_h0);
     cudaFree(c->d_static); cudaFree(c->d_sigma); cudaFree(c->d_invtau); cudaFree(c->d_coeff);
     cudaFree(c->d_psi0); cudaFree(c->d_bra); cudaFree(c->d_pops); cudaFree(c->d_corr); cudaFree(c->d_erracc);
     cudaFree(c->d_zz_omega); cudaFree(c->d_zz_coeff);
@@ -162,32 +160,36 @@ dq_status dq_set_hamiltonian_csr(dq_ctx* c, int n, const int* rowptr, const int*
     std::vector<double> vb, h0(n, 0.0);
     cl.reserve(nnz);
     vb.reserve(nnz);
+    // besides the split: whether every row's off-diagonal columns are sorted
+    // (the device builder of the packed coupling blocks merges sorted rows)
+    // and the bandwidth (it sizes the shared-memory windows)
+    bool sorted = true;
+    int bw = 0;
     for (int i = 0; i < n; ++i) {
+        int prev = -1;
         for (int p = rowptr[i]; p < rowptr[i + 1]; ++p) {
             int j = col[p];
             if (j < 0 || j >= n) return fail(c, DQ_ERR_ARG, "hamiltonian: column index out of range");
             if (!std::isfinite(val[p])) return fail(c, DQ_ERR_ARG, "hamiltonian: non-finite value");
-            if (j == i) h0[i] += val[p];
-            else { cl.push_back(j); vb.push_back(val[p]); }
+            if (j == i) {
+                h0[i] += val[p];
+            } else {
+                cl.push_back(j);
+                vb.push_back(val[p]);
+                if (j < prev) sorted = false;
+                prev = j;
+                bw = std::max(bw, std::abs(j - i));
+            }
         }
         rp[i + 1] = (int)cl.size();
     }
-    // the device builder of the packed coupling blocks merges sorted rows;
-    // the bandwidth sizes the shared-memory windows
-    bool sorted = true;
-    int bw = 0;
-    for (int i = 0; i < n; ++i)
-        for (int p = rp[i]; p < rp[i + 1]; ++p) {
-            if (p > rp[i] && cl[p] < cl[p - 1]) sorted = false;
-            bw = std::max(bw, std::abs(cl[p] - i));
-        }
     c->rows_sorted = sorted;
     c->bw = bw;
-    c->rowptr = rp;
-    c->col = cl;
-    c->val_base = vb;
-    c->h0diag = h0;
     c->nnz_off = (int)cl.size();
+    c->rowptr = std::move(rp);
+    c->col = std::move(cl);
+    c->val_base = std::move(vb);
+    c->h0diag = std::move(h0);
     c->cls.clear();
     c->scales.clear();
     dq_status st;
@@ -199,10 +201,8 @@ dq_status dq_set_hamiltonian_csr(dq_ctx* c, int n, const int* rowptr, const int*
         // keep valid (non-null) pointers for kernels
         static const int zi = 0;
         static const double zd = 0.0;
-        static const float zf = 0.f;
         if ((st = upload(c, &c->d_col, &zi, 1))) return st;
         if ((st = upload(c, &c->d_val, &zd, 1))) return st;
-        if ((st = upload(c, &c->d_valf, &zf, 1))) return st;
     }
     c->have_ham = true;
     c->ready = false;

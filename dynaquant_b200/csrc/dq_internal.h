@@ -64,7 +64,6 @@ struct dq_ctx {
     int* d_rowptr = nullptr;
     int* d_col = nullptr;
     double* d_val = nullptr;
-    float* d_valf = nullptr;
     double* d_h0 = nullptr;
     double* d_static = nullptr;            // explicit static energies (or null)
     double* d_sigma = nullptr;
