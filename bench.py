@@ -215,6 +215,16 @@ def dominant_kernel(s, B, m, staged, prof):
     return b, ms, b / (ms / 1e3) / 1e9
 
 
+def gather_floor_ms(p, reps=20):
+    """Device ms of the gathers alone of the context's packed coupling blocks (dq_time_gather_floor), or
+    None for a tiling without them."""
+    import dynaquant_b200 as dq
+    try:
+        return p.time_gather_floor(reps)
+    except dq.DQError:
+        return None
+
+
 def spmm_bytes(s, B):
     """Algorithmic HBM bytes of one SpMM+alpha launch (complex64 path):
     read q_j (8 B) and the diagonal (4 B), write w (8 B) per site-trajectory,
@@ -379,6 +389,7 @@ def large_leg():
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / K
     prof = p.profile_step(1)
+    gather_floor = gather_floor_ms(p)
     p.close()
     b, kms, achieved = dominant_kernel(s, B, 24, tiling["staged"], prof)
     peak, peak_kind = _peaks()
@@ -387,7 +398,9 @@ def large_leg():
             "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged")},
             "roofline": {"bound": "hbm", "kernel": SPMM_FORMS.get(tiling["staged"], ("SpMM + alpha",))[0],
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b, "ms_per_launch": kms},
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b, "ms_per_launch": kms,
+                         "gather_floor_ms": gather_floor,
+                         "frac_of_gather_floor": (gather_floor / kms) if gather_floor else None},
             "kernels_ms_per_launch": {k: v[0] for k, v in prof.items()}}
 
 
@@ -677,6 +690,7 @@ def run_ours(args, rank, world, local_rank):
     value = B * K * world / (ms / 1e3)
     # ---- per-kernel times (eager, events between kernels) ------------------
     prof = p.profile_step(2)
+    gather_floor = gather_floor_ms(p)
     p.close()
     peak, peak_kind = _peaks()
     bytes_spmm, spmm_ms, achieved = dominant_kernel(s, B, w["m"], tiling["staged"], prof)
@@ -759,7 +773,12 @@ def run_ours(args, rank, world, local_rank):
                      "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_spmm, "ms_per_launch": spmm_ms,
                      "traffic": traffic,
-                     "traffic_source": (traffic_src + " (ncu dram bytes, one launch)") if traffic_src else None},
+                     "traffic_source": (traffic_src + " (ncu dram bytes, one launch)") if traffic_src else None,
+                     "gather_floor_ms": gather_floor,
+                     "frac_of_gather_floor": (gather_floor / spmm_ms) if gather_floor else None,
+                     "gather_floor_note": "dq_time_gather_floor: the same row-block walk, records and 16-byte "
+                                          "gathers without the FMAs, diagonal, q_{j-1}, alpha and all but one "
+                                          "store per block"},
         "kernels_ms_per_launch": {k: v[0] for k, v in prof.items()},
         "eager_step_ms": step_ms_eager,
         "clocks": clocks,

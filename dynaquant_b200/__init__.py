@@ -154,6 +154,13 @@ class Propagator:
         self._check(self.L.dq_time_iteration(self.h, reps, C.byref(ms)))
         return ms.value
 
+    def time_gather_floor(self, reps=10):
+        """Mean device ms of the gathers alone of the current tiling's packed coupling blocks (complex64,
+        vec 2, rows_per_block <= 3): the floor under the L1-gather SpMM."""
+        ms = C.c_double()
+        self._check(self.L.dq_time_gather_floor(self.h, reps, C.byref(ms)))
+        return ms.value
+
     def debug_set_wait_cycles(self, cycles):
         """Test hook: budget of the TMA-fed SpMM forms' barrier waits on this device (0: default; negative:
         the ring form's CTAs first wait that many cycles on a barrier nothing completes, so they time out)."""

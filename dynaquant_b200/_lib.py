@@ -29,7 +29,7 @@ EXPORTS = [
     "dq_set_correlation_bra", "dq_set_trajectory_offset", "dq_get_observable_sums", "dq_set_observable_sums",
     "dq_set_initial_state", "dq_set_initial_dipole", "dq_reset", "dq_prop_step", "dq_run_plain", "dq_run", "dq_get_populations",
     "dq_get_correlation", "dq_get_states", "dq_get_error_accum", "dq_steps_done", "dq_get_spectrum",
-    "dq_get_noise_state", "dq_set_line_dressing", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration",
+    "dq_get_noise_state", "dq_set_line_dressing", "dq_profile_step", "dq_set_tiling", "dq_get_tiling", "dq_autotune", "dq_time_iteration", "dq_time_gather_floor",
     "dq_debug_set_wait_cycles", "dq_krylov_step_static", "dq_adjoint_setup", "dq_forward", "dq_backward", "dq_forward_shard", "dq_forward_reduced",
     "dq_group_create", "dq_group_destroy", "dq_group_last_error", "dq_group_run", "dq_group_run_timed",
     "dq_write_populations", "dq_write_states", "dq_write_spectrum", "dq_write_spectrum_mean",
@@ -145,6 +145,7 @@ def load(path: str = LIB_PATH):
     L.dq_get_tiling.argtypes = [vp, ip, ip, ip, ip, ip, ip]
     L.dq_autotune.argtypes = [vp, C.c_int, dp]
     L.dq_time_iteration.argtypes = [vp, C.c_int, dp]
+    L.dq_time_gather_floor.argtypes = [vp, C.c_int, dp]
     L.dq_debug_set_wait_cycles.argtypes = [vp, C.c_int]
     L.dq_krylov_step_static.argtypes = [C.c_int, vp, vp, vp, vp, vp, vp, C.c_int, C.c_double, C.c_double, C.c_int,
                                         C.c_int, vp, dp, C.c_char_p, C.c_int]

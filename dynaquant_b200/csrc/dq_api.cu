@@ -757,6 +757,18 @@ extern "C" dq_status dq_time_iteration(dq_ctx* c, int reps, double* ms) {
     return DQ_OK;
 }
 
+extern "C" dq_status dq_time_gather_floor(dq_ctx* c, int reps, double* ms) {
+    DeviceScope dev_scope(c);
+    if (!c || !ms) return DQ_ERR_ARG;
+    if (reps < 1) reps = 5;
+    dq_status st;
+    if ((st = ensure_batched(c))) return st;
+    if ((st = dq_reset(c))) return st;
+    if ((st = batched_time_gather_floor(c, reps, ms))) return st;
+    c->ready = false;
+    return DQ_OK;
+}
+
 extern "C" dq_status dq_debug_set_wait_cycles(dq_ctx* c, int cycles) {
     DeviceScope dev_scope(c);
     if (!c) return DQ_ERR_ARG;

@@ -4272,11 +4272,15 @@ dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
         else if (bs->TPT == 2) launch_pform<float, 2>(c, j);
         else launch_pform<float, 1>(c, j);
     };
+    // the standard forms are timed on iteration 2 (after one of iteration 1),
+    // whose SpMM also streams q_{j-1} like every later one
+    const int js = std::min(2, c->cfg.m);
     auto one = [&]() {
         if (fused) fused_iteration_any(c, jt);
         else if (pform) pf(jt);
-        else enqueue_iteration_any(c, 1);
+        else enqueue_iteration_any(c, js);
     };
+    if (!fused && !pform && js == 2) enqueue_iteration_any(c, 1);
     if (fused) {
         enqueue_iteration_any(c, 1);
         if (jt == 3) fused_iteration_any(c, 2);
@@ -4296,6 +4300,80 @@ dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms) {
     cudaEventDestroy(e1);
     *ms = t / reps;
     return check_cuda(c, cudaGetLastError(), "time iteration");
+}
+
+// Gather floor of the packed column-union form (complex64, R <= 3, 2
+// trajectories per lane): the row-block walk, record stream and 16-byte
+// gathers of k_spmm_blk in 512-thread CTAs over the same grid, with the
+// coupling FMAs, the diagonal, q_{j-1}, alpha and all but one store per block
+// left out.  Its time is what the gathers of this access pattern alone take
+// on this GPU, the measured floor under the SpMM forms that gather through L1.
+template <int R>
+__global__ void __launch_bounds__(512, 1) k_gather_floor(int n, int B, int TC, int bpc, int nb,
+                                                        const int* __restrict__ bptr, const float4* __restrict__ rec,
+                                                        const float* __restrict__ x, float* __restrict__ out) {
+    const int TPR = TC / 2;
+    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int RPC = blockDim.x / TPR;
+    const int b0 = blockIdx.y * TC + tr * 2;
+    const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
+    const float* src = x + 2 * (size_t)b0;
+    for (int k = k0 + rl; k < k1; k += RPC) {
+        const int pb = __ldg(bptr + k), pe = __ldg(bptr + k + 1);
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int e = pb; e < pe; e += 4) {   // a multiple of 4 records per block
+            float4 r[4], y[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) r[u] = __ldg(rec + e + u);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                y[u] = __ldg(reinterpret_cast<const float4*>(src + 2 * (size_t)__float_as_int(r[u].x) * B));
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a.x += y[u].x; a.y += y[u].y; a.z += y[u].z; a.w += y[u].w;
+            }
+        }
+        *reinterpret_cast<float4*>(out + 2 * ((size_t)min(k * R, n - 1) * B + b0)) = a;
+    }
+}
+
+dq_status batched_time_gather_floor(dq_ctx* c, int reps, double* ms) {
+    BatchedState* bs = c->bat;
+    const BlockFmt& f = bs->fmt[r_index(bs->R)];
+    if (!bs->mixed || bs->TPT != 2 || bs->R > 3 || !f.packed) {
+        c->err = "gather floor: needs the complex64 packed form (vec 2, rows_per_block <= 3)";
+        return DQ_ERR_STATE;
+    }
+    const size_t se = (size_t)c->n * bs->B;
+    float* slabs = (float*)bs->slabs;
+    const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
+    const dim3 grid(bs->gxs, bs->chunks);
+    auto launch = [&]() {
+        switch (bs->R) {
+            case 1: k_gather_floor<1><<<grid, 512, 0, c->stream>>>(c->n, bs->B, bs->TC, bs->bpc, f.nb, f.bptr, rec, slabs + 2 * se, slabs); break;
+            case 2: k_gather_floor<2><<<grid, 512, 0, c->stream>>>(c->n, bs->B, bs->TC, bs->bpc, f.nb, f.bptr, rec, slabs + 2 * se, slabs); break;
+            default: k_gather_floor<3><<<grid, 512, 0, c->stream>>>(c->n, bs->B, bs->TC, bs->bpc, f.nb, f.bptr, rec, slabs + 2 * se, slabs); break;
+        }
+    };
+    const int carve = cudaSharedmemCarveoutMaxL1;
+    cudaFuncSetAttribute((const void*)k_gather_floor<1>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    cudaFuncSetAttribute((const void*)k_gather_floor<2>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    cudaFuncSetAttribute((const void*)k_gather_floor<3>, cudaFuncAttributePreferredSharedMemoryCarveout, carve);
+    cudaGetLastError();
+    cudaEvent_t e0, e1;
+    DQ_CU(cudaEventCreate(&e0));
+    DQ_CU(cudaEventCreate(&e1));
+    launch();   // warm-up
+    DQ_CU(cudaEventRecord(e0, c->stream));
+    for (int r = 0; r < reps; ++r) launch();
+    DQ_CU(cudaEventRecord(e1, c->stream));
+    DQ_CU(cudaEventSynchronize(e1));
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / reps;
+    return check_cuda(c, cudaGetLastError(), "gather floor");
 }
 
 void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged, int* groups) {

@@ -186,6 +186,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
 void batched_get_tiling(dq_ctx* c, int* tc, int* tpt, int* cps, int* R, int* staged, int* groups);
 dq_status batched_invalidate_blocks(dq_ctx* c);
 dq_status batched_time_iteration(dq_ctx* c, int reps, double* ms);
+dq_status batched_time_gather_floor(dq_ctx* c, int reps, double* ms);
 dq_status batched_set_wait_cycles(dq_ctx* c, int cycles);
 void batched_noise_arrays(dq_ctx* c, const double** eps, const double** deps);
 // kernels of dq_batched.cu also launched by the Taylor-Krylov ensemble

@@ -274,6 +274,15 @@ DQ_API dq_status dq_autotune(dq_ctx *ctx, int reps, double *best_ms);
 /* Mean device time of one Lanczos iteration (SpMM + axpy) under the current
  * tiling, over reps launches; the ensemble restarts at the next dq_run. */
 DQ_API dq_status dq_time_iteration(dq_ctx *ctx, int reps, double *ms);
+/* Measurement, no reference counterpart: mean device time of one launch of
+ * the gathers alone of the current tiling's packed coupling blocks (complex64,
+ * vec 2, rows_per_block <= 3): the same row-block walk, record stream and
+ * 16-byte gathers of the trajectory rows as the L1-gather SpMM, without its
+ * FMAs, diagonal, q_{j-1} term, alpha and all but one store per block; the
+ * floor that access pattern sets on the GPU.  Overwrites the ensemble's work
+ * slab (the ensemble restarts at the next dq_run); DQ_ERR_STATE for other
+ * tilings. */
+DQ_API dq_status dq_time_gather_floor(dq_ctx *ctx, int reps, double *ms);
 /* Test hook, no reference counterpart: sets the budget (SM cycles) of the
  * bounded shared-memory barrier waits of the TMA-fed SpMM forms on the
  * context's device; 0 restores the default (about 2 s).  A negative value

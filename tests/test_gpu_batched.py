@@ -429,3 +429,32 @@ def test_device_block_format_matches_host_builder(R):
         p.close()
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_gather_floor_probe_runs_below_the_spmm_and_refuses_other_forms():
+    """dq_time_gather_floor times the gathers alone of the packed coupling blocks: it must take less time
+    than the SpMM that does those gathers and more, leave the ensemble restartable, and refuse the FP64
+    form (no packed records)."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(60, 100)
+    B = 128
+    p = dq.Propagator(s.n, m=12, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=2, dot=1,
+                      pop_every=4, max_steps=8, precision=dq.PREC_MIXED)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    p.set_initial_state(s.bright_state())
+    p.set_tiling(64, 2, 1, 3, 5, 1)
+    floor = p.time_gather_floor(10)
+    spmm = p.profile_step(1)["spmm_alpha"][0]
+    assert 0.0 < floor < spmm, (floor, spmm)
+    p.reset()
+    p.run(4)
+    assert np.allclose(p.populations()[-1].sum(), 1.0, atol=1e-6)
+    p.close()
+    q = dq.Propagator(s.n, m=12, n_traj=8, dt=0.5, precision=dq.PREC_FP64)
+    q.set_system(s)
+    q.set_initial_state(s.bright_state())
+    with pytest.raises(dq.DQError):
+        q.time_gather_floor(2)
+    q.close()
