@@ -201,7 +201,7 @@ def dominant_kernel(s, B, m, staged, prof):
         # fused forms: the dominant launch is the whole iteration
         ms = prof["fused_iter"][0]
     b = spmm_bytes(s, B)
-    if staged in (0, 5, 9, 10, 11):
+    if staged in (0, 5, 9, 10, 11, 12):
         # the L1 forms also read q_{j-1} (8 B per site-trajectory) in m - 1 of the step's m launches
         b += 8.0 * s.n * B * (m - 1) / m
     if staged in (2, 4):
@@ -249,7 +249,8 @@ SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", None),
                   None),
               10: ("k_spmm_wg (warp per row block, eight gathers in flight + alpha, minus beta q_{j-1})", None),
               11: ("k_spmm_wg with the axpy (one cooperative launch per iteration: SpMM + alpha, wait, r_{j+1}, beta)",
-                   "k_spmm_wg_tube60x500.md")}
+                   "k_spmm_wg_tube60x500.md"),
+              12: ("k_spmm_lean (L1 gathers at 32 warps per SM, 64 registers + alpha, minus beta q_{j-1})", None)}
 
 
 def measured_traffic(staged):

@@ -725,7 +725,7 @@ extern "C" dq_status dq_autotune(dq_ctx* c, int reps, double* best_ms) {
     double best = 1e30;
     const int vecs[2] = {2, 1};
     for (int groups = 1; groups <= 8; groups <<= 1)
-        for (int staged = 0; staged <= 11; ++staged)
+        for (int staged = 0; staged <= 12; ++staged)
             for (int vi = 0; vi < 2; ++vi)
                 for (int tc = 4; tc <= 64; tc <<= 1)
                     for (int cps = 1; cps <= 8; cps <<= 1)

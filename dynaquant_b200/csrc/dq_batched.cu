@@ -1219,6 +1219,150 @@ __global__ void __launch_bounds__(512, 1) k_spmm_wg(int n, int B, int bpc, int n
     }
 }
 
+// Lean row-blocked SpMM (staged = 12; complex64, packed records, R <= 3, 2
+// trajectories per lane) for 32 warps per SM: NT = 1024 threads in one CTA
+// per SM or NT = 512 in two, at most 64 registers a thread.  k_spmm_blk holds
+// about 124 registers (the block's own rows and diagonal, two record groups,
+// the next block's header, alpha sums and scalars across the gather loop), so
+// only 16 warps fit per SM and each warp's FMA and store work between its
+// gather waits is exposed.  Here a thread holds only the accumulators, the
+// group of four records and their four gathered rows: the records are loaded
+// where they are used (consecutive records share L1 lines), the own rows,
+// diagonal and q_{j-1} rows are prefetched into L1 at the block's start and
+// read after the gathers (minus beta q_{j-1} is added after the couplings),
+// the scalars are read again per block, and the FP64 alpha sums of each
+// thread live in shared memory.
+template <int R, bool kBilinear, bool kWrite, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT) k_spmm_lean(int n, int B, int TC, int bpc, int nb, int j,
+                                                            const int* __restrict__ bptr,
+                                                            const float4* __restrict__ rec,
+                                                            const float* __restrict__ d, const float* __restrict__ rj,
+                                                            const float* __restrict__ rjm, float* __restrict__ w,
+                                                            BatchedScalars S, int cy0, int nch) {
+    constexpr int TPT = 2;
+    const int TPR = TC / TPT;
+    const int tr = threadIdx.x % TPR, rl = threadIdx.x / TPR;
+    const int RPC = NT / TPR;
+    const int chunk = blockIdx.y + cy0;
+    if (chunk_converged(S, chunk)) return;
+    const int b0 = chunk * TC + tr * TPT;
+    const int k0 = blockIdx.x * bpc, k1 = min(nb, k0 + bpc);
+    // per-thread FP64 alpha (or norm) sums, then the reduction's scratch
+    __shared__ double2 sums[NT * TPT];
+    __shared__ double2 red[kMaxTC];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) sums[threadIdx.x * TPT + t] = make_double2(0.0, 0.0);
+    const float* src = rj + 2 * (size_t)b0;
+    for (int k = k0 + rl; k < k1; k += RPC) {
+        const int row0 = k * R;
+        const int pb = __ldg(bptr + k), pe = __ldg(bptr + k + 1);
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const size_t base = (size_t)min(row0 + i, n - 1) * B + b0;
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(rj + 2 * base));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(d + base));
+            if (rjm) asm volatile("prefetch.global.L1 [%0];" ::"l"(rjm + 2 * base));
+        }
+        CV<float, TPT> acc[R];
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+            for (int v = 0; v < 2 * TPT; ++v) acc[i].v[v] = 0.f;
+        for (int e = pb; e < pe; e += 4) {   // a multiple of 4 records per block
+            float4 r[4];
+            CV<float, TPT> y[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) r[u] = __ldg(rec + e + u);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) y[u] = ldv<float, TPT, true>(src, (size_t)__float_as_int(r[u].x) * B);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                cfma<float, TPT>(acc[0], r[u].y, y[u]);
+                if constexpr (R > 1) cfma<float, TPT>(acc[R > 1 ? 1 : 0], r[u].z, y[u]);
+                if constexpr (R > 2) cfma<float, TPT>(acc[R > 2 ? 2 : 0], r[u].w, y[u]);
+            }
+        }
+        // minus beta_{j-1} q_{j-1} and the diagonal, then w and the sums
+        double sc[TPT];
+        float fm[TPT];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+            sc[t] = S.sc[(size_t)j * B + b0 + t];
+            fm[t] = 0.f;
+            if (rjm) {
+                const size_t km = (size_t)(j - 1) * B + b0 + t;
+                fm[t] = sc[t] != 0.0 ? (float)(S.beta[km] * S.sc[km] / sc[t]) : 0.f;
+            }
+        }
+        double ar[TPT], ai[TPT];
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) { ar[t] = 0.0; ai[t] = 0.0; }
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const int row = row0 + i;
+            if (row >= n) break;
+            const size_t base = (size_t)row * B + b0;
+            const CV<float, TPT> x = ldv<float, TPT, true>(rj, base);
+            if (rjm) {
+                const CV<float, TPT> xm = ldv<float, TPT, true>(rjm, base);
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    acc[i].v[2 * t] = fmaf(-fm[t], xm.v[2 * t], acc[i].v[2 * t]);
+                    acc[i].v[2 * t + 1] = fmaf(-fm[t], xm.v[2 * t + 1], acc[i].v[2 * t + 1]);
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < TPT; ++t) {
+                const float dv = __ldg(d + base + t);
+                acc[i].v[2 * t] = fmaf(dv, x.v[2 * t], acc[i].v[2 * t]);
+                acc[i].v[2 * t + 1] = fmaf(dv, x.v[2 * t + 1], acc[i].v[2 * t + 1]);
+            }
+            if (kWrite) {
+                CV<float, TPT> o;
+#pragma unroll
+                for (int t = 0; t < TPT; ++t) {
+                    o.v[2 * t] = (float)(sc[t] * (double)acc[i].v[2 * t]);
+                    o.v[2 * t + 1] = (float)(sc[t] * (double)acc[i].v[2 * t + 1]);
+                    const double xr = x.v[2 * t], xi = x.v[2 * t + 1], ur = acc[i].v[2 * t], ui = acc[i].v[2 * t + 1];
+                    if (kBilinear) { ar[t] += xr * ur - xi * ui; ai[t] += xr * ui + xi * ur; }
+                    else { ar[t] += xr * ur + xi * ui; ai[t] += xr * ui - xi * ur; }
+                }
+                stv<float, TPT>(w, base, o);
+            } else {
+#pragma unroll
+                for (int t = 0; t < TPT; ++t)
+                    ar[t] += (double)acc[i].v[2 * t] * acc[i].v[2 * t] + (double)acc[i].v[2 * t + 1] * acc[i].v[2 * t + 1];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < TPT; ++t) {
+            double2& sm = sums[threadIdx.x * TPT + t];
+            sm.x += ar[t];
+            sm.y += ai[t];
+        }
+    }
+    double ar[TPT], ai[TPT];
+#pragma unroll
+    for (int t = 0; t < TPT; ++t) {
+        ar[t] = sums[threadIdx.x * TPT + t].x;
+        ai[t] = sums[threadIdx.x * TPT + t].y;
+    }
+    __syncthreads();   // the sums become the reduction's scratch
+    if (chunk_reduce_s<TPT>(ar, ai, TC, S.partial, S.tickets + (kWrite ? 0 : 2) * nch, red, chunk, sums)) {
+        if (threadIdx.x < TC) {
+            const int b = chunk * TC + threadIdx.x;
+            const double s = S.sc[(size_t)j * B + b];
+            const double2 v = red[threadIdx.x];
+            if (kWrite) {
+                S.alpha[2 * ((size_t)j * B + b)] = v.x * s * s;
+                S.alpha[2 * ((size_t)j * B + b) + 1] = v.y * s * s;
+            } else {
+                S.nav[b] = sqrt(v.x) * s;
+            }
+        }
+    }
+}
+
 // Warp-per-block SpMM (staged = 3; complex64, packed records, R <= 3).  All
 // 32 lanes of a warp work on one block of R rows for TC = 32 TPT
 // trajectories, so the block's column-union records are one warp-uniform
@@ -3228,6 +3372,21 @@ static void prefer_l1_r() {
 }
 
 template <int R>
+static void prefer_l1_lean() {
+    const int carve = cudaSharedmemCarveoutMaxL1;
+    auto set = [&](const void* f) { cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carve); };
+    set((const void*)k_spmm_lean<R, false, true, 1024>);
+    set((const void*)k_spmm_lean<R, true, true, 1024>);
+    set((const void*)k_spmm_lean<R, false, false, 1024>);
+    set((const void*)k_spmm_lean<R, true, false, 1024>);
+    set((const void*)k_spmm_lean<R, false, true, 512>);
+    set((const void*)k_spmm_lean<R, true, true, 512>);
+    set((const void*)k_spmm_lean<R, false, false, 512>);
+    set((const void*)k_spmm_lean<R, true, false, 512>);
+    cudaGetLastError();   // a hint: a refusal changes nothing
+}
+
+template <int R>
 static void prefer_l1_wg() {
     const int carve = cudaSharedmemCarveoutMaxL1;
     auto set = [&](const void* f) { cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, carve); };
@@ -3258,7 +3417,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (!bs->mixed && tpt != 1) return DQ_ERR_ARG;
     if (tc < tpt || tc > kMaxTC || (tc & (tc - 1)) || B % tc || tc / tpt > kBThreads) return DQ_ERR_ARG;
     if (ctas_per_sm < 1 || ctas_per_sm > 16) return DQ_ERR_ARG;
-    if (staged < 0 || staged > 11) return DQ_ERR_ARG;
+    if (staged < 0 || staged > 12) return DQ_ERR_ARG;
     // reorthogonalisation runs between the axpy and the next SpMM: not in the fused forms
     if ((c->cfg.reorth || c->cfg.m_min > 0) && (staged == 2 || staged == 4 || staged == 8 || staged == 11))
         return DQ_ERR_ARG;
@@ -3271,6 +3430,8 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     // the same restrictions, chunk groups allowed
     if ((staged == 10 || staged == 11) && (!bs->mixed || R > 3 || tc != 64 || tpt != 2 || ctas_per_sm != 1))
         return DQ_ERR_ARG;
+    // lean SpMM for 32 warps per SM: one 1024-thread CTA or two 512-thread CTAs per SM
+    if (staged == 12 && (!bs->mixed || R > 3 || tpt != 2 || ctas_per_sm > 2)) return DQ_ERR_ARG;
     // ring SpMM: complex64 packed records, 32 trajectories per chunk, 2 per lane in the other
     // kernels (the ring itself takes 2 per lane with staged 6, 4 with staged 7), one CTA per SM
     const bool ring = staged == 6 || staged == 7;
@@ -3285,7 +3446,7 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
     if (groups < 1 || chunks % groups) return DQ_ERR_ARG;
     const int cpg = chunks / groups;   // chunks per launch of the per-iteration kernels
     const int TPR = tc / tpt, RPC = kBThreads / TPR;
-    const int RPC_spmm = (staged == 5 || staged >= 8 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
+    const int RPC_spmm = (staged == 12 ? (ctas_per_sm == 1 ? 1024 : 512) : staged == 5 || staged >= 8 ? 512 : kBThreads) / TPR;   // row blocks in flight per SpMM CTA
     // bandwidth-bound per-row kernels (noise, axpy, combine) always run wide:
     // one wave of kStreamCtasPerSm CTAs per SM while every thread still walks
     // several rows, twice as many CTAs when that wave would leave each thread
@@ -3467,6 +3628,13 @@ dq_status batched_set_tiling(dq_ctx* c, int tc, int tpt, int ctas_per_sm, int R,
             case 1: prefer_l1_wg<1>(); break;
             case 2: prefer_l1_wg<2>(); break;
             default: prefer_l1_wg<3>(); break;
+        }
+    }
+    if (staged == 12) {
+        switch (R) {
+            case 1: prefer_l1_lean<1>(); break;
+            case 2: prefer_l1_lean<2>(); break;
+            default: prefer_l1_lean<3>(); break;
         }
     }
     if (staged == 11) {
@@ -3795,6 +3963,30 @@ static void launch_spmm(dq_ctx* c, int j, const Real* rj, const Real* rjm, Real*
                 default: DQ_CPA_R(3); break;
             }
 #undef DQ_CPA_R
+        }
+        return;
+    }
+    if (bs->staged == 12) {
+        if constexpr (sizeof(Real) == 4 && TPT == 2) {
+            const dim3 grid(bs->gxs, ncy);
+            const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
+#define DQ_LEAN_R(RR, NT)                                                                                         \
+    k_spmm_lean<RR, kBil, kWrite, NT><<<grid, NT, 0, c->stream>>>(n, B, TC, bs->bpc, f.nb, j, f.bptr, rec, d, rj, rjm, \
+                                                                  w, bs->s, cy0, bs->chunks)
+            if (bs->ctas_per_sm == 1) {
+                switch (bs->R) {
+                    case 1: DQ_LEAN_R(1, 1024); break;
+                    case 2: DQ_LEAN_R(2, 1024); break;
+                    default: DQ_LEAN_R(3, 1024); break;
+                }
+            } else {
+                switch (bs->R) {
+                    case 1: DQ_LEAN_R(1, 512); break;
+                    case 2: DQ_LEAN_R(2, 512); break;
+                    default: DQ_LEAN_R(3, 512); break;
+                }
+            }
+#undef DQ_LEAN_R
         }
         return;
     }

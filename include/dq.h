@@ -259,7 +259,10 @@ DQ_API dq_status dq_run(dq_ctx *ctx, int n_steps);
  * ctas_per_sm 1, rows_per_block <= 3), 11 is form 10 with the axpy in the
  * same launch: a cooperative launch in which each CTA waits (bounded) for its
  * chunk's alpha_j and then forms r_{j+1} for its own rows while w and q_j are
- * still in L2 (no reorthogonalisation or adaptive m).  groups splits the trajectory chunks
+ * still in L2 (no reorthogonalisation or adaptive m), 12 is the L1 form at
+ * 32 warps per SM and at most 64 registers a thread (complex64, vec 2,
+ * rows_per_block <= 3; ctas_per_sm 1: one 1024-thread CTA per SM, 2: two
+ * 512-thread CTAs).  groups splits the trajectory chunks
  * into groups whose m Lanczos iterations run one group after another, so a
  * group's Krylov slabs stay resident in L2 (must divide n_traj / traj_chunk).  Changing it restarts the ensemble at the next dq_run
  * (as dq_reset does). */

@@ -458,3 +458,32 @@ def test_gather_floor_probe_runs_below_the_spmm_and_refuses_other_forms():
     with pytest.raises(dq.DQError):
         q.time_gather_floor(2)
     q.close()
+
+
+@pytest.mark.parametrize("tc,cps", [(64, 1), (64, 2), (32, 2)])
+@pytest.mark.parametrize("dot", [1, 0])
+@pytest.mark.parametrize("R", [1, 2, 3])
+def test_lean_spmm_mixed_tube_matches_oracle(oracle, dot, R, tc, cps):
+    """The 64-register L1 SpMM (staged = 12: one 1024-thread CTA or two 512-thread CTAs per SM, 32 warps
+    per SM) against the FP64 oracle on the dipole-coupled tube."""
+    import dynaquant_b200 as dq
+    from dynaquant_b200 import systems
+    s = systems.tube(20, 24)
+    rp, col, val, diag = s.off_diagonal()
+    S = oracle.System(rp, col, val, diag, m=20, dt=0.5, dot_mode=dot, noise=2, sigma=250.0, tau=50.0,
+                      sigma_static=150.0, seed=9)
+    B, T = 128, 40
+    psi0 = s.bright_state()
+    ref = S.run(B, T, psi0, pop_every=8, threads=4)
+    p = dq.Propagator(s.n, m=20, n_traj=B, dt=0.5, noise=dq.NOISE_OU, sigma_static=150.0, seed=9, dot=dot,
+                      pop_every=8, max_steps=T, precision=dq.PREC_MIXED)
+    p.set_system(s)
+    p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
+    p.set_initial_state(psi0)
+    p.set_tiling(tc, 2, cps, R, 12, 1)
+    assert p.get_tiling() == (tc, 2, cps, R, 12, 1)
+    p.run(T)
+    assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
+    assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
+    assert np.allclose(p.error_accum(), ref["err"], rtol=1e-2, atol=1e-12)
+    p.close()
