@@ -250,7 +250,8 @@ SPMM_FORMS = {0: ("k_spmm_blk (L1 gathers + alpha, minus beta q_{j-1})", None),
               10: ("k_spmm_wg (warp per row block, eight gathers in flight + alpha, minus beta q_{j-1})", None),
               11: ("k_spmm_wg with the axpy (one cooperative launch per iteration: SpMM + alpha, wait, r_{j+1}, beta)",
                    "k_spmm_wg_tube60x500.md"),
-              12: ("k_spmm_lean (L1 gathers at 32 warps per SM, 64 registers + alpha, minus beta q_{j-1})", None)}
+              12: ("k_spmm_lean (L1 gathers at 32 warps per SM, 64 registers + alpha, minus beta q_{j-1})",
+                   "k_spmm_lean_tube60x500.md")}
 
 
 def measured_traffic(staged):
@@ -392,11 +393,12 @@ def large_leg():
     prof = p.profile_step(1)
     gather_floor = gather_floor_ms(p)
     p.close()
-    b, kms, achieved = dominant_kernel(s, B, 24, tiling["staged"], prof)
+    # with chunk groups each launch covers B / groups trajectories
+    b, kms, achieved = dominant_kernel(s, B // tiling.get("groups", 1), 24, tiling["staged"], prof)
     peak, peak_kind = _peaks()
     return {"workload": "tube120x1000_B1024_m24", "n_sites": s.n, "nnz_per_row": (s.nnz - s.n) / s.n,
             "value": B / (ms / 1e3), "unit": "traj-steps/s", "ms_per_step": ms,
-            "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged")},
+            "tiling": {k: tiling[k] for k in ("traj_chunk", "vec", "ctas_per_sm", "rows_per_block", "staged", "groups")},
             "roofline": {"bound": "hbm", "kernel": SPMM_FORMS.get(tiling["staged"], ("SpMM + alpha",))[0],
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b, "ms_per_launch": kms,
@@ -694,7 +696,7 @@ def run_ours(args, rank, world, local_rank):
     gather_floor = gather_floor_ms(p)
     p.close()
     peak, peak_kind = _peaks()
-    bytes_spmm, spmm_ms, achieved = dominant_kernel(s, B, w["m"], tiling["staged"], prof)
+    bytes_spmm, spmm_ms, achieved = dominant_kernel(s, B // tiling.get("groups", 1), w["m"], tiling["staged"], prof)
     step_ms_eager = sum(v[0] * v[1] for v in prof.values()) / 2
     kernels_per_step = sum(v[1] for v in prof.values()) // 2
     # ---- end to end through the C ABI with host buffers --------------------
