@@ -1230,8 +1230,8 @@ __global__ void __launch_bounds__(512, 1) k_spmm_wg(int n, int B, int bpc, int n
 // where they are used (consecutive records share L1 lines), the own rows,
 // diagonal and q_{j-1} rows are prefetched into L1 at the block's start and
 // read after the gathers (minus beta q_{j-1} is added after the couplings),
-// the scalars are read again per block, and the FP64 alpha sums of each
-// thread live in shared memory.
+// the chunk's scalars are staged once in shared memory and read per block,
+// and the FP64 alpha sums of each thread live in shared memory.
 template <int R, bool kBilinear, bool kWrite, int NT>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_spmm_lean(int n, int B, int TC, int bpc, int nb, int j,
                                                             const int* __restrict__ bptr,
@@ -1250,8 +1250,25 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_spmm_lean(int n, int B, int T
     // per-thread FP64 alpha (or norm) sums, then the reduction's scratch
     __shared__ double2 sums[NT * TPT];
     __shared__ double2 red[kMaxTC];
+    // the chunk's sc_j and beta_{j-1} sc_{j-1} / sc_j, read per block from here
+    __shared__ double sc_s[kMaxTC];
+    __shared__ float fm_s[kMaxTC];
 #pragma unroll
     for (int t = 0; t < TPT; ++t) sums[threadIdx.x * TPT + t] = make_double2(0.0, 0.0);
+    if (threadIdx.x < TC) {
+        const int b = chunk * TC + threadIdx.x;
+        const double scb = S.sc[(size_t)j * B + b];
+        float f = 0.f;
+        if (rjm) {
+            // sc_j = 0 only after a breakdown, where beta_{j-1} = 0 as well
+            const size_t km = (size_t)(j - 1) * B + b;
+            f = scb != 0.0 ? (float)(S.beta[km] * S.sc[km] / scb) : 0.f;
+        }
+        sc_s[threadIdx.x] = scb;
+        fm_s[threadIdx.x] = f;
+    }
+    __syncthreads();
+    const int tl = tr * TPT;   // this thread's first trajectory within the chunk
     const float* src = rj + 2 * (size_t)b0;
     for (int k = k0 + rl; k < k1; k += RPC) {
         const int row0 = k * R;
@@ -1271,6 +1288,9 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_spmm_lean(int n, int B, int T
         for (int e = pb; e < pe; e += 4) {   // a multiple of 4 records per block
             float4 r[4];
             CV<float, TPT> y[4];
+            // the record line two groups ahead, within the block (the gathers'
+            // addresses depend on the records)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(rec + min(e + 8, pe - 1)));
 #pragma unroll
             for (int u = 0; u < 4; ++u) r[u] = __ldg(rec + e + u);
 #pragma unroll
@@ -1287,12 +1307,8 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_spmm_lean(int n, int B, int T
         float fm[TPT];
 #pragma unroll
         for (int t = 0; t < TPT; ++t) {
-            sc[t] = S.sc[(size_t)j * B + b0 + t];
-            fm[t] = 0.f;
-            if (rjm) {
-                const size_t km = (size_t)(j - 1) * B + b0 + t;
-                fm[t] = sc[t] != 0.0 ? (float)(S.beta[km] * S.sc[km] / sc[t]) : 0.f;
-            }
+            sc[t] = sc_s[tl + t];
+            fm[t] = fm_s[tl + t];
         }
         double ar[TPT], ai[TPT];
 #pragma unroll
