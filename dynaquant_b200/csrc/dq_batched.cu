@@ -4555,7 +4555,8 @@ dq_status batched_time_gather_floor(dq_ctx* c, int reps, double* ms) {
     const size_t se = (size_t)c->n * bs->B;
     float* slabs = (float*)bs->slabs;
     const float4* rec = reinterpret_cast<const float4*>(f.bcoef);
-    const dim3 grid(bs->gxs, bs->chunks);
+    // one launch's chunks (with chunk groups, an SpMM launch covers one group)
+    const dim3 grid(bs->gxs, bs->chunks / bs->groups);
     auto launch = [&]() {
         switch (bs->R) {
             case 1: k_gather_floor<1><<<grid, 512, 0, c->stream>>>(c->n, bs->B, bs->TC, bs->bpc, f.nb, f.bptr, rec, slabs + 2 * se, slabs); break;

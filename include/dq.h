@@ -281,8 +281,9 @@ DQ_API dq_status dq_time_iteration(dq_ctx *ctx, int reps, double *ms);
  * the gathers alone of the current tiling's packed coupling blocks (complex64,
  * vec 2, rows_per_block <= 3): the same row-block walk, record stream and
  * 16-byte gathers of the trajectory rows as the L1-gather SpMM, without its
- * FMAs, diagonal, q_{j-1} term, alpha and all but one store per block; the
- * floor that access pattern sets on the GPU.  Overwrites the ensemble's work
+ * FMAs, diagonal, q_{j-1} term, alpha and all but one store per block, over
+ * the chunks of one SpMM launch (one chunk group); the floor that access
+ * pattern sets on the GPU.  Overwrites the ensemble's work
  * slab (the ensemble restarts at the next dq_run); DQ_ERR_STATE for other
  * tilings. */
 DQ_API dq_status dq_time_gather_floor(dq_ctx *ctx, int reps, double *ms);
