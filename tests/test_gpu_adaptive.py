@@ -33,7 +33,7 @@ def _oracle_dims(S, psi0):
 
 
 @pytest.mark.parametrize("precision,tiling", [("fp64", None), ("mixed", None), ("mixed", (32, 2, 1, 3, 6, 1)),
-                                              ("mixed", (8, 2, 2, 3, 0, 2))])
+                                              ("mixed", (8, 2, 2, 3, 0, 2)), ("mixed", (8, 2, 1, 3, 12, 2))])
 def test_adaptive_dimension_matches_oracle(oracle, precision, tiling):
     import dynaquant_b200 as dq
     s, S = _setup(oracle)

@@ -372,11 +372,12 @@ def test_async_copy_gather_spmm_mixed_tube_matches_oracle(oracle, dot, R, staged
     p.close()
 
 
+@pytest.mark.parametrize("staged,tc", [(11, 64), (12, 32)])
 @pytest.mark.parametrize("groups", [1, 2])
-def test_cooperative_iteration_chunk_groups_match_oracle(oracle, groups):
-    """Staged 11 (SpMM and axpy in one cooperative launch, a bounded wait per chunk for alpha) with
-    the chunks run as one launch or as two groups of one chunk each, against the FP64 oracle; the
-    group run also matches the one-launch run to FP32 rounding."""
+def test_cooperative_iteration_chunk_groups_match_oracle(oracle, groups, staged, tc):
+    """Staged 11 (SpMM and axpy in one cooperative launch, a bounded wait per chunk for alpha) and the
+    lean SpMM of staged 12, with the chunks run as one launch or as two groups, against the FP64
+    oracle."""
     import dynaquant_b200 as dq
     from dynaquant_b200 import systems
     s = systems.tube(20, 24)
@@ -391,8 +392,8 @@ def test_cooperative_iteration_chunk_groups_match_oracle(oracle, groups):
     p.set_system(s)
     p.set_noise_params(np.full(s.n, 250.0), np.full(s.n, 50.0))
     p.set_initial_state(psi0)
-    p.set_tiling(64, 2, 1, 3, 11, groups)
-    assert p.get_tiling() == (64, 2, 1, 3, 11, groups)
+    p.set_tiling(tc, 2, 1, 3, staged, groups)
+    assert p.get_tiling() == (tc, 2, 1, 3, staged, groups)
     p.run(T)
     assert np.abs(p.populations() - ref["pops"]).max() < POP_TOL_MIXED
     assert np.abs(p.correlation() - ref["corr"]).max() < POP_TOL_MIXED * 10
