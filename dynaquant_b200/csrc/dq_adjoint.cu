@@ -242,7 +242,7 @@ __global__ void k_adj_small(int m, int B, double tau_im, BatchedScalars SV, Batc
 // Sums over the CTA's trajectories go to gsite/gcpl[row][traj group] (one
 // writer each, deterministic); |lambda|^2 partials to lpart[cta][b].
 template <typename Real, int MM>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_grad(int n, int B, int m, int rows_per_cta, int G,
+__global__ void __launch_bounds__(kAdjThreads, 2) k_adj_grad(int n, int B, int m, int rows_per_cta, int G,
                                                          const Real* __restrict__ sV, Real* sW, size_t slab_reals,
                                                          const Real* __restrict__ d, const cd* __restrict__ psi0,
                                                          const cd* __restrict__ Gt, double invB, int write_lam,
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_grad(int n, int B, int m, i
 // skip0, class-0 entries are left out: their sum follows on the host from the
 // total off-diagonal form (free from the Lanczos relation in k_adj_grad).
 template <typename Real, int MM>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_cls(int n, int B, int m, int rows_per_cta, int G, int C,
+__global__ void __launch_bounds__(kAdjThreads, 2) k_adj_cls(int n, int B, int m, int rows_per_cta, int G, int C,
                                                         const Real* __restrict__ sV, const Real* __restrict__ sW,
                                                         size_t slab_reals, const int* __restrict__ rowptr,
                                                         const int* __restrict__ col, const int* __restrict__ cls,
